@@ -1,0 +1,154 @@
+"""ctypes mirror of include/fivo2d.h and the loader for the CUDA library.
+
+The structs here are byte-for-byte the C ABI the Julia shim (julia/FivoGPU.jl)
+binds with `ccall`; Python is the host language of this repository's tests and
+benchmark because no Julia toolchain is installed where they run.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import pathlib
+
+FIVO_ABI_VERSION = 1
+
+FIVO_OK, FIVO_ERR_ARG, FIVO_ERR_CONFIG, FIVO_ERR_CUDA, FIVO_ERR_NOMEM, FIVO_ERR_DEVICE = range(6)
+
+FIVO_EOS_CONFORMAL_HQ = 0
+FIVO_EOS_LATTICE_HRG = 1
+FIVO_SHEAR_ZERO, FIVO_SHEAR_QGP = 0, 1
+FIVO_BULK_ZERO, FIVO_BULK_LORENTZ, FIVO_BULK_GAUSS = 0, 1, 2
+FIVO_BC_OUTFLOW, FIVO_BC_PERIODIC = 0, 1
+FIVO_SSPRK2, FIVO_SSPRK3 = 2, 3
+
+# Terms register (src/terms.jl:82-104), one bit per field in field order.
+TERM_NAMES = (
+    "nu_gradalpha", "fm_gradT", "fm_inertial", "fm_nu_gradu", "fm_expansion", "fm_dlnh",
+    "m2_nu_gradient", "m2_bg_gradu", "m2_bg_DlnT", "m2_bg_Dalpha", "m2_expansion",
+    "m2_pi_sigma", "m2_PiQ_sigma", "m2_vorticity", "m2_projector", "m2_accel_nu",
+    "m2_nu_gradTh", "shear_vorticity",
+)
+TERM_BIT = {n: 1 << k for k, n in enumerate(TERM_NAMES)}
+FIVO_TERMS_DEFAULT = 0x1DFFF
+
+
+class FivoParams(C.Structure):
+    _fields_ = [
+        ("g_eff", C.c_double), ("m_hq", C.c_double), ("g_hq", C.c_double),
+        ("lhrg_a", C.c_double * 4), ("lhrg_b", C.c_double * 4),
+        ("lhrg_c", C.c_double), ("lhrg_d", C.c_double), ("canon_factor", C.c_double),
+        ("kappa_coeff", C.c_double), ("tauN_coeff", C.c_double), ("deltaN_factor", C.c_double),
+        ("nu_clip_factor", C.c_double), ("vacuum_n_lo", C.c_double), ("vacuum_n_hi", C.c_double),
+        ("eta_over_s", C.c_double), ("tauShear_coeff", C.c_double),
+        ("deltaShear_factor", C.c_double), ("taupi_pi_factor", C.c_double),
+        ("lambda_pi_Pi_factor", C.c_double), ("pi_clip_factor", C.c_double),
+        ("zeta_over_s", C.c_double), ("tauPi_coeff", C.c_double), ("bulk_T0", C.c_double),
+        ("bulk_width", C.c_double), ("deltaPi_factor", C.c_double),
+        ("lambda_Pi_pi_factor", C.c_double), ("Pi_clip_factor", C.c_double),
+        ("r_domain", C.c_double), ("T_vac_cut", C.c_double), ("E_vac_cut", C.c_double),
+        ("primrec_tol", C.c_double),
+        ("eos_kind", C.c_int32), ("hq_times_fmGeV3", C.c_int32), ("with_charge", C.c_int32),
+        ("enable_diff", C.c_int32), ("enable_shear", C.c_int32), ("enable_bulk", C.c_int32),
+        ("shear_kind", C.c_int32), ("bulk_kind", C.c_int32),
+        ("advect_nu", C.c_int32), ("relax_advect_nu", C.c_int32),
+        ("advect_pi", C.c_int32), ("relax_advect_pi", C.c_int32),
+        ("advect_Pi", C.c_int32), ("relax_advect_Pi", C.c_int32),
+        ("vacuum_ramp_relax", C.c_int32),
+        ("shear_projected_deriv", C.c_int32), ("diff_projected_deriv", C.c_int32),
+        ("shear_constraint_project", C.c_int32),
+        ("consistent_fm", C.c_int32), ("consistent_m2", C.c_int32),
+        ("primrec_maxit", C.c_int32), ("terms", C.c_uint32),
+    ]
+
+
+class FivoCounters(C.Structure):
+    _fields_ = [
+        ("nprimfail", C.c_int64), ("nvacuum", C.c_int64), ("primfail_index", C.c_int64),
+        ("primfail_reason", C.c_int32), ("pad0", C.c_int32), ("primfail_resnorm", C.c_double),
+        ("amax", C.c_double), ("nmood", C.c_int64), ("nhalve", C.c_int64),
+    ]
+
+
+class FivoRunResult(C.Structure):
+    _fields_ = [
+        ("ok", C.c_int32), ("pad0", C.c_int32), ("tau", C.c_double), ("nsteps", C.c_int64),
+        ("nprimfail", C.c_int64), ("nvacuum", C.c_int64), ("max_shear_res", C.c_double),
+        ("maxu", C.c_double), ("dQ", C.c_double), ("Q0", C.c_double), ("Q1", C.c_double),
+        ("minPtot", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("pad")}
+
+
+PKG_DIR = pathlib.Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR.parent / "csrc" / "libfivo2d.so"
+
+_D = C.POINTER(C.c_double)
+_U8 = C.POINTER(C.c_uint8)
+_I64 = C.c_int64
+
+# name -> (restype, argtypes), exactly the declarations of include/fivo2d.h
+SIGNATURES = {
+    "fivo_abi_version": (C.c_int, []),
+    "fivo_last_error": (C.c_char_p, []),
+    "fivo_params_default": (None, [C.POINTER(FivoParams)]),
+    "fivo_ctx_create": (C.c_int, [C.POINTER(FivoParams), C.c_int, C.c_int, C.c_int, C.c_double,
+                                  C.c_double, C.POINTER(C.c_void_p)]),
+    "fivo_ctx_destroy": (C.c_int, [C.c_void_p]),
+    "fivo_ctx_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int64), _D]),
+    "fivo_upload_state": (C.c_int, [C.c_void_p, _D, C.c_int, _I64]),
+    "fivo_download_state": (C.c_int, [C.c_void_p, _D, C.c_int, _I64]),
+    "fivo_upload_history": (C.c_int, [C.c_void_p, _I64] + [_D] * 8),
+    "fivo_download_history": (C.c_int, [C.c_void_p, _I64] + [_D] * 8),
+    "fivo_reset_history": (C.c_int, [C.c_void_p]),
+    "fivo_get_primitives": (C.c_int, [C.c_void_p, _I64] + [_D] * 9 + [_U8]),
+    "fivo_get_counters": (C.c_int, [C.c_void_p, C.POINTER(FivoCounters)]),
+    "fivo_rhs": (C.c_int, [C.c_void_p, C.c_double, C.c_int, _U8, _D]),
+    "fivo_step": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
+                            _D, C.POINTER(C.c_int)]),
+    "fivo_update_primitives": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.POINTER(C.c_int64)]),
+    "fivo_relax": (C.c_int, [C.c_void_p, C.c_double, C.c_double]),
+    "fivo_project_shear": (C.c_int, [C.c_void_p, _D, _D]),
+    "fivo_compute_dt": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, _D]),
+    "fivo_run": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                           C.c_int, _I64, C.c_int, C.POINTER(FivoRunResult)]),
+    "fivo_finalize_ic": (C.c_int, [C.c_void_p, C.c_double, C.c_int]),
+    "fivo_set_cells": (C.c_int, [C.POINTER(FivoParams), _I64, C.c_double] + [_D] * 10 + [_D, _U8]),
+    "fivo_eos_Pne": (C.c_int, [C.POINTER(FivoParams), _I64, _D, _D, _D, _D, _D]),
+    "fivo_cons_to_prim": (C.c_int, [C.POINTER(FivoParams), _I64, C.c_double, _D, _D, _D, _U8, _U8]),
+    "fivo_sync": (C.c_int, [C.c_void_p]),
+}
+
+_LIB = None
+
+
+class FivoError(RuntimeError):
+    """A C-ABI call returned a non-zero status (see fivo_last_error)."""
+
+
+def load_library(path: str | os.PathLike | None = None):
+    """Load libfivo2d.so (the CUDA build). Raises if it is missing: there is no
+    CPU fallback for the stage."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = pathlib.Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FivoError(f"libfivo2d.so not built at {p}; run __graft_entry__.build()")
+    lib = C.CDLL(str(p))
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    if lib.fivo_abi_version() != FIVO_ABI_VERSION:
+        raise FivoError("libfivo2d ABI version mismatch")
+    if path is None:
+        _LIB = lib
+    return lib
+
+
+def check(lib, status: int, what: str = ""):
+    if status != FIVO_OK:
+        msg = lib.fivo_last_error()
+        raise FivoError(f"{what}: status {status}: {msg.decode() if msg else ''}")

@@ -1,0 +1,268 @@
+/*
+ * fivo2d.h — C ABI of the B200 finite-volume stage for FiVoHydro's 2+1D solver.
+ *
+ * The library replaces, behind plain pointers and sizes, the Julia functions the
+ * 2+1D driver `run_sim_2d!` (main2D.jl:371-561) calls once per time step:
+ *
+ *   step_ssprk2_2d! / step_ssprk3_2d!   src2d/timestepper2d.jl:74-103, 148-188
+ *   rhs_2d!                             src2d/rhs2d.jl:169-249
+ *   update_primitives_2d!               src2d/rhs2d.jl:57-65
+ *   relax_dissipative_2d!               src2d/dissipation2d.jl:293-363
+ *   compute_dt_2d                       src2d/timestepper2d.jl:37-47
+ *   project_shear!                      main2D.jl:332-358
+ *   prim_to_cons_2d! (IC path)          src2d/primrec2d.jl:753-796
+ *   finalize_ic!                        main2D.jl:164-171
+ *
+ * Conventions
+ *   - State U is the reference's `Matrix{Float64}(nv, Ntot)`: column-major, so
+ *     cell i, field a lives at U[i*nv + a] (AoS per cell). Flat cell index
+ *     i = ix*Nytot + iy (0-based; y is the fast index), src2d/grid2d.jl:85.
+ *   - Field order is StateLayout2D's (src2d/state_layout2d.jl:61-84):
+ *     Dtau, Sx, Sy, E, [nux, nuy], [Pi], [pixx, pixy, piyy, pieta].
+ *   - Every function returns an int status: FIVO_OK (0) or a positive error
+ *     code; fivo_last_error() returns the message of the last failure on the
+ *     calling thread. A time step that the scheme cannot accept is NOT an
+ *     error: it reports ok = 0, as step_ssprk2_2d! returns (false, Δ).
+ *   - All host pointers are only read or written during the call.
+ *   - One context owns one CUDA stream on the device that was current when the
+ *     context was created; calls are synchronous unless named *_async.
+ */
+#ifndef FIVO2D_H
+#define FIVO2D_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FIVO_ABI_VERSION 1
+
+/* status codes */
+#define FIVO_OK              0
+#define FIVO_ERR_ARG         1   /* invalid argument / size mismatch          */
+#define FIVO_ERR_CONFIG      2   /* model knob not implemented (reference refuses it too) */
+#define FIVO_ERR_CUDA        3   /* CUDA runtime error                        */
+#define FIVO_ERR_NOMEM       4   /* device allocation failed                  */
+#define FIVO_ERR_DEVICE      5   /* a device-side loop hit its iteration cap  */
+
+/* equation of state: src/eos.jl:39-84 (ConformalHQEOS), :318-519 (LatticeHRGEOS) */
+#define FIVO_EOS_CONFORMAL_HQ  0
+#define FIVO_EOS_LATTICE_HRG   1
+
+/* shear / bulk transport models: src/primitives.jl:347-409 */
+#define FIVO_SHEAR_ZERO        0   /* ZeroViscosity                             */
+#define FIVO_SHEAR_QGP         1   /* QGPViscosity(eta/s, C_s)                  */
+#define FIVO_BULK_ZERO         0   /* ZeroBulkViscosity                         */
+#define FIVO_BULK_LORENTZ      1   /* SimpleBulkViscosity: Lorentzian at 0.175 GeV */
+#define FIVO_BULK_GAUSS        2   /* Gaussian zeta/s(T) peak (new BulkViscosity subtype) */
+
+/* boundary conditions: src2d/bc2d.jl:14-65 */
+#define FIVO_BC_OUTFLOW        0
+#define FIVO_BC_PERIODIC       1
+
+/* integrators: main2D.jl:382 */
+#define FIVO_SSPRK2            2
+#define FIVO_SSPRK3            3
+
+/* Terms register bits, in the field order of `Terms` (src/terms.jl:82-104). */
+#define FIVO_TERM_NU_GRADALPHA     (1u << 0)
+#define FIVO_TERM_FM_GRADT         (1u << 1)
+#define FIVO_TERM_FM_INERTIAL      (1u << 2)
+#define FIVO_TERM_FM_NU_GRADU      (1u << 3)
+#define FIVO_TERM_FM_EXPANSION     (1u << 4)
+#define FIVO_TERM_FM_DLNH          (1u << 5)
+#define FIVO_TERM_M2_NU_GRADIENT   (1u << 6)
+#define FIVO_TERM_M2_BG_GRADU      (1u << 7)
+#define FIVO_TERM_M2_BG_DLNT       (1u << 8)
+#define FIVO_TERM_M2_BG_DALPHA     (1u << 9)
+#define FIVO_TERM_M2_EXPANSION     (1u << 10)
+#define FIVO_TERM_M2_PI_SIGMA      (1u << 11)
+#define FIVO_TERM_M2_PIQ_SIGMA     (1u << 12)
+#define FIVO_TERM_M2_VORTICITY     (1u << 13)
+#define FIVO_TERM_M2_PROJECTOR     (1u << 14)
+#define FIVO_TERM_M2_ACCEL_NU      (1u << 15)
+#define FIVO_TERM_M2_NU_GRADTH     (1u << 16)
+#define FIVO_TERM_SHEAR_VORTICITY  (1u << 17)
+/* Terms() defaults: every term on except m2_vorticity and shear_vorticity */
+#define FIVO_TERMS_DEFAULT         0x1DFFFu
+
+/*
+ * Flattened IdealDiffVisc2DModel (src2d/primitives2d.jl:41-210) plus the EOS,
+ * transport models and layout switches of build_model_2d (main2D.jl:85-123).
+ * fivo_params_default() fills the reference's keyword defaults.
+ * Doubles first, then 32-bit integers, so the struct has no interior padding.
+ */
+typedef struct fivo_params {
+  /* --- EOS --- */
+  double g_eff;             /* ConformalHQEOS g_eff (default 40)                 */
+  double m_hq;              /* heavy-quark mass [GeV] (1.5)                      */
+  double g_hq;              /* heavy-quark degeneracy (6)                        */
+  double lhrg_a[4];         /* LatticeHRGEOS a1..a4                              */
+  double lhrg_b[4];         /* LatticeHRGEOS b1..b4                              */
+  double lhrg_c, lhrg_d;    /* LatticeHRGEOS c, d                                */
+  double canon_factor;      /* LatticeHRGEOS canonical suppression I1/I0         */
+  /* --- charge diffusion --- */
+  double kappa_coeff;       /* D_s T [GeV fm]                                    */
+  double tauN_coeff;        /* multiplies tau_n (1)                              */
+  double deltaN_factor;     /* delta_N = factor * tau_n (0)                      */
+  double nu_clip_factor;    /* |nu| <= f n u^tau, off when <= 0 (-1)             */
+  double vacuum_n_lo;       /* charge-sector density ramp (1e-6)                 */
+  double vacuum_n_hi;       /* (2e-3)                                            */
+  /* --- shear --- */
+  double eta_over_s;        /* QGPViscosity eta/s                                */
+  double tauShear_coeff;    /* QGPViscosity C_s                                  */
+  double deltaShear_factor; /* delta_pipi = factor * tau_pi (4/3)                */
+  double taupi_pi_factor;   /* tau_pipi = factor * tau_pi (0)                    */
+  double lambda_pi_Pi_factor; /* lambda_piPi = factor * tau_pi (0)               */
+  double pi_clip_factor;    /* |pi^ij| <= f |P|, off when <= 0 (-1)              */
+  /* --- bulk --- */
+  double zeta_over_s;       /* peak zeta/s                                       */
+  double tauPi_coeff;       /* C_zeta (15)                                       */
+  double bulk_T0;           /* peak position [GeV] (Lorentzian: 0.175)           */
+  double bulk_width;        /* width [GeV] (Lorentzian: 0.024)                   */
+  double deltaPi_factor;    /* delta_PiPi = factor * tau_Pi (0)                  */
+  double lambda_Pi_pi_factor; /* lambda_Pipi = factor * tau_Pi (0)              */
+  double Pi_clip_factor;    /* |Pi| <= f |P|, off when <= 0 (-1)                 */
+  /* --- domain / vacuum --- */
+  double r_domain;          /* evolve only r <= r_domain (+Inf = whole box)      */
+  double T_vac_cut;         /* vacuum cut temperature [GeV] (0.05)               */
+  double E_vac_cut;         /* vacuum cut energy; <= 0 derives it from T_vac_cut */
+  /* --- primitive recovery numerics (src2d/primrec2d.jl:465-472) --- */
+  double primrec_tol;       /* row-scaled residual tolerance (1e-12)             */
+  /* --- integers --- */
+  int32_t eos_kind;         /* FIVO_EOS_*                                        */
+  int32_t hq_times_fmGeV3;  /* multiply HQ (P,n,e) by fmGeV3                     */
+  int32_t with_charge;      /* layout: nux, nuy present                          */
+  int32_t enable_diff;
+  int32_t enable_shear;     /* also: layout carries pixx, pixy, piyy, pieta      */
+  int32_t enable_bulk;      /* also: layout carries Pi                           */
+  int32_t shear_kind;       /* FIVO_SHEAR_*                                      */
+  int32_t bulk_kind;        /* FIVO_BULK_*                                       */
+  int32_t advect_nu, relax_advect_nu;
+  int32_t advect_pi, relax_advect_pi;
+  int32_t advect_Pi, relax_advect_Pi;
+  int32_t vacuum_ramp_relax;
+  int32_t shear_projected_deriv, diff_projected_deriv;
+  int32_t shear_constraint_project; /* 1 = :project, 0 = :monitor                */
+  int32_t consistent_fm, consistent_m2; /* charm closures: not built, must be 0  */
+  int32_t primrec_maxit;    /* Newton iteration cap (80)                         */
+  uint32_t terms;           /* FIVO_TERM_* bitmask                               */
+} fivo_params;
+
+/* Diagnostics of the last call (run_sim_2d! NamedTuple, main2D.jl:558-560). */
+typedef struct fivo_counters {
+  int64_t nprimfail;        /* recovery failures (non-vacuum), last pass         */
+  int64_t nvacuum;          /* PRR_VACUUM cells, last pass                       */
+  int64_t primfail_index;   /* one representative failing cell, -1 if none      */
+  int32_t primfail_reason;  /* its PrimRecReason (src/constants.jl:51-62)        */
+  int32_t pad0;
+  double  primfail_resnorm; /* its scaled residual                               */
+  double  amax;             /* largest HLLE signal speed of the last rhs         */
+  int64_t nmood;            /* MOOD stage retries in the last step               */
+  int64_t nhalve;           /* dt halvings in the last step                      */
+} fivo_counters;
+
+/* Result of fivo_run (run_sim_2d!, main2D.jl:558-560). */
+typedef struct fivo_run_result {
+  int32_t ok;
+  int32_t pad0;
+  double  tau;
+  int64_t nsteps;
+  int64_t nprimfail;
+  int64_t nvacuum;
+  double  max_shear_res;
+  double  maxu;
+  double  dQ, Q0, Q1;
+  double  minPtot;
+} fivo_run_result;
+
+typedef struct fivo_ctx fivo_ctx;
+
+/* --- library --- */
+int         fivo_abi_version(void);
+const char* fivo_last_error(void);
+void        fivo_params_default(fivo_params* p);
+
+/* --- context (Grid2D + Work2D mirror), src2d/grid2d.jl:52-71, src2d/work2d.jl:387-411 --- */
+int  fivo_ctx_create(const fivo_params* p, int nx, int ny, int nghost,
+                     double xmax, double ymax, fivo_ctx** out);
+int  fivo_ctx_destroy(fivo_ctx* ctx);
+int  fivo_ctx_info(const fivo_ctx* ctx, int* nv, int64_t* ntot, double* E_vac_cut);
+
+/* --- state and history transfer --- */
+int  fivo_upload_state(fivo_ctx* ctx, const double* U, int nv, int64_t ntot);
+int  fivo_download_state(fivo_ctx* ctx, double* U, int nv, int64_t ntot);
+/* Warm starts and dtau history (Work2D x0_*, *_prev); any pointer may be NULL. */
+int  fivo_upload_history(fivo_ctx* ctx, int64_t ntot,
+                         const double* x0_yT, const double* x0_phi,
+                         const double* x0_ux, const double* x0_uy,
+                         const double* ux_prev, const double* uy_prev,
+                         const double* alpha_prev, const double* T_prev);
+int  fivo_download_history(fivo_ctx* ctx, int64_t ntot,
+                           double* x0_yT, double* x0_phi, double* x0_ux, double* x0_uy,
+                           double* ux_prev, double* uy_prev,
+                           double* alpha_prev, double* T_prev);
+/* NaN-seed every history vector (run_sim_2d! reset_history, main2D.jl:407-415). */
+int  fivo_reset_history(fivo_ctx* ctx);
+/* Cell primitives of the last recovery (Work2D yT..ok); any pointer may be NULL. */
+int  fivo_get_primitives(fivo_ctx* ctx, int64_t ntot,
+                         double* yT, double* phi, double* mu, double* alpha,
+                         double* ux, double* uy, double* P, double* n, double* e,
+                         uint8_t* ok);
+int  fivo_get_counters(fivo_ctx* ctx, fivo_counters* out);
+
+/* --- the stage --- */
+/* rhs_2d!: BCs, primitive pass, MUSCL, HLLE, sources. mask = force_first_order
+ * (Ntot bytes, NULL = none). dU (nv x Ntot AoS, may be NULL) receives the RHS. */
+int  fivo_rhs(fivo_ctx* ctx, double tau, int bc, const uint8_t* mask, double* dU);
+/* step_ssprk2_2d! / step_ssprk3_2d! on the resident state. */
+int  fivo_step(fivo_ctx* ctx, int integrator, double tau, double dtau,
+               int max_halve, int max_mood, int bc, double* dtau_used, int* ok);
+/* update_primitives_2d!: BCs + primitive pass; returns the failure count. */
+int  fivo_update_primitives(fivo_ctx* ctx, double tau, int bc, int64_t* nprimfail);
+/* relax_dissipative_2d!: operator-split IS/DNMR relaxation, once per step. */
+int  fivo_relax(fivo_ctx* ctx, double tau, double dtau);
+/* project_shear!: pieta from tracelessness; returns max and mean residual. */
+int  fivo_project_shear(fivo_ctx* ctx, double* max_res, double* mean_res);
+/* compute_dt_2d from the amax of the last rhs. */
+int  fivo_compute_dt(fivo_ctx* ctx, double tau, double cfl, double cfltau, double* dt);
+/* run_sim_2d! (main2D.jl:371-561) on the resident state, without dumps. */
+int  fivo_run(fivo_ctx* ctx, double tau0, double taufinal, double cfl, double cfltau,
+              int integrator, int bc, int64_t max_steps, int reset_history,
+              fivo_run_result* out);
+
+/* --- initial conditions --- */
+/* finalize_ic! (main2D.jl:164-171) on the resident state. */
+int  fivo_finalize_ic(fivo_ctx* ctx, double tau0, int bc);
+/* set_cell! / prim_to_cons_2d! for ncell cells at once (main2D.jl:142-154):
+ * inputs are per-cell arrays (T, alpha = mu/T, ux, uy, Pi, pixx, pixy, piyy,
+ * nux, nuy; the dissipative ones may be NULL = 0); pieta comes from
+ * tracelessness. U receives nv x ncell (AoS), ok one byte per cell. */
+int  fivo_set_cells(const fivo_params* p, int64_t ncell, double tau,
+                    const double* T, const double* alpha,
+                    const double* ux, const double* uy,
+                    const double* Pi, const double* pixx, const double* pixy,
+                    const double* piyy, const double* nux, const double* nuy,
+                    double* U, uint8_t* ok);
+
+/* --- equation of state (for IC builders and tests) --- */
+/* eos_Pne (src/eos.jl:53-84, 483-519) for n points. */
+int  fivo_eos_Pne(const fivo_params* p, int64_t n, const double* T, const double* mu,
+                  double* P, double* nq, double* e);
+
+/* --- one-cell recovery (src2d/primrec2d.jl:465-486) for n independent cells --- */
+/* cons[k*11 + j] = (D, Sx, Sy, E, nux, nuy, Pi, pixx, pixy, piyy, pieta) of cell k;
+ * warm[k*4 + j] = (yT0, phi0, ux0, uy0) or NULL for a cold start.
+ * prim[k*7 + j] = (T, mu, ux, uy, n, e, P); ok and reason one byte per cell. */
+int  fivo_cons_to_prim(const fivo_params* p, int64_t n, double tau,
+                       const double* cons, const double* warm,
+                       double* prim, uint8_t* ok, uint8_t* reason);
+
+/* --- synchronisation --- */
+int  fivo_sync(fivo_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FIVO2D_H */

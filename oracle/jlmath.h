@@ -1,0 +1,253 @@
+/*
+ * oracle/jlmath.h — scalar math for the CPU oracle (TEST INFRASTRUCTURE ONLY).
+ *
+ * The reference is Julia; its arithmetic runs on Julia's own exp/log, on
+ * `Base.Math.pow_body` for float^integer, on NaN-propagating min/max and on
+ * SpecialFunctions.jl (Amos) for scaled Bessel K. None of those libraries is
+ * available here, so this file restates each one from a published method:
+ *
+ *   o_exp   Cody–Waite reduction x = k ln2 + r (ln2 split into a 32-bit head and
+ *           a tail), degree-13 Taylor polynomial in Horner form with fma, and
+ *           scaling by 2^k through the exponent bits.
+ *   o_log   x = 2^e m, m in [1/sqrt2, sqrt2); log m = 2 atanh(s), s=(m-1)/(m+1),
+ *           odd series to s^23; log x = e ln2 + log m.
+ *   o_pow4  Julia's literal T^4 is `pow_body(T, 4)`: exponentiation by squaring
+ *           carrying the low parts of each square (error-free products with
+ *           fma), then one rounding of head + tail.
+ *   o_min/o_max  Julia's Float64 min/max: NaN propagates, -0.0 < 0.0.
+ *   o_clamp The reference's own clamp (src/utils.jl:6), NaN passes through.
+ *   o_hypot Julia's hypot algorithm: order, early-out for widely varying
+ *           operands, 2^+-563 rescaling, sqrt(fma(ax,ax,ay*ay)) and one
+ *           fma-based correction step.
+ *   o_besselkx  e^x K_nu(x), nu = 0, 1 (then upward recurrence):
+ *           x < 1   power series of A&S 9.6.10-9.6.13 (K0, K1 via I0, I1 and
+ *                   the digamma sums), times e^x;
+ *           x >= 1  trapezoidal rule (34 nodes, step 1/5) on the Laplace-type
+ *                   representation DLMF 10.32.8 after t = s^2:
+ *                   e^x K_nu(x) = sqrt(pi/2x)/Gamma(nu+1/2) *
+ *                                 int_R e^{-s^2} |s|^{2nu} (1+s^2/2x)^{nu-1/2} ds;
+ *           x >= 1e4  the reference's three-term asymptotic series
+ *                   (safe_besselkx, src/eos.jl:27-34), verbatim in arithmetic.
+ *           Checked against mpmath to <= 6e-16 relative (tests/test_oracle_math.py).
+ *
+ * The CUDA library implements the same algorithms with the same operation
+ * order, and both are compiled without floating-point contraction, so the
+ * oracle and the device produce identical bits.
+ */
+#ifndef FIVO_ORACLE_JLMATH_H
+#define FIVO_ORACLE_JLMATH_H
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+
+namespace orc {
+
+static const double O_INF = std::numeric_limits<double>::infinity();
+static const double O_NAN = std::numeric_limits<double>::quiet_NaN();
+static const double O_PI = 3.141592653589793;
+
+static inline uint64_t o_bits(double x) { uint64_t u; std::memcpy(&u, &x, 8); return u; }
+static inline double o_from_bits(uint64_t u) { double x; std::memcpy(&x, &u, 8); return x; }
+static inline bool o_isnan(double x) { return x != x; }
+static inline bool o_isfinite(double x) { return std::isfinite(x); }
+static inline bool o_signbit(double x) { return (o_bits(x) >> 63) != 0; }
+
+/* Julia Base min/max for Float64 (NaN-propagating, -0.0 < 0.0). */
+static inline double o_min(double x, double y) {
+  bool take_y = (y < x) || (o_signbit(y) && !o_signbit(x));
+  return take_y ? (o_isnan(x) ? x : y) : (o_isnan(y) ? y : x);
+}
+static inline double o_max(double x, double y) {
+  bool take_y = (y > x) || (!o_signbit(y) && o_signbit(x));
+  return take_y ? (o_isnan(x) ? x : y) : (o_isnan(y) ? y : x);
+}
+/* src/utils.jl:6 — `clamp(x, a, b) = x < a ? a : (x > b ? b : x)` */
+static inline double o_clamp(double x, double a, double b) { return x < a ? a : (x > b ? b : x); }
+/* Julia sign: NaN -> NaN, +-0 -> +-0, else +-1 */
+static inline double o_sign(double x) {
+  if (o_isnan(x)) return x;
+  if (x == 0.0) return x;
+  return x > 0.0 ? 1.0 : -1.0;
+}
+
+/* 2^k * p for p in [0.5, 2), k in [-1100, 1100] */
+static inline double o_scale2(double p, int k) {
+  if (k > 1023) { p = p * 8.98846567431158e307; k -= 1023; if (k > 1023) k = 1023; }  /* 2^1023 */
+  if (k < -1022) {
+    p = p * o_from_bits((uint64_t)(k + 1000 + 1023) << 52);
+    return p * o_from_bits((uint64_t)(1023 - 1000) << 52);
+  }
+  return p * o_from_bits((uint64_t)(k + 1023) << 52);
+}
+
+static const double O_LN2_HI = 0.6931471803691238;     /* 32 leading bits of ln 2 */
+static const double O_LN2_LO = 1.9082149292705877e-10; /* ln 2 - O_LN2_HI          */
+static const double O_INV_LN2 = 1.4426950408889634;
+
+static inline double o_exp(double x) {
+  if (o_isnan(x)) return x;
+  if (x > 709.782712893384) return O_INF;
+  if (x < -745.1332191019412) return 0.0;
+  double kd = std::nearbyint(x * O_INV_LN2);
+  double r = std::fma(-kd, O_LN2_HI, x);
+  r = std::fma(-kd, O_LN2_LO, r);
+  double p = 1.6059043836821613e-10;            /* 1/13! */
+  p = std::fma(p, r, 2.08767569878681e-09);      /* 1/12! */
+  p = std::fma(p, r, 2.505210838544172e-08);
+  p = std::fma(p, r, 2.755731922398589e-07);
+  p = std::fma(p, r, 2.7557319223985893e-06);
+  p = std::fma(p, r, 2.48015873015873e-05);
+  p = std::fma(p, r, 0.0001984126984126984);
+  p = std::fma(p, r, 0.001388888888888889);
+  p = std::fma(p, r, 0.008333333333333333);
+  p = std::fma(p, r, 0.041666666666666664);
+  p = std::fma(p, r, 0.16666666666666666);
+  p = std::fma(p, r, 0.5);
+  p = std::fma(p, r, 1.0);
+  p = std::fma(p, r, 1.0);
+  return o_scale2(p, (int)kd);
+}
+
+static inline double o_log(double x) {
+  if (o_isnan(x)) return x;
+  if (x < 0.0) return O_NAN;
+  if (x == 0.0) return -O_INF;
+  if (x == O_INF) return x;
+  int e = 0;
+  if (x < 2.2250738585072014e-308) { x = x * 18014398509481984.0; e = -54; }  /* 2^54 */
+  uint64_t u = o_bits(x);
+  e += (int)((u >> 52) & 0x7ff) - 1023;
+  double m = o_from_bits((u & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL);
+  if (m > 1.4142135623730951) { m = m * 0.5; e += 1; }
+  double f = m - 1.0;
+  double s = f / (2.0 + f);
+  double z = s * s;
+  double q = 0.043478260869565216;               /* 1/23 */
+  q = std::fma(q, z, 0.047619047619047616);       /* 1/21 */
+  q = std::fma(q, z, 0.05263157894736842);
+  q = std::fma(q, z, 0.058823529411764705);
+  q = std::fma(q, z, 0.06666666666666667);
+  q = std::fma(q, z, 0.07692307692307693);
+  q = std::fma(q, z, 0.09090909090909091);
+  q = std::fma(q, z, 0.1111111111111111);
+  q = std::fma(q, z, 0.14285714285714285);
+  q = std::fma(q, z, 0.2);
+  q = std::fma(q, z, 0.3333333333333333);
+  double lm = std::fma(2.0 * s, z * q, 2.0 * s);
+  double ed = (double)e;
+  return std::fma(ed, O_LN2_HI, std::fma(ed, O_LN2_LO, lm));
+}
+
+/* Julia `x^4` for Float64 (literal_pow -> pow_body(x, 4)). */
+static inline double o_pow4(double x) {
+  double x2 = x * x;
+  double e2 = std::fma(x, x, -x2);
+  double err = (x2 * 2.0) * e2;
+  double x4 = x2 * x2;
+  double lo = std::fma(x2, x2, -x4) + err;
+  if (o_isfinite(x4) && o_isfinite(lo)) return x4 + lo;
+  return x4;
+}
+
+static inline double o_hypot(double x, double y) {
+  if (std::isinf(x) || std::isinf(y)) return O_INF;
+  double ax = std::fabs(x), ay = std::fabs(y);
+  if (ay > ax) { double t = ax; ax = ay; ay = t; }
+  if (ay <= ax * 1.0536712127723509e-08) return ax;      /* sqrt(eps/2) */
+  double scale = 1.0;
+  if (ax > 9.480751908109176e153) {                        /* sqrt(floatmax/2) */
+    ax = ax * 3.312168642111238e-170; ay = ay * 3.312168642111238e-170;  /* 2^-563 */
+    scale = 3.019169939857233e169;
+  } else if (ay < 1.4916681462400413e-154) {               /* sqrt(floatmin) */
+    ax = ax * 3.019169939857233e169; ay = ay * 3.019169939857233e169;
+    scale = 3.312168642111238e-170;
+  }
+  double h = std::sqrt(std::fma(ax, ax, ay * ay));
+  double hsq = h * h, axsq = ax * ax;
+  h -= (std::fma(-ay, ay, hsq - axsq) + std::fma(h, h, -hsq) - std::fma(ax, ax, -axsq)) / (2.0 * h);
+  return h * scale;
+}
+
+/* ---------------- scaled modified Bessel K ---------------- */
+
+static const double O_BESSEL_S2[34] = {
+  0.0, 0.04, 0.16, 0.36, 0.64, 1.0, 1.44, 1.96, 2.56, 3.24, 4.0, 4.84, 5.76, 6.76,
+  7.84, 9.0, 10.24, 11.56, 12.96, 14.44, 16.0, 17.64, 19.36, 21.16, 23.04, 25.0,
+  27.04, 29.16, 31.36, 33.64, 36.0, 38.44, 40.96, 43.56};
+static const double O_BESSEL_W[34] = {
+  0.11283791670955126, 0.21682695742097263, 0.19230825976786156, 0.15744868634285744,
+  0.11899715725149379, 0.08302149948411894, 0.05346886940070783, 0.03178834153545557,
+  0.017445811726789072, 0.008838344666402213, 0.004133397070818411, 0.001784431012983241,
+  0.0007111297361755495, 0.00026161000994465633, 8.884158884113332e-05, 2.785061038934957e-05,
+  8.059527106647123e-06, 2.1529842073361357e-06, 5.309193689433173e-07, 1.2085725786444936e-07,
+  2.5396469343733115e-08, 4.926408197336689e-09, 8.821529389366844e-10, 1.4581890004763904e-10,
+  2.225052137962172e-11, 3.134173306203467e-12, 4.075325146752109e-13, 4.89167914078347e-14,
+  5.420134984939562e-15, 5.543942072256747e-16, 5.2346024784985296e-17, 4.5625240909092945e-18,
+  3.670988941398298e-19, 2.726574842629012e-20};
+static const double O_EULER_GAMMA = 0.5772156649015329;
+
+/* e^x K0(x), e^x K1(x) for 0 < x < 1e4 */
+static inline void o_k01x(double x, double* k0x, double* k1x) {
+  if (x < 1.0) {
+    double t = 0.25 * x * x;
+    double term = 1.0, i0 = 1.0, s0 = 0.0, hk = 0.0;
+    double term1 = 1.0, i1 = 1.0;
+    double s1 = (-O_EULER_GAMMA) + (1.0 - O_EULER_GAMMA);
+    for (int k = 1; k <= 15; ++k) {
+      double kk = (double)k;
+      term = term * (t / (kk * kk));
+      hk = hk + 1.0 / kk;
+      i0 = i0 + term;
+      s0 = s0 + hk * term;
+      term1 = term1 * (t / (kk * (kk + 1.0)));
+      i1 = i1 + term1;
+      s1 = s1 + (2.0 * (hk - O_EULER_GAMMA) + 1.0 / (kk + 1.0)) * term1;
+    }
+    double lx = o_log(0.5 * x);
+    double k0 = -(lx + O_EULER_GAMMA) * i0 + s0;
+    double I1 = 0.5 * x * i1;
+    double k1 = 1.0 / x + lx * I1 - 0.25 * x * s1;
+    double ex = o_exp(x);
+    *k0x = k0 * ex;
+    *k1x = k1 * ex;
+    return;
+  }
+  double inv2x = 1.0 / (2.0 * x);
+  double a0 = 0.0, a1 = 0.0;
+  for (int k = 33; k >= 0; --k) {
+    double s2 = O_BESSEL_S2[k];
+    double q = std::sqrt(1.0 + s2 * inv2x);
+    a0 = a0 + O_BESSEL_W[k] / q;
+    a1 = a1 + (O_BESSEL_W[k] * s2) * q;
+  }
+  double pre = std::sqrt(O_PI / (2.0 * x));
+  *k0x = pre * a0;
+  *k1x = pre * (2.0 * a1);
+}
+
+/* safe_besselkx(nu, x), src/eos.jl:27-34: 0 for x <= 0 or non-finite, the
+ * asymptotic series for x >= 1e4, else e^x K_nu(x) by upward recurrence. */
+static inline double o_besselkx(int nu, double x) {
+  if (!(o_isfinite(x) && x > 0.0)) return 0.0;
+  if (x >= 1.0e4) {
+    double mu = 4.0 * ((double)nu * (double)nu);
+    double ix = 1.0 / (8.0 * x);
+    double s = 1.0 + (mu - 1.0) * ix * (1.0 + (mu - 9.0) * ix / 2.0 * (1.0 + (mu - 25.0) * ix / 3.0));
+    return std::sqrt(O_PI / (2.0 * x)) * s;
+  }
+  double k0, k1;
+  o_k01x(x, &k0, &k1);
+  if (nu == 0) return k0;
+  if (nu == 1) return k1;
+  double km = k0, kc = k1;
+  for (int n = 1; n < nu; ++n) {
+    double kn = km + ((2.0 * n) / x) * kc;
+    km = kc; kc = kn;
+  }
+  return kc;
+}
+
+}  // namespace orc
+#endif

@@ -1,0 +1,223 @@
+"""ctypes wrapper of the CPU oracle (oracle/liboracle_fivo2d.so) for the tests.
+
+The oracle is test infrastructure: only tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg use this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+import subprocess
+import sys
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+sys.path.insert(0, str(ROOT / "fivohydro.jl_b200"))
+
+from fivo2d import _abi as A  # noqa: E402
+
+ORACLE_DIR = ROOT / "oracle"
+ORACLE_SO = ORACLE_DIR / "liboracle_fivo2d.so"
+
+_D = C.POINTER(C.c_double)
+_U8 = C.POINTER(C.c_uint8)
+_lib = None
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if a.dtype == np.uint8:
+        return a.ctypes.data_as(_U8)
+    return a.ctypes.data_as(_D)
+
+
+def build_oracle():
+    subprocess.run(["make", "-s", "-C", str(ORACLE_DIR)], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not ORACLE_SO.exists():
+            build_oracle()
+        L = C.CDLL(str(ORACLE_SO))
+        P = C.POINTER(A.FivoParams)
+        sig = {
+            "oracle_last_error": (C.c_char_p, []),
+            "oracle_ctx_create": (C.c_void_p, [P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double]),
+            "oracle_ctx_destroy": (None, [C.c_void_p]),
+            "oracle_ctx_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int64), _D]),
+            "oracle_set_state": (None, [C.c_void_p, _D]),
+            "oracle_get_state": (None, [C.c_void_p, _D]),
+            "oracle_set_history": (None, [C.c_void_p] + [_D] * 8),
+            "oracle_get_history": (None, [C.c_void_p] + [_D] * 8),
+            "oracle_reset_history": (None, [C.c_void_p]),
+            "oracle_get_primitives": (None, [C.c_void_p] + [_D] * 9 + [_U8]),
+            "oracle_get_counters": (None, [C.c_void_p, C.POINTER(A.FivoCounters)]),
+            "oracle_rhs": (None, [C.c_void_p, C.c_double, C.c_int, _U8, _D]),
+            "oracle_step": (None, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
+                                   _D, C.POINTER(C.c_int)]),
+            "oracle_update_primitives": (C.c_int64, [C.c_void_p, C.c_double, C.c_int]),
+            "oracle_relax": (None, [C.c_void_p, C.c_double, C.c_double]),
+            "oracle_project_shear": (None, [C.c_void_p, _D, _D]),
+            "oracle_compute_dt": (C.c_double, [C.c_void_p, C.c_double, C.c_double, C.c_double]),
+            "oracle_run": (None, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                                  C.c_int, C.c_int64, C.c_int, C.POINTER(A.FivoRunResult)]),
+            "oracle_finalize_ic": (None, [C.c_void_p, C.c_double, C.c_int]),
+            "oracle_set_cells": (C.c_int, [P, C.c_int64, C.c_double] + [_D] * 10 + [_D, _U8]),
+            "oracle_eos_Pne": (None, [P, C.c_int64, _D, _D, _D, _D, _D]),
+            "oracle_eos_cs2": (None, [P, C.c_int64, _D, _D, _D]),
+            "oracle_cons_to_prim": (None, [P, C.c_int64, C.c_double, _D, _D, _D, _U8, _U8]),
+            "oracle_besselkx": (None, [C.c_int, C.c_int64, _D, _D]),
+            "oracle_exp": (None, [C.c_int64, _D, _D]),
+            "oracle_log": (None, [C.c_int64, _D, _D]),
+            "oracle_pow4": (None, [C.c_int64, _D, _D]),
+            "oracle_hypot": (None, [C.c_int64, _D, _D, _D]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def vec(fn, x, *more):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.empty_like(x)
+    args = [np.ascontiguousarray(m, dtype=np.float64) for m in more]
+    fn(x.size, _ptr(x), *[_ptr(a) for a in args], _ptr(out))
+    return out
+
+
+def besselkx(nu, x):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.empty_like(x)
+    lib().oracle_besselkx(nu, x.size, _ptr(x), _ptr(out))
+    return out
+
+
+def set_cells(params, tau, T, alpha, ux, uy, nv, Pi=None, pixx=None, pixy=None, piyy=None, nux=None, nuy=None):
+    n = len(T)
+    U = np.zeros((n, nv))
+    ok = np.zeros(n, dtype=np.uint8)
+    cv = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)  # noqa: E731
+    arrs = [cv(a) for a in (T, alpha, ux, uy, Pi, pixx, pixy, piyy, nux, nuy)]
+    st = lib().oracle_set_cells(C.byref(params), n, tau, *[_ptr(a) for a in arrs], _ptr(U), _ptr(ok))
+    assert st == 0, lib().oracle_last_error()
+    return U, ok
+
+
+def eos_Pne(params, T, mu):
+    T = np.ascontiguousarray(T, dtype=np.float64)
+    mu = np.ascontiguousarray(mu, dtype=np.float64)
+    P, n, e = np.empty_like(T), np.empty_like(T), np.empty_like(T)
+    lib().oracle_eos_Pne(C.byref(params), T.size, _ptr(T), _ptr(mu), _ptr(P), _ptr(n), _ptr(e))
+    return P, n, e
+
+
+def cons_to_prim(params, tau, cons, warm=None):
+    cons = np.ascontiguousarray(cons, dtype=np.float64).reshape(-1, 11)
+    n = cons.shape[0]
+    prim = np.empty((n, 7))
+    ok = np.zeros(n, dtype=np.uint8)
+    reason = np.zeros(n, dtype=np.uint8)
+    w = None if warm is None else np.ascontiguousarray(warm, dtype=np.float64).reshape(-1, 4)
+    lib().oracle_cons_to_prim(C.byref(params), n, tau, _ptr(cons), _ptr(w), _ptr(prim), _ptr(ok), _ptr(reason))
+    return prim, ok.astype(bool), reason
+
+
+class OracleSolver:
+    """Same surface as fivo2d.solver.GPUSolver, on the CPU oracle."""
+
+    def __init__(self, model, g):
+        self.model, self.g = model, g
+        self.h = lib().oracle_ctx_create(C.byref(model.params), g.Nx, g.Ny, g.nghost, g.xmax, g.ymax)
+        if not self.h:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        self.nv = model.nv
+        self.N = g.Ntot
+
+    def close(self):
+        if self.h:
+            lib().oracle_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_state(self, U):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        assert U.size == self.nv * self.N
+        lib().oracle_set_state(self.h, _ptr(U))
+
+    def get_state(self):
+        U = np.empty((self.N, self.nv))
+        lib().oracle_get_state(self.h, _ptr(U))
+        return U
+
+    def set_history(self, **kw):
+        names = ("x0_yT", "x0_phi", "x0_ux", "x0_uy", "ux_prev", "uy_prev", "alpha_prev", "T_prev")
+        arrs = [None if kw.get(n) is None else np.ascontiguousarray(kw[n], dtype=np.float64) for n in names]
+        lib().oracle_set_history(self.h, *[_ptr(a) for a in arrs])
+
+    def get_history(self):
+        names = ("x0_yT", "x0_phi", "x0_ux", "x0_uy", "ux_prev", "uy_prev", "alpha_prev", "T_prev")
+        arrs = [np.empty(self.N) for _ in names]
+        lib().oracle_get_history(self.h, *[_ptr(a) for a in arrs])
+        return dict(zip(names, arrs))
+
+    def reset_history(self):
+        lib().oracle_reset_history(self.h)
+
+    def primitives(self):
+        names = ("yT", "phi", "mu", "alpha", "ux", "uy", "P", "n", "e")
+        arrs = [np.empty(self.N) for _ in names]
+        ok = np.empty(self.N, dtype=np.uint8)
+        lib().oracle_get_primitives(self.h, *[_ptr(a) for a in arrs], _ptr(ok))
+        d = dict(zip(names, arrs))
+        d["ok"] = ok
+        return d
+
+    def counters(self):
+        c = A.FivoCounters()
+        lib().oracle_get_counters(self.h, C.byref(c))
+        return c
+
+    def rhs(self, tau, bc=0, mask=None):
+        dU = np.empty((self.N, self.nv))
+        m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+        lib().oracle_rhs(self.h, tau, bc, _ptr(m), _ptr(dU))
+        return dU
+
+    def step(self, integrator, tau, dtau, max_halve=12, max_mood=2, bc=0):
+        used = C.c_double(0)
+        ok = C.c_int(0)
+        lib().oracle_step(self.h, integrator, tau, dtau, max_halve, max_mood, bc, C.byref(used), C.byref(ok))
+        return bool(ok.value), used.value
+
+    def update_primitives(self, tau, bc=0):
+        return lib().oracle_update_primitives(self.h, tau, bc)
+
+    def relax(self, tau, dtau):
+        lib().oracle_relax(self.h, tau, dtau)
+
+    def project_shear(self):
+        a, b = C.c_double(0), C.c_double(0)
+        lib().oracle_project_shear(self.h, C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def compute_dt(self, tau, cfl=0.2, cfltau=0.05):
+        return lib().oracle_compute_dt(self.h, tau, cfl, cfltau)
+
+    def run(self, tau0, taufinal, cfl=0.2, cfltau=0.05, integrator=A.FIVO_SSPRK2, bc=0,
+            max_steps=2_000_000, reset_history=True):
+        r = A.FivoRunResult()
+        lib().oracle_run(self.h, tau0, taufinal, cfl, cfltau, integrator, bc, max_steps, int(reset_history),
+                         C.byref(r))
+        return r.as_dict()
+
+    def finalize_ic(self, tau0, bc=0):
+        lib().oracle_finalize_ic(self.h, tau0, bc)
