@@ -1,0 +1,816 @@
+/*
+ * fivo2d.cu — the C ABI of include/fivo2d.h on one B200 (sm_100a).
+ *
+ * A context mirrors Grid2D + Work2D (src2d/grid2d.jl, src2d/work2d.jl) in HBM:
+ * four state buffers (U, U1, U2 and a scratch) of nv planes each, the cell
+ * primitives, warm starts and dtau history, three MOOD masks and a flag block.
+ * The RK buffers are addressed by role indices, so "copy U1 into U" is a role
+ * swap, and the relaxation double-buffers only the dissipative planes.
+ *
+ * Control flow (halving, MOOD escalation, the time loop) stays on the host,
+ * exactly as in src2d/timestepper2d.jl and main2D.jl:371-561; the device
+ * reports the admissibility count and the signal speed after every stage.
+ */
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+
+using namespace fv;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess) return fail(FIVO_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define CKL()                                                                             \
+  do {                                                                                    \
+    cudaError_t e_ = cudaGetLastError();                                                  \
+    if (e_ != cudaSuccess) return fail(FIVO_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+inline unsigned nblk(long long n, int b) { return (unsigned)((n + b - 1) / b); }
+
+/* reject_unwired_knobs_2d + check_terms (src2d/primitives2d.jl:246-272, src/terms.jl) */
+int validate(const fivo_params* p) {
+  if (p->consistent_fm || p->consistent_m2)
+    return fail(FIVO_ERR_CONFIG, "consistent_fm / consistent_m2 (the charm closures) are not built");
+  if (p->eos_kind != FIVO_EOS_CONFORMAL_HQ && p->eos_kind != FIVO_EOS_LATTICE_HRG)
+    return fail(FIVO_ERR_CONFIG, "unknown eos_kind");
+  if (p->enable_shear && p->shear_kind != FIVO_SHEAR_QGP && p->shear_kind != FIVO_SHEAR_ZERO)
+    return fail(FIVO_ERR_CONFIG, "unknown shear_kind");
+  if (p->enable_bulk && (p->bulk_kind < FIVO_BULK_ZERO || p->bulk_kind > FIVO_BULK_GAUSS))
+    return fail(FIVO_ERR_CONFIG, "unknown bulk_kind");
+  if (p->enable_bulk && p->bulk_kind == FIVO_BULK_GAUSS && !(p->bulk_width > 0))
+    return fail(FIVO_ERR_CONFIG, "GaussianBulkViscosity needs bulk_width > 0");
+  if (p->enable_diff && !p->with_charge)
+    return fail(FIVO_ERR_CONFIG, "enable_diff needs a layout with charge (with_charge = true)");
+  /* a term switched away from its default whose sector is off cannot act */
+  const uint32_t diff = (p->terms ^ FIVO_TERMS_DEFAULT);
+  const uint32_t fm = 0x3Eu, m2 = 0x1FFC0u;
+  if ((diff & FIVO_TERM_NU_GRADALPHA) && !p->enable_diff)
+    return fail(FIVO_ERR_CONFIG, "Terms: nu_gradalpha switched but enable_diff is off");
+  if ((diff & FIVO_TERM_SHEAR_VORTICITY) && !p->enable_shear)
+    return fail(FIVO_ERR_CONFIG, "Terms: shear_vorticity switched but enable_shear is off");
+  if ((diff & fm) || (diff & m2))
+    return fail(FIVO_ERR_CONFIG, "Terms: a charm-closure term is switched but its sector is not built");
+  if (p->primrec_maxit < 1 || !(p->primrec_tol > 0))
+    return fail(FIVO_ERR_CONFIG, "primrec_maxit must be >= 1 and primrec_tol > 0");
+  return FIVO_OK;
+}
+
+/* Layout, grid and derived constants. The derived constants are the same
+ * expressions the per-call code of the reference evaluates, computed once. */
+DevParams make_devparams(const fivo_params* p, int nx, int ny, int ng, double xmax, double ymax) {
+  DevParams d;
+  std::memset(&d, 0, sizeof(d));
+  d.p = *p;
+  int k = 0;
+  d.iDtau = k++; d.iSx = k++; d.iSy = k++; d.iE = k++;
+  d.hasNu = p->with_charge != 0; d.iNux = d.hasNu ? k++ : -1; d.iNuy = d.hasNu ? k++ : -1;
+  d.hasPi = p->enable_bulk != 0; d.iPi = d.hasPi ? k++ : -1;
+  d.hasShear = p->enable_shear != 0;
+  d.iPixx = d.hasShear ? k++ : -1; d.iPixy = d.hasShear ? k++ : -1;
+  d.iPiyy = d.hasShear ? k++ : -1; d.iPieta = d.hasShear ? k++ : -1;
+  d.nv = k;
+  d.ncharge = (p->eos_kind == FIVO_EOS_CONFORMAL_HQ) ? (p->g_hq > 0.0) : 1;
+  d.Nx = nx; d.Ny = ny; d.ng = ng; d.Nxtot = nx + 2 * ng; d.Nytot = ny + 2 * ng;
+  d.Ntot = (long long)d.Nxtot * d.Nytot;
+  d.xmin = -xmax; d.ymin = -ymax;
+  d.dx = (xmax - d.xmin) / nx; d.dy = (ymax - d.ymin) / ny;
+  const double fmgev = 1.0 / 0.1973269804;
+  d.fmgev3 = (fmgev * fmgev) * fmgev;
+  d.pi2 = FX_PI * FX_PI;
+  d.aSB = (d.pi2 / 90.0) * p->g_eff;
+  double m = p->m_hq, g = p->g_hq;
+  d.A_conf = (g * (m * m)) / (2.0 * d.pi2);
+  d.A_lhrg = ((p->canon_factor * g) * (m * m)) / (2.0 * d.pi2);
+  d.lA = 0.01 * (p->lhrg_d * p->lhrg_d);
+  d.lB = 0.1 * (p->lhrg_c * p->lhrg_c);
+  d.log_T_min = fx_log(FV_T_MIN);
+  d.log_T_solve_max = fx_log(FV_T_SOLVE_MAX);
+  d.log_seed_T = fx_log(jmax(0.15, FV_T_MIN));
+  /* build_model_2d derives E_vac_cut from T_vac_cut (main2D.jl:102-108) */
+  if (p->E_vac_cut > 0.0) d.E_vac_cut = p->E_vac_cut;
+  else {
+    double P, n, e;
+    if (p->eos_kind == FIVO_EOS_CONFORMAL_HQ) eos_Pne<FIVO_EOS_CONFORMAL_HQ>(p->T_vac_cut, 0.0, d, &P, &n, &e);
+    else eos_Pne<FIVO_EOS_LATTICE_HRG>(p->T_vac_cut, 0.0, d, &P, &n, &e);
+    d.E_vac_cut = e;
+  }
+  return d;
+}
+
+}  // namespace
+
+struct fivo_ctx {
+  DevParams dp;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  double* slab = nullptr;
+  DevState S[4];
+  int iU = 0, iU1 = 1, iU2 = 2, iT = 3;
+  double* pbuf = nullptr;
+  DevPrims w;
+  double* hbuf = nullptr;
+  DevHist h;
+  uint8_t* masks = nullptr;   /* bad | mask | tmp, Ntot bytes each */
+  DevFlags* fl = nullptr;
+  DevFlags* flh = nullptr;    /* pinned mirror */
+  double* dU = nullptr;       /* lazily allocated RHS planes for fivo_rhs */
+  double* stage = nullptr;    /* nv x Ntot AoS staging for uploads and downloads */
+  bool hist_valid = false;
+  fivo_counters cnt;
+  long long rep_none = 0;
+};
+
+namespace {
+
+const long long REP_NONE = 0x7fffffffffffffffLL;
+
+/* ---------------------------------------------------------- launch helpers */
+
+int launch_bc(fivo_ctx* c, const DevState& U, int bc) {
+  const DevParams& d = c->dp;
+  long long nframe = d.Ntot - (long long)d.Nx * d.Ny;
+  k_bc<<<nblk(nframe, 256), 256, 0, c->st>>>(d, U, bc);
+  CKL();
+  return FIVO_OK;
+}
+
+/* what: see k_reset_flags. amax is reset to 0 only by an rhs pass (rhs_2d!
+ * fills amax_tls, src2d/rhs2d.jl:193); other passes leave it alone. */
+int reset_flags(fivo_ctx* c, int what) {
+  k_reset_flags<<<1, 32, 0, c->st>>>(c->fl, what, 0ULL);
+  CKL();
+  return FIVO_OK;
+}
+
+int launch_primitive(fivo_ctx* c, const DevState& U, double tau) {
+  const DevParams& d = c->dp;
+  unsigned g = nblk(d.Ntot, 128);
+  if (d.p.eos_kind == FIVO_EOS_LATTICE_HRG)
+    k_primitive<FIVO_EOS_LATTICE_HRG, true><<<g, 128, 0, c->st>>>(d, U, c->w, c->h, tau, c->fl);
+  else if (d.ncharge)
+    k_primitive<FIVO_EOS_CONFORMAL_HQ, true><<<g, 128, 0, c->st>>>(d, U, c->w, c->h, tau, c->fl);
+  else
+    k_primitive<FIVO_EOS_CONFORMAL_HQ, false><<<g, 128, 0, c->st>>>(d, U, c->w, c->h, tau, c->fl);
+  CKL();
+  return FIVO_OK;
+}
+
+template <int EOS, bool NCH>
+int launch_stage_t(fivo_ctx* c, const StageArgs& a) {
+  const DevParams& d = c->dp;
+  size_t smem = (size_t)(ST_NFX + ST_NFY) * d.nv * sizeof(double);
+  static bool attr_set = false;
+  if (!attr_set) {
+    CK(cudaFuncSetAttribute(k_stage<EOS, NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, 120 * 1024));
+    attr_set = true;
+  }
+  dim3 grid((d.Nxtot + ST_CX - 1) / ST_CX, (d.Nytot + ST_CY - 1) / ST_CY);
+  k_stage<EOS, NCH><<<grid, 256, smem, c->st>>>(d, a);
+  CKL();
+  return FIVO_OK;
+}
+
+int launch_stage(fivo_ctx* c, const StageArgs& a) {
+  if (c->dp.p.eos_kind == FIVO_EOS_LATTICE_HRG) return launch_stage_t<FIVO_EOS_LATTICE_HRG, true>(c, a);
+  if (c->dp.ncharge) return launch_stage_t<FIVO_EOS_CONFORMAL_HQ, true>(c, a);
+  return launch_stage_t<FIVO_EOS_CONFORMAL_HQ, false>(c, a);
+}
+
+int sync_flags(fivo_ctx* c, bool read_amax) {
+  CK(cudaMemcpyAsync(c->flh, c->fl, sizeof(DevFlags), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  const DevFlags& f = *c->flh;
+  c->cnt.nprimfail = f.nprimfail;
+  c->cnt.nvacuum = f.nvacuum;
+  if (f.rep != (unsigned long long)REP_NONE) {
+    c->cnt.primfail_index = (int64_t)(f.rep >> 8);
+    c->cnt.primfail_reason = (int32_t)(f.rep & 0xff);
+  } else {
+    c->cnt.primfail_index = -1;
+    c->cnt.primfail_reason = 0;
+  }
+  c->cnt.primfail_resnorm = fx::nan_();
+  if (read_amax) {
+    uint64_t ab = f.amax_bits;
+    double am; std::memcpy(&am, &ab, 8);
+    c->cnt.amax = am;
+  }
+  return FIVO_OK;
+}
+
+/* rhs_2d! + combination + sanitize + admissibility on the given roles.
+ * ub = base (and combination input), uo = output, uold = blend partner.
+ * Returns FIVO_OK; *nbad = inadmissible interior cells. */
+int run_stage(fivo_ctx* c, int ub, int uo, int uold, double tau, double tau_state, double dt, double wold,
+              double wnew, int mode, const uint8_t* mask, int bc, long long* nbad, double* dU) {
+  int rc;
+  if ((rc = launch_bc(c, c->S[ub], bc))) return rc;
+  if ((rc = reset_flags(c, 1 | 2))) return rc;
+  if ((rc = launch_primitive(c, c->S[ub], tau))) return rc;
+  StageArgs a;
+  a.Ub = c->S[ub]; a.Uold = c->S[uold]; a.Uout = c->S[uo]; a.w = c->w; a.ffo = mask;
+  a.bad = c->masks; a.dU = dU; a.tau = tau; a.tau_state = tau_state; a.dt = dt; a.wold = wold;
+  a.wnew = wnew; a.mode = mode; a.fl = c->fl;
+  if ((rc = launch_stage(c, a))) return rc;
+  if (mode != COMB_RHS_ONLY)
+    if ((rc = launch_bc(c, c->S[uo], bc))) return rc;
+  if ((rc = sync_flags(c, true))) return rc;
+  if (nbad) *nbad = c->flh->nbad;
+  return FIVO_OK;
+}
+
+/* _stage_2d! with the MOOD escalation, src2d/timestepper2d.jl:113-140 */
+int stage_mood(fivo_ctx* c, int ub, int uo, int uold, double tau, double tau_state, double dt, double wold,
+               double wnew, int bc, int max_mood, bool* ok) {
+  const DevParams& d = c->dp;
+  const uint8_t* mask = nullptr;
+  uint8_t* bad = c->masks;
+  uint8_t* m1 = c->masks + d.Ntot;
+  uint8_t* m2 = c->masks + 2 * d.Ntot;
+  int mode = (wnew == 0.0) ? COMB_EULER : COMB_BLEND;
+  for (int attempt = 0; attempt <= max_mood; ++attempt) {
+    long long nbad = 0;
+    int rc = run_stage(c, ub, uo, uold, tau, tau_state, dt, wold, wnew, mode, mask, bc, &nbad, nullptr);
+    if (rc) return rc;
+    if (nbad == 0) { *ok = true; return FIVO_OK; }
+    if (attempt == max_mood) { *ok = false; return FIVO_OK; }
+    c->cnt.nmood += 1;
+    /* expand_bad_2d!(radius = 1 + attempt): bad -> m1 -> m2 -> ... */
+    const uint8_t* src = bad;
+    uint8_t* dst = m1;
+    for (int r = 0; r < 1 + attempt; ++r) {
+      k_expand_bad<<<nblk(d.Ntot, 256), 256, 0, c->st>>>(d, src, dst);
+      CKL();
+      src = dst;
+      dst = (dst == m1) ? m2 : m1;
+    }
+    mask = src;
+  }
+  *ok = false;
+  return FIVO_OK;
+}
+
+int copy_state(fivo_ctx* c, int dst, int src) {
+  const DevParams& d = c->dp;
+  k_copy_planes<<<nblk(d.Ntot, 256), 256, 0, c->st>>>(c->S[dst], c->S[src], 0, d.nv, d.Ntot);
+  CKL();
+  return FIVO_OK;
+}
+
+/* step_ssprk2_2d!, src2d/timestepper2d.jl:74-103 */
+int step2(fivo_ctx* c, double tau, double dtau, int max_halve, int max_mood, int bc, double* used, int* okout) {
+  double D = dtau;
+  c->cnt.nmood = 0; c->cnt.nhalve = 0;
+  for (int h = 0; h <= max_halve; ++h) {
+    int rc;
+    if ((rc = copy_state(c, c->iU2, c->iU))) return rc;
+    bool ok1 = false, ok2 = false;
+    if ((rc = stage_mood(c, c->iU, c->iU1, c->iU2, tau, tau + D, D, 1.0, 0.0, bc, max_mood, &ok1))) return rc;
+    if (ok1) {
+      if ((rc = stage_mood(c, c->iU1, c->iT, c->iU2, tau + D, tau + D, D, 0.5, 0.5, bc, max_mood, &ok2))) return rc;
+      if (ok2) { std::swap(c->iU, c->iT); *used = D; *okout = 1; return FIVO_OK; }
+    }
+    std::swap(c->iU, c->iU2);   /* copyto!(U, work.U2) */
+    D *= 0.5;
+    c->cnt.nhalve += 1;
+  }
+  *used = D; *okout = 0;
+  return FIVO_OK;
+}
+
+/* step_ssprk3_2d!, src2d/timestepper2d.jl:148-188 */
+int step3(fivo_ctx* c, double tau, double dtau, int max_halve, int bc, double* used, int* okout) {
+  double D = dtau;
+  c->cnt.nmood = 0; c->cnt.nhalve = 0;
+  for (int h = 0; h <= max_halve; ++h) {
+    int rc;
+    long long nbad = 0;
+    if ((rc = copy_state(c, c->iU2, c->iU))) return rc;
+    if ((rc = run_stage(c, c->iU, c->iU1, c->iU2, tau, tau + D, D, 1.0, 0.0, COMB_EULER, nullptr, bc, &nbad, nullptr))) return rc;
+    if (nbad) { std::swap(c->iU, c->iU2); D *= 0.5; c->cnt.nhalve += 1; continue; }
+    if ((rc = run_stage(c, c->iU1, c->iT, c->iU2, tau + D, tau + D, D, 0.75, 0.25, COMB_BLEND, nullptr, bc, &nbad, nullptr))) return rc;
+    std::swap(c->iU1, c->iT);
+    if (nbad) { std::swap(c->iU, c->iU2); D *= 0.5; c->cnt.nhalve += 1; continue; }
+    if ((rc = run_stage(c, c->iU1, c->iT, c->iU2, tau + (0.5 * D), tau + D, D, 0.0, 0.0, COMB_THIRD, nullptr, bc, &nbad, nullptr))) return rc;
+    std::swap(c->iU, c->iT);
+    if (!nbad) { *used = D; *okout = 1; return FIVO_OK; }
+    std::swap(c->iU, c->iU2);
+    D *= 0.5;
+    c->cnt.nhalve += 1;
+  }
+  *used = D; *okout = 0;
+  return FIVO_OK;
+}
+
+/* update_primitives_2d!, src2d/rhs2d.jl:57-65 */
+int update_prims(fivo_ctx* c, double tau, int bc) {
+  int rc;
+  if ((rc = launch_bc(c, c->S[c->iU], bc))) return rc;
+  if ((rc = reset_flags(c, 1))) return rc;
+  if ((rc = launch_primitive(c, c->S[c->iU], tau))) return rc;
+  return FIVO_OK;
+}
+
+/* relax_dissipative_2d! (+ project_shear! when project != 0) on U */
+int relax_project(fivo_ctx* c, double tau, double D, int do_relax, int do_project) {
+  const DevParams& d = c->dp;
+  if (d.nv <= 4) return FIVO_OK;
+  DevState Uq = c->S[c->iU], Uo = c->S[c->iT];
+  int rc = reset_flags(c, 4);
+  if (rc) return rc;
+  unsigned g = nblk(d.Ntot, 128);
+  if (d.p.eos_kind == FIVO_EOS_LATTICE_HRG)
+    k_relax<FIVO_EOS_LATTICE_HRG><<<g, 128, 0, c->st>>>(d, Uq, Uo, c->w, c->h, tau, D, do_relax, do_project, c->fl);
+  else
+    k_relax<FIVO_EOS_CONFORMAL_HQ><<<g, 128, 0, c->st>>>(d, Uq, Uo, c->w, c->h, tau, D, do_relax, do_project, c->fl);
+  CKL();
+  /* the dissipative planes of U are now those of the scratch state */
+  for (int a = 4; a < d.nv; ++a) std::swap(c->S[c->iU].f[a], c->S[c->iT].f[a]);
+  if (do_relax) {
+    CK(cudaMemcpyAsync(c->h.ux_prev, c->w.ux, d.Ntot * 8, cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaMemcpyAsync(c->h.uy_prev, c->w.uy, d.Ntot * 8, cudaMemcpyDeviceToDevice, c->st));
+  }
+  return FIVO_OK;
+}
+
+int read_shear(fivo_ctx* c, double* maxr, double* meanr) {
+  CK(cudaMemcpyAsync(c->flh, c->fl, sizeof(DevFlags), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  uint64_t b = c->flh->shear_max_bits;
+  double m; std::memcpy(&m, &b, 8);
+  if (maxr) *maxr = m;
+  long long cnt = (long long)c->dp.Nx * c->dp.Ny;
+  if (meanr) *meanr = cnt > 0 ? c->flh->shear_sum / cnt : 0.0;
+  return FIVO_OK;
+}
+
+int fill_nan(fivo_ctx* c, double* p, long long n) {
+  k_fill_nan<<<nblk(n, 256), 256, 0, c->st>>>(p, n);
+  CKL();
+  return FIVO_OK;
+}
+
+int reset_history(fivo_ctx* c) {
+  int rc;
+  /* x0_* and the four *_prev planes are contiguous in hbuf */
+  if ((rc = fill_nan(c, c->hbuf, 8 * c->dp.Ntot))) return rc;
+  c->hist_valid = false;
+  return FIVO_OK;
+}
+
+int diag(fivo_ctx* c, bool want_u, double* sumD, double* maxu, double* minPtot) {
+  const DevParams& d = c->dp;
+  int rc = reset_flags(c, 8);
+  if (rc) return rc;
+  k_diag<<<nblk((long long)d.Nx * d.Ny, 256), 256, 0, c->st>>>(d, c->S[c->iU], c->w, c->fl, want_u ? 1 : 0);
+  CKL();
+  CK(cudaMemcpyAsync(c->flh, c->fl, sizeof(DevFlags), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  *sumD = c->flh->sumD;
+  if (maxu) *maxu = c->flh->maxu;
+  if (minPtot) *minPtot = c->flh->minPtot;
+  return FIVO_OK;
+}
+
+}  // namespace
+
+/* ==================================================================== ABI */
+
+extern "C" {
+
+int fivo_abi_version(void) { return FIVO_ABI_VERSION; }
+
+const char* fivo_last_error(void) { return g_err.c_str(); }
+
+void fivo_params_default(fivo_params* p) {
+  std::memset(p, 0, sizeof(*p));
+  /* LatticeHRGEOS() (src/eos.jl:318-345) */
+  const double a[4] = {-15.526548963383643, 18.6159584620131, -10.731808109698516, 2.7413302179949346};
+  const double b[4] = {-3.3147904483107595, 5.310983721567554, -4.653922019495976, 1.8600649533271152};
+  for (int k = 0; k < 4; ++k) { p->lhrg_a[k] = a[k]; p->lhrg_b[k] = b[k]; }
+  p->lhrg_c = -1.0465330501411811; p->lhrg_d = 0.09551531822245873;
+  p->g_eff = 40.0; p->m_hq = 1.5; p->g_hq = 6.0;
+  p->canon_factor = 0.9524014587885937;
+  p->eos_kind = FIVO_EOS_LATTICE_HRG; p->hq_times_fmGeV3 = 1;
+  /* IdealDiffVisc2DModel / build_model_2d defaults (src2d/primitives2d.jl:41-210, main2D.jl:85-93) */
+  p->with_charge = 1;
+  p->tauN_coeff = 1.0; p->nu_clip_factor = -1.0; p->vacuum_n_lo = 1e-6; p->vacuum_n_hi = 2e-3;
+  p->eta_over_s = 0.1; p->tauShear_coeff = 0.2; p->deltaShear_factor = 4.0 / 3.0; p->pi_clip_factor = -1.0;
+  p->zeta_over_s = 0.1; p->tauPi_coeff = 15.0; p->bulk_T0 = 0.175; p->bulk_width = 0.024;
+  p->Pi_clip_factor = -1.0;
+  p->r_domain = fx::inf_(); p->T_vac_cut = 0.05; p->E_vac_cut = -1.0;
+  p->primrec_tol = 1e-12; p->primrec_maxit = 80;
+  p->relax_advect_nu = 1; p->relax_advect_pi = 1; p->relax_advect_Pi = 1; p->vacuum_ramp_relax = 1;
+  p->shear_projected_deriv = 1; p->diff_projected_deriv = 1; p->shear_constraint_project = 1;
+  p->terms = FIVO_TERMS_DEFAULT;
+}
+
+int fivo_ctx_create(const fivo_params* p, int nx, int ny, int nghost, double xmax, double ymax, fivo_ctx** out) {
+  if (!p || !out) return fail(FIVO_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (nx <= 8 || ny <= 8) return fail(FIVO_ERR_ARG, "make_grid2d: Nx and Ny must exceed 8");
+  if (nghost != 3) return fail(FIVO_ERR_ARG, "the stage is built for nghost = 3");
+  if (!(xmax > 0) || !(ymax > 0)) return fail(FIVO_ERR_ARG, "xmax and ymax must be positive");
+  int rc = validate(p);
+  if (rc) return rc;
+  fivo_ctx* c = new fivo_ctx();
+  c->dp = make_devparams(p, nx, ny, nghost, xmax, ymax);
+  const DevParams& d = c->dp;
+  std::memset(&c->cnt, 0, sizeof(c->cnt));
+  c->cnt.primfail_index = -1;
+  auto cleanup = [&](int code) { fivo_ctx_destroy(c); return code; };
+  if (cudaGetDevice(&c->device) != cudaSuccess) return cleanup(fail(FIVO_ERR_CUDA, "no CUDA device"));
+  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess)
+    return cleanup(fail(FIVO_ERR_CUDA, "cudaStreamCreate failed"));
+  size_t N = (size_t)d.Ntot;
+  if (cudaMalloc(&c->slab, 4 * (size_t)d.nv * N * 8) != cudaSuccess ||
+      cudaMalloc(&c->pbuf, 9 * N * 8 + N) != cudaSuccess ||
+      cudaMalloc(&c->hbuf, 8 * N * 8) != cudaSuccess ||
+      cudaMalloc(&c->masks, 3 * N) != cudaSuccess ||
+      cudaMalloc(&c->fl, sizeof(DevFlags)) != cudaSuccess ||
+      cudaMalloc(&c->stage, (size_t)d.nv * N * 8) != cudaSuccess)
+    return cleanup(fail(FIVO_ERR_NOMEM, "device allocation failed"));
+  if (cudaMallocHost(&c->flh, sizeof(DevFlags)) != cudaSuccess)
+    return cleanup(fail(FIVO_ERR_NOMEM, "pinned allocation failed"));
+  for (int s = 0; s < 4; ++s)
+    for (int a = 0; a < FV_MAXV; ++a) c->S[s].f[a] = a < d.nv ? c->slab + ((size_t)s * d.nv + a) * N : nullptr;
+  double* q = c->pbuf;
+  c->w.yT = q; q += N; c->w.phi = q; q += N; c->w.mu = q; q += N; c->w.alpha = q; q += N;
+  c->w.ux = q; q += N; c->w.uy = q; q += N; c->w.P = q; q += N; c->w.n = q; q += N; c->w.e = q; q += N;
+  c->w.ok = (uint8_t*)q;
+  q = c->hbuf;
+  c->h.x0_yT = q; q += N; c->h.x0_phi = q; q += N; c->h.x0_ux = q; q += N; c->h.x0_uy = q; q += N;
+  c->h.ux_prev = q; q += N; c->h.uy_prev = q; q += N; c->h.alpha_prev = q; q += N; c->h.T_prev = q;
+  /* Work2D(): zeros, NaN history (src2d/work2d.jl:387-411) */
+  if (cudaMemsetAsync(c->slab, 0, 4 * (size_t)d.nv * N * 8, c->st) != cudaSuccess ||
+      cudaMemsetAsync(c->pbuf, 0, 9 * N * 8 + N, c->st) != cudaSuccess ||
+      cudaMemsetAsync(c->masks, 0, 3 * N, c->st) != cudaSuccess)
+    return cleanup(fail(FIVO_ERR_CUDA, "memset failed"));
+  if ((rc = reset_history(c))) return cleanup(rc);
+  if ((rc = reset_flags(c, 1 | 2 | 4 | 8))) return cleanup(rc);
+  if (cudaStreamSynchronize(c->st) != cudaSuccess) return cleanup(fail(FIVO_ERR_CUDA, "sync failed"));
+  *out = c;
+  return FIVO_OK;
+}
+
+int fivo_ctx_destroy(fivo_ctx* c) {
+  if (!c) return FIVO_OK;
+  if (c->st) cudaStreamSynchronize(c->st);
+  cudaFree(c->slab); cudaFree(c->pbuf); cudaFree(c->hbuf); cudaFree(c->masks); cudaFree(c->fl);
+  cudaFree(c->dU); cudaFree(c->stage);
+  if (c->flh) cudaFreeHost(c->flh);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+  return FIVO_OK;
+}
+
+int fivo_ctx_info(const fivo_ctx* c, int* nv, int64_t* ntot, double* evac) {
+  if (!c) return fail(FIVO_ERR_ARG, "null context");
+  if (nv) *nv = c->dp.nv;
+  if (ntot) *ntot = c->dp.Ntot;
+  if (evac) *evac = c->dp.E_vac_cut;
+  return FIVO_OK;
+}
+
+int fivo_upload_state(fivo_ctx* c, const double* U, int nv, int64_t ntot) {
+  if (!c || !U) return fail(FIVO_ERR_ARG, "null argument");
+  if (nv != c->dp.nv || ntot != c->dp.Ntot) return fail(FIVO_ERR_ARG, "state size mismatch");
+  /* stage the AoS block, then transpose into the U planes */
+  double* stage = c->stage;
+  CK(cudaMemcpyAsync(stage, U, (size_t)nv * ntot * 8, cudaMemcpyHostToDevice, c->st));
+  k_aos_to_soa<<<nblk((long long)nv * ntot, 256), 256, 0, c->st>>>(c->S[c->iU], stage, nv, ntot);
+  CKL();
+  CK(cudaStreamSynchronize(c->st));
+  return FIVO_OK;
+}
+
+int fivo_download_state(fivo_ctx* c, double* U, int nv, int64_t ntot) {
+  if (!c || !U) return fail(FIVO_ERR_ARG, "null argument");
+  if (nv != c->dp.nv || ntot != c->dp.Ntot) return fail(FIVO_ERR_ARG, "state size mismatch");
+  double* stage = c->stage;
+  k_soa_to_aos<<<nblk((long long)nv * ntot, 256), 256, 0, c->st>>>(c->S[c->iU], stage, nv, ntot);
+  CKL();
+  CK(cudaMemcpyAsync(U, stage, (size_t)nv * ntot * 8, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return FIVO_OK;
+}
+
+int fivo_upload_history(fivo_ctx* c, int64_t ntot, const double* x0_yT, const double* x0_phi,
+                        const double* x0_ux, const double* x0_uy, const double* ux_prev,
+                        const double* uy_prev, const double* alpha_prev, const double* T_prev) {
+  if (!c) return fail(FIVO_ERR_ARG, "null context");
+  if (ntot != c->dp.Ntot) return fail(FIVO_ERR_ARG, "history size mismatch");
+  const double* src[8] = {x0_yT, x0_phi, x0_ux, x0_uy, ux_prev, uy_prev, alpha_prev, T_prev};
+  double* dst[8] = {c->h.x0_yT, c->h.x0_phi, c->h.x0_ux, c->h.x0_uy, c->h.ux_prev, c->h.uy_prev,
+                    c->h.alpha_prev, c->h.T_prev};
+  for (int k = 0; k < 8; ++k)
+    if (src[k]) CK(cudaMemcpyAsync(dst[k], src[k], (size_t)ntot * 8, cudaMemcpyHostToDevice, c->st));
+  if (alpha_prev) c->hist_valid = fx::isfinite_(alpha_prev[0]);
+  CK(cudaStreamSynchronize(c->st));
+  return FIVO_OK;
+}
+
+int fivo_download_history(fivo_ctx* c, int64_t ntot, double* x0_yT, double* x0_phi, double* x0_ux,
+                          double* x0_uy, double* ux_prev, double* uy_prev, double* alpha_prev, double* T_prev) {
+  if (!c) return fail(FIVO_ERR_ARG, "null context");
+  if (ntot != c->dp.Ntot) return fail(FIVO_ERR_ARG, "history size mismatch");
+  double* dst[8] = {x0_yT, x0_phi, x0_ux, x0_uy, ux_prev, uy_prev, alpha_prev, T_prev};
+  const double* src[8] = {c->h.x0_yT, c->h.x0_phi, c->h.x0_ux, c->h.x0_uy, c->h.ux_prev, c->h.uy_prev,
+                          c->h.alpha_prev, c->h.T_prev};
+  for (int k = 0; k < 8; ++k)
+    if (dst[k]) CK(cudaMemcpyAsync(dst[k], src[k], (size_t)ntot * 8, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return FIVO_OK;
+}
+
+int fivo_reset_history(fivo_ctx* c) {
+  if (!c) return fail(FIVO_ERR_ARG, "null context");
+  int rc = reset_history(c);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->st));
+  return FIVO_OK;
+}
+
+int fivo_get_primitives(fivo_ctx* c, int64_t ntot, double* yT, double* phi, double* mu, double* alpha,
+                        double* ux, double* uy, double* P, double* n, double* e, uint8_t* ok) {
+  if (!c) return fail(FIVO_ERR_ARG, "null context");
+  if (ntot != c->dp.Ntot) return fail(FIVO_ERR_ARG, "size mismatch");
+  double* dst[9] = {yT, phi, mu, alpha, ux, uy, P, n, e};
+  const double* src[9] = {c->w.yT, c->w.phi, c->w.mu, c->w.alpha, c->w.ux, c->w.uy, c->w.P, c->w.n, c->w.e};
+  for (int k = 0; k < 9; ++k)
+    if (dst[k]) CK(cudaMemcpyAsync(dst[k], src[k], (size_t)ntot * 8, cudaMemcpyDeviceToHost, c->st));
+  if (ok) CK(cudaMemcpyAsync(ok, c->w.ok, (size_t)ntot, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return FIVO_OK;
+}
+
+int fivo_get_counters(fivo_ctx* c, fivo_counters* out) {
+  if (!c || !out) return fail(FIVO_ERR_ARG, "null argument");
+  *out = c->cnt;
+  return FIVO_OK;
+}
+
+int fivo_rhs(fivo_ctx* c, double tau, int bc, const uint8_t* mask, double* dU) {
+  if (!c) return fail(FIVO_ERR_ARG, "null context");
+  const DevParams& d = c->dp;
+  const uint8_t* dmask = nullptr;
+  if (mask) {
+    CK(cudaMemcpyAsync(c->masks + d.Ntot, mask, (size_t)d.Ntot, cudaMemcpyHostToDevice, c->st));
+    dmask = c->masks + d.Ntot;
+  }
+  if (dU && !c->dU) CK(cudaMalloc(&c->dU, (size_t)d.nv * d.Ntot * 8));
+  if (dU) CK(cudaMemsetAsync(c->dU, 0, (size_t)d.nv * d.Ntot * 8, c->st));
+  int rc = run_stage(c, c->iU, c->iT, c->iU, tau, tau, 0.0, 0.0, 0.0, COMB_RHS_ONLY, dmask, bc, nullptr,
+                     dU ? c->dU : nullptr);
+  if (rc) return rc;
+  if (dU) {
+    /* planes -> AoS on the host side */
+    std::vector<double> tmp((size_t)d.nv * d.Ntot);
+    CK(cudaMemcpy(tmp.data(), c->dU, tmp.size() * 8, cudaMemcpyDeviceToHost));
+    for (long long i = 0; i < d.Ntot; ++i)
+      for (int a = 0; a < d.nv; ++a) dU[i * d.nv + a] = tmp[(size_t)a * d.Ntot + i];
+  }
+  return FIVO_OK;
+}
+
+int fivo_step(fivo_ctx* c, int integrator, double tau, double dtau, int max_halve, int max_mood, int bc,
+              double* dtau_used, int* ok) {
+  if (!c || !dtau_used || !ok) return fail(FIVO_ERR_ARG, "null argument");
+  if (integrator == FIVO_SSPRK3) return step3(c, tau, dtau, max_halve, bc, dtau_used, ok);
+  if (integrator == FIVO_SSPRK2) return step2(c, tau, dtau, max_halve, max_mood, bc, dtau_used, ok);
+  return fail(FIVO_ERR_ARG, "integrator must be FIVO_SSPRK2 or FIVO_SSPRK3");
+}
+
+int fivo_update_primitives(fivo_ctx* c, double tau, int bc, int64_t* nprimfail) {
+  if (!c) return fail(FIVO_ERR_ARG, "null context");
+  int rc = update_prims(c, tau, bc);
+  if (rc) return rc;
+  if ((rc = sync_flags(c, false))) return rc;
+  if (nprimfail) *nprimfail = c->cnt.nprimfail;
+  return FIVO_OK;
+}
+
+int fivo_relax(fivo_ctx* c, double tau, double dtau) {
+  if (!c) return fail(FIVO_ERR_ARG, "null context");
+  const fivo_params& p = c->dp.p;
+  if (!(p.enable_shear || p.enable_bulk || p.enable_diff)) return FIVO_OK;
+  int rc = relax_project(c, tau, dtau, 1, 0);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->st));
+  return FIVO_OK;
+}
+
+int fivo_project_shear(fivo_ctx* c, double* max_res, double* mean_res) {
+  if (!c) return fail(FIVO_ERR_ARG, "null context");
+  if (!c->dp.hasShear) { if (max_res) *max_res = 0.0; if (mean_res) *mean_res = 0.0; return FIVO_OK; }
+  int rc = relax_project(c, 0.0, 1.0, 0, 1);
+  if (rc) return rc;
+  return read_shear(c, max_res, mean_res);
+}
+
+int fivo_compute_dt(fivo_ctx* c, double tau, double cfl, double cfltau, double* dt) {
+  if (!c || !dt) return fail(FIVO_ERR_ARG, "null argument");
+  /* compute_dt_2d, src2d/timestepper2d.jl:37-47 */
+  double amax = 0.0;
+  if (c->cnt.amax > amax) amax = c->cnt.amax;
+  amax = jmax(amax, 1e-6);
+  double dt_cfl = (cfl * jmin(c->dp.dx, c->dp.dy)) / amax;
+  double dt_tau = cfltau * tau;
+  *dt = jmin(dt_cfl, dt_tau);
+  return FIVO_OK;
+}
+
+int fivo_run(fivo_ctx* c, double tau0, double taufinal, double cfl, double cfltau, int integrator, int bc,
+             int64_t max_steps, int reset_hist, fivo_run_result* out) {
+  if (!c || !out) return fail(FIVO_ERR_ARG, "null argument");
+  if (integrator != FIVO_SSPRK2 && integrator != FIVO_SSPRK3)
+    return fail(FIVO_ERR_ARG, "integrator must be FIVO_SSPRK2 or FIVO_SSPRK3");
+  const DevParams& d = c->dp;
+  const fivo_params& p = d.p;
+  int rc;
+  std::memset(out, 0, sizeof(*out));
+  if (reset_hist && (rc = reset_history(c))) return rc;
+  /* one RHS pass to populate primitives and signal speeds (main2D.jl:418) */
+  if ((rc = run_stage(c, c->iU, c->iT, c->iU, tau0, tau0, 0.0, 0.0, 0.0, COMB_RHS_ONLY, nullptr, bc, nullptr, nullptr))) return rc;
+  double Qin = 0.0;
+  if ((rc = diag(c, false, &Qin, nullptr, nullptr))) return rc;
+  double tau = tau0;
+  int64_t nsteps = 0, nprimfail = 0, nvacuum = 0;
+  double max_shear_res = 0.0;
+  const bool any_sector = p.enable_shear || p.enable_bulk || p.enable_diff;
+  while (tau < taufinal && nsteps < max_steps) {
+    double D;
+    fivo_compute_dt(c, tau, cfl, cfltau, &D);
+    D = jmin(D, taufinal - tau);
+    if (D <= 0) break;
+    if (c->hist_valid || nsteps > 0) {
+      k_snapshot<<<nblk(d.Ntot, 256), 256, 0, c->st>>>(d, c->w, c->h);
+      CKL();
+      c->hist_valid = true;
+    }
+    double used = 0.0;
+    int ok = 0;
+    if (integrator == FIVO_SSPRK3) rc = step3(c, tau, D, 12, bc, &used, &ok);
+    else rc = step2(c, tau, D, 12, 2, bc, &used, &ok);
+    if (rc) return rc;
+    if (!ok) {
+      out->ok = 0; out->tau = tau; out->nsteps = nsteps; out->nprimfail = nprimfail; out->nvacuum = nvacuum;
+      out->max_shear_res = max_shear_res; out->maxu = fx::nan_(); out->dQ = fx::nan_(); out->Q0 = Qin;
+      out->Q1 = fx::nan_(); out->minPtot = fx::nan_();
+      return FIVO_OK;
+    }
+    tau += used;
+    nsteps += 1;
+    if (any_sector) {
+      if ((rc = update_prims(c, tau, bc))) return rc;
+      if ((rc = relax_project(c, tau, used, 1, d.hasShear))) return rc;
+      if ((rc = sync_flags(c, false))) return rc;
+      if (d.hasShear) {
+        uint64_t b = c->flh->shear_max_bits;
+        double r; std::memcpy(&r, &b, 8);
+        max_shear_res = jmax(max_shear_res, r);
+      }
+    } else if (d.hasShear) {
+      if ((rc = relax_project(c, tau, used, 0, 1))) return rc;
+      double r;
+      if ((rc = read_shear(c, &r, nullptr))) return rc;
+      max_shear_res = jmax(max_shear_res, r);
+    }
+    nprimfail += c->cnt.nprimfail;
+    nvacuum += c->cnt.nvacuum;
+  }
+  double Qout = 0.0, maxu = 0.0, minPtot = 0.0;
+  if ((rc = diag(c, true, &Qout, &maxu, &minPtot))) return rc;
+  out->ok = 1; out->tau = tau; out->nsteps = nsteps; out->nprimfail = nprimfail; out->nvacuum = nvacuum;
+  out->max_shear_res = max_shear_res; out->maxu = maxu;
+  out->dQ = fx::fabs_(Qin) > 0 ? fx::fabs_(Qout - Qin) / fx::fabs_(Qin) : 0.0;
+  out->Q0 = Qin; out->Q1 = Qout; out->minPtot = minPtot;
+  return FIVO_OK;
+}
+
+int fivo_finalize_ic(fivo_ctx* c, double tau0, int bc) {
+  if (!c) return fail(FIVO_ERR_ARG, "null context");
+  const DevParams& d = c->dp;
+  k_finalize_ic<<<nblk((long long)d.Nx * d.Ny, 256), 256, 0, c->st>>>(d, c->S[c->iU], tau0);
+  CKL();
+  int rc = launch_bc(c, c->S[c->iU], bc);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->st));
+  return FIVO_OK;
+}
+
+int fivo_sync(fivo_ctx* c) {
+  if (!c) return fail(FIVO_ERR_ARG, "null context");
+  CK(cudaStreamSynchronize(c->st));
+  return FIVO_OK;
+}
+
+/* ------------------------------------------------- batched one-shot helpers */
+
+namespace {
+struct DevBuf {
+  void* p = nullptr;
+  ~DevBuf() { if (p) cudaFree(p); }
+};
+int up(DevBuf& b, const double* src, long long n) {
+  if (!src) return FIVO_OK;
+  CK(cudaMalloc(&b.p, n * 8));
+  CK(cudaMemcpy(b.p, src, n * 8, cudaMemcpyHostToDevice));
+  return FIVO_OK;
+}
+}  // namespace
+
+int fivo_set_cells(const fivo_params* p, int64_t ncell, double tau, const double* T, const double* alpha,
+                   const double* ux, const double* uy, const double* Pi, const double* pixx, const double* pixy,
+                   const double* piyy, const double* nux, const double* nuy, double* U, uint8_t* ok) {
+  if (!p || !T || !alpha || !ux || !uy || !U || !ok) return fail(FIVO_ERR_ARG, "null argument");
+  if (ncell <= 0) return FIVO_OK;
+  int rc = validate(p);
+  if (rc) return rc;
+  DevParams d = make_devparams(p, 9, 9, 3, 1.0, 1.0);
+  DevBuf bT, ba, bx, by, bP, bxx, bxy, byy, bnx, bny, bU, bok;
+  const double* srcs[10] = {T, alpha, ux, uy, Pi, pixx, pixy, piyy, nux, nuy};
+  DevBuf* bufs[10] = {&bT, &ba, &bx, &by, &bP, &bxx, &bxy, &byy, &bnx, &bny};
+  for (int k = 0; k < 10; ++k) if ((rc = up(*bufs[k], srcs[k], ncell))) return rc;
+  CK(cudaMalloc(&bU.p, (size_t)ncell * d.nv * 8));
+  CK(cudaMemcpy(bU.p, U, (size_t)ncell * d.nv * 8, cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&bok.p, (size_t)ncell));
+  auto P_ = [](DevBuf& b) { return (const double*)b.p; };
+  if (p->eos_kind == FIVO_EOS_LATTICE_HRG)
+    k_set_cells<FIVO_EOS_LATTICE_HRG><<<nblk(ncell, 128), 128>>>(d, ncell, tau, P_(bT), P_(ba), P_(bx), P_(by), P_(bP), P_(bxx), P_(bxy), P_(byy), P_(bnx), P_(bny), (double*)bU.p, (uint8_t*)bok.p);
+  else
+    k_set_cells<FIVO_EOS_CONFORMAL_HQ><<<nblk(ncell, 128), 128>>>(d, ncell, tau, P_(bT), P_(ba), P_(bx), P_(by), P_(bP), P_(bxx), P_(bxy), P_(byy), P_(bnx), P_(bny), (double*)bU.p, (uint8_t*)bok.p);
+  CKL();
+  CK(cudaMemcpy(U, bU.p, (size_t)ncell * d.nv * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(ok, bok.p, (size_t)ncell, cudaMemcpyDeviceToHost));
+  return FIVO_OK;
+}
+
+int fivo_eos_Pne(const fivo_params* p, int64_t n, const double* T, const double* mu, double* P, double* nq,
+                 double* e) {
+  if (!p || !T || !mu || !P || !nq || !e) return fail(FIVO_ERR_ARG, "null argument");
+  if (n <= 0) return FIVO_OK;
+  int rc = validate(p);
+  if (rc) return rc;
+  DevParams d = make_devparams(p, 9, 9, 3, 1.0, 1.0);
+  DevBuf bT, bm, bo;
+  if ((rc = up(bT, T, n)) || (rc = up(bm, mu, n))) return rc;
+  CK(cudaMalloc(&bo.p, 3 * (size_t)n * 8));
+  double* o = (double*)bo.p;
+  if (p->eos_kind == FIVO_EOS_LATTICE_HRG)
+    k_eos<FIVO_EOS_LATTICE_HRG><<<nblk(n, 128), 128>>>(d, n, (const double*)bT.p, (const double*)bm.p, o, o + n, o + 2 * n);
+  else
+    k_eos<FIVO_EOS_CONFORMAL_HQ><<<nblk(n, 128), 128>>>(d, n, (const double*)bT.p, (const double*)bm.p, o, o + n, o + 2 * n);
+  CKL();
+  CK(cudaMemcpy(P, o, n * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(nq, o + n, n * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(e, o + 2 * n, n * 8, cudaMemcpyDeviceToHost));
+  return FIVO_OK;
+}
+
+int fivo_cons_to_prim(const fivo_params* p, int64_t n, double tau, const double* cons, const double* warm,
+                      double* prim, uint8_t* ok, uint8_t* reason) {
+  if (!p || !cons || !prim || !ok) return fail(FIVO_ERR_ARG, "null argument");
+  if (n <= 0) return FIVO_OK;
+  int rc = validate(p);
+  if (rc) return rc;
+  DevParams d = make_devparams(p, 9, 9, 3, 1.0, 1.0);
+  DevBuf bc, bw, bp, bo, br;
+  if ((rc = up(bc, cons, 11 * n)) || (rc = up(bw, warm, 4 * n))) return rc;
+  CK(cudaMalloc(&bp.p, 7 * (size_t)n * 8));
+  CK(cudaMalloc(&bo.p, (size_t)n));
+  CK(cudaMalloc(&br.p, (size_t)n));
+  const double* c_ = (const double*)bc.p;
+  const double* w_ = (const double*)bw.p;
+  if (p->eos_kind == FIVO_EOS_LATTICE_HRG)
+    k_cons_to_prim<FIVO_EOS_LATTICE_HRG, true><<<nblk(n, 128), 128>>>(d, n, tau, c_, w_, (double*)bp.p, (uint8_t*)bo.p, (uint8_t*)br.p);
+  else if (d.ncharge)
+    k_cons_to_prim<FIVO_EOS_CONFORMAL_HQ, true><<<nblk(n, 128), 128>>>(d, n, tau, c_, w_, (double*)bp.p, (uint8_t*)bo.p, (uint8_t*)br.p);
+  else
+    k_cons_to_prim<FIVO_EOS_CONFORMAL_HQ, false><<<nblk(n, 128), 128>>>(d, n, tau, c_, w_, (double*)bp.p, (uint8_t*)bo.p, (uint8_t*)br.p);
+  CKL();
+  CK(cudaMemcpy(prim, bp.p, 7 * (size_t)n * 8, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(ok, bo.p, (size_t)n, cudaMemcpyDeviceToHost));
+  if (reason) CK(cudaMemcpy(reason, br.p, (size_t)n, cudaMemcpyDeviceToHost));
+  return FIVO_OK;
+}
+
+}  /* extern "C" */

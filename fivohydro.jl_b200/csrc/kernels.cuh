@@ -1,0 +1,950 @@
+/*
+ * kernels.cuh — CUDA kernels of the 2+1D stage (sm_100a, FP64).
+ *
+ * Data layout in HBM (structure of arrays): every state row a is a plane of
+ * Ntot doubles, cell i = ix*Nytot + iy (y contiguous, so a warp covers 32
+ * consecutive y cells and every plane access is a coalesced 256-byte stream).
+ * Primitives, warm starts and history are planes of the same shape.
+ *
+ * Per RK stage (rhs_2d! + the stage combination + sanitize_stage_2d! +
+ * state_ok_2d, src2d/timestepper2d.jl:113-140):
+ *   k_bc          ghost frame of U_base               (apply_bc_2d!)
+ *   k_primitive   Newton recovery, every cell          (_primitive_pass!)
+ *   k_stage       per tile: MUSCL + prim->cons + HLLE on all faces touching
+ *                 the tile (amax over every face, ghosts included), then for
+ *                 each interior cell: divergence + Bjorken source, RK
+ *                 combination, floors, S-E and nu bounds, admissibility
+ *   k_bc          ghost frame of U_out
+ * Relaxation (relax_dissipative_2d! + project_shear!): k_relax, one thread per
+ * cell, reading the pre-relaxation dissipative planes and writing a second set.
+ */
+#ifndef FIVO_KERNELS_CUH
+#define FIVO_KERNELS_CUH
+
+#include "physics.cuh"
+
+namespace fv {
+
+#define FV_MAXV 11
+
+struct DevState { double* f[FV_MAXV]; };
+
+struct DevPrims {
+  double *yT, *phi, *mu, *alpha, *ux, *uy, *P, *n, *e;
+  uint8_t* ok;
+};
+
+struct DevHist { double *x0_yT, *x0_phi, *x0_ux, *x0_uy, *ux_prev, *uy_prev, *alpha_prev, *T_prev; };
+
+/* device-side flags and reductions, mirrored into pinned host memory */
+struct DevFlags {
+  unsigned long long amax_bits;   /* max over faces of max(|sL|,|sR|), as ordered bits */
+  unsigned long long rep;         /* (first failing cell << 8) | reason                */
+  long long nprimfail, nvacuum;
+  long long nbad;                 /* inadmissible interior cells of the last stage     */
+  unsigned long long shear_max_bits;
+  double shear_sum;
+  double sumD, maxu, minPtot;     /* end-of-run diagnostics                             */
+  int status;                     /* nonzero: a device loop hit its cap                 */
+  int pad;
+};
+
+__device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) {
+  /* v >= 0 and not NaN: the IEEE bit pattern orders like the value */
+  if (v > 0.0) atomicMax(a, (unsigned long long)__double_as_longlong(v));
+}
+
+/* slot of layout row a in the flux vector (0..3 conserved, 4..10 dissipatives) */
+__device__ __forceinline__ int slot_of(const DevParams& d, int a) {
+  if (a < 4) return a;
+  if (d.hasNu && a == d.iNux) return 4;
+  if (d.hasNu && a == d.iNuy) return 5;
+  if (d.hasPi && a == d.iPi) return 6;
+  if (a == d.iPixx) return 7;
+  if (a == d.iPixy) return 8;
+  if (a == d.iPiyy) return 9;
+  return 10;
+}
+
+__device__ __forceinline__ void load_dis(const DevParams& d, const DevState& U, long long i, double dis[7]) {
+  dis[0] = d.hasNu ? U.f[d.iNux][i] : 0.0;
+  dis[1] = d.hasNu ? U.f[d.iNuy][i] : 0.0;
+  dis[2] = d.hasPi ? U.f[d.iPi][i] : 0.0;
+  dis[3] = d.hasShear ? U.f[d.iPixx][i] : 0.0;
+  dis[4] = d.hasShear ? U.f[d.iPixy][i] : 0.0;
+  dis[5] = d.hasShear ? U.f[d.iPiyy][i] : 0.0;
+  dis[6] = d.hasShear ? U.f[d.iPieta][i] : 0.0;
+}
+
+/* ---------------------------------------------------------------- boundary */
+
+/* apply_bc_2d!, src2d/bc2d.jl:14-65. Both passes together leave every ghost
+ * cell equal to U[clamp(ix), clamp(iy)] (outflow) or U[wrap(ix), wrap(iy)]
+ * (periodic), which is what one thread per ghost cell writes. */
+__global__ void k_bc(DevParams d, DevState U, int bc) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int ng = d.ng, Nx = d.Nx, Ny = d.Ny;
+  const long long nframe = (long long)d.Nxtot * d.Nytot - (long long)Nx * Ny;
+  if (t >= nframe) return;
+  /* enumerate the ghost frame: rows ix < ng or ix >= ng+Nx fully, else the y edges */
+  int ix, iy;
+  long long full = (long long)ng * d.Nytot;
+  if (t < full) { ix = (int)(t / d.Nytot); iy = (int)(t % d.Nytot); }
+  else if (t < 2 * full) { t -= full; ix = ng + Nx + (int)(t / d.Nytot); iy = (int)(t % d.Nytot); }
+  else {
+    t -= 2 * full;
+    int per = 2 * ng;
+    ix = ng + (int)(t / per);
+    int r = (int)(t % per);
+    iy = r < ng ? r : ng + Ny + (r - ng);
+  }
+  int sx, sy;
+  if (bc == FIVO_BC_PERIODIC) {
+    sx = ix < ng ? ix + Nx : (ix >= ng + Nx ? ix - Nx : ix);
+    sy = iy < ng ? iy + Ny : (iy >= ng + Ny ? iy - Ny : iy);
+  } else {
+    sx = ix < ng ? ng : (ix >= ng + Nx ? ng + Nx - 1 : ix);
+    sy = iy < ng ? ng : (iy >= ng + Ny ? ng + Ny - 1 : iy);
+  }
+  long long dst = (long long)ix * d.Nytot + iy, src = (long long)sx * d.Nytot + sy;
+  for (int a = 0; a < d.nv; ++a) U.f[a][dst] = U.f[a][src];
+}
+
+/* ------------------------------------------------------- primitive recovery */
+
+/* _primitive_pass!, src2d/rhs2d.jl:67-160, one thread per cell (ghosts too) */
+template <int EOS, bool NCH>
+__global__ void __launch_bounds__(128) k_primitive(DevParams d, DevState U, DevPrims w, DevHist h,
+                                                   double tau, DevFlags* fl) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.Ntot) return;
+  CellCons c;
+  c.D = safe_div(U.f[d.iDtau][i], tau);
+  c.Sx = U.f[d.iSx][i]; c.Sy = U.f[d.iSy][i]; c.E = U.f[d.iE][i];
+  double dis[7];
+  load_dis(d, U, i, dis);
+  c.nux = dis[0]; c.nuy = dis[1]; c.Pi = dis[2]; c.pixx = dis[3]; c.pixy = dis[4]; c.piyy = dis[5];
+  c.pieta = dis[6];
+  Recovery r = recover<EOS, NCH>(c, d, h.x0_yT[i], h.x0_phi[i], h.x0_ux[i], h.x0_uy[i],
+                                 d.p.primrec_maxit, d.p.primrec_tol);
+  double T = r.T, mu = r.mu, ux = r.ux, uy = r.uy, n = r.n, en = r.e, P = r.P;
+  if (!r.ok) {
+    if (r.reason == PRR_VACUUM) atomicAdd((unsigned long long*)&fl->nvacuum, 1ULL);
+    else {
+      atomicAdd((unsigned long long*)&fl->nprimfail, 1ULL);
+      atomicMin(&fl->rep, ((unsigned long long)i << 8) | r.reason);
+    }
+    T = FV_T_MIN; mu = 0.0; ux = 0.0; uy = 0.0;
+    eos_Pne<EOS>(T, mu, d, &P, &n, &en);
+    en = jmax(en, 0.0); n = 0.0;
+  }
+  double Tm = jmax(T, FV_T_MIN);
+  double yT = fx_log(Tm);
+  double phi = jclamp((mu - d.p.m_hq) / Tm, -FV_PHI_CAP, FV_PHI_CAP);
+  w.yT[i] = yT; w.phi[i] = phi; w.mu[i] = mu; w.alpha[i] = mu / Tm;
+  w.ux[i] = ux; w.uy[i] = uy; w.P[i] = P; w.n[i] = n; w.e[i] = en; w.ok[i] = r.ok;
+  if (r.ok) { h.x0_yT[i] = yT; h.x0_phi[i] = phi; h.x0_ux[i] = ux; h.x0_uy[i] = uy; }
+  else { double q = nan_(); h.x0_yT[i] = q; h.x0_phi[i] = q; h.x0_ux[i] = q; h.x0_uy[i] = q; }
+}
+
+/* ------------------------------------------------------------------ faces */
+
+/* One face between cell i (left) and ip = i + st: reconstructed face states
+ * (reconstruct_muscl_2d!), prim_to_cons with the first-order and vacuum-floor
+ * fallbacks (_faces_2d!), HLLE (hlle_flux_2d!). Writes nv fluxes (layout order)
+ * to Fh and returns max(|sL|, |sR|). k = 0-based index of the left cell along
+ * the face normal, kmax = cells along it. */
+template <int EOS, bool XDIR>
+__device__ double face_flux(const DevParams& d, const DevState& U, const DevPrims& w, long long i,
+                            long long st, int k, int kmax, double tau, const uint8_t* ffo, double* Fh) {
+  const long long ip = i + st;
+  const int ng = d.ng;
+  double disL[7], disR[7];
+  load_dis(d, U, i, disL);
+  load_dis(d, U, ip, disR);
+  bool forced = ffo != nullptr && (ffo[i] || ffo[ip]);
+  bool good = false;
+  Prim pL, pR;
+  double ucL[4], ucR[4];
+  bool floorL = false, floorR = false;
+  if (!forced) {
+    double l[4], r[4];
+    const double* fld[4] = {w.yT, w.phi, w.ux, w.uy};
+    bool first = (k + 1 <= ng) || (k + 1 >= kmax - ng);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double* v = fld[q];
+      double vi = v[i], vp = v[ip];
+      if (first) { l[q] = vi; r[q] = vp; continue; }
+      double vm = v[i - st], vpp = v[ip + st];
+      double si = mc_limiter(vi - vm, vp - vi);
+      double sp = mc_limiter(vp - vi, vpp - vp);
+      double a = vi + 0.5 * si;
+      double b = vp - 0.5 * sp;
+      l[q] = jclamp(a, jmin(jmin(vm, vi), vp), jmax(jmax(vm, vi), vp));
+      r[q] = jclamp(b, jmin(jmin(vi, vp), vpp), jmax(jmax(vi, vp), vpp));
+    }
+    double TL = fx_exp(l[0]); double muL = d.p.m_hq + (TL * l[1]);
+    double TR = fx_exp(r[0]); double muR = d.p.m_hq + (TR * r[1]);
+    bool okL = prim_to_cons<EOS>(ucL, pL, TL, muL, l[2], l[3], disL, tau, d);
+    bool okR = prim_to_cons<EOS>(ucR, pR, TR, muR, r[2], r[3], disR, tau, d);
+    good = okL && okR && ucL[0] >= 0.0 && ucR[0] >= 0.0 && ucL[3] >= FV_E_FLOOR && ucR[3] >= FV_E_FLOOR;
+  }
+  if (!good) {
+    double TLc = fx_exp(w.yT[i]), muLc = w.mu[i];
+    double TRc = fx_exp(w.yT[ip]), muRc = w.mu[ip];
+    bool okL = prim_to_cons<EOS>(ucL, pL, TLc, muLc, w.ux[i], w.uy[i], disL, tau, d);
+    bool okR = prim_to_cons<EOS>(ucR, pR, TRc, muRc, w.ux[ip], w.uy[ip], disR, tau, d);
+    if (!(okL && okR)) {
+      /* _floor_prim_2d!, src2d/rhs2d.jl:259-268 */
+      if (!okL) {
+        floorL = true;
+        ucL[0] = 0.0; ucL[1] = 0.0; ucL[2] = 0.0; ucL[3] = FV_E_FLOOR;
+        pL.T = FV_T_MIN; pL.mu = 0.0; pL.ux = 0.0; pL.uy = 0.0; pL.n = 0.0; pL.e = FV_E_FLOOR; pL.P = 0.0;
+        pL.nux = pL.nuy = pL.Pi = pL.pixx = pL.pixy = pL.piyy = pL.pieta = 0.0;
+      }
+      if (!okR) {
+        floorR = true;
+        ucR[0] = 0.0; ucR[1] = 0.0; ucR[2] = 0.0; ucR[3] = FV_E_FLOOR;
+        pR.T = FV_T_MIN; pR.mu = 0.0; pR.ux = 0.0; pR.uy = 0.0; pR.n = 0.0; pR.e = FV_E_FLOOR; pR.P = 0.0;
+        pR.nux = pR.nuy = pR.Pi = pR.pixx = pR.pixy = pR.piyy = pR.pieta = 0.0;
+      }
+    }
+  }
+  if (floorL) pL.cs2 = eos_cs2<EOS>(FV_T_MIN, d);
+  if (floorR) pR.cs2 = eos_cs2<EOS>(FV_T_MIN, d);
+  double FL[11], FR[11];
+  flux_cell<XDIR>(FL, pL, tau, d);
+  flux_cell<XDIR>(FR, pR, tau, d);
+  double lmL, lpL, lmR, lpR;
+  wavespeeds<XDIR>(pL, XDIR ? pL.pixx : pL.piyy, &lmL, &lpL);
+  wavespeeds<XDIR>(pR, XDIR ? pR.pixx : pR.piyy, &lmR, &lpR);
+  double sL = jmin(lmL, lmR), sR = jmax(lpL, lpR);
+  /* conserved columns of the two states incl. the stored dissipatives (zero when floored) */
+  double cl[11], cr[11];
+  cl[0] = ucL[0]; cl[1] = ucL[1]; cl[2] = ucL[2]; cl[3] = ucL[3];
+  cr[0] = ucR[0]; cr[1] = ucR[1]; cr[2] = ucR[2]; cr[3] = ucR[3];
+#pragma unroll
+  for (int q = 0; q < 7; ++q) { cl[4 + q] = floorL ? 0.0 : disL[q]; cr[4 + q] = floorR ? 0.0 : disR[q]; }
+  if (sL >= 0) {
+    for (int a = 0; a < d.nv; ++a) Fh[a] = FL[slot_of(d, a)];
+  } else if (sR <= 0) {
+    for (int a = 0; a < d.nv; ++a) Fh[a] = FR[slot_of(d, a)];
+  } else {
+    double inv = 1.0 / ((sR - sL) + FV_TINY);
+    for (int a = 0; a < d.nv; ++a) {
+      int s = slot_of(d, a);
+      Fh[a] = (((sR * FL[s]) - (sL * FR[s])) + ((sR * sL) * (cr[s] - cl[s]))) * inv;
+    }
+  }
+  return jmax(fabs_(sL), fabs_(sR));
+}
+
+/* --------------------------------------------------------------- the stage */
+
+/* combination modes (src2d/timestepper2d.jl:122-130, 158-178) */
+enum { COMB_EULER = 0, COMB_BLEND = 1, COMB_THIRD = 2, COMB_RHS_ONLY = 3 };
+
+struct StageArgs {
+  DevState Ub;      /* state the RHS is evaluated on (= U_in of the combination) */
+  DevState Uold;    /* the step's entry state (blended stages)                    */
+  DevState Uout;
+  DevPrims w;
+  const uint8_t* ffo;   /* force_first_order mask or null */
+  uint8_t* bad;         /* per-cell inadmissible flag (interior)                   */
+  double* dU;           /* optional: RHS planes (nv x Ntot), for fivo_rhs          */
+  double tau, tau_state, dt, wold, wnew;
+  int mode;
+  DevFlags* fl;
+};
+
+#define ST_CX 8
+#define ST_CY 32
+#define ST_NFX ((ST_CX + 1) * ST_CY)
+#define ST_NFY (ST_CX * (ST_CY + 1))
+
+__device__ __forceinline__ double peff_of(const DevParams& d, const double u[FV_MAXV], double Pw) {
+  double Peff = 0.0;
+  if (isfinite_(Pw)) Peff = jmax(Pw, 0.0);
+  if (d.hasPi) { double v = u[d.iPi]; if (isfinite_(v)) Peff += fabs_(v); }
+  if (d.hasShear) {
+    double v;
+    v = u[d.iPixx]; if (isfinite_(v)) Peff += fabs_(v);
+    v = u[d.iPixy]; if (isfinite_(v)) Peff += fabs_(v);
+    v = u[d.iPiyy]; if (isfinite_(v)) Peff += fabs_(v);
+    v = u[d.iPieta]; if (isfinite_(v)) Peff += fabs_(v);
+  }
+  return Peff;
+}
+
+/* enforce_floors_2d! + enforce_S_energy_constraint_2d! + enforce_nu_charge_constraint_2d!
+ * for one interior cell (src2d/floors2d.jl:24-210). Pw = work.P (NaN if absent). */
+__device__ void sanitize_cell(const DevParams& d, double u[FV_MAXV], int ix, int iy, double tau_state,
+                              double Pw, bool haveP, double Emin) {
+  double Evac = jmax(Emin, d.E_vac_cut);
+  double rdom = d.p.r_domain;
+  bool blank = false, done = false;
+  if (isfinite_(rdom)) {
+    double x = d.xmin + (((double)(ix + 1 - d.ng)) - 0.5) * d.dx;
+    double y = d.ymin + (((double)(iy + 1 - d.ng)) - 0.5) * d.dy;
+    if ((x * x) + (y * y) > rdom * rdom) { u[d.iE] = Emin; blank = true; done = true; }
+  }
+  if (!done) {
+    double Ei = u[d.iE];
+    if (!isfinite_(Ei)) { u[d.iE] = Emin; blank = true; done = true; }
+    else if (Ei < Evac) { u[d.iE] = Emin; blank = true; done = true; }
+    else if (Ei <= 1e6 * Emin) blank = true;
+  }
+  if (blank) {
+    u[d.iSx] = 0.0; u[d.iSy] = 0.0; u[d.iDtau] = 0.0;
+    if (d.hasNu) { u[d.iNux] = 0.0; u[d.iNuy] = 0.0; }
+    if (d.hasPi) u[d.iPi] = 0.0;
+    if (d.hasShear) { u[d.iPixx] = 0.0; u[d.iPixy] = 0.0; u[d.iPiyy] = 0.0; u[d.iPieta] = 0.0; }
+  }
+  if (!done) {
+    double Di = u[d.iDtau];
+    if (!isfinite_(Di) || Di < 0.0) u[d.iDtau] = 0.0;
+    if (!isfinite_(u[d.iSx])) u[d.iSx] = 0.0;
+    if (!isfinite_(u[d.iSy])) u[d.iSy] = 0.0;
+    for (int a = 4; a < d.nv; ++a) if (!isfinite_(u[a])) u[a] = 0.0;
+  }
+  /* S-E bound */
+  {
+    double Ei = u[d.iE], Sx = u[d.iSx], Sy = u[d.iSy];
+    if (isfinite_(Ei) && isfinite_(Sx) && isfinite_(Sy) && !(Ei <= 0)) {
+      double Peff = peff_of(d, u, haveP ? Pw : nan_());
+      double Smax = FV_CHI_SRE * (Ei + Peff);
+      double aS = fx_hypot(Sx, Sy);
+      if (aS > Smax) {
+        double sc = Smax / (aS + FV_TINY);
+        u[d.iSx] = Sx * sc; u[d.iSy] = Sy * sc;
+      }
+    }
+  }
+  /* nu bound */
+  if (d.hasNu) {
+    double Dt = u[d.iDtau] / tau_state;
+    double nux = u[d.iNux], nuy = u[d.iNuy];
+    if (isfinite_(Dt) && isfinite_(nux) && isfinite_(nuy)) {
+      if (Dt <= 0.0) { u[d.iNux] = 0.0; u[d.iNuy] = 0.0; }
+      else {
+        double cap = 0.999 * Dt;
+        double an = fx_hypot(nux, nuy);
+        if (an > cap) {
+          double sc = cap / (an + FV_TINY);
+          u[d.iNux] = nux * sc; u[d.iNuy] = nuy * sc;
+        }
+      }
+    }
+  }
+}
+
+/* cell_admissible_2d, src2d/floors2d.jl:281-337 */
+template <int EOS, bool NCH>
+__device__ bool cell_admissible(const DevParams& d, const double u[FV_MAXV], double tau, bool okw,
+                                double ux, double uy, double Pw) {
+  const double Emin = FV_E_FLOOR;
+  double E = u[d.iE], Sx = u[d.iSx], Sy = u[d.iSy], Dt = u[d.iDtau];
+  if (!(isfinite_(E) && isfinite_(Sx) && isfinite_(Sy) && isfinite_(Dt))) return false;
+  if (!(E >= Emin)) return false;
+  if (!(Dt >= 0.0)) return false;
+  for (int a = 4; a < d.nv; ++a) if (!isfinite_(u[a])) return false;
+  if (E <= 1e6 * Emin) return true;
+  if (okw) {
+    double ut = utau(ux, uy);
+    double iu = safe_inv(ut);
+    double vx = ux * iu, vy = uy * iu;
+    if (!(isfinite_(vx) && isfinite_(vy))) return false;
+    double lim = (1.0 - 1e-12) * (1.0 - 1e-12);
+    if (!((vx * vx) + (vy * vy) < lim)) return false;
+  }
+  double Peff = peff_of(d, u, Pw);
+  if (fx_hypot(Sx, Sy) <= ((FV_SR_MARGIN * FV_CHI_SRE) * (E + Peff))) return true;
+  CellCons c;
+  c.D = safe_div(Dt, tau); c.Sx = Sx; c.Sy = Sy; c.E = E;
+  c.nux = d.hasNu ? u[d.iNux] : 0.0; c.nuy = d.hasNu ? u[d.iNuy] : 0.0;
+  c.Pi = d.hasPi ? u[d.iPi] : 0.0;
+  c.pixx = d.hasShear ? u[d.iPixx] : 0.0; c.pixy = d.hasShear ? u[d.iPixy] : 0.0;
+  c.piyy = d.hasShear ? u[d.iPiyy] : 0.0; c.pieta = d.hasShear ? u[d.iPieta] : 0.0;
+  Recovery r = recover<EOS, NCH>(c, d, nan_(), nan_(), nan_(), nan_(), 80, 1e-12);
+  return r.ok || r.reason == PRR_VACUUM;
+}
+
+/* rhs_2d! (faces, sources, assembly) fused with the stage combination, the
+ * sanitiser and the admissibility test. One CTA per ST_CX x ST_CY tile of the
+ * full (ghost-inclusive) grid. */
+template <int EOS, bool NCH>
+__global__ void __launch_bounds__(256) k_stage(DevParams d, StageArgs s) {
+  extern __shared__ double sm[];
+  double* Fx = sm;                              /* ST_NFX x nv */
+  double* Fy = sm + (size_t)ST_NFX * d.nv;      /* ST_NFY x nv */
+  const int cx0 = blockIdx.x * ST_CX, cy0 = blockIdx.y * ST_CY;
+  const int tid = threadIdx.x;
+  double amax = 0.0;
+  /* ---- faces ---- */
+  for (int f = tid; f < ST_NFX + ST_NFY; f += blockDim.x) {
+    if (f < ST_NFX) {
+      int lx = f / ST_CY, ly = f % ST_CY;
+      int ix = cx0 - 1 + lx, iy = cy0 + ly;
+      if (ix < 0 || ix > d.Nxtot - 2 || iy >= d.Nytot) continue;
+      long long i = (long long)ix * d.Nytot + iy;
+      double a = face_flux<EOS, true>(d, s.Ub, s.w, i, d.Nytot, ix, d.Nxtot, s.tau, s.ffo,
+                                      Fx + (size_t)f * d.nv);
+      if (a > amax) amax = a;
+    } else {
+      int g = f - ST_NFX;
+      int lx = g / (ST_CY + 1), ly = g % (ST_CY + 1);
+      int ix = cx0 + lx, iy = cy0 - 1 + ly;
+      if (iy < 0 || iy > d.Nytot - 2 || ix >= d.Nxtot) continue;
+      long long i = (long long)ix * d.Nytot + iy;
+      double a = face_flux<EOS, false>(d, s.Ub, s.w, i, 1, iy, d.Nytot, s.tau, s.ffo,
+                                       Fy + (size_t)g * d.nv);
+      if (a > amax) amax = a;
+    }
+  }
+  /* block max of amax -> one atomic */
+  for (int o = 16; o > 0; o >>= 1) amax = jmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+  __shared__ double red[8];
+  if ((tid & 31) == 0) red[tid >> 5] = amax;
+  __syncthreads();
+  if (tid == 0) {
+    double m = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) m = jmax(m, red[k]);
+    atomic_max_pos(&s.fl->amax_bits, m);
+  }
+  /* ---- cells ---- */
+  const int lx = tid / ST_CY, ly = tid % ST_CY;
+  const int ix = cx0 + lx, iy = cy0 + ly;
+  const int ng = d.ng;
+  if (ix < ng || ix >= ng + d.Nx || iy < ng || iy >= ng + d.Ny) return;
+  const long long i = (long long)ix * d.Nytot + iy;
+  const int nv = d.nv;
+  const double invdx = 1.0 / d.dx, invdy = 1.0 / d.dy;
+  const double* fxR = Fx + (size_t)((lx + 1) * ST_CY + ly) * nv;
+  const double* fxL = Fx + (size_t)(lx * ST_CY + ly) * nv;
+  const double* fyT = Fy + (size_t)(lx * (ST_CY + 1) + ly + 1) * nv;
+  const double* fyB = Fy + (size_t)(lx * (ST_CY + 1) + ly) * nv;
+  double ub[FV_MAXV];
+  for (int a = 0; a < nv; ++a) ub[a] = s.Ub.f[a][i];
+  const double Pw = s.w.P[i];
+  /* source_cell_2d!, src2d/fluxes2d.jl:166-177 (+ the advected-scalar divv terms) */
+  double Sr[FV_MAXV];
+  for (int a = 0; a < nv; ++a) Sr[a] = 0.0;
+  {
+    double itau = safe_inv(s.tau);
+    double Pi = d.hasPi ? ub[d.iPi] : 0.0, pieta = d.hasShear ? ub[d.iPieta] : 0.0;
+    Sr[d.iSx] = (-ub[d.iSx]) * itau;
+    Sr[d.iSy] = (-ub[d.iSy]) * itau;
+    Sr[d.iE] = (-((ub[d.iE] + (Pw + Pi)) + pieta)) * itau;
+    bool an = d.hasNu && d.p.advect_nu, aP = d.hasPi && d.p.advect_Pi, ap = d.hasShear && d.p.advect_pi;
+    if (an || aP || ap) {
+      /* compute_divv_2d!, src2d/rhs2d.jl:29-41 */
+      const long long ixm = i - d.Nytot, ixp = i + d.Nytot;
+      double vxp = s.w.ux[ixp] * safe_inv(utau(s.w.ux[ixp], s.w.uy[ixp]));
+      double vxm = s.w.ux[ixm] * safe_inv(utau(s.w.ux[ixm], s.w.uy[ixm]));
+      double vyp = s.w.uy[i + 1] * safe_inv(utau(s.w.ux[i + 1], s.w.uy[i + 1]));
+      double vym = s.w.uy[i - 1] * safe_inv(utau(s.w.ux[i - 1], s.w.uy[i - 1]));
+      double divv = ((0.5 * (vxp - vxm)) * invdx) + ((0.5 * (vyp - vym)) * invdy);
+      if (an) { Sr[d.iNux] += ub[d.iNux] * divv; Sr[d.iNuy] += ub[d.iNuy] * divv; }
+      if (aP) Sr[d.iPi] += ub[d.iPi] * divv;
+      if (ap) {
+        Sr[d.iPixx] += ub[d.iPixx] * divv; Sr[d.iPixy] += ub[d.iPixy] * divv;
+        Sr[d.iPiyy] += ub[d.iPiyy] * divv; Sr[d.iPieta] += ub[d.iPieta] * divv;
+      }
+    }
+  }
+  double u[FV_MAXV];
+  for (int a = 0; a < nv; ++a) {
+    double k = (((-(fxR[a] - fxL[a])) * invdx) - ((fyT[a] - fyB[a]) * invdy)) + Sr[a];
+    if (s.dU) s.dU[(size_t)a * d.Ntot + i] = k;
+    if (s.mode == COMB_EULER) u[a] = ub[a] + (s.dt * k);
+    else if (s.mode == COMB_BLEND) u[a] = (s.wold * s.Uold.f[a][i]) + (s.wnew * (ub[a] + (s.dt * k)));
+    else if (s.mode == COMB_THIRD) u[a] = (s.Uold.f[a][i] + (2.0 * (ub[a] + (s.dt * k)))) / 3.0;
+  }
+  if (s.mode == COMB_RHS_ONLY) return;
+  sanitize_cell(d, u, ix, iy, s.tau_state, Pw, true, FV_E_FLOOR);
+  bool adm = cell_admissible<EOS, NCH>(d, u, s.tau_state, s.w.ok[i] != 0, s.w.ux[i], s.w.uy[i], Pw);
+  s.bad[i] = adm ? 0 : 1;
+  if (!adm) atomicAdd((unsigned long long*)&s.fl->nbad, 1ULL);
+  for (int a = 0; a < nv; ++a) s.Uout.f[a][i] = u[a];
+}
+
+/* expand_bad_2d! one radius step, src2d/floors2d.jl:369-383 */
+__global__ void k_expand_bad(DevParams d, const uint8_t* bad, uint8_t* out) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.Ntot) return;
+  int ix = (int)(i / d.Nytot), iy = (int)(i % d.Nytot);
+  uint8_t b = bad[i];
+  if (ix >= d.ng && ix < d.ng + d.Nx && iy >= d.ng && iy < d.ng + d.Ny && !b)
+    b = (bad[i - 1] || bad[i + 1] || bad[i - d.Nytot] || bad[i + d.Nytot]) ? 1 : 0;
+  out[i] = b;
+}
+
+/* finalize_ic! floors/bounds without a pressure (main2D.jl:164-171), interior */
+__global__ void k_finalize_ic(DevParams d, DevState U, double tau0) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)d.Nx * d.Ny) return;
+  int ix = d.ng + (int)(t / d.Ny), iy = d.ng + (int)(t % d.Ny);
+  long long i = (long long)ix * d.Nytot + iy;
+  double u[FV_MAXV];
+  for (int a = 0; a < d.nv; ++a) u[a] = U.f[a][i];
+  sanitize_cell(d, u, ix, iy, tau0, 0.0, false, FV_E_FLOOR);
+  for (int a = 0; a < d.nv; ++a) U.f[a][i] = u[a];
+}
+
+/* ------------------------------------------------------------- relaxation */
+
+/* MC-limited face-reconstructed gradient of alpha at interior cell i
+ * (compute_alpha_grad_fv_2d!, src2d/dissipation2d.jl:225-260) */
+__device__ __forceinline__ double alpha_grad(const double* a, long long i, long long st, int k, int kmax,
+                                             int ng, double invd) {
+  double am2 = a[i - 2 * st], am1 = a[i - st], a0 = a[i], ap1 = a[i + st], ap2 = a[i + 2 * st];
+  double slm = mc_limiter(am1 - am2, a0 - am1);
+  double sl0 = mc_limiter(a0 - am1, ap1 - a0);
+  double slp = mc_limiter(ap1 - a0, ap2 - ap1);
+  /* face[i] (left cell k) and face[i-st] (left cell k-1) */
+  double fi = (k + 1 <= ng || k + 1 >= kmax - ng) ? 0.5 * (a0 + ap1)
+                                                   : 0.5 * ((a0 + (0.5 * sl0)) + (ap1 - (0.5 * slp)));
+  double fm = (k <= ng || k >= kmax - ng) ? 0.5 * (am1 + a0)
+                                          : 0.5 * ((am1 + (0.5 * slm)) + (a0 - (0.5 * sl0)));
+  return (fi - fm) * invd;
+}
+
+/* transport coefficients at one cell (src/primitives.jl:357-409,
+ * src2d/transport2d.jl:19-155) */
+template <int EOS>
+__device__ void diff_tauN(const DevParams& d, double Tm, double alpha, double* taun) {
+  const double m = d.p.m_hq;
+  const double DsT = d.p.kappa_coeff, tauD = d.p.tauN_coeff;
+  double z = m / Tm;
+  if (EOS == FIVO_EOS_LATTICE_HRG) {
+    if (z <= 0.0) { *taun = 0.0; return; }
+    double b1, b2;
+    if (z >= 1.0e4) { b1 = fx_besselkx_asym(1, z); b2 = fx_besselkx_asym(2, z); }
+    else { double k0, k1; fx_k01x(z, &k0, &k1); b1 = k1; b2 = k0 + (2.0 / z) * k1; }
+    double b3 = b1 + ((4.0 / z) * b2);
+    double b4 = b2 + ((6.0 / z) * b3);
+    double b5 = b3 + ((8.0 / z) * b4);
+    double ex = fx_exp(jclamp(alpha - z, -700.0, 700.0));
+    double tauq = (((d.p.g_hq * (DsT / ((96.0 * d.pi2) * ((Tm * Tm) * Tm)))) * fx_pow5(m)) * ex) *
+                  (((2.0 * b1) - (3.0 * b3)) + b5);
+    /* _fluidum_single_hadron_normalization_2d at max(Tm, T_MIN) */
+    double Tn = jmax(Tm, FV_T_MIN);
+    double zn = m / Tn;
+    double b2n = b2, exn = ex;
+    if (Tn != Tm) { b2n = fx_besselkx(2, zn); exn = fx_exp(jclamp(alpha - zn, -700.0, 700.0)); }
+    double norm = ((((d.p.g_hq * (Tn / (2.0 * d.pi2))) * (m * m)) * exn) * b2n) * d.fmgev3;
+    if (fabs_(norm) <= FV_TINY) { *taun = 0.0; return; }
+    double tn = (tauq / norm) * (FV_FMGEV * FV_FMGEV);
+    if (!isfinite_(tn)) { *taun = 0.0; return; }
+    *taun = jmax(tn, 0.0) * tauD;
+    return;
+  }
+  if (z <= 0) { *taun = 0.0; return; }
+  if (z > 50.0) {
+    double K2a = fx_besselkx(2, z), K3a = fx_besselkx(3, z);
+    double tg = fabs_(K2a) > FV_TINY ? (((DsT * z) * (K3a / K2a)) / Tm) : ((DsT * z) / Tm);
+    *taun = jmin((tg / FV_FMGEV) * tauD, 1e20);
+    return;
+  }
+  double K1x = fx_besselkx(1, z), K2x = fx_besselkx(2, z), K3x = fx_besselkx(3, z), K5x = fx_besselkx(5, z);
+  double numerator = ((2.0 * K1x) - (3.0 * K3x)) + K5x;
+  double denominator = jmax(fabs_(K2x), FV_TINY);
+  double ratio = (numerator / denominator) * jsign(K2x == 0 ? 1.0 : K2x);
+  double z3 = ((z * z) * z) / Tm;
+  if (!isfinite_(z3) || z3 > 1e50) z3 = 1e50;
+  double tg = ((DsT / 48.0) * z3) * ratio;
+  if (!isfinite_(tg) || fabs_(tg) > 1e50) { *taun = 1e50 * jsign(tg); return; }
+  *taun = (tg / FV_FMGEV) * tauD;
+}
+
+/* pi_sigma_contractions_2d, src2d/hq_consistent_m2_2d.jl:201-210 */
+__device__ void pi_sigma(double ux, double uy, double pxx, double pxy, double pyy, double peta,
+                         double sxx, double sxy, double syy, double seta,
+                         double* ps, double* cxx, double* cxy, double* cyy) {
+  double ux2 = ux * ux, uy2 = uy * uy, ux3 = (ux * ux) * ux, uy3 = (uy * uy) * uy, ux4 = fx_pow4(ux);
+  double opuy2 = 1.0 + uy2;
+  double u2 = (1.0 + ux2) + uy2;
+  double num = ((((((((((((((((2.0 * pxy) * sxy) + (pyy * syy)) + (((2.0 * pxy) * sxy) * ux2)) +
+      (((2.0 * pyy) * syy) * ux2)) + ((pyy * syy) * ux4)) - ((((2.0 * pxy) * sxx) * ux) * uy)) -
+      ((((2.0 * pyy) * sxy) * ux) * uy)) - ((((2.0 * pxy) * syy) * ux) * uy)) -
+      ((((2.0 * pyy) * sxy) * ux3) * uy)) - ((((2.0 * pxy) * syy) * ux3) * uy)) +
+      (((2.0 * pxy) * sxy) * uy2)) + (((pyy * sxx) * ux2) * uy2)) + ((((4.0 * pxy) * sxy) * ux2) * uy2)) -
+      ((((2.0 * pxy) * sxx) * ux) * uy3)) + ((pxx * sxx) * (opuy2 * opuy2))) +
+      ((peta * seta) * (u2 * u2));
+  num = num + (((pxx * ux) * uy) * (((syy * ux) * uy) - ((2.0 * sxy) * opuy2)));
+  *ps = num / (u2 * u2);
+  *cxx = ((pxx * sxx) + (pxy * sxy)) - ((((pxx * ux) + (pxy * uy)) * ((sxx * ux) + (sxy * uy))) / u2);
+  *cyy = ((pxy * sxy) + (pyy * syy)) - ((((pxy * ux) + (pyy * uy)) * ((sxy * ux) + (syy * uy))) / u2);
+  double t1 = pyy * ((sxy + (sxy * ux2)) - ((sxx * ux) * uy));
+  double t2 = pxy * ((((sxx + syy) + (syy * ux2)) - (((2.0 * sxy) * ux) * uy)) + (sxx * uy2));
+  double t3 = pxx * ((sxy - ((syy * ux) * uy)) + (sxy * uy2));
+  *cxy = ((t1 + t2) + t3) / (2.0 * u2);
+}
+
+struct Kin { double th, ax, ay, at, dxux, dxuy, dyux, dyuy; };
+
+/* ns_shear_target_2d, src2d/dissipation2d.jl:181-192 */
+__device__ __forceinline__ void ns_shear(double ux, double uy, double ut, double tau, const Kin& k,
+                                         double eta, double* xx, double* xy, double* yy, double* et) {
+  double third = k.th / 3.0;
+  double sxx = (k.dxux + (ux * k.ax)) - (third * (1.0 + (ux * ux)));
+  double syy = (k.dyuy + (uy * k.ay)) - (third * (1.0 + (uy * uy)));
+  double sxy = ((0.5 * (k.dxuy + k.dyux)) + (0.5 * ((ux * k.ay) + (uy * k.ax)))) - (third * (ux * uy));
+  double seta = (ut * safe_inv(tau)) - third;
+  double m2 = -2.0 * eta;
+  *xx = m2 * sxx; *xy = m2 * sxy; *yy = m2 * syy; *et = m2 * seta;
+}
+
+/* vorticity_coupling_2d, src2d/hq_consistent_m2_2d.jl:442-468 */
+__device__ void vorticity_coupling(double ux, double uy, double ut, double pxx, double pxy, double pyy,
+                                   double ax, double ay, double dtux, double dtuy, double dxux, double dxuy,
+                                   double dyux, double dyuy, double* wxx, double* wxy, double* wyy) {
+  double iu = safe_inv(ut);
+  double at = ((ux * ax) + (uy * ay)) * iu;
+  double dxut = ((ux * dxux) + (uy * dxuy)) * iu;
+  double dyut = ((ux * dyux) + (uy * dyuy)) * iu;
+  double Atx = (-dtux) + (ut * ax), Axt = dxut + (ux * at);
+  double Aty = (-dtuy) + (ut * ay), Ayt = dyut + (uy * at);
+  double Axy = dxuy + (ux * ay), Ayx = dyux + (uy * ax);
+  double wtx = 0.5 * (Atx - Axt), wty = 0.5 * (Aty - Ayt), wxy_ = 0.5 * (Axy - Ayx);
+  PiC pc = shear_tensor(ux, uy, ut, pxx, pxy, pyy);
+  double Mxx = ((-pc.tx) * wtx) - (pc.xy * wxy_);
+  double Mxy = ((-pc.tx) * wty) + (pc.xx * wxy_);
+  double Myx = ((-pc.ty) * wtx) - (pc.yy * wxy_);
+  double Myy = ((-pc.ty) * wty) + (pc.xy * wxy_);
+  *wxx = 2.0 * Mxx; *wxy = Mxy + Myx; *wyy = 2.0 * Myy;
+}
+
+/* relax_dissipative_2d! (src2d/dissipation2d.jl:293-705) fused with
+ * project_shear! (main2D.jl:332-358). Reads the dissipative planes of Uq (the
+ * pre-relaxation snapshot), writes them to Uo; the conserved planes are shared.
+ * Every cell writes its dissipative rows: interior ok cells relaxed, the rest
+ * copied. Then the shear projection of every interior cell. */
+template <int EOS>
+__global__ void __launch_bounds__(128) k_relax(DevParams d, DevState Uq, DevState Uo, DevPrims w,
+                                               DevHist h, double tau, double D, int do_relax,
+                                               int do_project, DevFlags* fl) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.Ntot) return;
+  const int nv = d.nv;
+  const int ix = (int)(i / d.Nytot), iy = (int)(i % d.Nytot);
+  const int ng = d.ng;
+  const bool interior = ix >= ng && ix < ng + d.Nx && iy >= ng && iy < ng + d.Ny;
+  double u[FV_MAXV];
+  for (int a = 4; a < nv; ++a) u[a] = Uq.f[a][i];
+  const fivo_params& p = d.p;
+  const double ux = w.ux[i], uy = w.uy[i];
+  const double ut = utau(ux, uy);
+  if (do_relax && interior && w.ok[i]) {
+    const double invdx = 1.0 / d.dx, invdy = 1.0 / d.dy;
+    const long long st = d.Nytot;
+    auto upw = [&](int a) {
+      const double* Q = Uq.f[a];
+      double q0 = Q[i];
+      double dqx = ux >= 0 ? (q0 - Q[i - st]) * invdx : (Q[i + st] - q0) * invdx;
+      double dqy = uy >= 0 ? (q0 - Q[i - 1]) * invdy : (Q[i + 1] - q0) * invdy;
+      return (ux * dqx) + (uy * dqy);
+    };
+    /* kinematics_2d, src2d/dissipation2d.jl:141-167 */
+    Kin k;
+    {
+      double ix2 = 1.0 / (2.0 * d.dx), iy2 = 1.0 / (2.0 * d.dy);
+      k.dxux = (w.ux[i + st] - w.ux[i - st]) * ix2;
+      k.dxuy = (w.uy[i + st] - w.uy[i - st]) * ix2;
+      k.dyux = (w.ux[i + 1] - w.ux[i - 1]) * iy2;
+      k.dyuy = (w.uy[i + 1] - w.uy[i - 1]) * iy2;
+      double uxp = h.ux_prev[i], uyp = h.uy_prev[i];
+      bool have_prev = isfinite_(uxp) && isfinite_(uyp);
+      double dtux = have_prev ? (ux - uxp) / D : 0.0;
+      double dtuy = have_prev ? (uy - uyp) / D : 0.0;
+      double dtut = ((ux * dtux) + (uy * dtuy)) * safe_inv(ut);
+      k.th = ((dtut + k.dxux) + k.dyuy) + (ut * safe_inv(tau));
+      k.ax = ((ut * dtux) + (ux * k.dxux)) + (uy * k.dyux);
+      k.ay = ((ut * dtuy) + (ux * k.dxuy)) + (uy * k.dyuy);
+      k.at = ((ux * k.ax) + (uy * k.ay)) * safe_inv(ut);
+    }
+    const double T = fx_exp(w.yT[i]), mu = w.mu[i], n = w.n[i], en = w.e[i], P = w.P[i];
+    /* local_thermo: entropy and (bulk only) cs2 */
+    const double s_ent = eos_entropy(T, mu, n, en, P);
+    /* ---- bulk ---- */
+    if (p.enable_bulk && d.hasPi) {
+      double Pin = u[d.iPi];
+      double zeta = 0.0, tPi = 0.0;
+      if (p.bulk_kind != FIVO_BULK_ZERO) {
+        double cs2 = eos_cs2<EOS>(T, d);
+        double peak;
+        if (p.bulk_kind == FIVO_BULK_LORENTZ) { double q = (T - 0.175) / 0.024; peak = p.zeta_over_s / (1.0 + (q * q)); }
+        else { double q = (T - p.bulk_T0) / p.bulk_width; peak = p.zeta_over_s * fx_exp(-0.5 * (q * q)); }
+        zeta = (peak * FV_INVFMGEV) * jmax(s_ent, 0.0);
+        double sp = posden(s_ent);
+        double Dl = jmax(fabs_((1.0 / 3.0) - cs2), 1e-8);
+        tPi = (safe_div(zeta, ((posden(T) * sp) * posden(p.tauPi_coeff))) * (1.0 / (Dl * Dl))) + 0.1;
+      }
+      double PiNS = (-zeta) * k.th;
+      double A = safe_div(tPi * ut, D);
+      double adv = p.relax_advect_Pi ? (-tPi) * upw(d.iPi) : 0.0;
+      double dPi = p.deltaPi_factor * tPi;
+      if (p.lambda_Pi_pi_factor != 0.0 && p.enable_shear && d.hasShear) {
+        double sxx, sxy, syy, se, ps, c1, c2, c3;
+        ns_shear(ux, uy, ut, tau, k, -0.5, &sxx, &sxy, &syy, &se);
+        pi_sigma(ux, uy, u[d.iPixx], u[d.iPixy], u[d.iPiyy], u[d.iPieta], sxx, sxy, syy, se, &ps, &c1, &c2, &c3);
+        adv = adv - ((p.lambda_Pi_pi_factor * tPi) * ps);
+      }
+      double num = ((A * Pin) + PiNS) + adv;
+      Pin = dPi == 0.0 ? num / (A + 1.0) : num / jmax((A + 1.0) + (dPi * k.th), 0.5 * (A + 1.0));
+      Pin = jmax(Pin, -0.99 * jmax(P, 0.0));
+      if (p.Pi_clip_factor > 0) { double cap = p.Pi_clip_factor * fabs_(P); Pin = jclamp(Pin, -cap, cap); }
+      u[d.iPi] = Pin;
+    }
+    /* ---- shear ---- */
+    if (p.enable_shear && d.hasShear) {
+      double eta = 0.0, tpi = 0.0, dpi = 0.0;
+      if (p.shear_kind == FIVO_SHEAR_QGP) {
+        eta = (jmax(p.eta_over_s, 0.0) * jmax(s_ent, 0.0)) * FV_INVFMGEV;
+        double Ts = posden(T) * posden(s_ent);
+        tpi = safe_div(eta, (Ts * posden(p.tauShear_coeff)));
+        dpi = p.deltaShear_factor * tpi;
+      } else {
+        dpi = p.deltaShear_factor * 0.0;
+      }
+      double pixx = u[d.iPixx], pixy = u[d.iPixy], piyy = u[d.iPiyy], pieta = u[d.iPieta];
+      double nsxx, nsxy, nsyy, nse;
+      ns_shear(ux, uy, ut, tau, k, eta, &nsxx, &nsxy, &nsyy, &nse);
+      PiC pc = shear_tensor(ux, uy, ut, pixx, pixy, piyy);
+      double cx = (((-pc.tx) * k.at) + (pc.xx * k.ax)) + (pc.xy * k.ay);
+      double cy = (((-pc.ty) * k.at) + (pc.xy * k.ax)) + (pc.yy * k.ay);
+      double A = safe_div(tpi * ut, D);
+      double den = jmax((A + 1.0) + (dpi * k.th), 0.5 * (A + 1.0));
+      double pd = p.shear_projected_deriv ? tpi : 0.0;
+      bool ra = p.relax_advect_pi != 0;
+      double axx = ra ? (-tpi) * upw(d.iPixx) : 0.0;
+      double axy = ra ? (-tpi) * upw(d.iPixy) : 0.0;
+      double ayy = ra ? (-tpi) * upw(d.iPiyy) : 0.0;
+      if (p.terms & FIVO_TERM_SHEAR_VORTICITY) {
+        double iu = safe_inv(ut);
+        double dtux = ((k.ax - (ux * k.dxux)) - (uy * k.dyux)) * iu;
+        double dtuy = ((k.ay - (ux * k.dxuy)) - (uy * k.dyuy)) * iu;
+        double wxx, wxy, wyy;
+        vorticity_coupling(ux, uy, ut, pixx, pixy, piyy, k.ax, k.ay, dtux, dtuy, k.dxux, k.dxuy,
+                           k.dyux, k.dyuy, &wxx, &wxy, &wyy);
+        axx -= tpi * wxx; axy -= tpi * wxy; ayy -= tpi * wyy;
+      }
+      if (p.taupi_pi_factor != 0.0 || p.lambda_pi_Pi_factor != 0.0) {
+        double sxx, sxy, syy, se;
+        ns_shear(ux, uy, ut, tau, k, -0.5, &sxx, &sxy, &syy, &se);
+        if (p.taupi_pi_factor != 0.0) {
+          double tpp = p.taupi_pi_factor * tpi;
+          double ps, cxx, cxy, cyy;
+          pi_sigma(ux, uy, pixx, pixy, piyy, pieta, sxx, sxy, syy, se, &ps, &cxx, &cxy, &cyy);
+          axx -= tpp * (cxx - (((1.0 + (ux * ux)) * ps) / 3.0));
+          axy -= tpp * (cxy - (((ux * uy) * ps) / 3.0));
+          ayy -= tpp * (cyy - (((1.0 + (uy * uy)) * ps) / 3.0));
+        }
+        if (p.lambda_pi_Pi_factor != 0.0 && p.enable_bulk && d.hasPi) {
+          /* bulk already updated above, as in the reference (bulk runs first) */
+          double lP = (p.lambda_pi_Pi_factor * tpi) * u[d.iPi];
+          axx -= lP * sxx; axy -= lP * sxy; ayy -= lP * syy;
+        }
+      }
+      pixx = ((((A * pixx) + nsxx) + (pd * ((2.0 * ux) * cx))) + axx) / den;
+      pixy = ((((A * pixy) + nsxy) + (pd * ((ux * cy) + (uy * cx)))) + axy) / den;
+      piyy = ((((A * piyy) + nsyy) + (pd * ((2.0 * uy) * cy))) + ayy) / den;
+      if (p.pi_clip_factor > 0) {
+        double cap = p.pi_clip_factor * fabs_(P);
+        pixx = jclamp(pixx, -cap, cap); pixy = jclamp(pixy, -cap, cap); piyy = jclamp(piyy, -cap, cap);
+      }
+      double pe = project_traceless(ux, uy, ut, pixx, pixy, piyy);
+      u[d.iPixx] = pixx; u[d.iPixy] = pixy; u[d.iPiyy] = piyy; u[d.iPieta] = pe;
+    }
+    /* ---- charge ---- */
+    if (p.enable_diff && d.hasNu) {
+      double wv;
+      {
+        double lo = p.vacuum_n_lo, hi = p.vacuum_n_hi;
+        wv = hi <= lo ? 1.0 : (n <= lo ? 0.0 : (n >= hi ? 1.0 : (n - lo) / (hi - lo)));
+      }
+      if (wv <= 0.0) { u[d.iNux] = 0.0; u[d.iNuy] = 0.0; }
+      else {
+        double Tm = posden(T);
+        double alpha = mu / Tm;
+        double kappa = (safe_div(p.kappa_coeff, Tm) * jmax(n, 0.0)) / FV_FMGEV;
+        double tn;
+        diff_tauN<EOS>(d, Tm, alpha, &tn);
+        double dN = p.deltaN_factor * tn;
+        double nux = u[d.iNux], nuy = u[d.iNuy];
+        double dxa = alpha_grad(w.alpha, i, st, ix, d.Nxtot, ng, invdx);
+        double dya = alpha_grad(w.alpha, i, 1, iy, d.Nytot, ng, invdy);
+        double ap = h.alpha_prev[i];
+        double dta = isfinite_(ap) ? (w.alpha[i] - ap) / D : 0.0;
+        double nsx = 0.0, nsy = 0.0;
+        if (p.terms & FIVO_TERM_NU_GRADALPHA) {
+          double Da = ((ut * dta) + (ux * dxa)) + (uy * dya);
+          nsx = (-kappa) * (dxa + (ux * Da));
+          nsy = (-kappa) * (dya + (uy * Da));
+        }
+        nsx *= wv; nsy *= wv;
+        if (p.vacuum_ramp_relax) { tn = wv * tn; dN = wv * dN; }
+        double nut = nu_tau(ux, uy, ut, nux, nuy);
+        double nua = (((-nut) * k.at) + (nux * k.ax)) + (nuy * k.ay);
+        double A = safe_div(tn * ut, D);
+        double den = jmax((A + 1.0) + (dN * k.th), 0.5 * (A + 1.0));
+        double pdn = p.diff_projected_deriv ? tn : 0.0;
+        double anx = p.relax_advect_nu ? (-tn) * upw(d.iNux) : 0.0;
+        double any_ = p.relax_advect_nu ? (-tn) * upw(d.iNuy) : 0.0;
+        nux = ((((A * nux) + nsx) + ((pdn * ux) * nua)) + anx) / den;
+        nuy = ((((A * nuy) + nsy) + ((pdn * uy) * nua)) + any_) / den;
+        if (p.nu_clip_factor > 0) {
+          double cap = (p.nu_clip_factor * jmax(n, 0.0)) * ut;
+          double mag = fx_hypot(nux, nuy);
+          if (mag > cap && mag > FV_TINY) { double sc = cap / mag; nux *= sc; nuy *= sc; }
+        }
+        u[d.iNux] = nux; u[d.iNuy] = nuy;
+      }
+    }
+  }
+  /* project_shear!: residual monitor and pieta from tracelessness, interior cells */
+  if (do_project && d.hasShear && interior) {
+    double rel = shear_residual_rel(ux, uy, ut, u[d.iPixx], u[d.iPixy], u[d.iPiyy], u[d.iPieta]);
+    atomic_max_pos(&fl->shear_max_bits, rel);
+    atomicAdd(&fl->shear_sum, rel);
+    if (p.shear_constraint_project) u[d.iPieta] = project_traceless(ux, uy, ut, u[d.iPixx], u[d.iPixy], u[d.iPiyy]);
+  }
+  for (int a = 4; a < nv; ++a) Uo.f[a][i] = u[a];
+}
+
+/* --------------------------------------------------------------- utilities */
+
+/* flag resets on the device (no host staging, so nothing races a queued copy).
+ * what: 1 = per-pass counters, 2 = amax (set to amax_bits), 4 = shear monitor,
+ * 8 = end-of-run diagnostics */
+__global__ void k_reset_flags(DevFlags* fl, int what, unsigned long long amax_bits) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (what & 1) { fl->nprimfail = 0; fl->nvacuum = 0; fl->rep = 0x7fffffffffffffffULL; fl->nbad = 0; }
+  if (what & 2) fl->amax_bits = amax_bits;
+  if (what & 4) { fl->shear_max_bits = 0; fl->shear_sum = 0.0; }
+  if (what & 8) { fl->sumD = 0.0; fl->maxu = 0.0; fl->minPtot = inf_(); }
+  fl->status = 0;
+}
+
+__global__ void k_fill_nan(double* p, long long n) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = nan_();
+}
+
+/* run_sim_2d! history snapshot (main2D.jl:458-463): alpha_prev = alpha, T_prev = exp(yT) */
+__global__ void k_snapshot(DevParams d, DevPrims w, DevHist h) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.Ntot) return;
+  h.alpha_prev[i] = w.alpha[i];
+  h.T_prev[i] = fx_exp(w.yT[i]);
+}
+
+__global__ void k_copy_planes(DevState dst, DevState src, int a0, int a1, long long n) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int a = a0; a < a1; ++a) dst.f[a][i] = src.f[a][i];
+}
+
+/* AoS (Julia U[a, i]) <-> SoA planes */
+__global__ void k_aos_to_soa(DevState U, const double* aos, int nv, long long n) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * nv) return;
+  long long i = t / nv; int a = (int)(t % nv);
+  U.f[a][i] = aos[t];
+}
+__global__ void k_soa_to_aos(DevState U, double* aos, int nv, long long n) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * nv) return;
+  long long i = t / nv; int a = (int)(t % nv);
+  aos[t] = U.f[a][i];
+}
+
+/* run_sim_2d! diagnostics over the interior (main2D.jl:421-426, 542-556) */
+__global__ void k_diag(DevParams d, DevState U, DevPrims w, DevFlags* fl, int want_u) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double sD = 0.0, mu = 0.0, mp = inf_();
+  if (t < (long long)d.Nx * d.Ny) {
+    int ix = d.ng + (int)(t / d.Ny), iy = d.ng + (int)(t % d.Ny);
+    long long i = (long long)ix * d.Nytot + iy;
+    sD = U.f[d.iDtau][i];
+    if (want_u) {
+      mu = fx_hypot(w.ux[i], w.uy[i]);
+      if (w.P[i] > 0) mp = w.P[i] + (d.hasPi ? U.f[d.iPi][i] : 0.0);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    sD += __shfl_xor_sync(0xffffffffu, sD, o);
+    mu = jmax(mu, __shfl_xor_sync(0xffffffffu, mu, o));
+    mp = jmin(mp, __shfl_xor_sync(0xffffffffu, mp, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&fl->sumD, sD);
+    if (want_u) {
+      atomic_max_pos((unsigned long long*)&fl->maxu, mu);
+      /* minPtot: min over positive and negative values via a CAS loop */
+      double old = fl->minPtot;
+      while (mp < old) {
+        unsigned long long o = __double_as_longlong(old);
+        unsigned long long r = atomicCAS((unsigned long long*)&fl->minPtot, o, (unsigned long long)__double_as_longlong(mp));
+        if (r == o) break;
+        old = __longlong_as_double((long long)r);
+      }
+    }
+  }
+}
+
+/* one-shot helpers for the C ABI's batched entry points */
+template <int EOS>
+__global__ void k_set_cells(DevParams d, long long n, double tau, const double* T, const double* alpha,
+                            const double* ux, const double* uy, const double* Pi, const double* pixx,
+                            const double* pixy, const double* piyy, const double* nux, const double* nuy,
+                            double* U, uint8_t* ok) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double vx = ux[i], vy = uy[i];
+  double ut = utau(vx, vy);
+  double pxx = pixx ? pixx[i] : 0.0, pxy = pixy ? pixy[i] : 0.0, pyy = piyy ? piyy[i] : 0.0;
+  double pieta = project_traceless(vx, vy, ut, pxx, pxy, pyy);
+  double dis[7] = {nux ? nux[i] : 0.0, nuy ? nuy[i] : 0.0, Pi ? Pi[i] : 0.0, pxx, pxy, pyy, pieta};
+  double uc[4];
+  Prim pr;
+  bool r = prim_to_cons<EOS>(uc, pr, T[i], alpha[i] * T[i], vx, vy, dis, tau, d);
+  if (r) {
+    double* col = U + i * d.nv;
+    col[d.iDtau] = uc[0]; col[d.iSx] = uc[1]; col[d.iSy] = uc[2]; col[d.iE] = uc[3];
+    if (d.hasNu) { col[d.iNux] = dis[0]; col[d.iNuy] = dis[1]; }
+    if (d.hasPi) col[d.iPi] = dis[2];
+    if (d.hasShear) { col[d.iPixx] = dis[3]; col[d.iPixy] = dis[4]; col[d.iPiyy] = dis[5]; col[d.iPieta] = dis[6]; }
+  }
+  ok[i] = r ? 1 : 0;
+}
+
+template <int EOS>
+__global__ void k_eos(DevParams d, long long n, const double* T, const double* mu, double* P, double* nq,
+                      double* e) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  eos_Pne<EOS>(T[i], mu[i], d, P + i, nq + i, e + i);
+}
+
+template <int EOS, bool NCH>
+__global__ void k_cons_to_prim(DevParams d, long long n, double tau, const double* cons, const double* warm,
+                               double* prim, uint8_t* ok, uint8_t* reason) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double* c = cons + 11 * i;
+  CellCons cc;
+  cc.D = c[0]; cc.Sx = c[1]; cc.Sy = c[2]; cc.E = c[3]; cc.nux = c[4]; cc.nuy = c[5]; cc.Pi = c[6];
+  cc.pixx = c[7]; cc.pixy = c[8]; cc.piyy = c[9]; cc.pieta = c[10];
+  double y0 = nan_(), f0 = nan_(), x0 = nan_(), v0 = nan_();
+  if (warm) { y0 = warm[4 * i]; f0 = warm[4 * i + 1]; x0 = warm[4 * i + 2]; v0 = warm[4 * i + 3]; }
+  Recovery r = recover<EOS, NCH>(cc, d, y0, f0, x0, v0, d.p.primrec_maxit, d.p.primrec_tol);
+  double* o = prim + 7 * i;
+  o[0] = r.T; o[1] = r.mu; o[2] = r.ux; o[3] = r.uy; o[4] = r.n; o[5] = r.e; o[6] = r.P;
+  ok[i] = r.ok;
+  if (reason) reason[i] = r.reason;
+}
+
+}  // namespace fv
+#endif
