@@ -1,0 +1,379 @@
+#!/usr/bin/env python
+"""bench.py — zone-updates/s of the 2+1D finite-volume stage on B200.
+
+Workload (one GPU): a viscous single event, shear + bulk IS/DNMR (eta/s = 0.16,
+C_s = 0.2 so tau_pi = 5 eta/(e+P), delta_pipi = 4/3 tau_pi; zeta/s Gaussian peak
+0.05 at 0.180 GeV, width 0.024 GeV), diffusing charm (D_s T = 0.5), LatticeHRG
+EOS, 384 x 384 cells on [-15, 15] fm, SSPRK3, CFL 0.2 / CFLtau 0.05, starting
+at tau0 = 0.6 fm/c from a seeded MC-Glauber Pb+Pb event (seed 1001 + rank).
+
+A step is one iteration of run_sim_2d!'s loop (main2D.jl:436-513): the CFL dt,
+the three SSPRK3 stages (each: BCs, primitive recovery on every cell, MUSCL +
+HLLE + sources, combination, floors/bounds/admissibility), the primitive
+refresh, the IS/DNMR relaxation and the shear projection. A zone-update is one
+interior cell advanced through one accepted step.
+
+  value  device-resident: per-step CUDA events on the library's stream, L2
+         flushed (256 MB write) between steps, sum over K steps, max over ranks.
+  e2e    the same steps through the C ABI with the state in pinned host memory:
+         every step uploads U, advances, downloads U (the drop-in usage from a
+         host driver that keeps U on the host).
+
+`--impl reference` times the reference's CPU path (the C++ restatement in
+oracle/, all host threads) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "fivohydro.jl_b200"))
+
+N_CELLS = 384
+BOX = 15.0
+TAU0 = 0.6
+CFL, CFLTAU = 0.2, 0.05
+SEED = 1001
+WORKLOAD = "viscous_event_384x384_ssprk3_lhrg_shear_bulk_diffusion"
+METRIC = "zone-updates/s on 1 B200: batched learned+FP32 vs plain FP64, L2(T)<=1e-6"
+UNIT = "zone-updates/s"
+
+
+def model_and_grid():
+    import fivo2d
+    g = fivo2d.make_grid2d(N_CELLS, N_CELLS, xmax=BOX, ymax=BOX)
+    m = fivo2d.build_model_2d(eos=fivo2d.LatticeHRGEOS(), enable_shear=True, enable_bulk=True,
+                              enable_diff=True, eta_over_s=0.16, tauShear_coeff=0.2,
+                              deltaShear_factor=4 / 3, zeta_over_s=0.05, bulk_model="gaussian",
+                              bulk_T0=0.180, bulk_width=0.024, kappa_coeff=0.5)
+    return g, m
+
+
+def ic_fields(g, seed):
+    from fivo2d import ic
+    T, a, ux, uy, ev = ic.glauber_fields(g, TAU0, seed)
+    return T, a, ux, uy
+
+
+# ----------------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (clocks and throttle reasons)."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        for line in pathlib.Path(self.f.name).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------- roofline
+
+# Algorithmic bytes per cell of each kernel class: every field read or written
+# once per pass (FP64 = 8 B, flags 1 B). nv = 11 state rows here.
+def algorithmic_bytes(kclass, nv, ntot, nint):
+    ndis = nv - 4
+    if kclass == "primitive":   # U (nv) + warm start (4) in; 9 primitives + ok + warm start (4) out
+        return ntot * ((nv + 4) * 8 + 9 * 8 + 1 + 4 * 8)
+    if kclass == "stage":       # U_in (nv), U_old (nv, 2 of 3 stages), 6 prims + ok in; U_out (nv) + bad out
+        return nint * (nv * 8 + (2 / 3) * nv * 8 + 6 * 8 + 1 + nv * 8 + 1)
+    if kclass == "relax":       # dissipatives in/out, 8 primitives + ok, 3 history planes
+        return ntot * (2 * ndis * 8 + 8 * 8 + 1 + 3 * 8)
+    return None
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_from_profiles(kclass):
+    """Per-launch DRAM bytes from the committed ncu summary, if present."""
+    f = ROOT / "profiles" / f"{kclass}_kernel_traffic.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch_full_workload:"):
+            return float(line.split(":")[1])
+    return None
+
+
+# ----------------------------------------------------------------------------- our arm
+
+def run_gpu(args):
+    import numpy as np
+    import torch
+
+    import fivo2d
+    from fivo2d import _abi as A
+    from fivo2d.solver import GPUWork2D, set_cells
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    lib = A.load_library()
+    g, m = model_and_grid()
+    T, a, ux, uy = ic_fields(g, SEED + rank)
+    U0, ok = set_cells(m, TAU0, T, a, ux, uy, lib=lib)
+    w = GPUWork2D(m, g, lib=lib)
+    stream = torch.cuda.Stream()
+    A.check(lib, lib.fivo_ctx_set_stream(w.h, C.c_void_p(stream.cuda_stream)), "set_stream")
+    w.set_state(U0)
+    w.finalize_ic(TAU0)
+    nint = g.Nx * g.Ny
+
+    # prime primitives and signal speeds (run_sim_2d!, main2D.jl:418)
+    w.rhs(TAU0)
+    tau = TAU0
+    res = A.FivoRunResult()
+
+    def advance(n):
+        nonlocal tau
+        A.check(lib, lib.fivo_advance(w.h, tau, 1e9, CFL, CFLTAU, A.FIVO_SSPRK3, A.FIVO_BC_OUTFLOW, n,
+                                      C.byref(res)), "fivo_advance")
+        if not res.ok:
+            raise RuntimeError(f"step failed at tau={tau}")
+        tau = res.tau
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def l2_flush():
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+
+    for _ in range(args.warmup):
+        advance(1)
+
+    # ---------------- device-resident timing
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    A.check(lib, lib.fivo_profile(w.h, 1), "profile")
+    kt = A.FivoKernelTimes()
+    lib.fivo_profile_read(w.h, C.byref(kt), 1)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    tau_start = tau
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            l2_flush()
+            starts[k].record(stream)
+            advance(1)
+            stops[k].record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, stops))
+    lib.fivo_profile_read(w.h, C.byref(kt), 1)
+    A.check(lib, lib.fivo_profile(w.h, 0), "profile")
+    clocks = clk.summary()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = args.steps * nint * world / (ms_max / 1e3)
+
+    # ---------------- end to end through the C ABI, state in pinned host memory
+    Uh = torch.empty((g.Ntot, m.nv), dtype=torch.float64, pin_memory=True)
+    Up = C.cast(Uh.data_ptr(), C.POINTER(C.c_double))
+    lib.fivo_download_state(w.h, Up, m.nv, g.Ntot)
+    e2e_steps = max(1, min(args.steps, 10))
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(e2e_steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(e2e_steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for k in range(e2e_steps):
+        l2_flush()
+        ev0[k].record(stream)
+        A.check(lib, lib.fivo_upload_state(w.h, Up, m.nv, g.Ntot), "upload")
+        advance(1)
+        A.check(lib, lib.fivo_download_state(w.h, Up, m.nv, g.Ntot), "download")
+        ev1[k].record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = sum(a_.elapsed_time(b_) for a_, b_ in zip(ev0, ev1))
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    e2e_value = e2e_steps * nint * world / (float(t.item()) / 1e3)
+    state_bytes = g.Ntot * m.nv * 8
+
+    # ---------------- roofline of the dominant kernel
+    classes = A.KERNEL_CLASSES
+    tot = {c: kt.ms[i] for i, c in enumerate(classes)}
+    dom = max(("primitive", "stage", "relax"), key=lambda c: tot[c])
+    di = classes.index(dom)
+    avg_ms = kt.ms[di] / max(1, kt.launches[di])
+    bytes_launch = algorithmic_bytes(dom, m.nv, g.Ntot, nint)
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_launch / (avg_ms / 1e3) / 1e9
+    traffic = traffic_from_profiles(dom)
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "kernel": f"k_{dom}", "peak_source": peak_kind,
+            "bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms,
+            "kernel_share": {c: tot[c] / max(1e-30, sum(tot.values())) for c in classes},
+            "note": "FP64-ALU bound Newton; bytes-based fraction per the contract, FP64-pipe utilisation in profiles/"}
+
+    w.close()
+    if dist:
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded MC-Glauber event)",
+        "config": {"workload": WORKLOAD, "grid": [N_CELLS, N_CELLS], "box_fm": BOX, "tau0": TAU0,
+                   "tau_window": [tau_start, tau], "integrator": "ssprk3", "cfl": CFL, "cfltau": CFLTAU,
+                   "events_per_gpu": 1, "seed": SEED, "l2": "flushed (256 MB write) between timed steps",
+                   "parallelism": f"replicas{world}"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
+                "d2h_bytes_per_step": state_bytes, "steps": e2e_steps},
+        "gpu_launches": int(kt.total_launches),
+        "roofline": roof,
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.cpu_steps)
+    return line
+
+
+# ----------------------------------------------------------------------------- CPU legs
+
+def oracle_event():
+    sys.path.insert(0, str(ROOT / "tests"))
+    import _oracle as O
+    g, m = model_and_grid()
+    T, a, ux, uy = ic_fields(g, SEED)
+    U, ok = O.set_cells(m.params, TAU0, T, a, ux, uy, m.nv)
+    o = O.OracleSolver(m, g)
+    o.set_state(U)
+    o.finalize_ic(TAU0)
+    return O, g, m, o
+
+
+def oracle_steps(o, tau, n):
+    """n iterations of run_sim_2d!'s loop on the oracle (oracle_advance)."""
+    from fivo2d import _abi as A
+    r = o.advance(tau, 1e9, CFL, CFLTAU, A.FIVO_SSPRK3, 0, n)
+    if not r["ok"] or r["nsteps"] != n:
+        raise RuntimeError("oracle step failed")
+    return r["tau"]
+
+
+def cpu_baseline(nsteps):
+    O, g, m, o = oracle_event()
+    o.rhs(TAU0)
+    t0 = time.perf_counter()
+    oracle_steps(o, TAU0, nsteps)
+    dt = time.perf_counter() - t0
+    return {"value": nsteps * g.Nx * g.Ny / dt, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{nsteps} run_sim_2d! steps of the {N_CELLS}x{N_CELLS} event from tau0 (oracle/, OpenMP)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return None
+    O, g, m, o = oracle_event()
+    o.rhs(TAU0)
+    tau = TAU0
+    tau = oracle_steps(o, tau, args.warmup)
+    t0 = time.perf_counter()
+    oracle_steps(o, tau, args.steps)
+    dt = time.perf_counter() - t0
+    value = args.steps * g.Nx * g.Ny / dt
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded MC-Glauber event)",
+        "config": {"workload": WORKLOAD, "grid": [N_CELLS, N_CELLS], "box_fm": BOX, "tau0": TAU0,
+                   "integrator": "ssprk3", "cfl": CFL, "cfltau": CFLTAU, "seed": SEED},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"{args.steps} run_sim_2d! steps after {args.warmup} warm-up steps; "
+                                   "reference is Julia (not installed), timed via its C++ restatement"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=30)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    if args.impl == "reference":
+        line = run_reference(args)
+    else:
+        line = run_gpu(args)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -134,19 +134,71 @@ struct fivo_ctx {
   double* dU = nullptr;       /* lazily allocated RHS planes for fivo_rhs */
   double* stage = nullptr;    /* nv x Ntot AoS staging for uploads and downloads */
   bool hist_valid = false;
+  long long nsteps_run = 0;            /* accepted steps since fivo_run started */
   fivo_counters cnt;
-  long long rep_none = 0;
+  cudaStream_t own_st = nullptr;       /* the context's own stream (st may be a caller's) */
+  /* per-kernel CUDA-event timing (fivo_profile) */
+  bool profiling = false;
+  struct Pend { int cls; cudaEvent_t a, b; };
+  std::vector<Pend> pend;
+  std::vector<cudaEvent_t> pool;
+  fivo_kernel_times kt;
 };
 
 namespace {
 
 const long long REP_NONE = 0x7fffffffffffffffLL;
 
+/* ------------------------------------------------------------ kernel timing */
+
+cudaEvent_t pool_get(fivo_ctx* c) {
+  if (!c->pool.empty()) { cudaEvent_t e = c->pool.back(); c->pool.pop_back(); return e; }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+/* bracket one launch of kernel class cls (0 primitive, 1 stage, 2 relax, 3 other) */
+struct KTimer {
+  fivo_ctx* c; int cls; cudaEvent_t a = nullptr;
+  KTimer(fivo_ctx* c_, int cls_) : c(c_), cls(cls_) {
+    if (!c->profiling) return;
+    a = pool_get(c);
+    cudaEventRecord(a, c->st);
+  }
+  ~KTimer() {
+    if (!c->profiling || !a) return;
+    cudaEvent_t b = pool_get(c);
+    cudaEventRecord(b, c->st);
+    c->pend.push_back({cls, a, b});
+  }
+};
+
+/* after a stream synchronisation: fold finished launches into the totals */
+void prof_flush(fivo_ctx* c) {
+  for (auto& q : c->pend) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, q.a, q.b) == cudaSuccess) c->kt.ms[q.cls] += ms;
+    c->kt.launches[q.cls] += 1;
+    c->kt.total_launches += 1;
+    c->pool.push_back(q.a);
+    c->pool.push_back(q.b);
+  }
+  c->pend.clear();
+}
+
+cudaError_t ctx_sync(fivo_ctx* c) {
+  cudaError_t e = cudaStreamSynchronize(c->st);
+  if (e == cudaSuccess) prof_flush(c);
+  return e;
+}
+
 /* ---------------------------------------------------------- launch helpers */
 
 int launch_bc(fivo_ctx* c, const DevState& U, int bc) {
   const DevParams& d = c->dp;
   long long nframe = d.Ntot - (long long)d.Nx * d.Ny;
+  KTimer t_(c, 3);
   k_bc<<<nblk(nframe, 256), 256, 0, c->st>>>(d, U, bc);
   CKL();
   return FIVO_OK;
@@ -155,6 +207,7 @@ int launch_bc(fivo_ctx* c, const DevState& U, int bc) {
 /* what: see k_reset_flags. amax is reset to 0 only by an rhs pass (rhs_2d!
  * fills amax_tls, src2d/rhs2d.jl:193); other passes leave it alone. */
 int reset_flags(fivo_ctx* c, int what) {
+  KTimer t_(c, 3);
   k_reset_flags<<<1, 32, 0, c->st>>>(c->fl, what, 0ULL);
   CKL();
   return FIVO_OK;
@@ -163,6 +216,7 @@ int reset_flags(fivo_ctx* c, int what) {
 int launch_primitive(fivo_ctx* c, const DevState& U, double tau) {
   const DevParams& d = c->dp;
   unsigned g = nblk(d.Ntot, 128);
+  KTimer t_(c, 0);
   if (d.p.eos_kind == FIVO_EOS_LATTICE_HRG)
     k_primitive<FIVO_EOS_LATTICE_HRG, true><<<g, 128, 0, c->st>>>(d, U, c->w, c->h, tau, c->fl);
   else if (d.ncharge)
@@ -177,12 +231,10 @@ template <int EOS, bool NCH>
 int launch_stage_t(fivo_ctx* c, const StageArgs& a) {
   const DevParams& d = c->dp;
   size_t smem = (size_t)(ST_NFX + ST_NFY) * d.nv * sizeof(double);
-  static bool attr_set = false;
-  if (!attr_set) {
-    CK(cudaFuncSetAttribute(k_stage<EOS, NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, 120 * 1024));
-    attr_set = true;
-  }
+  /* per device context; cheap enough to set on every launch */
+  CK(cudaFuncSetAttribute(k_stage<EOS, NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid((d.Nxtot + ST_CX - 1) / ST_CX, (d.Nytot + ST_CY - 1) / ST_CY);
+  KTimer t_(c, 1);
   k_stage<EOS, NCH><<<grid, 256, smem, c->st>>>(d, a);
   CKL();
   return FIVO_OK;
@@ -196,7 +248,7 @@ int launch_stage(fivo_ctx* c, const StageArgs& a) {
 
 int sync_flags(fivo_ctx* c, bool read_amax) {
   CK(cudaMemcpyAsync(c->flh, c->fl, sizeof(DevFlags), cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
+  CK(ctx_sync(c));
   const DevFlags& f = *c->flh;
   c->cnt.nprimfail = f.nprimfail;
   c->cnt.nvacuum = f.nvacuum;
@@ -257,6 +309,7 @@ int stage_mood(fivo_ctx* c, int ub, int uo, int uold, double tau, double tau_sta
     const uint8_t* src = bad;
     uint8_t* dst = m1;
     for (int r = 0; r < 1 + attempt; ++r) {
+      KTimer t_(c, 3);
       k_expand_bad<<<nblk(d.Ntot, 256), 256, 0, c->st>>>(d, src, dst);
       CKL();
       src = dst;
@@ -270,6 +323,7 @@ int stage_mood(fivo_ctx* c, int ub, int uo, int uold, double tau, double tau_sta
 
 int copy_state(fivo_ctx* c, int dst, int src) {
   const DevParams& d = c->dp;
+  KTimer t_(c, 3);
   k_copy_planes<<<nblk(d.Ntot, 256), 256, 0, c->st>>>(c->S[dst], c->S[src], 0, d.nv, d.Ntot);
   CKL();
   return FIVO_OK;
@@ -337,11 +391,14 @@ int relax_project(fivo_ctx* c, double tau, double D, int do_relax, int do_projec
   int rc = reset_flags(c, 4);
   if (rc) return rc;
   unsigned g = nblk(d.Ntot, 128);
+  {
+  KTimer t_(c, 2);
   if (d.p.eos_kind == FIVO_EOS_LATTICE_HRG)
     k_relax<FIVO_EOS_LATTICE_HRG><<<g, 128, 0, c->st>>>(d, Uq, Uo, c->w, c->h, tau, D, do_relax, do_project, c->fl);
   else
     k_relax<FIVO_EOS_CONFORMAL_HQ><<<g, 128, 0, c->st>>>(d, Uq, Uo, c->w, c->h, tau, D, do_relax, do_project, c->fl);
   CKL();
+  }
   /* the dissipative planes of U are now those of the scratch state */
   for (int a = 4; a < d.nv; ++a) std::swap(c->S[c->iU].f[a], c->S[c->iT].f[a]);
   if (do_relax) {
@@ -353,7 +410,7 @@ int relax_project(fivo_ctx* c, double tau, double D, int do_relax, int do_projec
 
 int read_shear(fivo_ctx* c, double* maxr, double* meanr) {
   CK(cudaMemcpyAsync(c->flh, c->fl, sizeof(DevFlags), cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
+  CK(ctx_sync(c));
   uint64_t b = c->flh->shear_max_bits;
   double m; std::memcpy(&m, &b, 8);
   if (maxr) *maxr = m;
@@ -363,6 +420,7 @@ int read_shear(fivo_ctx* c, double* maxr, double* meanr) {
 }
 
 int fill_nan(fivo_ctx* c, double* p, long long n) {
+  KTimer t_(c, 3);
   k_fill_nan<<<nblk(n, 256), 256, 0, c->st>>>(p, n);
   CKL();
   return FIVO_OK;
@@ -370,6 +428,7 @@ int fill_nan(fivo_ctx* c, double* p, long long n) {
 
 int reset_history(fivo_ctx* c) {
   int rc;
+  c->nsteps_run = 0;
   /* x0_* and the four *_prev planes are contiguous in hbuf */
   if ((rc = fill_nan(c, c->hbuf, 8 * c->dp.Ntot))) return rc;
   c->hist_valid = false;
@@ -380,10 +439,11 @@ int diag(fivo_ctx* c, bool want_u, double* sumD, double* maxu, double* minPtot) 
   const DevParams& d = c->dp;
   int rc = reset_flags(c, 8);
   if (rc) return rc;
+  KTimer t_(c, 3);
   k_diag<<<nblk((long long)d.Nx * d.Ny, 256), 256, 0, c->st>>>(d, c->S[c->iU], c->w, c->fl, want_u ? 1 : 0);
   CKL();
   CK(cudaMemcpyAsync(c->flh, c->fl, sizeof(DevFlags), cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
+  CK(ctx_sync(c));
   *sumD = c->flh->sumD;
   if (maxu) *maxu = c->flh->maxu;
   if (minPtot) *minPtot = c->flh->minPtot;
@@ -438,8 +498,10 @@ int fivo_ctx_create(const fivo_params* p, int nx, int ny, int nghost, double xma
   c->cnt.primfail_index = -1;
   auto cleanup = [&](int code) { fivo_ctx_destroy(c); return code; };
   if (cudaGetDevice(&c->device) != cudaSuccess) return cleanup(fail(FIVO_ERR_CUDA, "no CUDA device"));
-  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess)
+  if (cudaStreamCreateWithFlags(&c->own_st, cudaStreamNonBlocking) != cudaSuccess)
     return cleanup(fail(FIVO_ERR_CUDA, "cudaStreamCreate failed"));
+  c->st = c->own_st;
+  std::memset(&c->kt, 0, sizeof(c->kt));
   size_t N = (size_t)d.Ntot;
   if (cudaMalloc(&c->slab, 4 * (size_t)d.nv * N * 8) != cudaSuccess ||
       cudaMalloc(&c->pbuf, 9 * N * 8 + N) != cudaSuccess ||
@@ -466,7 +528,7 @@ int fivo_ctx_create(const fivo_params* p, int nx, int ny, int nghost, double xma
     return cleanup(fail(FIVO_ERR_CUDA, "memset failed"));
   if ((rc = reset_history(c))) return cleanup(rc);
   if ((rc = reset_flags(c, 1 | 2 | 4 | 8))) return cleanup(rc);
-  if (cudaStreamSynchronize(c->st) != cudaSuccess) return cleanup(fail(FIVO_ERR_CUDA, "sync failed"));
+  if (ctx_sync(c) != cudaSuccess) return cleanup(fail(FIVO_ERR_CUDA, "sync failed"));
   *out = c;
   return FIVO_OK;
 }
@@ -474,10 +536,12 @@ int fivo_ctx_create(const fivo_params* p, int nx, int ny, int nghost, double xma
 int fivo_ctx_destroy(fivo_ctx* c) {
   if (!c) return FIVO_OK;
   if (c->st) cudaStreamSynchronize(c->st);
+  for (auto& q : c->pend) { cudaEventDestroy(q.a); cudaEventDestroy(q.b); }
+  for (auto e : c->pool) cudaEventDestroy(e);
   cudaFree(c->slab); cudaFree(c->pbuf); cudaFree(c->hbuf); cudaFree(c->masks); cudaFree(c->fl);
   cudaFree(c->dU); cudaFree(c->stage);
   if (c->flh) cudaFreeHost(c->flh);
-  if (c->st) cudaStreamDestroy(c->st);
+  if (c->own_st) cudaStreamDestroy(c->own_st);
   delete c;
   return FIVO_OK;
 }
@@ -496,9 +560,10 @@ int fivo_upload_state(fivo_ctx* c, const double* U, int nv, int64_t ntot) {
   /* stage the AoS block, then transpose into the U planes */
   double* stage = c->stage;
   CK(cudaMemcpyAsync(stage, U, (size_t)nv * ntot * 8, cudaMemcpyHostToDevice, c->st));
+  { KTimer t_(c, 3);
   k_aos_to_soa<<<nblk((long long)nv * ntot, 256), 256, 0, c->st>>>(c->S[c->iU], stage, nv, ntot);
-  CKL();
-  CK(cudaStreamSynchronize(c->st));
+  CKL(); }
+  CK(ctx_sync(c));
   return FIVO_OK;
 }
 
@@ -506,10 +571,11 @@ int fivo_download_state(fivo_ctx* c, double* U, int nv, int64_t ntot) {
   if (!c || !U) return fail(FIVO_ERR_ARG, "null argument");
   if (nv != c->dp.nv || ntot != c->dp.Ntot) return fail(FIVO_ERR_ARG, "state size mismatch");
   double* stage = c->stage;
+  { KTimer t_(c, 3);
   k_soa_to_aos<<<nblk((long long)nv * ntot, 256), 256, 0, c->st>>>(c->S[c->iU], stage, nv, ntot);
-  CKL();
+  CKL(); }
   CK(cudaMemcpyAsync(U, stage, (size_t)nv * ntot * 8, cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
+  CK(ctx_sync(c));
   return FIVO_OK;
 }
 
@@ -524,7 +590,7 @@ int fivo_upload_history(fivo_ctx* c, int64_t ntot, const double* x0_yT, const do
   for (int k = 0; k < 8; ++k)
     if (src[k]) CK(cudaMemcpyAsync(dst[k], src[k], (size_t)ntot * 8, cudaMemcpyHostToDevice, c->st));
   if (alpha_prev) c->hist_valid = fx::isfinite_(alpha_prev[0]);
-  CK(cudaStreamSynchronize(c->st));
+  CK(ctx_sync(c));
   return FIVO_OK;
 }
 
@@ -537,7 +603,7 @@ int fivo_download_history(fivo_ctx* c, int64_t ntot, double* x0_yT, double* x0_p
                           c->h.alpha_prev, c->h.T_prev};
   for (int k = 0; k < 8; ++k)
     if (dst[k]) CK(cudaMemcpyAsync(dst[k], src[k], (size_t)ntot * 8, cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
+  CK(ctx_sync(c));
   return FIVO_OK;
 }
 
@@ -545,7 +611,7 @@ int fivo_reset_history(fivo_ctx* c) {
   if (!c) return fail(FIVO_ERR_ARG, "null context");
   int rc = reset_history(c);
   if (rc) return rc;
-  CK(cudaStreamSynchronize(c->st));
+  CK(ctx_sync(c));
   return FIVO_OK;
 }
 
@@ -558,7 +624,7 @@ int fivo_get_primitives(fivo_ctx* c, int64_t ntot, double* yT, double* phi, doub
   for (int k = 0; k < 9; ++k)
     if (dst[k]) CK(cudaMemcpyAsync(dst[k], src[k], (size_t)ntot * 8, cudaMemcpyDeviceToHost, c->st));
   if (ok) CK(cudaMemcpyAsync(ok, c->w.ok, (size_t)ntot, cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
+  CK(ctx_sync(c));
   return FIVO_OK;
 }
 
@@ -614,7 +680,7 @@ int fivo_relax(fivo_ctx* c, double tau, double dtau) {
   if (!(p.enable_shear || p.enable_bulk || p.enable_diff)) return FIVO_OK;
   int rc = relax_project(c, tau, dtau, 1, 0);
   if (rc) return rc;
-  CK(cudaStreamSynchronize(c->st));
+  CK(ctx_sync(c));
   return FIVO_OK;
 }
 
@@ -638,30 +704,24 @@ int fivo_compute_dt(fivo_ctx* c, double tau, double cfl, double cfltau, double* 
   return FIVO_OK;
 }
 
-int fivo_run(fivo_ctx* c, double tau0, double taufinal, double cfl, double cfltau, int integrator, int bc,
-             int64_t max_steps, int reset_hist, fivo_run_result* out) {
-  if (!c || !out) return fail(FIVO_ERR_ARG, "null argument");
-  if (integrator != FIVO_SSPRK2 && integrator != FIVO_SSPRK3)
-    return fail(FIVO_ERR_ARG, "integrator must be FIVO_SSPRK2 or FIVO_SSPRK3");
+namespace {
+/* run_sim_2d!'s while loop (main2D.jl:436-513) */
+int advance_loop(fivo_ctx* c, double tau, double taufinal, double cfl, double cfltau, int integrator, int bc,
+                 int64_t max_steps, fivo_run_result* out) {
   const DevParams& d = c->dp;
   const fivo_params& p = d.p;
   int rc;
-  std::memset(out, 0, sizeof(*out));
-  if (reset_hist && (rc = reset_history(c))) return rc;
-  /* one RHS pass to populate primitives and signal speeds (main2D.jl:418) */
-  if ((rc = run_stage(c, c->iU, c->iT, c->iU, tau0, tau0, 0.0, 0.0, 0.0, COMB_RHS_ONLY, nullptr, bc, nullptr, nullptr))) return rc;
-  double Qin = 0.0;
-  if ((rc = diag(c, false, &Qin, nullptr, nullptr))) return rc;
-  double tau = tau0;
   int64_t nsteps = 0, nprimfail = 0, nvacuum = 0;
   double max_shear_res = 0.0;
   const bool any_sector = p.enable_shear || p.enable_bulk || p.enable_diff;
+  out->ok = 1;
   while (tau < taufinal && nsteps < max_steps) {
     double D;
     fivo_compute_dt(c, tau, cfl, cfltau, &D);
     D = jmin(D, taufinal - tau);
     if (D <= 0) break;
-    if (c->hist_valid || nsteps > 0) {
+    if (c->hist_valid || c->nsteps_run > 0) {
+      KTimer t_(c, 3);
       k_snapshot<<<nblk(d.Ntot, 256), 256, 0, c->st>>>(d, c->w, c->h);
       CKL();
       c->hist_valid = true;
@@ -671,14 +731,10 @@ int fivo_run(fivo_ctx* c, double tau0, double taufinal, double cfl, double cflta
     if (integrator == FIVO_SSPRK3) rc = step3(c, tau, D, 12, bc, &used, &ok);
     else rc = step2(c, tau, D, 12, 2, bc, &used, &ok);
     if (rc) return rc;
-    if (!ok) {
-      out->ok = 0; out->tau = tau; out->nsteps = nsteps; out->nprimfail = nprimfail; out->nvacuum = nvacuum;
-      out->max_shear_res = max_shear_res; out->maxu = fx::nan_(); out->dQ = fx::nan_(); out->Q0 = Qin;
-      out->Q1 = fx::nan_(); out->minPtot = fx::nan_();
-      return FIVO_OK;
-    }
+    if (!ok) { out->ok = 0; break; }
     tau += used;
     nsteps += 1;
+    c->nsteps_run += 1;
     if (any_sector) {
       if ((rc = update_prims(c, tau, bc))) return rc;
       if ((rc = relax_project(c, tau, used, 1, d.hasShear))) return rc;
@@ -697,29 +753,85 @@ int fivo_run(fivo_ctx* c, double tau0, double taufinal, double cfl, double cflta
     nprimfail += c->cnt.nprimfail;
     nvacuum += c->cnt.nvacuum;
   }
+  out->tau = tau; out->nsteps = nsteps; out->nprimfail = nprimfail; out->nvacuum = nvacuum;
+  out->max_shear_res = max_shear_res;
+  return FIVO_OK;
+}
+}  // namespace
+
+int fivo_run(fivo_ctx* c, double tau0, double taufinal, double cfl, double cfltau, int integrator, int bc,
+             int64_t max_steps, int reset_hist, fivo_run_result* out) {
+  if (!c || !out) return fail(FIVO_ERR_ARG, "null argument");
+  if (integrator != FIVO_SSPRK2 && integrator != FIVO_SSPRK3)
+    return fail(FIVO_ERR_ARG, "integrator must be FIVO_SSPRK2 or FIVO_SSPRK3");
+  int rc;
+  std::memset(out, 0, sizeof(*out));
+  if (reset_hist && (rc = reset_history(c))) return rc;
+  c->nsteps_run = 0;
+  /* one RHS pass to populate primitives and signal speeds (main2D.jl:418) */
+  if ((rc = run_stage(c, c->iU, c->iT, c->iU, tau0, tau0, 0.0, 0.0, 0.0, COMB_RHS_ONLY, nullptr, bc, nullptr, nullptr))) return rc;
+  double Qin = 0.0;
+  if ((rc = diag(c, false, &Qin, nullptr, nullptr))) return rc;
+  if ((rc = advance_loop(c, tau0, taufinal, cfl, cfltau, integrator, bc, max_steps, out))) return rc;
+  out->Q0 = Qin;
+  if (!out->ok) {
+    out->maxu = fx::nan_(); out->dQ = fx::nan_(); out->Q1 = fx::nan_(); out->minPtot = fx::nan_();
+    return FIVO_OK;
+  }
   double Qout = 0.0, maxu = 0.0, minPtot = 0.0;
   if ((rc = diag(c, true, &Qout, &maxu, &minPtot))) return rc;
-  out->ok = 1; out->tau = tau; out->nsteps = nsteps; out->nprimfail = nprimfail; out->nvacuum = nvacuum;
-  out->max_shear_res = max_shear_res; out->maxu = maxu;
+  out->maxu = maxu;
   out->dQ = fx::fabs_(Qin) > 0 ? fx::fabs_(Qout - Qin) / fx::fabs_(Qin) : 0.0;
-  out->Q0 = Qin; out->Q1 = Qout; out->minPtot = minPtot;
+  out->Q1 = Qout; out->minPtot = minPtot;
   return FIVO_OK;
+}
+
+int fivo_advance(fivo_ctx* c, double tau, double taufinal, double cfl, double cfltau, int integrator, int bc,
+                 int64_t max_steps, fivo_run_result* out) {
+  if (!c || !out) return fail(FIVO_ERR_ARG, "null argument");
+  if (integrator != FIVO_SSPRK2 && integrator != FIVO_SSPRK3)
+    return fail(FIVO_ERR_ARG, "integrator must be FIVO_SSPRK2 or FIVO_SSPRK3");
+  std::memset(out, 0, sizeof(*out));
+  return advance_loop(c, tau, taufinal, cfl, cfltau, integrator, bc, max_steps, out);
 }
 
 int fivo_finalize_ic(fivo_ctx* c, double tau0, int bc) {
   if (!c) return fail(FIVO_ERR_ARG, "null context");
   const DevParams& d = c->dp;
+  { KTimer t_(c, 3);
   k_finalize_ic<<<nblk((long long)d.Nx * d.Ny, 256), 256, 0, c->st>>>(d, c->S[c->iU], tau0);
-  CKL();
+  CKL(); }
   int rc = launch_bc(c, c->S[c->iU], bc);
   if (rc) return rc;
-  CK(cudaStreamSynchronize(c->st));
+  CK(ctx_sync(c));
   return FIVO_OK;
 }
 
 int fivo_sync(fivo_ctx* c) {
   if (!c) return fail(FIVO_ERR_ARG, "null context");
-  CK(cudaStreamSynchronize(c->st));
+  CK(ctx_sync(c));
+  return FIVO_OK;
+}
+
+int fivo_ctx_set_stream(fivo_ctx* c, void* stream) {
+  if (!c) return fail(FIVO_ERR_ARG, "null context");
+  CK(ctx_sync(c));
+  c->st = stream ? (cudaStream_t)stream : c->own_st;
+  return FIVO_OK;
+}
+
+int fivo_profile(fivo_ctx* c, int enable) {
+  if (!c) return fail(FIVO_ERR_ARG, "null context");
+  CK(ctx_sync(c));
+  c->profiling = enable != 0;
+  return FIVO_OK;
+}
+
+int fivo_profile_read(fivo_ctx* c, fivo_kernel_times* out, int reset) {
+  if (!c || !out) return fail(FIVO_ERR_ARG, "null argument");
+  CK(ctx_sync(c));
+  *out = c->kt;
+  if (reset) std::memset(&c->kt, 0, sizeof(c->kt));
   return FIVO_OK;
 }
 

@@ -81,6 +81,12 @@ class FivoRunResult(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("pad")}
 
 
+class FivoKernelTimes(C.Structure):
+    _fields_ = [("launches", C.c_int64 * 4), ("ms", C.c_double * 4), ("total_launches", C.c_int64)]
+
+
+KERNEL_CLASSES = ("primitive", "stage", "relax", "other")
+
 PKG_DIR = pathlib.Path(__file__).resolve().parent
 LIB_PATH = PKG_DIR.parent / "csrc" / "libfivo2d.so"
 
@@ -113,11 +119,16 @@ SIGNATURES = {
     "fivo_compute_dt": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, _D]),
     "fivo_run": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
                            C.c_int, _I64, C.c_int, C.POINTER(FivoRunResult)]),
+    "fivo_advance": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                               C.c_int, _I64, C.POINTER(FivoRunResult)]),
     "fivo_finalize_ic": (C.c_int, [C.c_void_p, C.c_double, C.c_int]),
     "fivo_set_cells": (C.c_int, [C.POINTER(FivoParams), _I64, C.c_double] + [_D] * 10 + [_D, _U8]),
     "fivo_eos_Pne": (C.c_int, [C.POINTER(FivoParams), _I64, _D, _D, _D, _D, _D]),
     "fivo_cons_to_prim": (C.c_int, [C.POINTER(FivoParams), _I64, C.c_double, _D, _D, _D, _U8, _U8]),
     "fivo_sync": (C.c_int, [C.c_void_p]),
+    "fivo_ctx_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "fivo_profile": (C.c_int, [C.c_void_p, C.c_int]),
+    "fivo_profile_read": (C.c_int, [C.c_void_p, C.POINTER(FivoKernelTimes), C.c_int]),
 }
 
 _LIB = None

@@ -208,11 +208,18 @@ def eos_params(eos, p: A.FivoParams | None = None) -> A.FivoParams:
     """Fill the EOS block of a fivo_params."""
     p = p if p is not None else A.FivoParams()
     if isinstance(eos, ConformalHQEOS):
+        lh = LatticeHRGEOS()                # unused by this EOS; fivo_params_default's values
+        for k, v in enumerate((lh.a1, lh.a2, lh.a3, lh.a4)):
+            p.lhrg_a[k] = v
+        for k, v in enumerate((lh.b1, lh.b2, lh.b3, lh.b4)):
+            p.lhrg_b[k] = v
+        p.lhrg_c, p.lhrg_d, p.canon_factor = lh.c, lh.d, lh.canon_factor
         p.eos_kind = A.FIVO_EOS_CONFORMAL_HQ
         p.g_eff, p.m_hq, p.g_hq = eos.g_eff, eos.m_hq, eos.g_hq
         p.hq_times_fmGeV3 = int(eos.hq_times_fmGeV3)
     elif isinstance(eos, LatticeHRGEOS):
         p.eos_kind = A.FIVO_EOS_LATTICE_HRG
+        p.g_eff = ConformalHQEOS.g_eff      # unused by this EOS; fivo_params_default's value
         for k, v in enumerate((eos.a1, eos.a2, eos.a3, eos.a4)):
             p.lhrg_a[k] = v
         for k, v in enumerate((eos.b1, eos.b2, eos.b3, eos.b4)):

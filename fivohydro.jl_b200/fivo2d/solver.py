@@ -149,6 +149,14 @@ class GPUWork2D:
                                    int(reset_history), C.byref(r)), "fivo_run")
         return r.as_dict()
 
+    def advance(self, tau, taufinal, cfl=0.2, cfltau=0.05, integrator=A.FIVO_SSPRK2, bc=A.FIVO_BC_OUTFLOW,
+                max_steps=1):
+        """run_sim_2d!'s loop body from tau for at most max_steps steps (a join)."""
+        r = A.FivoRunResult()
+        self._ck(self.lib.fivo_advance(self.h, tau, taufinal, cfl, cfltau, integrator, bc, max_steps,
+                                       C.byref(r)), "fivo_advance")
+        return r.as_dict()
+
     def finalize_ic(self, tau0, bc=A.FIVO_BC_OUTFLOW):
         self._ck(self.lib.fivo_finalize_ic(self.h, tau0, bc), "fivo_finalize_ic")
 

@@ -177,6 +177,15 @@ typedef struct fivo_run_result {
   double  minPtot;
 } fivo_run_result;
 
+/* CUDA-event timing of the library's kernels (fivo_profile). Kernel classes:
+ * 0 = primitive recovery, 1 = stage (faces + combination + sanitiser),
+ * 2 = relaxation + shear projection, 3 = everything else (BCs, copies, masks). */
+typedef struct fivo_kernel_times {
+  int64_t launches[4];
+  double  ms[4];
+  int64_t total_launches;   /* every kernel this context launched while enabled */
+} fivo_kernel_times;
+
 typedef struct fivo_ctx fivo_ctx;
 
 /* --- library --- */
@@ -232,6 +241,14 @@ int  fivo_run(fivo_ctx* ctx, double tau0, double taufinal, double cfl, double cf
               int integrator, int bc, int64_t max_steps, int reset_history,
               fivo_run_result* out);
 
+/* The loop body of run_sim_2d! (main2D.jl:436-513) from tau for at most
+ * max_steps steps (and not past taufinal), continuing the history and the
+ * signal speed of the previous call: no initial rhs, no history reset, no
+ * end-of-run diagnostics. out->tau is the new time, out->nsteps the steps taken.
+ * A host that calls on_dump between chunks uses this instead of fivo_run. */
+int  fivo_advance(fivo_ctx* ctx, double tau, double taufinal, double cfl, double cfltau,
+                  int integrator, int bc, int64_t max_steps, fivo_run_result* out);
+
 /* --- initial conditions --- */
 /* finalize_ic! (main2D.jl:164-171) on the resident state. */
 int  fivo_finalize_ic(fivo_ctx* ctx, double tau0, int bc);
@@ -259,8 +276,15 @@ int  fivo_cons_to_prim(const fivo_params* p, int64_t n, double tau,
                        const double* cons, const double* warm,
                        double* prim, uint8_t* ok, uint8_t* reason);
 
-/* --- synchronisation --- */
+/* --- streams, synchronisation, timing --- */
 int  fivo_sync(fivo_ctx* ctx);
+/* Run the context's later calls on a caller's CUDA stream (a cudaStream_t of
+ * the context's device, e.g. CUDA.jl's or torch's); NULL restores its own. */
+int  fivo_ctx_set_stream(fivo_ctx* ctx, void* stream);
+/* Enable (1) or disable (0) per-kernel CUDA-event timing. */
+int  fivo_profile(fivo_ctx* ctx, int enable);
+/* Accumulated kernel times since enabling or the last reset. */
+int  fivo_profile_read(fivo_ctx* ctx, fivo_kernel_times* out, int reset);
 
 #ifdef __cplusplus
 }

@@ -17,6 +17,7 @@ struct OCtx {
   Model m;
   Work w;
   std::vector<double> U;
+  int64_t nsteps_run = 0;
 };
 }  // namespace
 
@@ -79,6 +80,7 @@ void oracle_get_history(void* h, double* x0_yT, double* x0_phi, double* x0_ux, d
 
 void oracle_reset_history(void* h) {
   OCtx* c = (OCtx*)h;
+  c->nsteps_run = 0;
   for (auto* v : {&c->w.x0_yT, &c->w.x0_phi, &c->w.x0_ux, &c->w.x0_uy, &c->w.ux_prev, &c->w.uy_prev,
                   &c->w.alpha_prev, &c->w.T_prev})
     std::fill(v->begin(), v->end(), O_NAN);
@@ -148,6 +150,15 @@ void oracle_run(void* h, double tau0, double taufinal, double cfl, double cfltau
   OCtx* c = (OCtx*)h;
   run_sim_2d(c->U.data(), c->g, c->m, c->w, tau0, taufinal, cfl, cfltau, integrator, bc,
              reset_history != 0, max_steps, out);
+  c->nsteps_run = out->nsteps;
+}
+
+void oracle_advance(void* h, double tau, double taufinal, double cfl, double cfltau, int integrator, int bc,
+                    int64_t max_steps, fivo_run_result* out) {
+  OCtx* c = (OCtx*)h;
+  std::memset(out, 0, sizeof(*out));
+  advance_sim_2d(c->U.data(), c->g, c->m, c->w, tau, taufinal, cfl, cfltau, integrator, bc, max_steps,
+                 &c->nsteps_run, out);
 }
 
 void oracle_finalize_ic(void* h, double tau0, int bc) {

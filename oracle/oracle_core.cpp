@@ -1616,31 +1616,22 @@ void finalize_ic(double* U, const Grid& g, const Model& m, int bc, double Emin, 
   apply_bc_2d(U, g, m.L, bc);
 }
 
-/* run_sim_2d!, main2D.jl:371-561 (no dumps) */
-void run_sim_2d(double* U, const Grid& g, const Model& m, Work& w, double tau0, double taufinal,
-                double CFL, double CFLtau, int integrator, int bc, bool reset_history,
-                int64_t max_steps, fivo_run_result* res) {
+/* run_sim_2d!'s while loop (main2D.jl:436-513), from tau; nsteps_run is the
+ * count of accepted steps since the run began (run_sim_2d!'s local nsteps) */
+void advance_sim_2d(double* U, const Grid& g, const Model& m, Work& w, double tau, double taufinal,
+                    double CFL, double CFLtau, int integrator, int bc, int64_t max_steps,
+                    int64_t* nsteps_run, fivo_run_result* res) {
   const Layout& L = m.L;
   const fivo_params& p = m.p;
-  if (reset_history) {
-    std::fill(w.x0_yT.begin(), w.x0_yT.end(), O_NAN); std::fill(w.x0_phi.begin(), w.x0_phi.end(), O_NAN);
-    std::fill(w.x0_ux.begin(), w.x0_ux.end(), O_NAN); std::fill(w.x0_uy.begin(), w.x0_uy.end(), O_NAN);
-    std::fill(w.ux_prev.begin(), w.ux_prev.end(), O_NAN); std::fill(w.uy_prev.begin(), w.uy_prev.end(), O_NAN);
-    std::fill(w.alpha_prev.begin(), w.alpha_prev.end(), O_NAN); std::fill(w.T_prev.begin(), w.T_prev.end(), O_NAN);
-  }
-  rhs_2d(w.k.data(), U, g, tau0, m, w, bc, E_FLOOR, nullptr);
-  double Qin = 0.0;
-  for (int ix = g.ng; ix < g.ng + g.Nx; ++ix)
-    for (int iy = g.ng; iy < g.ng + g.Ny; ++iy) Qin += U[g.lin(ix, iy) * L.nv + L.iDtau];
-  double tau = tau0;
   int64_t nsteps = 0, nprimfail = 0, nvacuum = 0;
   double max_shear_res = 0.0;
   bool any_sector = p.enable_shear || p.enable_bulk || p.enable_diff;
+  res->ok = 1;
   while (tau < taufinal && nsteps < max_steps) {
     double D = compute_dt_2d(w, g, tau, CFL, CFLtau);
     D = o_min(D, taufinal - tau);
     if (D <= 0) break;
-    if (o_isfinite(w.alpha_prev[0]) || nsteps > 0) {
+    if (o_isfinite(w.alpha_prev[0]) || *nsteps_run > 0) {
       w.alpha_prev = w.alpha;
       for (int64_t j = 0; j < g.Ntot; ++j) w.T_prev[j] = o_exp(w.yT[j]);
     }
@@ -1648,14 +1639,10 @@ void run_sim_2d(double* U, const Grid& g, const Model& m, Work& w, double tau0, 
     bool ok = integrator == FIVO_SSPRK3
                   ? step_ssprk3_2d(U, g, tau, D, m, w, bc, 12, &used)
                   : step_ssprk2_2d(U, g, tau, D, m, w, bc, 12, 2, &used);
-    if (!ok) {
-      res->ok = 0; res->tau = tau; res->nsteps = nsteps; res->nprimfail = nprimfail;
-      res->nvacuum = nvacuum; res->max_shear_res = max_shear_res; res->maxu = O_NAN;
-      res->dQ = O_NAN; res->Q0 = Qin; res->Q1 = O_NAN; res->minPtot = O_NAN;
-      return;
-    }
+    if (!ok) { res->ok = 0; break; }
     tau += used;
     nsteps += 1;
+    *nsteps_run += 1;
     if (any_sector) {
       update_primitives_2d(U, g, tau, m, w, bc);
       relax_dissipative_2d(U, g, tau, used, m, w);
@@ -1667,6 +1654,32 @@ void run_sim_2d(double* U, const Grid& g, const Model& m, Work& w, double tau0, 
       project_shear(U, g, w, m, &r, &mr);
       max_shear_res = o_max(max_shear_res, r);
     }
+  }
+  res->tau = tau; res->nsteps = nsteps; res->nprimfail = nprimfail; res->nvacuum = nvacuum;
+  res->max_shear_res = max_shear_res;
+}
+
+/* run_sim_2d!, main2D.jl:371-561 (no dumps) */
+void run_sim_2d(double* U, const Grid& g, const Model& m, Work& w, double tau0, double taufinal,
+                double CFL, double CFLtau, int integrator, int bc, bool reset_history,
+                int64_t max_steps, fivo_run_result* res) {
+  const Layout& L = m.L;
+  if (reset_history) {
+    std::fill(w.x0_yT.begin(), w.x0_yT.end(), O_NAN); std::fill(w.x0_phi.begin(), w.x0_phi.end(), O_NAN);
+    std::fill(w.x0_ux.begin(), w.x0_ux.end(), O_NAN); std::fill(w.x0_uy.begin(), w.x0_uy.end(), O_NAN);
+    std::fill(w.ux_prev.begin(), w.ux_prev.end(), O_NAN); std::fill(w.uy_prev.begin(), w.uy_prev.end(), O_NAN);
+    std::fill(w.alpha_prev.begin(), w.alpha_prev.end(), O_NAN); std::fill(w.T_prev.begin(), w.T_prev.end(), O_NAN);
+  }
+  rhs_2d(w.k.data(), U, g, tau0, m, w, bc, E_FLOOR, nullptr);
+  double Qin = 0.0;
+  for (int ix = g.ng; ix < g.ng + g.Nx; ++ix)
+    for (int iy = g.ng; iy < g.ng + g.Ny; ++iy) Qin += U[g.lin(ix, iy) * L.nv + L.iDtau];
+  int64_t nsteps_run = 0;
+  advance_sim_2d(U, g, m, w, tau0, taufinal, CFL, CFLtau, integrator, bc, max_steps, &nsteps_run, res);
+  res->Q0 = Qin;
+  if (!res->ok) {
+    res->maxu = O_NAN; res->dQ = O_NAN; res->Q1 = O_NAN; res->minPtot = O_NAN;
+    return;
   }
   double minPtot = O_INF, maxu = 0.0, Qout = 0.0;
   for (int ix = g.ng; ix < g.ng + g.Nx; ++ix)
@@ -1680,9 +1693,9 @@ void run_sim_2d(double* U, const Grid& g, const Model& m, Work& w, double tau0, 
         if (pt < minPtot) minPtot = pt;
       }
     }
-  double dQ = std::fabs(Qin) > 0 ? std::fabs(Qout - Qin) / std::fabs(Qin) : 0.0;
-  res->ok = 1; res->tau = tau; res->nsteps = nsteps; res->nprimfail = nprimfail; res->nvacuum = nvacuum;
-  res->max_shear_res = max_shear_res; res->maxu = maxu; res->dQ = dQ; res->Q0 = Qin; res->Q1 = Qout;
+  res->maxu = maxu;
+  res->dQ = std::fabs(Qin) > 0 ? std::fabs(Qout - Qin) / std::fabs(Qin) : 0.0;
+  res->Q1 = Qout;
   res->minPtot = minPtot;
 }
 

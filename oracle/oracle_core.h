@@ -131,6 +131,9 @@ bool step_ssprk3_2d(double* U, const Grid& g, double tau, double dtau, const Mod
 int64_t relax_dissipative_2d(double* U, const Grid& g, double tau, double dtau, const Model& m, Work& w);
 void project_shear(double* U, const Grid& g, const Work& w, const Model& m, double* maxr, double* meanr);
 void finalize_ic(double* U, const Grid& g, const Model& m, int bc, double Emin, double tau0);
+void advance_sim_2d(double* U, const Grid& g, const Model& m, Work& w, double tau, double taufinal,
+                    double CFL, double CFLtau, int integrator, int bc, int64_t max_steps,
+                    int64_t* nsteps_run, fivo_run_result* res);
 void run_sim_2d(double* U, const Grid& g, const Model& m, Work& w, double tau0, double taufinal,
                 double CFL, double CFLtau, int integrator, int bc, bool reset_history,
                 int64_t max_steps, fivo_run_result* res);

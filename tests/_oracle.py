@@ -66,6 +66,8 @@ def lib():
             "oracle_run": (None, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
                                   C.c_int, C.c_int64, C.c_int, C.POINTER(A.FivoRunResult)]),
             "oracle_finalize_ic": (None, [C.c_void_p, C.c_double, C.c_int]),
+            "oracle_advance": (None, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                                      C.c_int, C.c_int64, C.POINTER(A.FivoRunResult)]),
             "oracle_set_cells": (C.c_int, [P, C.c_int64, C.c_double] + [_D] * 10 + [_D, _U8]),
             "oracle_eos_Pne": (None, [P, C.c_int64, _D, _D, _D, _D, _D]),
             "oracle_eos_cs2": (None, [P, C.c_int64, _D, _D, _D]),
@@ -217,6 +219,11 @@ class OracleSolver:
         r = A.FivoRunResult()
         lib().oracle_run(self.h, tau0, taufinal, cfl, cfltau, integrator, bc, max_steps, int(reset_history),
                          C.byref(r))
+        return r.as_dict()
+
+    def advance(self, tau, taufinal, cfl=0.2, cfltau=0.05, integrator=A.FIVO_SSPRK2, bc=0, max_steps=1):
+        r = A.FivoRunResult()
+        lib().oracle_advance(self.h, tau, taufinal, cfl, cfltau, integrator, bc, max_steps, C.byref(r))
         return r.as_dict()
 
     def finalize_ic(self, tau0, bc=0):

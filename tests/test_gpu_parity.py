@@ -228,6 +228,31 @@ def test_run_viscous_glauber_bitwise(gpu_lib, integrator):
     _assert_same_work(w, o, "viscous run")
 
 
+def test_advance_chunks_equal_one_run(gpu_lib):
+    """run_sim_2d! resumed step by step (fivo_advance, the on_dump join) gives the
+    bits of the oracle's continuous loop, and the kernel timers count launches."""
+    g, m, U = _glauber_setup(40)
+    w, o = _pair(m, g, U)
+    w.rhs(0.6)
+    o.rhs(0.6)
+    lib = w.lib
+    import ctypes as C
+    lib.fivo_profile(w.h, 1)
+    tau_w = tau_o = 0.6
+    for _ in range(6):
+        rw = w.advance(tau_w, 5.0, 0.2, 0.05, A.FIVO_SSPRK3, A.FIVO_BC_OUTFLOW, 1)
+        ro = o.advance(tau_o, 5.0, 0.2, 0.05, A.FIVO_SSPRK3, 0, 1)
+        assert rw["ok"] and ro["ok"] and rw["tau"] == ro["tau"] and rw["nsteps"] == 1
+        tau_w, tau_o = rw["tau"], ro["tau"]
+    kt = A.FivoKernelTimes()
+    lib.fivo_profile_read(w.h, C.byref(kt), 1)
+    # every stage is one recovery + one stage kernel; every step adds one refresh + one relaxation
+    assert kt.launches[2] == 6 and kt.launches[1] >= 6 * 3
+    assert kt.launches[0] == kt.launches[1] + kt.launches[2]
+    assert all(kt.ms[k] > 0 for k in range(3)) and kt.total_launches > sum(kt.launches[:3])
+    _assert_same_work(w, o, "advance")
+
+
 def test_failure_injection_maxit(gpu_lib):
     """Force the Newton to one iteration on an evolved state: the recovery-failure
     fallback (cold vacuum cells, NaN warm starts, PRR_RESIDUAL_TOO_LARGE) runs
