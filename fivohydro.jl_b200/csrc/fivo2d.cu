@@ -926,3 +926,118 @@ int fivo_cons_to_prim(const fivo_params* p, int64_t n, double tau, const double*
 }
 
 }  /* extern "C" */
+
+/* ======================================================== rhs without allocation
+ *
+ * Some hosts cannot call cudaMalloc: a Julia driver whose device memory is owned
+ * by CUDA.jl's pool allocator, a caller inside a captured or replayed CUDA
+ * graph, or a long-running service that forbids device allocation after start-up
+ * so its memory footprint stays fixed. fivo_rhs_noalloc serves them: its work
+ * memory (the cell primitives, the warm-start planes it starts cold from, and
+ * the flag block) is the file-scope array below, sized for
+ * FIVO_NOALLOC_MAX_CELLS cells (about 17 MB). The array exists on every GPU
+ * that loads this library until the process exits. The first call on a device
+ * looks up its device address (cudaGetSymbolAddress), so make that first call
+ * before any stream capture. Every call shares the array and it keeps the last
+ * call's contents, so each call clears what must start cleared (flags, warm
+ * starts); calls whose work overlaps on the GPU race on it.
+ */
+#include <mutex>
+
+namespace {
+constexpr size_t NOALLOC_PLANE_BYTES = (size_t)FIVO_NOALLOC_MAX_CELLS * 8;
+/* 9 primitive planes + 4 warm-start planes (doubles), the ok bytes, the flags */
+constexpr size_t NOALLOC_BYTES = 13 * NOALLOC_PLANE_BYTES + (((size_t)FIVO_NOALLOC_MAX_CELLS + 255) / 256) * 256 +
+                                 ((sizeof(DevFlags) + 255) / 256) * 256;
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
+
+namespace {
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[128] = {nullptr};
+
+int noalloc_scratch(unsigned char** out) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) return fail(FIVO_ERR_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_ptr[dev] = (unsigned char*)p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return FIVO_OK;
+}
+}  // namespace
+
+extern "C" int fivo_rhs_noalloc(const fivo_params* p, int nx, int ny, double xmax, double ymax, double tau,
+                                int bc, double* U, double* dU, double* amax, void* stream) {
+  if (!p || !U || !dU || !amax) return fail(FIVO_ERR_ARG, "null argument");
+  if (nx <= 8 || ny <= 8) return fail(FIVO_ERR_ARG, "make_grid2d: Nx and Ny must exceed 8");
+  if (!(xmax > 0) || !(ymax > 0)) return fail(FIVO_ERR_ARG, "xmax and ymax must be positive");
+  const long long ntot = (long long)(nx + 6) * (ny + 6);
+  if (ntot > FIVO_NOALLOC_MAX_CELLS)
+    return fail(FIVO_ERR_ARG, "fivo_rhs_noalloc: (nx+6)*(ny+6) = " + std::to_string(ntot) +
+                                  " cells exceeds FIVO_NOALLOC_MAX_CELLS = " +
+                                  std::to_string((long long)FIVO_NOALLOC_MAX_CELLS));
+  int rc = validate(p);
+  if (rc) return rc;
+  unsigned char* base = nullptr;
+  if ((rc = noalloc_scratch(&base))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  DevParams d = make_devparams(p, nx, ny, 3, xmax, ymax);
+  const size_t N = (size_t)d.Ntot;
+  DevState S;
+  for (int a = 0; a < FV_MAXV; ++a) S.f[a] = a < d.nv ? U + (size_t)a * N : nullptr;
+  double* q = (double*)base;
+  DevPrims w;
+  w.yT = q; q += N; w.phi = q; q += N; w.mu = q; q += N; w.alpha = q; q += N;
+  w.ux = q; q += N; w.uy = q; q += N; w.P = q; q += N; w.n = q; q += N; w.e = q; q += N;
+  DevHist h;
+  h.x0_yT = q; q += N; h.x0_phi = q; q += N; h.x0_ux = q; q += N; h.x0_uy = q; q += N;
+  h.ux_prev = h.uy_prev = h.alpha_prev = h.T_prev = nullptr;
+  unsigned char* okb = base + 13 * NOALLOC_PLANE_BYTES;
+  w.ok = (uint8_t*)okb;
+  DevFlags* fl = (DevFlags*)(okb + (((size_t)FIVO_NOALLOC_MAX_CELLS + 255) / 256) * 256);
+  /* clear what the pass must start from: NaN warm starts (a cold start), the flags */
+  k_fill_nan<<<nblk(4 * (long long)N, 256), 256, 0, st>>>(h.x0_yT, 4 * (long long)N);
+  CKL();
+  k_reset_flags<<<1, 32, 0, st>>>(fl, 1 | 2 | 4 | 8, 0ULL);
+  CKL();
+  CK(cudaMemsetAsync(dU, 0, (size_t)d.nv * N * 8, st));
+  /* rhs_2d!: BCs, primitive pass, faces + sources (src2d/rhs2d.jl:169-249) */
+  long long nframe = d.Ntot - (long long)d.Nx * d.Ny;
+  k_bc<<<nblk(nframe, 256), 256, 0, st>>>(d, S, bc);
+  CKL();
+  unsigned g = nblk(d.Ntot, 128);
+  if (d.p.eos_kind == FIVO_EOS_LATTICE_HRG)
+    k_primitive<FIVO_EOS_LATTICE_HRG, true><<<g, 128, 0, st>>>(d, S, w, h, tau, fl);
+  else if (d.ncharge)
+    k_primitive<FIVO_EOS_CONFORMAL_HQ, true><<<g, 128, 0, st>>>(d, S, w, h, tau, fl);
+  else
+    k_primitive<FIVO_EOS_CONFORMAL_HQ, false><<<g, 128, 0, st>>>(d, S, w, h, tau, fl);
+  CKL();
+  StageArgs a;
+  a.Ub = S; a.Uold = S; a.Uout = S; a.w = w; a.ffo = nullptr; a.bad = nullptr; a.dU = dU;
+  a.tau = tau; a.tau_state = tau; a.dt = 0.0; a.wold = 0.0; a.wnew = 0.0; a.mode = COMB_RHS_ONLY; a.fl = fl;
+  size_t smem = (size_t)(ST_NFX + ST_NFY) * d.nv * sizeof(double);
+  dim3 grid((d.Nxtot + ST_CX - 1) / ST_CX, (d.Nytot + ST_CY - 1) / ST_CY);
+  if (d.p.eos_kind == FIVO_EOS_LATTICE_HRG) {
+    CK(cudaFuncSetAttribute(k_stage<FIVO_EOS_LATTICE_HRG, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_stage<FIVO_EOS_LATTICE_HRG, true><<<grid, 256, smem, st>>>(d, a);
+  } else if (d.ncharge) {
+    CK(cudaFuncSetAttribute(k_stage<FIVO_EOS_CONFORMAL_HQ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_stage<FIVO_EOS_CONFORMAL_HQ, true><<<grid, 256, smem, st>>>(d, a);
+  } else {
+    CK(cudaFuncSetAttribute(k_stage<FIVO_EOS_CONFORMAL_HQ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_stage<FIVO_EOS_CONFORMAL_HQ, false><<<grid, 256, smem, st>>>(d, a);
+  }
+  CKL();
+  unsigned long long bits = 0;
+  CK(cudaMemcpyAsync(&bits, &fl->amax_bits, sizeof(bits), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  std::memcpy(amax, &bits, 8);
+  return FIVO_OK;
+}

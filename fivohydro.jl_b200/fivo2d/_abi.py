@@ -30,6 +30,7 @@ TERM_NAMES = (
 )
 TERM_BIT = {n: 1 << k for k, n in enumerate(TERM_NAMES)}
 FIVO_TERMS_DEFAULT = 0x1DFFF
+FIVO_NOALLOC_MAX_CELLS = 160000
 
 
 class FivoParams(C.Structure):
@@ -126,6 +127,8 @@ SIGNATURES = {
     "fivo_eos_Pne": (C.c_int, [C.POINTER(FivoParams), _I64, _D, _D, _D, _D, _D]),
     "fivo_cons_to_prim": (C.c_int, [C.POINTER(FivoParams), _I64, C.c_double, _D, _D, _D, _U8, _U8]),
     "fivo_sync": (C.c_int, [C.c_void_p]),
+    "fivo_rhs_noalloc": (C.c_int, [C.POINTER(FivoParams), C.c_int, C.c_int, C.c_double, C.c_double,
+                                   C.c_double, C.c_int, C.c_void_p, C.c_void_p, _D, C.c_void_p]),
     "fivo_ctx_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "fivo_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "fivo_profile_read": (C.c_int, [C.c_void_p, C.POINTER(FivoKernelTimes), C.c_int]),

@@ -276,6 +276,20 @@ int  fivo_cons_to_prim(const fivo_params* p, int64_t n, double tau,
                        const double* cons, const double* warm,
                        double* prim, uint8_t* ok, uint8_t* reason);
 
+/* --- rhs without device allocation --- */
+/* No counterpart in the reference: an extra entry point for hosts that cannot
+ * allocate device memory (see the comment block in fivo2d.cu). One rhs_2d!
+ * evaluation with a cold-started recovery (no warm starts are kept), reading the
+ * state U and writing the right-hand side dU, both caller-owned device buffers of
+ * nv planes x Ntot doubles (plane a at ptr + a*Ntot). The ghost frame of U is
+ * refilled in place, as rhs_2d! does. *amax (host) receives the largest HLLE
+ * signal speed. stream may be NULL (the default stream). Work memory is a
+ * fixed file-scope device array, so Ntot = (nx+6)*(ny+6) must not exceed
+ * FIVO_NOALLOC_MAX_CELLS; concurrent calls on overlapping streams race on it. */
+#define FIVO_NOALLOC_MAX_CELLS 160000
+int  fivo_rhs_noalloc(const fivo_params* p, int nx, int ny, double xmax, double ymax,
+                      double tau, int bc, double* U, double* dU, double* amax, void* stream);
+
 /* --- streams, synchronisation, timing --- */
 int  fivo_sync(fivo_ctx* ctx);
 /* Run the context's later calls on a caller's CUDA stream (a cudaStream_t of
