@@ -132,6 +132,9 @@ struct fivo_ctx {
   DevFlags* fl = nullptr;
   DevFlags* flh = nullptr;    /* pinned mirror */
   double* dU = nullptr;       /* lazily allocated RHS planes for fivo_rhs */
+  double* fh = nullptr;       /* face fluxes: x faces then y faces, nv planes each */
+  unsigned int* queues = nullptr;  /* deferred recoveries | deferred admissibility tests */
+  int nsm = 148;
   double* stage = nullptr;    /* nv x Ntot AoS staging for uploads and downloads */
   bool hist_valid = false;
   long long nsteps_run = 0;            /* accepted steps since fivo_run started */
@@ -139,10 +142,11 @@ struct fivo_ctx {
   cudaStream_t own_st = nullptr;       /* the context's own stream (st may be a caller's) */
   /* per-kernel CUDA-event timing (fivo_profile) */
   bool profiling = false;
-  struct Pend { int cls; cudaEvent_t a, b; };
+  struct Pend { int cls, nk; long long units; cudaEvent_t a, b; };
   std::vector<Pend> pend;
   std::vector<cudaEvent_t> pool;
   fivo_kernel_times kt;
+  int64_t tot_base_p = 0, tot_base_a = 0;   /* device deferred-cell totals at the last reset */
 };
 
 namespace {
@@ -158,10 +162,10 @@ cudaEvent_t pool_get(fivo_ctx* c) {
   return e;
 }
 
-/* bracket one launch of kernel class cls (0 primitive, 1 stage, 2 relax, 3 other) */
+/* bracket nk launches of kernel class cls (FIVO_KCLASS_*) that process `units` cells or faces */
 struct KTimer {
-  fivo_ctx* c; int cls; cudaEvent_t a = nullptr;
-  KTimer(fivo_ctx* c_, int cls_) : c(c_), cls(cls_) {
+  fivo_ctx* c; int cls, nk; long long units; cudaEvent_t a = nullptr;
+  KTimer(fivo_ctx* c_, int cls_, int nk_ = 1, long long units_ = 0) : c(c_), cls(cls_), nk(nk_), units(units_) {
     if (!c->profiling) return;
     a = pool_get(c);
     cudaEventRecord(a, c->st);
@@ -170,7 +174,7 @@ struct KTimer {
     if (!c->profiling || !a) return;
     cudaEvent_t b = pool_get(c);
     cudaEventRecord(b, c->st);
-    c->pend.push_back({cls, a, b});
+    c->pend.push_back({cls, nk, units, a, b});
   }
 };
 
@@ -180,7 +184,8 @@ void prof_flush(fivo_ctx* c) {
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, q.a, q.b) == cudaSuccess) c->kt.ms[q.cls] += ms;
     c->kt.launches[q.cls] += 1;
-    c->kt.total_launches += 1;
+    c->kt.total_launches += q.nk;
+    c->kt.units[q.cls] += q.units;
     c->pool.push_back(q.a);
     c->pool.push_back(q.b);
   }
@@ -198,7 +203,7 @@ cudaError_t ctx_sync(fivo_ctx* c) {
 int launch_bc(fivo_ctx* c, const DevState& U, int bc) {
   const DevParams& d = c->dp;
   long long nframe = d.Ntot - (long long)d.Nx * d.Ny;
-  KTimer t_(c, 3);
+  KTimer t_(c, FIVO_KCLASS_OTHER);
   k_bc<<<nblk(nframe, 256), 256, 0, c->st>>>(d, U, bc);
   CKL();
   return FIVO_OK;
@@ -207,36 +212,64 @@ int launch_bc(fivo_ctx* c, const DevState& U, int bc) {
 /* what: see k_reset_flags. amax is reset to 0 only by an rhs pass (rhs_2d!
  * fills amax_tls, src2d/rhs2d.jl:193); other passes leave it alone. */
 int reset_flags(fivo_ctx* c, int what) {
-  KTimer t_(c, 3);
+  KTimer t_(c, FIVO_KCLASS_OTHER);
   k_reset_flags<<<1, 32, 0, c->st>>>(c->fl, what, 0ULL);
   CKL();
   return FIVO_OK;
 }
 
-int launch_primitive(fivo_ctx* c, const DevState& U, double tau) {
+template <int EOS, bool NCH>
+int launch_primitive_t(fivo_ctx* c, const DevState& U, double tau) {
   const DevParams& d = c->dp;
-  unsigned g = nblk(d.Ntot, 128);
-  KTimer t_(c, 0);
-  if (d.p.eos_kind == FIVO_EOS_LATTICE_HRG)
-    k_primitive<FIVO_EOS_LATTICE_HRG, true><<<g, 128, 0, c->st>>>(d, U, c->w, c->h, tau, c->fl);
-  else if (d.ncharge)
-    k_primitive<FIVO_EOS_CONFORMAL_HQ, true><<<g, 128, 0, c->st>>>(d, U, c->w, c->h, tau, c->fl);
-  else
-    k_primitive<FIVO_EOS_CONFORMAL_HQ, false><<<g, 128, 0, c->st>>>(d, U, c->w, c->h, tau, c->fl);
-  CKL();
+  unsigned int* q = c->queues;
+  {
+    KTimer t_(c, FIVO_KCLASS_PRIM_FAST, 1, d.Ntot);
+    k_prim_fast<EOS, NCH><<<nblk(d.Ntot, 128), 128, 0, c->st>>>(d, U, c->w, c->h, tau, c->fl, q);
+    CKL();
+  }
+  {
+    KTimer t_(c, FIVO_KCLASS_PRIM_SLOW);
+    k_prim_slow<EOS, NCH><<<2 * c->nsm, 128, 0, c->st>>>(d, U, c->w, c->h, tau, c->fl, q);
+    CKL();
+  }
   return FIVO_OK;
 }
 
+/* _primitive_pass!: the two-phase recovery (k_prim_fast, then k_prim_slow on
+ * the cells it deferred). The flag block's pass counters must be reset first. */
+int launch_primitive(fivo_ctx* c, const DevState& U, double tau) {
+  const DevParams& d = c->dp;
+  if (d.p.eos_kind == FIVO_EOS_LATTICE_HRG) return launch_primitive_t<FIVO_EOS_LATTICE_HRG, true>(c, U, tau);
+  if (d.ncharge) return launch_primitive_t<FIVO_EOS_CONFORMAL_HQ, true>(c, U, tau);
+  return launch_primitive_t<FIVO_EOS_CONFORMAL_HQ, false>(c, U, tau);
+}
+
+/* rhs_2d! + combination + sanitiser + admissibility: k_faces (x, y), k_update,
+ * and k_adm_slow for the cells whose admissibility needs an inversion. */
 template <int EOS, bool NCH>
 int launch_stage_t(fivo_ctx* c, const StageArgs& a) {
   const DevParams& d = c->dp;
-  size_t smem = (size_t)(ST_NFX + ST_NFY) * d.nv * sizeof(double);
-  /* per device context; cheap enough to set on every launch */
-  CK(cudaFuncSetAttribute(k_stage<EOS, NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  dim3 grid((d.Nxtot + ST_CX - 1) / ST_CX, (d.Nytot + ST_CY - 1) / ST_CY);
-  KTimer t_(c, 1);
-  k_stage<EOS, NCH><<<grid, 256, smem, c->st>>>(d, a);
-  CKL();
+  double* fhx = c->fh;
+  double* fhy = c->fh + (size_t)d.nv * d.Ntot;
+  {
+    long long nfx = (long long)(d.Nxtot - 1) * d.Nytot, nfy = (long long)d.Nxtot * (d.Nytot - 1);
+    KTimer t_(c, FIVO_KCLASS_FACES, 2, nfx + nfy);
+    k_faces<EOS, true><<<nblk(nfx, 128), 128, 0, c->st>>>(d, a.Ub, a.w, a.tau, a.ffo, fhx, c->fl);
+    CKL();
+    k_faces<EOS, false><<<nblk(nfy, 128), 128, 0, c->st>>>(d, a.Ub, a.w, a.tau, a.ffo, fhy, c->fl);
+    CKL();
+  }
+  unsigned int* aq = c->queues + d.Ntot;
+  {
+    KTimer t_(c, FIVO_KCLASS_UPDATE, 1, (long long)d.Nx * d.Ny);
+    k_update<EOS, NCH><<<nblk((long long)d.Nx * d.Ny, 128), 128, 0, c->st>>>(d, a, fhx, fhy, aq);
+    CKL();
+  }
+  if (a.mode != COMB_RHS_ONLY) {
+    KTimer t_(c, FIVO_KCLASS_ADM_SLOW);
+    k_adm_slow<EOS, NCH><<<c->nsm, 128, 0, c->st>>>(d, a.Uout, a.tau_state, a.bad, c->fl, aq);
+    CKL();
+  }
   return FIVO_OK;
 }
 
@@ -309,7 +342,7 @@ int stage_mood(fivo_ctx* c, int ub, int uo, int uold, double tau, double tau_sta
     const uint8_t* src = bad;
     uint8_t* dst = m1;
     for (int r = 0; r < 1 + attempt; ++r) {
-      KTimer t_(c, 3);
+      KTimer t_(c, FIVO_KCLASS_OTHER);
       k_expand_bad<<<nblk(d.Ntot, 256), 256, 0, c->st>>>(d, src, dst);
       CKL();
       src = dst;
@@ -323,7 +356,7 @@ int stage_mood(fivo_ctx* c, int ub, int uo, int uold, double tau, double tau_sta
 
 int copy_state(fivo_ctx* c, int dst, int src) {
   const DevParams& d = c->dp;
-  KTimer t_(c, 3);
+  KTimer t_(c, FIVO_KCLASS_OTHER);
   k_copy_planes<<<nblk(d.Ntot, 256), 256, 0, c->st>>>(c->S[dst], c->S[src], 0, d.nv, d.Ntot);
   CKL();
   return FIVO_OK;
@@ -392,7 +425,7 @@ int relax_project(fivo_ctx* c, double tau, double D, int do_relax, int do_projec
   if (rc) return rc;
   unsigned g = nblk(d.Ntot, 128);
   {
-  KTimer t_(c, 2);
+  KTimer t_(c, FIVO_KCLASS_RELAX, 1, d.Ntot);
   if (d.p.eos_kind == FIVO_EOS_LATTICE_HRG)
     k_relax<FIVO_EOS_LATTICE_HRG><<<g, 128, 0, c->st>>>(d, Uq, Uo, c->w, c->h, tau, D, do_relax, do_project, c->fl);
   else
@@ -420,7 +453,7 @@ int read_shear(fivo_ctx* c, double* maxr, double* meanr) {
 }
 
 int fill_nan(fivo_ctx* c, double* p, long long n) {
-  KTimer t_(c, 3);
+  KTimer t_(c, FIVO_KCLASS_OTHER);
   k_fill_nan<<<nblk(n, 256), 256, 0, c->st>>>(p, n);
   CKL();
   return FIVO_OK;
@@ -439,7 +472,7 @@ int diag(fivo_ctx* c, bool want_u, double* sumD, double* maxu, double* minPtot) 
   const DevParams& d = c->dp;
   int rc = reset_flags(c, 8);
   if (rc) return rc;
-  KTimer t_(c, 3);
+  KTimer t_(c, FIVO_KCLASS_OTHER);
   k_diag<<<nblk((long long)d.Nx * d.Ny, 256), 256, 0, c->st>>>(d, c->S[c->iU], c->w, c->fl, want_u ? 1 : 0);
   CKL();
   CK(cudaMemcpyAsync(c->flh, c->fl, sizeof(DevFlags), cudaMemcpyDeviceToHost, c->st));
@@ -508,8 +541,12 @@ int fivo_ctx_create(const fivo_params* p, int nx, int ny, int nghost, double xma
       cudaMalloc(&c->hbuf, 8 * N * 8) != cudaSuccess ||
       cudaMalloc(&c->masks, 3 * N) != cudaSuccess ||
       cudaMalloc(&c->fl, sizeof(DevFlags)) != cudaSuccess ||
-      cudaMalloc(&c->stage, (size_t)d.nv * N * 8) != cudaSuccess)
+      cudaMalloc(&c->stage, (size_t)d.nv * N * 8) != cudaSuccess ||
+      cudaMalloc(&c->fh, 2 * (size_t)d.nv * N * 8) != cudaSuccess ||
+      cudaMalloc(&c->queues, 2 * N * sizeof(unsigned int)) != cudaSuccess)
     return cleanup(fail(FIVO_ERR_NOMEM, "device allocation failed"));
+  if (cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess || c->nsm < 1)
+    c->nsm = 148;
   if (cudaMallocHost(&c->flh, sizeof(DevFlags)) != cudaSuccess)
     return cleanup(fail(FIVO_ERR_NOMEM, "pinned allocation failed"));
   for (int s = 0; s < 4; ++s)
@@ -527,7 +564,7 @@ int fivo_ctx_create(const fivo_params* p, int nx, int ny, int nghost, double xma
       cudaMemsetAsync(c->masks, 0, 3 * N, c->st) != cudaSuccess)
     return cleanup(fail(FIVO_ERR_CUDA, "memset failed"));
   if ((rc = reset_history(c))) return cleanup(rc);
-  if ((rc = reset_flags(c, 1 | 2 | 4 | 8))) return cleanup(rc);
+  if ((rc = reset_flags(c, 1 | 2 | 4 | 8 | 16))) return cleanup(rc);
   if (ctx_sync(c) != cudaSuccess) return cleanup(fail(FIVO_ERR_CUDA, "sync failed"));
   *out = c;
   return FIVO_OK;
@@ -539,7 +576,7 @@ int fivo_ctx_destroy(fivo_ctx* c) {
   for (auto& q : c->pend) { cudaEventDestroy(q.a); cudaEventDestroy(q.b); }
   for (auto e : c->pool) cudaEventDestroy(e);
   cudaFree(c->slab); cudaFree(c->pbuf); cudaFree(c->hbuf); cudaFree(c->masks); cudaFree(c->fl);
-  cudaFree(c->dU); cudaFree(c->stage);
+  cudaFree(c->dU); cudaFree(c->stage); cudaFree(c->fh); cudaFree(c->queues);
   if (c->flh) cudaFreeHost(c->flh);
   if (c->own_st) cudaStreamDestroy(c->own_st);
   delete c;
@@ -560,7 +597,7 @@ int fivo_upload_state(fivo_ctx* c, const double* U, int nv, int64_t ntot) {
   /* stage the AoS block, then transpose into the U planes */
   double* stage = c->stage;
   CK(cudaMemcpyAsync(stage, U, (size_t)nv * ntot * 8, cudaMemcpyHostToDevice, c->st));
-  { KTimer t_(c, 3);
+  { KTimer t_(c, FIVO_KCLASS_OTHER);
   k_aos_to_soa<<<nblk((long long)nv * ntot, 256), 256, 0, c->st>>>(c->S[c->iU], stage, nv, ntot);
   CKL(); }
   CK(ctx_sync(c));
@@ -571,7 +608,7 @@ int fivo_download_state(fivo_ctx* c, double* U, int nv, int64_t ntot) {
   if (!c || !U) return fail(FIVO_ERR_ARG, "null argument");
   if (nv != c->dp.nv || ntot != c->dp.Ntot) return fail(FIVO_ERR_ARG, "state size mismatch");
   double* stage = c->stage;
-  { KTimer t_(c, 3);
+  { KTimer t_(c, FIVO_KCLASS_OTHER);
   k_soa_to_aos<<<nblk((long long)nv * ntot, 256), 256, 0, c->st>>>(c->S[c->iU], stage, nv, ntot);
   CKL(); }
   CK(cudaMemcpyAsync(U, stage, (size_t)nv * ntot * 8, cudaMemcpyDeviceToHost, c->st));
@@ -721,7 +758,7 @@ int advance_loop(fivo_ctx* c, double tau, double taufinal, double cfl, double cf
     D = jmin(D, taufinal - tau);
     if (D <= 0) break;
     if (c->hist_valid || c->nsteps_run > 0) {
-      KTimer t_(c, 3);
+      KTimer t_(c, FIVO_KCLASS_OTHER);
       k_snapshot<<<nblk(d.Ntot, 256), 256, 0, c->st>>>(d, c->w, c->h);
       CKL();
       c->hist_valid = true;
@@ -798,7 +835,7 @@ int fivo_advance(fivo_ctx* c, double tau, double taufinal, double cfl, double cf
 int fivo_finalize_ic(fivo_ctx* c, double tau0, int bc) {
   if (!c) return fail(FIVO_ERR_ARG, "null context");
   const DevParams& d = c->dp;
-  { KTimer t_(c, 3);
+  { KTimer t_(c, FIVO_KCLASS_OTHER);
   k_finalize_ic<<<nblk((long long)d.Nx * d.Ny, 256), 256, 0, c->st>>>(d, c->S[c->iU], tau0);
   CKL(); }
   int rc = launch_bc(c, c->S[c->iU], bc);
@@ -829,9 +866,17 @@ int fivo_profile(fivo_ctx* c, int enable) {
 
 int fivo_profile_read(fivo_ctx* c, fivo_kernel_times* out, int reset) {
   if (!c || !out) return fail(FIVO_ERR_ARG, "null argument");
+  CK(cudaMemcpyAsync(c->flh, c->fl, sizeof(DevFlags), cudaMemcpyDeviceToHost, c->st));
   CK(ctx_sync(c));
+  /* deferred cells are counted on the device; the profile owns those totals */
+  c->kt.units[FIVO_KCLASS_PRIM_SLOW] = (int64_t)c->flh->tot_p - c->tot_base_p;
+  c->kt.units[FIVO_KCLASS_ADM_SLOW] = (int64_t)c->flh->tot_a - c->tot_base_a;
   *out = c->kt;
-  if (reset) std::memset(&c->kt, 0, sizeof(c->kt));
+  if (reset) {
+    std::memset(&c->kt, 0, sizeof(c->kt));
+    c->tot_base_p = (int64_t)c->flh->tot_p;
+    c->tot_base_a = (int64_t)c->flh->tot_a;
+  }
   return FIVO_OK;
 }
 

@@ -15,8 +15,10 @@
  *            s = (m-1)/(m+1), odd series to s^23.
  *   fx_pow4  exponentiation by squaring with error-free squares (pow_body).
  *   fx_k01x  e^x K0(x), e^x K1(x): power series (A&S 9.6.10-9.6.13) for x < 1;
- *            34-node trapezoidal rule (step 1/5) on DLMF 10.32.8 with t = s^2
- *            for x >= 1; <= 6e-16 relative to 40-digit references.
+ *            Chebyshev series by Clenshaw's recurrence for 1 <= x < 1e4 (in
+ *            u = 2x - 3 below 2, in u = 4/x - 1 for sqrt(x) e^x K above), with
+ *            coefficients computed here from 50-digit values (gen_bessel_cheb.py);
+ *            <= 4e-16 relative to 40-digit references.
  *   fx_besselkx  safe_besselkx (src/eos.jl:27-34): 0 for x <= 0, the reference's
  *            three-term asymptotic series for x >= 1e4, else recurrence.
  */
@@ -202,30 +204,71 @@ FX_HD double fx_hypot(double x, double y) {
   return h * scale;
 }
 
-/* trapezoid nodes s_k^2 = (k/5)^2 and weights (1/5) e^{-s_k^2}/sqrt(pi) (doubled for k > 0) */
-#define FX_BESSEL_S2 { \
-  0.0, 0.04, 0.16, 0.36, 0.64, 1.0, 1.44, 1.96, 2.56, 3.24, 4.0, 4.84, 5.76, 6.76, \
-  7.84, 9.0, 10.24, 11.56, 12.96, 14.44, 16.0, 17.64, 19.36, 21.16, 23.04, 25.0, \
-  27.04, 29.16, 31.36, 33.64, 36.0, 38.44, 40.96, 43.56}
-#define FX_BESSEL_W { \
-  0.11283791670955126, 0.21682695742097263, 0.19230825976786156, 0.15744868634285744, \
-  0.11899715725149379, 0.08302149948411894, 0.05346886940070783, 0.03178834153545557, \
-  0.017445811726789072, 0.008838344666402213, 0.004133397070818411, 0.001784431012983241, \
-  0.0007111297361755495, 0.00026161000994465633, 8.884158884113332e-05, 2.785061038934957e-05, \
-  8.059527106647123e-06, 2.1529842073361357e-06, 5.309193689433173e-07, 1.2085725786444936e-07, \
-  2.5396469343733115e-08, 4.926408197336689e-09, 8.821529389366844e-10, 1.4581890004763904e-10, \
-  2.225052137962172e-11, 3.134173306203467e-12, 4.075325146752109e-13, 4.89167914078347e-14, \
-  5.420134984939562e-15, 5.543942072256747e-16, 5.2346024784985296e-17, 4.5625240909092945e-18, \
-  3.670988941398298e-19, 2.726574842629012e-20}
+/* Chebyshev coefficients (gen_bessel_cheb.py: 50-digit mpmath, rounded once):
+ * A: e^x K_nu(x) in u = 2x - 3 on [1, 2); B: sqrt(x) e^x K_nu(x) in u = 4/x - 1 on [2, 1e4). */
+#define FX_CHEB_K0A { \
+  0.975293670703631, -0.14911366079770616, 0.01739593810625341, -0.0022865321321120587, \
+  0.00031902053048988584, -4.617742767921652e-05, 6.855099419473594e-06, -1.0367102847936046e-06, \
+  1.590358485499584e-07, -2.4674715067053715e-08, 3.863812252910323e-09, -6.096897833322557e-10, \
+  9.683069016813046e-11, -1.5464054179684872e-11, 2.481515505543579e-12, -3.9988227436440834e-13, \
+  6.467756230057925e-14, -1.0495481280269401e-14, 1.7081563652123322e-15, -2.7874138983949704e-16, \
+  4.5594687260393236e-17, -7.47431382282828e-18}
+#define FX_CHEB_K1A { \
+  1.287716931284971, -0.29355526501238677, 0.04578781607810882, -0.0075606314967654195, \
+  0.0012725129170005956, -0.0002159483044944044, 3.679893234585295e-05, -6.2852010326152186e-06, \
+  1.0749808007083846e-06, -1.8401830928999913e-07, 3.151902199740263e-08, -5.4007938898647565e-09, \
+  9.256899680411872e-10, -1.5869503264192334e-10, 2.7209976034987024e-11, -4.665992426162454e-12, \
+  8.002016298795233e-13, -1.3724164584124254e-13, 2.353949688583712e-14, -4.037647655524712e-15, \
+  6.925895800834045e-16, -1.1880559867658363e-16}
+#define FX_CHEB_K0B { \
+  1.2201515410329777, -0.0314481013119645, 0.0015698838857300533, -0.00012849549581627802, \
+  1.39498137188765e-05, -1.8317555227191195e-06, 2.766813639445015e-07, -4.660489897687948e-08, \
+  8.574034017414225e-09, -1.6975345093890614e-09, 3.5773972814003283e-10, -7.957489244477396e-11, \
+  1.8559491149549264e-11, -4.514597883374519e-12, 1.1403405882073441e-12, -2.9800969231481784e-13, \
+  8.032890775068375e-14, -2.2275133267462965e-14, 6.340076476276646e-15, -1.848593377920907e-15, \
+  5.5120559994043335e-16, -1.6782311257549006e-16, 5.2103917776435543e-17, -1.6475805939842632e-17, \
+  5.3004337711773354e-18}
+#define FX_CHEB_K1B { \
+  1.3603130952422213, 0.10392373657681724, -0.002857816859622779, 0.00019521551847135162, \
+  -1.936197974166083e-05, 2.406484947837217e-06, -3.5019606030878126e-07, 5.7410841254500495e-08, \
+  -1.0345762465678097e-08, 2.0150497551970347e-09, -4.1903547593419254e-10, 9.218315187605315e-11, \
+  -2.129967838427791e-11, 5.139639673482343e-12, -1.2891739609498229e-12, 3.348419666052243e-13, \
+  -8.976705182010146e-14, 2.4771544242195988e-14, -7.0198370892147685e-15, 2.038703166239861e-15, \
+  -6.057047270643018e-16, 1.8380935752430455e-16, -5.689462849193648e-17, 1.7940510478863572e-17, \
+  -5.7567444820733025e-18}
+#define FX_CHEB_NA 22
+#define FX_CHEB_NB 25
 
 #define FX_EULER_GAMMA 0.5772156649015329
 
 #ifdef __CUDACC__
-__constant__ double FX_S2_DEV[34] = FX_BESSEL_S2;
-__constant__ double FX_W_DEV[34] = FX_BESSEL_W;
+__constant__ double FX_K0A_DEV[FX_CHEB_NA] = FX_CHEB_K0A;
+__constant__ double FX_K1A_DEV[FX_CHEB_NA] = FX_CHEB_K1A;
+__constant__ double FX_K0B_DEV[FX_CHEB_NB] = FX_CHEB_K0B;
+__constant__ double FX_K1B_DEV[FX_CHEB_NB] = FX_CHEB_K1B;
 #endif
-static const double FX_S2_HOST[34] = FX_BESSEL_S2;
-static const double FX_W_HOST[34] = FX_BESSEL_W;
+static const double FX_K0A_HOST[FX_CHEB_NA] = FX_CHEB_K0A;
+static const double FX_K1A_HOST[FX_CHEB_NA] = FX_CHEB_K1A;
+static const double FX_K0B_HOST[FX_CHEB_NB] = FX_CHEB_K0B;
+static const double FX_K1B_HOST[FX_CHEB_NB] = FX_CHEB_K1B;
+
+/* Clenshaw's recurrence for sum_k c_k T_k(u), two series at once:
+ * b_k = (2u b_{k+1} - b_{k+2}) + c_k, sum = (u b_1 - b_2) + c_0. */
+template <int N>
+FX_HD void fx_clenshaw2(const double* c0, const double* c1, double u, double* s0, double* s1) {
+  const double tu = 2.0 * u;
+  double p1 = 0.0, p2 = 0.0, q1 = 0.0, q2 = 0.0;
+#ifdef __CUDA_ARCH__
+#pragma unroll
+#endif
+  for (int k = N - 1; k >= 1; --k) {
+    double p = ((tu * p1) - p2) + c0[k];
+    double q = ((tu * q1) - q2) + c1[k];
+    p2 = p1; p1 = p; q2 = q1; q1 = q;
+  }
+  *s0 = ((u * p1) - p2) + c0[0];
+  *s1 = ((u * q1) - q2) + c1[0];
+}
 
 /* e^x K0(x), e^x K1(x) for 0 < x < 1e4 */
 FX_HD void fx_k01x(double x, double* k0x, double* k1x) {
@@ -256,27 +299,23 @@ FX_HD void fx_k01x(double x, double* k0x, double* k1x) {
     *k1x = k1 * ex;
     return;
   }
+  if (x < 2.0) {
 #ifdef __CUDA_ARCH__
-  const double* S2 = FX_S2_DEV;
-  const double* W = FX_W_DEV;
+    fx_clenshaw2<FX_CHEB_NA>(FX_K0A_DEV, FX_K1A_DEV, (2.0 * x) - 3.0, k0x, k1x);
 #else
-  const double* S2 = FX_S2_HOST;
-  const double* W = FX_W_HOST;
+    fx_clenshaw2<FX_CHEB_NA>(FX_K0A_HOST, FX_K1A_HOST, (2.0 * x) - 3.0, k0x, k1x);
 #endif
-  double inv2x = 1.0 / (2.0 * x);
-  double a0 = 0.0, a1 = 0.0;
-#ifdef __CUDA_ARCH__
-#pragma unroll 2
-#endif
-  for (int k = 33; k >= 0; --k) {
-    double s2 = S2[k];
-    double q = sqrt_(1.0 + s2 * inv2x);
-    a0 = a0 + W[k] / q;
-    a1 = a1 + (W[k] * s2) * q;
+    return;
   }
-  double pre = sqrt_(FX_PI / (2.0 * x));
-  *k0x = pre * a0;
-  *k1x = pre * (2.0 * a1);
+  double g0, g1;
+#ifdef __CUDA_ARCH__
+  fx_clenshaw2<FX_CHEB_NB>(FX_K0B_DEV, FX_K1B_DEV, (4.0 / x) - 1.0, &g0, &g1);
+#else
+  fx_clenshaw2<FX_CHEB_NB>(FX_K0B_HOST, FX_K1B_HOST, (4.0 / x) - 1.0, &g0, &g1);
+#endif
+  double rs = 1.0 / sqrt_(x);
+  *k0x = g0 * rs;
+  *k1x = g1 * rs;
 }
 
 /* the reference's asymptotic series (safe_besselkx, src/eos.jl:30-33) */

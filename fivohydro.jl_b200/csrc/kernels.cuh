@@ -22,6 +22,7 @@
 #define FIVO_KERNELS_CUH
 
 #include "physics.cuh"
+#include "coop.cuh"
 
 namespace fv {
 
@@ -47,6 +48,9 @@ struct DevFlags {
   double sumD, maxu, minPtot;     /* end-of-run diagnostics                             */
   int status;                     /* nonzero: a device loop hit its cap                 */
   int pad;
+  unsigned int qcount_p, qnext_p; /* deferred recoveries of the current pass           */
+  unsigned int qcount_a, qnext_a; /* deferred admissibility inversions of the stage     */
+  unsigned long long tot_p, tot_a;/* deferred cells summed over passes (kernel timing)   */
 };
 
 __device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) {
@@ -820,10 +824,14 @@ __global__ void __launch_bounds__(128) k_relax(DevParams d, DevState Uq, DevStat
  * 8 = end-of-run diagnostics */
 __global__ void k_reset_flags(DevFlags* fl, int what, unsigned long long amax_bits) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  if (what & 1) { fl->nprimfail = 0; fl->nvacuum = 0; fl->rep = 0x7fffffffffffffffULL; fl->nbad = 0; }
+  if (what & 1) {
+    fl->nprimfail = 0; fl->nvacuum = 0; fl->rep = 0x7fffffffffffffffULL; fl->nbad = 0;
+    fl->qcount_p = 0; fl->qnext_p = 0; fl->qcount_a = 0; fl->qnext_a = 0;
+  }
   if (what & 2) fl->amax_bits = amax_bits;
   if (what & 4) { fl->shear_max_bits = 0; fl->shear_sum = 0.0; }
   if (what & 8) { fl->sumD = 0.0; fl->maxu = 0.0; fl->minPtot = inf_(); }
+  if (what & 16) { fl->tot_p = 0; fl->tot_a = 0; }
   fl->status = 0;
 }
 
@@ -944,6 +952,279 @@ __global__ void k_cons_to_prim(DevParams d, long long n, double tau, const doubl
   o[0] = r.T; o[1] = r.mu; o[2] = r.ux; o[3] = r.uy; o[4] = r.n; o[5] = r.e; o[6] = r.P;
   ok[i] = r.ok;
   if (reason) reason[i] = r.reason;
+}
+
+/* ======================================================================
+ * Two-phase recovery and the split stage (the context path).
+ *
+ * A warp runs as long as its slowest lane. Almost every cell converges from
+ * its warm start in a few Newton iterations, but a few cells per pass need the
+ * fresh seed (3 x 60 bisection steps) and a long Newton, and they set the time
+ * of their whole warp. So the recovery runs in two kernels:
+ *   k_prim_fast  every cell; vacuum cells and warm starts that converge within
+ *                FAST_BUDGET iterations finish here; every other cell is
+ *                appended to a queue.
+ *   k_prim_slow  one warp per queued cell runs the whole cons_to_prim_2d!
+ *                from the start (recover_warp, coop.cuh).
+ * A cell's result does not depend on which kernel computed it: the fast kernel
+ * accepts only a first attempt whose Newton loop converged, which is exactly
+ * what the full algorithm returns for it, and the slow kernel recomputes
+ * everything else from scratch.
+ * The stage is split the same way: k_faces (one thread per face, no block
+ * barrier) writes the HLLE fluxes to planes, k_update combines and sanitises
+ * each cell and queues the rare cells whose admissibility needs an inversion,
+ * which k_adm_slow settles.
+ * ====================================================================== */
+
+#define FAST_BUDGET 6
+
+/* _primitive_pass! body after the recovery (src2d/rhs2d.jl:89-155) */
+template <int EOS>
+__device__ __forceinline__ void store_recovery(const DevParams& d, const DevPrims& w, const DevHist& h,
+                                               long long i, const Recovery& r) {
+  double T = r.T, mu = r.mu, ux = r.ux, uy = r.uy, n = r.n, en = r.e, P = r.P;
+  if (!r.ok) {
+    T = FV_T_MIN; mu = 0.0; ux = 0.0; uy = 0.0;
+    eos_Pne<EOS>(T, mu, d, &P, &n, &en);
+    en = jmax(en, 0.0); n = 0.0;
+  }
+  double Tm = jmax(T, FV_T_MIN);
+  double yT = fx_log(Tm);
+  double phi = jclamp((mu - d.p.m_hq) / Tm, -FV_PHI_CAP, FV_PHI_CAP);
+  w.yT[i] = yT; w.phi[i] = phi; w.mu[i] = mu; w.alpha[i] = mu / Tm;
+  w.ux[i] = ux; w.uy[i] = uy; w.P[i] = P; w.n[i] = n; w.e[i] = en; w.ok[i] = r.ok;
+  if (r.ok) { h.x0_yT[i] = yT; h.x0_phi[i] = phi; h.x0_ux[i] = ux; h.x0_uy[i] = uy; }
+  else { double q = nan_(); h.x0_yT[i] = q; h.x0_phi[i] = q; h.x0_ux[i] = q; h.x0_uy[i] = q; }
+}
+
+__device__ __forceinline__ void load_cons(const DevParams& d, const DevState& U, long long i, double tau,
+                                          CellCons& c) {
+  c.D = safe_div(U.f[d.iDtau][i], tau);
+  c.Sx = U.f[d.iSx][i]; c.Sy = U.f[d.iSy][i]; c.E = U.f[d.iE][i];
+  double dis[7];
+  load_dis(d, U, i, dis);
+  c.nux = dis[0]; c.nuy = dis[1]; c.Pi = dis[2]; c.pixx = dis[3]; c.pixy = dis[4]; c.piyy = dis[5];
+  c.pieta = dis[6];
+}
+
+template <int EOS, bool NCH>
+__global__ void __launch_bounds__(128) k_prim_fast(DevParams d, DevState U, DevPrims w, DevHist h, double tau,
+                                                   DevFlags* fl, unsigned int* queue) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  bool vac = false, defer = false;
+  if (i < d.Ntot) {
+    CellCons c;
+    load_cons(d, U, i, tau, c);
+    const double yT0 = h.x0_yT[i], ux0 = h.x0_ux[i], uy0 = h.x0_uy[i];
+    const bool vacuum = !isfinite_(c.E) || c.E <= FV_E_VAC || !isfinite_(c.D) || c.D < FV_D_VAC;
+    if (vacuum) {
+      Recovery r = recover_attempt<EOS, NCH>(c, d, yT0, h.x0_phi[i], ux0, uy0, d.p.primrec_maxit, d.p.primrec_tol);
+      store_recovery<EOS>(d, w, h, i, r);
+      vac = true;
+    } else if (!(isfinite_(yT0) && isfinite_(ux0) && isfinite_(uy0))) {
+      defer = true;
+    } else {
+      bool over = false;
+      Recovery r = recover_attempt<EOS, NCH>(c, d, yT0, h.x0_phi[i], ux0, uy0, d.p.primrec_maxit,
+                                             d.p.primrec_tol, FAST_BUDGET, &over);
+      if (over || !r.ok) defer = true;
+      else store_recovery<EOS>(d, w, h, i, r);
+    }
+  }
+  /* warp-aggregated counters and queue appends (the grid holds whole warps) */
+  const unsigned lane = threadIdx.x & 31;
+  unsigned mv = __ballot_sync(0xffffffffu, vac);
+  if (lane == 0 && mv) atomicAdd((unsigned long long*)&fl->nvacuum, (unsigned long long)__popc(mv));
+  unsigned md = __ballot_sync(0xffffffffu, defer);
+  if (md) {
+    unsigned base = 0;
+    if (lane == 0) base = atomicAdd(&fl->qcount_p, (unsigned)__popc(md));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (defer) queue[base + __popc(md & ((1u << lane) - 1u))] = (unsigned)i;
+  }
+}
+
+/* The deferred cells, one warp per cell (recover_warp), taken from the queue
+ * one at a time so that long and short recoveries balance over the warps. */
+template <int EOS, bool NCH>
+__global__ void __launch_bounds__(128) k_prim_slow(DevParams d, DevState U, DevPrims w, DevHist h, double tau,
+                                                   DevFlags* fl, const unsigned int* queue) {
+  const unsigned n = *(volatile unsigned int*)&fl->qcount_p;
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&fl->tot_p, (unsigned long long)n);
+  const int lane = threadIdx.x & 31;
+  while (true) {
+    unsigned q = 0;
+    if (lane == 0) q = atomicAdd(&fl->qnext_p, 1u);
+    q = __shfl_sync(FV_FULL, q, 0);
+    if (q >= n) break;
+    const long long i = queue[q];
+    CellCons c;
+    load_cons(d, U, i, tau, c);
+    Recovery r = recover_warp<EOS, NCH>(c, d, h.x0_yT[i], h.x0_phi[i], h.x0_ux[i], h.x0_uy[i],
+                                        d.p.primrec_maxit, d.p.primrec_tol, lane);
+    if (lane == 0) {
+      if (!r.ok) {
+        if (r.reason == PRR_VACUUM) atomicAdd((unsigned long long*)&fl->nvacuum, 1ULL);
+        else {
+          atomicAdd((unsigned long long*)&fl->nprimfail, 1ULL);
+          atomicMin(&fl->rep, ((unsigned long long)i << 8) | r.reason);
+        }
+      }
+      store_recovery<EOS>(d, w, h, i, r);
+    }
+  }
+}
+
+/* one thread per face of one direction, every face of the (ghost-inclusive) grid */
+template <int EOS, bool XDIR>
+__global__ void __launch_bounds__(128) k_faces(DevParams d, DevState Ub, DevPrims w, double tau,
+                                               const uint8_t* ffo, double* Fh, DevFlags* fl) {
+  const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nf = XDIR ? (long long)(d.Nxtot - 1) * d.Nytot : (long long)d.Nxtot * (d.Nytot - 1);
+  double amax = 0.0;
+  if (f < nf) {
+    long long i;
+    int k, kmax;
+    if (XDIR) { i = f; k = (int)(f / d.Nytot); kmax = d.Nxtot; }
+    else {
+      int ix = (int)(f / (d.Nytot - 1)), iy = (int)(f % (d.Nytot - 1));
+      i = (long long)ix * d.Nytot + iy; k = iy; kmax = d.Nytot;
+    }
+    double out[FV_MAXV];
+    double a = face_flux<EOS, XDIR>(d, Ub, w, i, XDIR ? d.Nytot : 1, k, kmax, tau, ffo, out);
+    if (a > amax) amax = a;
+    for (int q = 0; q < d.nv; ++q) Fh[(size_t)q * d.Ntot + i] = out[q];
+  }
+  for (int o = 16; o > 0; o >>= 1) amax = jmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+  __shared__ double red[4];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = amax;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = jmax(jmax(red[0], red[1]), jmax(red[2], red[3]));
+    atomic_max_pos(&fl->amax_bits, m);
+  }
+}
+
+/* cell_admissible_2d up to (not including) the inversion: 0 inadmissible,
+ * 1 admissible, 2 settle by inverting (src2d/floors2d.jl:281-337) */
+__device__ __forceinline__ int adm_prefilter(const DevParams& d, const double u[FV_MAXV], bool okw, double ux,
+                                             double uy, double Pw) {
+  const double Emin = FV_E_FLOOR;
+  double E = u[d.iE], Sx = u[d.iSx], Sy = u[d.iSy], Dt = u[d.iDtau];
+  if (!(isfinite_(E) && isfinite_(Sx) && isfinite_(Sy) && isfinite_(Dt))) return 0;
+  if (!(E >= Emin)) return 0;
+  if (!(Dt >= 0.0)) return 0;
+  for (int a = 4; a < d.nv; ++a) if (!isfinite_(u[a])) return 0;
+  if (E <= 1e6 * Emin) return 1;
+  if (okw) {
+    double ut = utau(ux, uy);
+    double iu = safe_inv(ut);
+    double vx = ux * iu, vy = uy * iu;
+    if (!(isfinite_(vx) && isfinite_(vy))) return 0;
+    double lim = (1.0 - 1e-12) * (1.0 - 1e-12);
+    if (!((vx * vx) + (vy * vy) < lim)) return 0;
+  }
+  double Peff = peff_of(d, u, Pw);
+  if (fx_hypot(Sx, Sy) <= ((FV_SR_MARGIN * FV_CHI_SRE) * (E + Peff))) return 1;
+  return 2;
+}
+
+/* per interior cell: flux divergence + source (rhs_2d! assembly), the stage
+ * combination, sanitize_stage_2d!'s floors and bounds, and the admissibility
+ * test up to the inversion */
+template <int EOS, bool NCH>
+__global__ void __launch_bounds__(128) k_update(DevParams d, StageArgs s, const double* Fhx, const double* Fhy,
+                                                unsigned int* aqueue) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int verdict = 1;
+  long long i = 0;
+  if (t < (long long)d.Nx * d.Ny) {
+    const int ix = d.ng + (int)(t / d.Ny), iy = d.ng + (int)(t % d.Ny);
+    i = (long long)ix * d.Nytot + iy;
+    const int nv = d.nv;
+    const size_t N = (size_t)d.Ntot;
+    const double invdx = 1.0 / d.dx, invdy = 1.0 / d.dy;
+    double ub[FV_MAXV];
+    for (int a = 0; a < nv; ++a) ub[a] = s.Ub.f[a][i];
+    const double Pw = s.w.P[i];
+    /* source_cell_2d!, src2d/fluxes2d.jl:166-177 (+ the advected-scalar divv terms) */
+    double Sr[FV_MAXV];
+    for (int a = 0; a < nv; ++a) Sr[a] = 0.0;
+    {
+      double itau = safe_inv(s.tau);
+      double Pi = d.hasPi ? ub[d.iPi] : 0.0, pieta = d.hasShear ? ub[d.iPieta] : 0.0;
+      Sr[d.iSx] = (-ub[d.iSx]) * itau;
+      Sr[d.iSy] = (-ub[d.iSy]) * itau;
+      Sr[d.iE] = (-((ub[d.iE] + (Pw + Pi)) + pieta)) * itau;
+      bool an = d.hasNu && d.p.advect_nu, aP = d.hasPi && d.p.advect_Pi, ap = d.hasShear && d.p.advect_pi;
+      if (an || aP || ap) {
+        /* compute_divv_2d!, src2d/rhs2d.jl:29-41 */
+        const long long ixm = i - d.Nytot, ixp = i + d.Nytot;
+        double vxp = s.w.ux[ixp] * safe_inv(utau(s.w.ux[ixp], s.w.uy[ixp]));
+        double vxm = s.w.ux[ixm] * safe_inv(utau(s.w.ux[ixm], s.w.uy[ixm]));
+        double vyp = s.w.uy[i + 1] * safe_inv(utau(s.w.ux[i + 1], s.w.uy[i + 1]));
+        double vym = s.w.uy[i - 1] * safe_inv(utau(s.w.ux[i - 1], s.w.uy[i - 1]));
+        double divv = ((0.5 * (vxp - vxm)) * invdx) + ((0.5 * (vyp - vym)) * invdy);
+        if (an) { Sr[d.iNux] += ub[d.iNux] * divv; Sr[d.iNuy] += ub[d.iNuy] * divv; }
+        if (aP) Sr[d.iPi] += ub[d.iPi] * divv;
+        if (ap) {
+          Sr[d.iPixx] += ub[d.iPixx] * divv; Sr[d.iPixy] += ub[d.iPixy] * divv;
+          Sr[d.iPiyy] += ub[d.iPiyy] * divv; Sr[d.iPieta] += ub[d.iPieta] * divv;
+        }
+      }
+    }
+    double u[FV_MAXV];
+    for (int a = 0; a < nv; ++a) {
+      const double* fx = Fhx + (size_t)a * N;
+      const double* fy = Fhy + (size_t)a * N;
+      double k = (((-(fx[i] - fx[i - d.Nytot])) * invdx) - ((fy[i] - fy[i - 1]) * invdy)) + Sr[a];
+      if (s.dU) s.dU[(size_t)a * N + i] = k;
+      if (s.mode == COMB_EULER) u[a] = ub[a] + (s.dt * k);
+      else if (s.mode == COMB_BLEND) u[a] = (s.wold * s.Uold.f[a][i]) + (s.wnew * (ub[a] + (s.dt * k)));
+      else if (s.mode == COMB_THIRD) u[a] = (s.Uold.f[a][i] + (2.0 * (ub[a] + (s.dt * k)))) / 3.0;
+    }
+    if (s.mode != COMB_RHS_ONLY) {
+      sanitize_cell(d, u, ix, iy, s.tau_state, Pw, true, FV_E_FLOOR);
+      verdict = adm_prefilter(d, u, s.w.ok[i] != 0, s.w.ux[i], s.w.uy[i], Pw);
+      s.bad[i] = verdict == 0 ? 1 : 0;
+      for (int a = 0; a < nv; ++a) s.Uout.f[a][i] = u[a];
+    }
+  }
+  const unsigned lane = threadIdx.x & 31;
+  unsigned mb = __ballot_sync(0xffffffffu, verdict == 0);
+  if (lane == 0 && mb) atomicAdd((unsigned long long*)&s.fl->nbad, (unsigned long long)__popc(mb));
+  unsigned mq = __ballot_sync(0xffffffffu, verdict == 2);
+  if (mq) {
+    unsigned base = 0;
+    if (lane == 0) base = atomicAdd(&s.fl->qcount_a, (unsigned)__popc(mq));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (verdict == 2) aqueue[base + __popc(mq & ((1u << lane) - 1u))] = (unsigned)i;
+  }
+}
+
+/* the inversion of cell_admissible_2d for the queued cells (src2d/floors2d.jl:329-335),
+ * one warp per cell */
+template <int EOS, bool NCH>
+__global__ void __launch_bounds__(128) k_adm_slow(DevParams d, DevState Uout, double tau_state, uint8_t* bad,
+                                                  DevFlags* fl, const unsigned int* aqueue) {
+  const unsigned n = *(volatile unsigned int*)&fl->qcount_a;
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&fl->tot_a, (unsigned long long)n);
+  const int lane = threadIdx.x & 31;
+  while (true) {
+    unsigned q = 0;
+    if (lane == 0) q = atomicAdd(&fl->qnext_a, 1u);
+    q = __shfl_sync(FV_FULL, q, 0);
+    if (q >= n) break;
+    const long long i = aqueue[q];
+    CellCons c;
+    load_cons(d, Uout, i, tau_state, c);
+    Recovery r = recover_warp<EOS, NCH>(c, d, nan_(), nan_(), nan_(), nan_(), 80, 1e-12, lane);
+    if (lane == 0) {
+      bool adm = r.ok || r.reason == PRR_VACUUM;
+      bad[i] = adm ? 0 : 1;
+      if (!adm) atomicAdd((unsigned long long*)&fl->nbad, 1ULL);
+    }
+  }
 }
 
 }  // namespace fv

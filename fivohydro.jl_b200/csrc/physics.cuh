@@ -440,7 +440,8 @@ FX_HD void solve_phi_bisect(double D, double T, double ux, double uy, double nux
 /* _cons_to_prim_attempt_2d!, src2d/primrec2d.jl:511-742 */
 template <int EOS, bool NCH>
 FX_HD Recovery recover_attempt(const CellCons& c, const DevParams& d, double yT0, double phi0,
-                               double ux0, double uy0, int maxit, double tol) {
+                               double ux0, double uy0, int maxit, double tol,
+                               int budget = 0x7fffffff, bool* over_budget = nullptr) {
   Recovery out;
   const double yT_lo = d.log_T_min, yT_hi = d.log_T_solve_max;
   const double m = d.p.m_hq;
@@ -491,6 +492,8 @@ FX_HD Recovery recover_attempt(const CellCons& c, const DevParams& d, double yT0
     for (int r = r_lo; r < 4; ++r) nrm = jmax(nrm, fabs_(F[r] * rs[r]));
     last_nrm = nrm;
     if (nrm < tol) { converged = true; out.reason = PRR_CONVERGED; break; }
+    /* iteration budget of the fast pass: leave the cell to the full pass */
+    if (it > budget) { *over_budget = true; return out; }
     bool ok_jac = true;
 #pragma unroll
     for (int k = 0; k < NU; ++k) {

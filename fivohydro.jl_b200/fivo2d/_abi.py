@@ -82,11 +82,15 @@ class FivoRunResult(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("pad")}
 
 
+FIVO_KCLASS_N = 8
+KERNEL_CLASSES = ("prim_fast", "prim_slow", "faces", "update", "adm_slow", "relax", "other", "unused")
+(FIVO_KCLASS_PRIM_FAST, FIVO_KCLASS_PRIM_SLOW, FIVO_KCLASS_FACES, FIVO_KCLASS_UPDATE, FIVO_KCLASS_ADM_SLOW,
+ FIVO_KCLASS_RELAX, FIVO_KCLASS_OTHER) = range(7)
+
+
 class FivoKernelTimes(C.Structure):
-    _fields_ = [("launches", C.c_int64 * 4), ("ms", C.c_double * 4), ("total_launches", C.c_int64)]
-
-
-KERNEL_CLASSES = ("primitive", "stage", "relax", "other")
+    _fields_ = [("launches", C.c_int64 * FIVO_KCLASS_N), ("ms", C.c_double * FIVO_KCLASS_N),
+                ("units", C.c_int64 * FIVO_KCLASS_N), ("total_launches", C.c_int64)]
 
 PKG_DIR = pathlib.Path(__file__).resolve().parent
 LIB_PATH = PKG_DIR.parent / "csrc" / "libfivo2d.so"

@@ -177,12 +177,28 @@ typedef struct fivo_run_result {
   double  minPtot;
 } fivo_run_result;
 
-/* CUDA-event timing of the library's kernels (fivo_profile). Kernel classes:
- * 0 = primitive recovery, 1 = stage (faces + combination + sanitiser),
- * 2 = relaxation + shear projection, 3 = everything else (BCs, copies, masks). */
+/* CUDA-event timing of the library's kernels (fivo_profile), by kernel class:
+ *   PRIM_FAST  recovery of every cell from its warm start, small iteration budget
+ *   PRIM_SLOW  full cons_to_prim_2d! of the cells the fast pass deferred
+ *   FACES      MUSCL + prim->cons + HLLE, x then y faces
+ *   UPDATE     flux divergence + source, stage combination, floors, bounds
+ *   ADM_SLOW   the inversions of cell_admissible_2d the update deferred
+ *   RELAX      relaxation + shear projection
+ *   OTHER      boundary frames, copies, masks, flag resets
+ * launches[k] counts launch brackets of class k (FACES launches two kernels per
+ * bracket); units[k] the cells (faces, for FACES) those launches processed. */
+#define FIVO_KCLASS_PRIM_FAST 0
+#define FIVO_KCLASS_PRIM_SLOW 1
+#define FIVO_KCLASS_FACES     2
+#define FIVO_KCLASS_UPDATE    3
+#define FIVO_KCLASS_ADM_SLOW  4
+#define FIVO_KCLASS_RELAX     5
+#define FIVO_KCLASS_OTHER     6
+#define FIVO_KCLASS_N         8
 typedef struct fivo_kernel_times {
-  int64_t launches[4];
-  double  ms[4];
+  int64_t launches[FIVO_KCLASS_N];
+  double  ms[FIVO_KCLASS_N];
+  int64_t units[FIVO_KCLASS_N];
   int64_t total_launches;   /* every kernel this context launched while enabled */
 } fivo_kernel_times;
 

@@ -22,13 +22,14 @@
  *   o_besselkx  e^x K_nu(x), nu = 0, 1 (then upward recurrence):
  *           x < 1   power series of A&S 9.6.10-9.6.13 (K0, K1 via I0, I1 and
  *                   the digamma sums), times e^x;
- *           x >= 1  trapezoidal rule (34 nodes, step 1/5) on the Laplace-type
- *                   representation DLMF 10.32.8 after t = s^2:
- *                   e^x K_nu(x) = sqrt(pi/2x)/Gamma(nu+1/2) *
- *                                 int_R e^{-s^2} |s|^{2nu} (1+s^2/2x)^{nu-1/2} ds;
+ *           1 <= x < 2  Chebyshev series of e^x K_nu in u = 2x - 3;
+ *           2 <= x < 1e4  Chebyshev series of sqrt(x) e^x K_nu in u = 4/x - 1;
+ *                   both summed by Clenshaw's recurrence, coefficients from
+ *                   50-digit mpmath values (the library's gen_bessel_cheb.py
+ *                   writes the same tables);
  *           x >= 1e4  the reference's three-term asymptotic series
  *                   (safe_besselkx, src/eos.jl:27-34), verbatim in arithmetic.
- *           Checked against mpmath to <= 6e-16 relative (tests/test_oracle_math.py).
+ *           Checked against mpmath to <= 4e-16 relative (tests/test_oracle_math.py).
  *
  * The CUDA library implements the same algorithms with the same operation
  * order, and both are compiled without floating-point contraction, so the
@@ -172,21 +173,49 @@ static inline double o_hypot(double x, double y) {
 
 /* ---------------- scaled modified Bessel K ---------------- */
 
-static const double O_BESSEL_S2[34] = {
-  0.0, 0.04, 0.16, 0.36, 0.64, 1.0, 1.44, 1.96, 2.56, 3.24, 4.0, 4.84, 5.76, 6.76,
-  7.84, 9.0, 10.24, 11.56, 12.96, 14.44, 16.0, 17.64, 19.36, 21.16, 23.04, 25.0,
-  27.04, 29.16, 31.36, 33.64, 36.0, 38.44, 40.96, 43.56};
-static const double O_BESSEL_W[34] = {
-  0.11283791670955126, 0.21682695742097263, 0.19230825976786156, 0.15744868634285744,
-  0.11899715725149379, 0.08302149948411894, 0.05346886940070783, 0.03178834153545557,
-  0.017445811726789072, 0.008838344666402213, 0.004133397070818411, 0.001784431012983241,
-  0.0007111297361755495, 0.00026161000994465633, 8.884158884113332e-05, 2.785061038934957e-05,
-  8.059527106647123e-06, 2.1529842073361357e-06, 5.309193689433173e-07, 1.2085725786444936e-07,
-  2.5396469343733115e-08, 4.926408197336689e-09, 8.821529389366844e-10, 1.4581890004763904e-10,
-  2.225052137962172e-11, 3.134173306203467e-12, 4.075325146752109e-13, 4.89167914078347e-14,
-  5.420134984939562e-15, 5.543942072256747e-16, 5.2346024784985296e-17, 4.5625240909092945e-18,
-  3.670988941398298e-19, 2.726574842629012e-20};
+/* Chebyshev coefficients of e^x K_nu (piece A, u = 2x - 3, 1 <= x < 2) and of
+ * sqrt(x) e^x K_nu (piece B, u = 4/x - 1, 2 <= x < 1e4), from 50-digit values */
+static const double O_CHEB_K0A[] = {
+  0.975293670703631, -0.14911366079770616, 0.01739593810625341, -0.0022865321321120587,
+  0.00031902053048988584, -4.617742767921652e-05, 6.855099419473594e-06, -1.0367102847936046e-06,
+  1.590358485499584e-07, -2.4674715067053715e-08, 3.863812252910323e-09, -6.096897833322557e-10,
+  9.683069016813046e-11, -1.5464054179684872e-11, 2.481515505543579e-12, -3.9988227436440834e-13,
+  6.467756230057925e-14, -1.0495481280269401e-14, 1.7081563652123322e-15, -2.7874138983949704e-16,
+  4.5594687260393236e-17, -7.47431382282828e-18};
+static const double O_CHEB_K1A[] = {
+  1.287716931284971, -0.29355526501238677, 0.04578781607810882, -0.0075606314967654195,
+  0.0012725129170005956, -0.0002159483044944044, 3.679893234585295e-05, -6.2852010326152186e-06,
+  1.0749808007083846e-06, -1.8401830928999913e-07, 3.151902199740263e-08, -5.4007938898647565e-09,
+  9.256899680411872e-10, -1.5869503264192334e-10, 2.7209976034987024e-11, -4.665992426162454e-12,
+  8.002016298795233e-13, -1.3724164584124254e-13, 2.353949688583712e-14, -4.037647655524712e-15,
+  6.925895800834045e-16, -1.1880559867658363e-16};
+static const double O_CHEB_K0B[] = {
+  1.2201515410329777, -0.0314481013119645, 0.0015698838857300533, -0.00012849549581627802,
+  1.39498137188765e-05, -1.8317555227191195e-06, 2.766813639445015e-07, -4.660489897687948e-08,
+  8.574034017414225e-09, -1.6975345093890614e-09, 3.5773972814003283e-10, -7.957489244477396e-11,
+  1.8559491149549264e-11, -4.514597883374519e-12, 1.1403405882073441e-12, -2.9800969231481784e-13,
+  8.032890775068375e-14, -2.2275133267462965e-14, 6.340076476276646e-15, -1.848593377920907e-15,
+  5.5120559994043335e-16, -1.6782311257549006e-16, 5.2103917776435543e-17, -1.6475805939842632e-17,
+  5.3004337711773354e-18};
+static const double O_CHEB_K1B[] = {
+  1.3603130952422213, 0.10392373657681724, -0.002857816859622779, 0.00019521551847135162,
+  -1.936197974166083e-05, 2.406484947837217e-06, -3.5019606030878126e-07, 5.7410841254500495e-08,
+  -1.0345762465678097e-08, 2.0150497551970347e-09, -4.1903547593419254e-10, 9.218315187605315e-11,
+  -2.129967838427791e-11, 5.139639673482343e-12, -1.2891739609498229e-12, 3.348419666052243e-13,
+  -8.976705182010146e-14, 2.4771544242195988e-14, -7.0198370892147685e-15, 2.038703166239861e-15,
+  -6.057047270643018e-16, 1.8380935752430455e-16, -5.689462849193648e-17, 1.7940510478863572e-17,
+  -5.7567444820733025e-18};
 static const double O_EULER_GAMMA = 0.5772156649015329;
+
+/* Clenshaw: b_k = (2u b_{k+1} - b_{k+2}) + c_k for k = n-1..1; sum = (u b_1 - b_2) + c_0 */
+static inline double o_clenshaw(const double* c, int n, double u) {
+  double tu = 2.0 * u, b1 = 0.0, b2 = 0.0;
+  for (int k = n - 1; k >= 1; --k) {
+    double b = ((tu * b1) - b2) + c[k];
+    b2 = b1; b1 = b;
+  }
+  return ((u * b1) - b2) + c[0];
+}
 
 /* e^x K0(x), e^x K1(x) for 0 < x < 1e4 */
 static inline void o_k01x(double x, double* k0x, double* k1x) {
@@ -214,17 +243,18 @@ static inline void o_k01x(double x, double* k0x, double* k1x) {
     *k1x = k1 * ex;
     return;
   }
-  double inv2x = 1.0 / (2.0 * x);
-  double a0 = 0.0, a1 = 0.0;
-  for (int k = 33; k >= 0; --k) {
-    double s2 = O_BESSEL_S2[k];
-    double q = std::sqrt(1.0 + s2 * inv2x);
-    a0 = a0 + O_BESSEL_W[k] / q;
-    a1 = a1 + (O_BESSEL_W[k] * s2) * q;
+  const int na = (int)(sizeof(O_CHEB_K0A) / sizeof(double));
+  const int nb = (int)(sizeof(O_CHEB_K0B) / sizeof(double));
+  if (x < 2.0) {
+    double u = (2.0 * x) - 3.0;
+    *k0x = o_clenshaw(O_CHEB_K0A, na, u);
+    *k1x = o_clenshaw(O_CHEB_K1A, na, u);
+    return;
   }
-  double pre = std::sqrt(O_PI / (2.0 * x));
-  *k0x = pre * a0;
-  *k1x = pre * (2.0 * a1);
+  double u = (4.0 / x) - 1.0;
+  double rs = 1.0 / std::sqrt(x);
+  *k0x = o_clenshaw(O_CHEB_K0B, nb, u) * rs;
+  *k1x = o_clenshaw(O_CHEB_K1B, nb, u) * rs;
 }
 
 /* safe_besselkx(nu, x), src/eos.jl:27-34: 0 for x <= 0 or non-finite, the

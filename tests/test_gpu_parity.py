@@ -246,10 +246,18 @@ def test_advance_chunks_equal_one_run(gpu_lib):
         tau_w, tau_o = rw["tau"], ro["tau"]
     kt = A.FivoKernelTimes()
     lib.fivo_profile_read(w.h, C.byref(kt), 1)
-    # every stage is one recovery + one stage kernel; every step adds one refresh + one relaxation
-    assert kt.launches[2] == 6 and kt.launches[1] >= 6 * 3
-    assert kt.launches[0] == kt.launches[1] + kt.launches[2]
-    assert all(kt.ms[k] > 0 for k in range(3)) and kt.total_launches > sum(kt.launches[:3])
+    # every stage is one recovery pass (fast + slow) + faces + update + deferred
+    # admissibility; every step adds one refresh pass + one relaxation
+    L = kt.launches
+    assert L[A.FIVO_KCLASS_RELAX] == 6 and L[A.FIVO_KCLASS_UPDATE] >= 6 * 3
+    assert L[A.FIVO_KCLASS_PRIM_FAST] == L[A.FIVO_KCLASS_UPDATE] + L[A.FIVO_KCLASS_RELAX]
+    assert L[A.FIVO_KCLASS_PRIM_SLOW] == L[A.FIVO_KCLASS_PRIM_FAST]
+    assert L[A.FIVO_KCLASS_FACES] == L[A.FIVO_KCLASS_UPDATE] == L[A.FIVO_KCLASS_ADM_SLOW]
+    for k in (A.FIVO_KCLASS_PRIM_FAST, A.FIVO_KCLASS_FACES, A.FIVO_KCLASS_UPDATE, A.FIVO_KCLASS_RELAX):
+        assert kt.ms[k] > 0
+    assert kt.units[A.FIVO_KCLASS_PRIM_FAST] == L[A.FIVO_KCLASS_PRIM_FAST] * g.Ntot
+    assert 0 <= kt.units[A.FIVO_KCLASS_PRIM_SLOW] <= kt.units[A.FIVO_KCLASS_PRIM_FAST]
+    assert kt.total_launches > sum(L)
     _assert_same_work(w, o, "advance")
 
 

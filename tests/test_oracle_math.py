@@ -6,6 +6,7 @@ they are pinned here against numpy (correctly rounded to within an ulp) and
 against 40-digit mpmath values (tests/golden/besselkx.json).
 """
 import json
+import re
 import pathlib
 
 import numpy as np
@@ -14,6 +15,7 @@ import pytest
 import _oracle as O
 
 GOLDEN = pathlib.Path(__file__).resolve().parent / "golden"
+ROOT = pathlib.Path(__file__).resolve().parent.parent
 
 
 def test_exp_log_within_an_ulp():
@@ -79,7 +81,23 @@ def test_besselkx_reference_branches():
 
 @pytest.mark.parametrize("nu", [0, 1, 2])
 def test_besselkx_continuity_at_branch_points(nu):
-    for x0 in (1.0, 1e4):
+    for x0 in (1.0, 2.0, 1e4):
         xs = np.array([np.nextafter(x0, 0), x0])
         v = O.besselkx(nu, xs)
         assert abs(v[1] / v[0] - 1) < 1e-13
+
+
+def _c_table(text, name):
+    """The numbers of a C initialiser `name ... { a, b, ... }` in a source file."""
+    m = re.search(re.escape(name) + r"[^{]*\{([^}]*)\}", text)
+    assert m, name
+    return [float(v) for v in m.group(1).replace("\\", " ").split(",") if v.strip()]
+
+
+def test_bessel_tables_same_in_oracle_and_library():
+    """The oracle and the CUDA library sum the same Chebyshev coefficients."""
+    orc = (ROOT / "oracle" / "jlmath.h").read_text()
+    lib = (ROOT / "fivohydro.jl_b200" / "csrc" / "fmath.cuh").read_text()
+    for t in ("K0A", "K1A", "K0B", "K1B"):
+        a, b = _c_table(orc, "O_CHEB_" + t), _c_table(lib, "#define FX_CHEB_" + t)
+        assert a == b and len(a) >= 20, t
