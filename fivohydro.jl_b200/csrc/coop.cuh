@@ -14,7 +14,10 @@
  *                 the tree with the ballot of the 31 predicates;
  *   Jacobian      the 2 x NU central-difference evaluations, one per lane;
  *   line search   the 12 step lengths alpha, alpha/2, ..., one per lane; the
- *                 first accepted one is taken, as the sequential loop would.
+ *                 first accepted one is taken, as the sequential loop would;
+ *                 in the same round, 2 x NU more lanes evaluate the Jacobian
+ *                 points of the next iteration around the full step, which is
+ *                 the trial usually accepted, so an iteration costs one round.
  *
  * Every value a lane computes is computed with the same operations as in
  * recover_attempt (physics.cuh), and every decision is taken from the same
@@ -148,23 +151,48 @@ __device__ __forceinline__ double pick4(const double x[4], int s) {
   return s == 0 ? x[0] : (s == 1 ? x[1] : (s == 2 ? x[2] : x[3]));
 }
 
+/* trial point of the line search: x + al * delta with the bounds of the unknowns
+ * (src2d/primrec2d.jl:660-668) */
+template <bool NCH>
+__device__ __forceinline__ void trial_point(const double x[4], const double delta[4], double al, double yT_lo,
+                                            double yT_hi, double xt[4]) {
+  xt[0] = x[0]; xt[1] = x[1]; xt[2] = x[2]; xt[3] = x[3];
+  if (NCH) {
+    xt[0] = x[0] + al * delta[0]; xt[1] = x[1] + al * delta[1];
+    xt[2] = x[2] + al * delta[2]; xt[3] = x[3] + al * delta[3];
+  } else {
+    xt[0] = x[0] + al * delta[0]; xt[2] = x[2] + al * delta[1]; xt[3] = x[3] + al * delta[2];
+  }
+  xt[0] = jclamp(xt[0], yT_lo, yT_hi);
+  if (NCH) xt[1] = jclamp(xt[1], -FV_PHI_CAP, FV_PHI_CAP);
+  xt[2] = jclamp(xt[2], -FV_U_CAP, FV_U_CAP);
+  xt[3] = jclamp(xt[3], -FV_U_CAP, FV_U_CAP);
+}
+
+/* point j of the central differences at x: x +- h e_s for unknown k = j / 2
+ * (+ for even j), h = 1e-6 max(1, |x_s|) (src2d/primrec2d.jl:605-618) */
+template <bool NCH>
+__device__ __forceinline__ void jac_point(const double x[4], int j, double xl[4]) {
+  const int k = j >> 1;
+  const int s = NCH ? k : (k == 0 ? 0 : k + 1);
+  double xs = pick4(x, s);
+  double h = 1e-6 * jmax(1.0, fabs_(xs));
+  double xv = (j & 1) ? xs - h : xs + h;
+  double a0 = x[0], a1 = x[1], a2 = x[2], a3 = x[3];
+  xl[0] = s == 0 ? xv : a0; xl[1] = s == 1 ? xv : a1;
+  xl[2] = s == 2 ? xv : a2; xl[3] = s == 3 ? xv : a3;
+}
+
 /* _cons_to_prim_attempt_2d! (src2d/primrec2d.jl:511-742), one warp */
 template <int EOS, bool NCH>
-__device__ Recovery attempt_warp(const CellCons& c, const DevParams& d, double yT0, double phi0, double ux0,
+__device__ __noinline__ Recovery attempt_warp(const CellCons& c, const DevParams& d, double yT0, double phi0, double ux0,
                                  double uy0, int maxit, double tol, int lane) {
   Recovery out;
   const double yT_lo = d.log_T_min, yT_hi = d.log_T_solve_max;
   const double m = d.p.m_hq;
   out.reason = PRR_UNSET; out.resnorm = nan_();
   const double D = c.D, Sx = c.Sx, Sy = c.Sy, E = c.E;
-  if (!isfinite_(E) || E <= FV_E_VAC || !isfinite_(D) || D < FV_D_VAC) {
-    out.reason = PRR_VACUUM; out.resnorm = 0.0;
-    double P, n, en;
-    eos_Pne<EOS>(FV_T_MIN, 0.0, d, &P, &n, &en);
-    out.T = FV_T_MIN; out.mu = 0.0; out.ux = 0.0; out.uy = 0.0; out.n = 0.0; out.e = jmax(E, 0.0);
-    out.P = P; out.ok = 0;
-    return out;
-  }
+  if (is_vacuum(c)) return vacuum_recovery<EOS>(c, d);
   const int NU = NCH ? 4 : 3;
   EosMemo memo; memo.reset();
   double x[4], F[4], J[4][4], delta[4];
@@ -196,6 +224,11 @@ __device__ Recovery attempt_warp(const CellCons& c, const DevParams& d, double y
   double last_nrm = nan_();
   const int r_lo = NCH ? 0 : 1;
 
+  /* Fj: on lanes < 2 NU, the Jacobian evaluations at the current x (valid when
+   * have_jac); jac_ok: all of them finite */
+  double Fj[4] = {0.0, 0.0, 0.0, 0.0};
+  bool have_jac = false, jac_ok = true;
+  const unsigned spec_mask = ((1u << (2 * NU)) - 1u) << 12;
   for (int it = 1; it <= maxit; ++it) {
     double nrm = 0.0;
 #pragma unroll
@@ -203,21 +236,17 @@ __device__ Recovery attempt_warp(const CellCons& c, const DevParams& d, double y
     last_nrm = nrm;
     if (nrm < tol) { converged = true; out.reason = PRR_CONVERGED; break; }
     /* ---- Jacobian: lane 2k evaluates x + h e_s, lane 2k+1 x - h e_s (s = unknown k) */
-    double Fj[4] = {0.0, 0.0, 0.0, 0.0};
-    bool fin = true;
-    if (lane < 2 * NU) {
-      const int k = lane >> 1;
-      const int s = NCH ? k : (k == 0 ? 0 : k + 1);
-      double xs = pick4(x, s);
-      double h = 1e-6 * jmax(1.0, fabs_(xs));
-      double xv = (lane & 1) ? xs - h : xs + h;
+    if (!have_jac) {
+      bool fin = true;
       double xl[4];
-      xl[0] = s == 0 ? xv : x[0]; xl[1] = s == 1 ? xv : x[1];
-      xl[2] = s == 2 ? xv : x[2]; xl[3] = s == 3 ? xv : x[3];
-      evalF<EOS, NCH>(Fj, xl, c, d, memo);
-      fin = finite4(Fj);
+      jac_point<NCH>(x, lane & 7, xl);
+      if (lane < 2 * NU) {
+        evalF<EOS, NCH>(Fj, xl, c, d, memo);
+        fin = finite4(Fj);
+      }
+      jac_ok = __all_sync(FV_FULL, fin);
     }
-    if (!__all_sync(FV_FULL, fin)) { out.reason = PRR_NONFINITE_JACOBIAN; break; }
+    if (!jac_ok) { out.reason = PRR_NONFINITE_JACOBIAN; break; }
 #pragma unroll
     for (int k = 0; k < NU; ++k) {
       const int s = NCH ? k : (k == 0 ? 0 : k + 1);
@@ -245,25 +274,26 @@ __device__ Recovery attempt_warp(const CellCons& c, const DevParams& d, double y
       double ad = fabs_(delta[k]);
       if (ad > 1.0) alpha = jmin(alpha, 1.0 / ad);
     }
-    /* ---- line search: lane l tries alpha * 2^-l (12 halvings at most) */
-    double xt[4] = {x[0], x[1], x[2], x[3]};
-    double Ft[4] = {0.0, 0.0, 0.0, 0.0};
-    bool acc = false;
+    /* ---- one round: lane l < 12 tries alpha * 2^-l (the line search); lanes
+     * 12 .. 12 + 2 NU - 1 evaluate the Jacobian at the first trial point, which
+     * the next iteration uses when that trial is the one accepted */
+    double xt[4];
+    double al = alpha;
     if (lane < 12) {
-      double al = alpha;
       for (int q = 0; q < lane; ++q) al *= 0.5;
-      if (NCH) {
-        xt[0] = x[0] + al * delta[0]; xt[1] = x[1] + al * delta[1];
-        xt[2] = x[2] + al * delta[2]; xt[3] = x[3] + al * delta[3];
-      } else {
-        xt[0] = x[0] + al * delta[0]; xt[2] = x[2] + al * delta[1]; xt[3] = x[3] + al * delta[2];
-      }
-      xt[0] = jclamp(xt[0], yT_lo, yT_hi);
-      if (NCH) xt[1] = jclamp(xt[1], -FV_PHI_CAP, FV_PHI_CAP);
-      xt[2] = jclamp(xt[2], -FV_U_CAP, FV_U_CAP);
-      xt[3] = jclamp(xt[3], -FV_U_CAP, FV_U_CAP);
-      evalF<EOS, NCH>(Ft, xt, c, d, memo);
-      if (finite4(Ft)) {
+      trial_point<NCH>(x, delta, al, yT_lo, yT_hi, xt);
+    } else {
+      double x0[4];
+      trial_point<NCH>(x, delta, alpha, yT_lo, yT_hi, x0);
+      jac_point<NCH>(x0, (lane - 12) & 7, xt);
+    }
+    double Ft[4] = {0.0, 0.0, 0.0, 0.0};
+    bool acc = false, fspec = true;
+    if (lane < 12 + 2 * NU) {
+      evalF<EOS, NCH>(Ft, xt, c, d, memo);   /* one call site for the whole round */
+      const bool fin = finite4(Ft);
+      if (lane >= 12) fspec = fin;
+      else if (fin) {
         double trial = 0.0;
 #pragma unroll
         for (int r = r_lo; r < 4; ++r) trial = jmax(trial, fabs_(Ft[r] * rs[r]));
@@ -271,10 +301,22 @@ __device__ Recovery attempt_warp(const CellCons& c, const DevParams& d, double y
       }
     }
     unsigned ab = __ballot_sync(FV_FULL, acc);
+    unsigned fb = __ballot_sync(FV_FULL, fspec);
     const int src = ab ? (__ffs(ab) - 1) : 11;
+    double Fs[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) { x[q] = shfl_d(xt[q], src); F[q] = shfl_d(Ft[q], src); }
+    for (int q = 0; q < 4; ++q) {
+      x[q] = shfl_d(xt[q], src);
+      Fs[q] = shfl_d(Ft[q], (lane + 12) & 31);
+      F[q] = shfl_d(Ft[q], src);
+    }
     if (!ab) { out.reason = PRR_LINESEARCH_FAILED; break; }
+    have_jac = (src == 0);
+    if (have_jac) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) Fj[q] = Fs[q];
+      jac_ok = (fb & spec_mask) == spec_mask;
+    }
   }
   out.resnorm = last_nrm;
   double T = jclamp(fx_exp(x[0]), FV_T_MIN, FV_T_SOLVE_MAX);

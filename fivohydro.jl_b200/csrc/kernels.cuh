@@ -1016,10 +1016,8 @@ __global__ void __launch_bounds__(128) k_prim_fast(DevParams d, DevState U, DevP
     CellCons c;
     load_cons(d, U, i, tau, c);
     const double yT0 = h.x0_yT[i], ux0 = h.x0_ux[i], uy0 = h.x0_uy[i];
-    const bool vacuum = !isfinite_(c.E) || c.E <= FV_E_VAC || !isfinite_(c.D) || c.D < FV_D_VAC;
-    if (vacuum) {
-      Recovery r = recover_attempt<EOS, NCH>(c, d, yT0, h.x0_phi[i], ux0, uy0, d.p.primrec_maxit, d.p.primrec_tol);
-      store_recovery<EOS>(d, w, h, i, r);
+    if (is_vacuum(c)) {
+      store_recovery<EOS>(d, w, h, i, vacuum_recovery<EOS>(c, d));
       vac = true;
     } else if (!(isfinite_(yT0) && isfinite_(ux0) && isfinite_(uy0))) {
       defer = true;

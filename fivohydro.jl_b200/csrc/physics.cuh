@@ -437,6 +437,22 @@ FX_HD void solve_phi_bisect(double D, double T, double ux, double uy, double nux
   *phi = f; *ok = isfinite_(nf);
 }
 
+/* the vacuum test and result of _cons_to_prim_attempt_2d! (src2d/primrec2d.jl:527-534) */
+FX_HD bool is_vacuum(const CellCons& c) {
+  return !isfinite_(c.E) || c.E <= FV_E_VAC || !isfinite_(c.D) || c.D < FV_D_VAC;
+}
+
+template <int EOS>
+FX_HD Recovery vacuum_recovery(const CellCons& c, const DevParams& d) {
+  Recovery out;
+  out.reason = PRR_VACUUM; out.resnorm = 0.0;
+  double P, n, en;
+  eos_Pne<EOS>(FV_T_MIN, 0.0, d, &P, &n, &en);
+  out.T = FV_T_MIN; out.mu = 0.0; out.ux = 0.0; out.uy = 0.0; out.n = 0.0; out.e = jmax(c.E, 0.0);
+  out.P = P; out.ok = 0;
+  return out;
+}
+
 /* _cons_to_prim_attempt_2d!, src2d/primrec2d.jl:511-742 */
 template <int EOS, bool NCH>
 FX_HD Recovery recover_attempt(const CellCons& c, const DevParams& d, double yT0, double phi0,
@@ -447,14 +463,7 @@ FX_HD Recovery recover_attempt(const CellCons& c, const DevParams& d, double yT0
   const double m = d.p.m_hq;
   out.reason = PRR_UNSET; out.resnorm = nan_();
   const double D = c.D, Sx = c.Sx, Sy = c.Sy, E = c.E;
-  if (!isfinite_(E) || E <= FV_E_VAC || !isfinite_(D) || D < FV_D_VAC) {
-    out.reason = PRR_VACUUM; out.resnorm = 0.0;
-    double P, n, en;
-    eos_Pne<EOS>(FV_T_MIN, 0.0, d, &P, &n, &en);
-    out.T = FV_T_MIN; out.mu = 0.0; out.ux = 0.0; out.uy = 0.0; out.n = 0.0; out.e = jmax(E, 0.0);
-    out.P = P; out.ok = 0;
-    return out;
-  }
+  if (is_vacuum(c)) return vacuum_recovery<EOS>(c, d);
   const int NU = NCH ? 4 : 3;
   EosMemo memo; memo.reset();
   double x[4], F[4], Fp[4], Fm[4], J[4][4], delta[4];
