@@ -24,7 +24,10 @@
  * predicate values, so the result has the bits of the sequential algorithm.
  * The EOS memo is per lane; it only changes which evaluations are repeated.
  * All 32 lanes must call these functions together with the same arguments;
- * every lane returns the same result.
+ * every lane returns the same result. A `stop` flag set by another warp ends an
+ * attempt early with an unusable result: the warm and the cold attempt of a
+ * cell run on two warps at once, and the cold one is abandoned when the warm
+ * one succeeds (cons_to_prim_2d! would not have run it).
  */
 #ifndef FIVO_COOP_CUH
 #define FIVO_COOP_CUH
@@ -36,6 +39,14 @@ namespace fv {
 #define FV_FULL 0xffffffffu
 
 __device__ __forceinline__ double shfl_d(double v, int src) { return __shfl_sync(FV_FULL, v, src); }
+
+/* Warp-uniform read of a stop flag another warp may set (null: never stops). */
+__device__ __forceinline__ bool stop_requested(const volatile int* stop) {
+  if (!stop) return false;
+  int v = 0;
+  if ((threadIdx.x & 31) == 0) v = *stop;
+  return __shfl_sync(FV_FULL, v, 0) != 0;
+}
 
 /* Interval of node (lane + 1) of a bisection tree rooted at (lo, hi), heap
  * order: the children of node k are 2k ("predicate true": hi = mid) and 2k + 1
@@ -69,10 +80,12 @@ __device__ __forceinline__ bool bisect_walk(unsigned bal, int levels, double* lo
 
 /* _invert_e_for_T (src2d/primrec2d.jl:300-314), 60 levels in 12 rounds of 5 */
 template <int EOS>
-__device__ double invert_e_warp(double e_target, double phi, const DevParams& d, int lane) {
+__device__ double invert_e_warp(double e_target, double phi, const DevParams& d, int lane,
+                                const volatile int* stop) {
   double lo = d.log_T_min, hi = d.log_T_solve_max;
   if (e_target <= 0.0) return lo;
   for (int it = 0; it < 60; it += 5) {
+    if (stop_requested(stop)) break;
     double a, b;
     bisect_node(lane, lo, hi, &a, &b);
     bool pred = false;
@@ -92,7 +105,7 @@ __device__ double invert_e_warp(double e_target, double phi, const DevParams& d,
 /* seed_from_conserved_2d (src2d/primrec2d.jl:323-347) */
 template <int EOS>
 __device__ void seed_warp(double E, double Sx, double Sy, double phi, const DevParams& d, double* yT,
-                          double* ux, double* uy, int lane) {
+                          double* ux, double* uy, int lane, const volatile int* stop) {
   double M = sqrt_((Sx * Sx) + (Sy * Sy));
   if (!isfinite_(E) || E <= 0.0) { *yT = d.log_seed_T; *ux = 0.0; *uy = 0.0; return; }
   double P = E / 3.0;
@@ -103,7 +116,7 @@ __device__ void seed_warp(double E, double Sx, double Sy, double phi, const DevP
     v = denom > FV_TINY ? jmin(M / denom, 0.999999) : 0.0;
     double ee = (denom * (1.0 - (v * v))) - P;
     if (ee <= 0.0) ee = jmax(E, FV_TINY);
-    y = invert_e_warp<EOS>(ee, phi, d, lane);
+    y = invert_e_warp<EOS>(ee, phi, d, lane, stop);
     double T = fx_exp(y);
     double Pn, en;
     eos_Pe_2d<EOS>(T, d.p.m_hq + (T * phi), d, &Pn, &en);
@@ -185,8 +198,8 @@ __device__ __forceinline__ void jac_point(const double x[4], int j, double xl[4]
 
 /* _cons_to_prim_attempt_2d! (src2d/primrec2d.jl:511-742), one warp */
 template <int EOS, bool NCH>
-__device__ __noinline__ Recovery attempt_warp(const CellCons& c, const DevParams& d, double yT0, double phi0, double ux0,
-                                 double uy0, int maxit, double tol, int lane) {
+__device__ __forceinline__ Recovery attempt_warp(const CellCons& c, const DevParams& d, double yT0, double phi0, double ux0,
+                                 double uy0, int maxit, double tol, int lane, const volatile int* stop) {
   Recovery out;
   const double yT_lo = d.log_T_min, yT_hi = d.log_T_solve_max;
   const double m = d.p.m_hq;
@@ -203,7 +216,7 @@ __device__ __noinline__ Recovery attempt_warp(const CellCons& c, const DevParams
     x[3] = jclamp(uy0, -FV_U_CAP, FV_U_CAP);
   } else {
     double sy, sx_, syy;
-    seed_warp<EOS>(E, Sx, Sy, x[1], d, &sy, &sx_, &syy, lane);
+    seed_warp<EOS>(E, Sx, Sy, x[1], d, &sy, &sx_, &syy, lane, stop);
     x[0] = jclamp(sy, yT_lo, yT_hi); x[2] = sx_; x[3] = syy;
   }
   evalF<EOS, NCH>(F, x, c, d, memo);
@@ -235,6 +248,7 @@ __device__ __noinline__ Recovery attempt_warp(const CellCons& c, const DevParams
     for (int r = r_lo; r < 4; ++r) nrm = jmax(nrm, fabs_(F[r] * rs[r]));
     last_nrm = nrm;
     if (nrm < tol) { converged = true; out.reason = PRR_CONVERGED; break; }
+    if (stop_requested(stop)) { out.ok = 0; out.reason = PRR_UNSET; return out; }
     /* ---- Jacobian: lane 2k evaluates x + h e_s, lane 2k+1 x - h e_s (s = unknown k) */
     if (!have_jac) {
       bool fin = true;
@@ -357,11 +371,16 @@ __device__ __noinline__ Recovery attempt_warp(const CellCons& c, const DevParams
 template <int EOS, bool NCH>
 __device__ Recovery recover_warp(const CellCons& c, const DevParams& d, double yT0, double phi0, double ux0,
                                  double uy0, int maxit, double tol, int lane) {
-  Recovery r = attempt_warp<EOS, NCH>(c, d, yT0, phi0, ux0, uy0, maxit, tol, lane);
-  if (r.ok) return r;
-  if (r.reason == PRR_VACUUM) return r;
-  if (!(isfinite_(yT0) && isfinite_(ux0) && isfinite_(uy0))) return r;
-  return attempt_warp<EOS, NCH>(c, d, nan_(), nan_(), nan_(), nan_(), maxit, tol, lane);
+  /* one call site for both attempts keeps a single inlined copy of the solver */
+  const bool warm = isfinite_(yT0) && isfinite_(ux0) && isfinite_(uy0);
+  Recovery r;
+  for (int a = 0; a < 2; ++a) {
+    const bool first = a == 0;
+    r = attempt_warp<EOS, NCH>(c, d, first ? yT0 : nan_(), first ? phi0 : nan_(), first ? ux0 : nan_(),
+                               first ? uy0 : nan_(), maxit, tol, lane, nullptr);
+    if (r.ok || r.reason == PRR_VACUUM || !warm) break;
+  }
+  return r;
 }
 
 }  // namespace fv

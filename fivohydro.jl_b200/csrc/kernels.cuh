@@ -1023,8 +1023,8 @@ __global__ void __launch_bounds__(128) k_prim_fast(DevParams d, DevState U, DevP
       defer = true;
     } else {
       bool over = false;
-      Recovery r = recover_attempt<EOS, NCH>(c, d, yT0, h.x0_phi[i], ux0, uy0, d.p.primrec_maxit,
-                                             d.p.primrec_tol, FAST_BUDGET, &over);
+      Recovery r = recover_fast<EOS, NCH>(c, d, yT0, h.x0_phi[i], ux0, uy0, d.p.primrec_maxit,
+                                          d.p.primrec_tol, FAST_BUDGET, &over);
       if (over || !r.ok) defer = true;
       else store_recovery<EOS>(d, w, h, i, r);
     }
@@ -1042,25 +1042,53 @@ __global__ void __launch_bounds__(128) k_prim_fast(DevParams d, DevState U, DevP
   }
 }
 
-/* The deferred cells, one warp per cell (recover_warp), taken from the queue
- * one at a time so that long and short recoveries balance over the warps. */
+/* Barrier of the two warps of pair p of a block (named barrier 1 + p, 64 threads). */
+__device__ __forceinline__ void pair_sync(int p) {
+  asm volatile("bar.sync %0, 64;" :: "r"(1 + p) : "memory");
+}
+
+/* The deferred cells. Each cell is taken by a pair of warps: the first runs the
+ * warm-started attempt, the second at the same time the cold (seeded) attempt
+ * that cons_to_prim_2d! runs when the warm one fails; the second stops early
+ * when the first succeeds. The pair takes cells from the queue one at a time so
+ * that long and short recoveries balance over the pairs. */
 template <int EOS, bool NCH>
 __global__ void __launch_bounds__(128) k_prim_slow(DevParams d, DevState U, DevPrims w, DevHist h, double tau,
                                                    DevFlags* fl, const unsigned int* queue) {
+  __shared__ unsigned int s_q[2];
+  __shared__ int s_stop[2];
+  __shared__ Recovery s_cold[2];
   const unsigned n = *(volatile unsigned int*)&fl->qcount_p;
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&fl->tot_p, (unsigned long long)n);
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int pair = warp >> 1;
+  const bool lead = (warp & 1) == 0;
   while (true) {
-    unsigned q = 0;
-    if (lane == 0) q = atomicAdd(&fl->qnext_p, 1u);
-    q = __shfl_sync(FV_FULL, q, 0);
+    if (lead && lane == 0) {
+      s_q[pair] = atomicAdd(&fl->qnext_p, 1u);
+      s_stop[pair] = 0;
+    }
+    pair_sync(pair);
+    const unsigned q = *(volatile unsigned int*)&s_q[pair];
     if (q >= n) break;
     const long long i = queue[q];
     CellCons c;
     load_cons(d, U, i, tau, c);
-    Recovery r = recover_warp<EOS, NCH>(c, d, h.x0_yT[i], h.x0_phi[i], h.x0_ux[i], h.x0_uy[i],
-                                        d.p.primrec_maxit, d.p.primrec_tol, lane);
-    if (lane == 0) {
+    const double yT0 = h.x0_yT[i], phi0 = h.x0_phi[i], ux0 = h.x0_ux[i], uy0 = h.x0_uy[i];
+    const bool warm = isfinite_(yT0) && isfinite_(ux0) && isfinite_(uy0);
+    Recovery r;
+    r.ok = 0; r.reason = PRR_UNSET;
+    if (!lead || warm) {   /* one call site: the lead's warm attempt or the partner's cold one */
+      r = attempt_warp<EOS, NCH>(c, d, lead ? yT0 : nan_(), lead ? phi0 : nan_(), lead ? ux0 : nan_(),
+                                 lead ? uy0 : nan_(), d.p.primrec_maxit, d.p.primrec_tol, lane,
+                                 lead ? nullptr : &s_stop[pair]);
+      if (lead && lane == 0 && (r.ok || r.reason == PRR_VACUUM)) *(volatile int*)&s_stop[pair] = 1;
+      if (!lead && lane == 0) s_cold[pair] = r;
+    }
+    pair_sync(pair);
+    if (lead && lane == 0) {
+      /* cons_to_prim_2d!: the warm result if it succeeded (or found vacuum), else the cold one */
+      if (!(warm && (r.ok || r.reason == PRR_VACUUM))) r = s_cold[pair];
       if (!r.ok) {
         if (r.reason == PRR_VACUUM) atomicAdd((unsigned long long*)&fl->nvacuum, 1ULL);
         else {

@@ -604,6 +604,217 @@ FX_HD Recovery recover(const CellCons& c, const DevParams& d, double yT0, double
   return recover_attempt<EOS, NCH>(c, d, nan_(), nan_(), nan_(), nan_(), maxit, tol);
 }
 
+/* ---------------------------------------------------------------------------
+ * The warm-started attempt of the fast pass, with the EOS memo replaced by
+ * explicit temperature parts. The memo of EOSCache2D only saves work: a hit
+ * returns the bits of a fresh evaluation. Here the T-only part of the
+ * LatticeHRG EOS (light P, e and e^x K2) is computed once per temperature and
+ * handed to the evaluations that share it, so the 2 x NU Jacobian evaluations
+ * of an iteration are straight-line independent code (two new temperatures,
+ * T e^{+-h}, plus the current one for the other unknowns) that the compiler can
+ * overlap, instead of a chain of calls that each branch on the memo.
+ * ------------------------------------------------------------------------- */
+struct TPart { double x, Pl, el, K2; };
+
+/* the T-only part of eos_Pne_memo (src2d/primrec2d.jl:170-197) at T (before the floor) */
+template <int EOS>
+FX_HD void tpart(double T, const DevParams& d, TPart& tp) {
+  if (EOS != FIVO_EOS_LATTICE_HRG) return;
+  const double Tm = jmax(T, FV_T_MIN);
+  tp.x = lhrg_x(Tm, d);
+  double dP;
+  light_eos<3>(Tm, d, &tp.Pl, &dP, nullptr);
+  tp.el = (-tp.Pl) + (Tm * dP);
+  tp.K2 = lhrg_K2(tp.x);
+}
+
+template <int EOS>
+FX_HD void eos_tp(double T, double mu, const DevParams& d, const TPart& tp, double* P, double* n, double* en) {
+  if (EOS != FIVO_EOS_LATTICE_HRG) { eos_Pne<EOS>(T, mu, d, P, n, en); return; }
+  const double Tm = jmax(T, FV_T_MIN);
+  lhrg_assemble(Tm, mu, d, tp.x, tp.Pl, tp.el, tp.K2, P, n, en);
+}
+
+/* evalF_2d! (src2d/primrec2d.jl:360-390) with tp the T-part of exp(x[0]) */
+template <int EOS, bool NCH>
+FX_HD void evalF_tp(double F[4], const double x[4], double T, const CellCons& c, const DevParams& d,
+                    const TPart& tp) {
+  double yT = x[0], phi = x[1], ux = x[2], uy = x[3];
+  if (!(isfinite_(yT) && isfinite_(phi) && isfinite_(ux) && isfinite_(uy))) {
+    F[0] = F[1] = F[2] = F[3] = inf_(); return;
+  }
+  double mu = d.p.m_hq + (T * phi);
+  double ut = utau(ux, uy);
+  double P, n, en;
+  eos_tp<EOS>(T, mu, d, tp, &P, &n, &en);
+  if (!(isfinite_(P) && isfinite_(n) && isfinite_(en))) { F[0] = F[1] = F[2] = F[3] = inf_(); return; }
+  double weff = (en + P) + c.Pi;
+  double Ptot = P + c.Pi;
+  PiC pc = shear_tensor(ux, uy, ut, c.pixx, c.pixy, c.piyy);
+  F[0] = NCH ? (((n * ut) + nu_tau(ux, uy, ut, c.nux, c.nuy)) - c.D) : 0.0;
+  F[1] = (((weff * ut) * ux) + pc.tx) - c.Sx;
+  F[2] = (((weff * ut) * uy) + pc.ty) - c.Sy;
+  F[3] = ((((weff * ut) * ut) - Ptot) + pc.tt) - c.E;
+}
+
+/* recover_attempt from a finite warm start (x0 already clamped), with the
+ * iteration budget of the fast pass; the same arithmetic, rounded the same way */
+template <int EOS, bool NCH>
+FX_HD Recovery recover_fast(const CellCons& c, const DevParams& d, double yT0, double phi0, double ux0,
+                            double uy0, int maxit, double tol, int budget, bool* over_budget) {
+  Recovery out;
+  const double yT_lo = d.log_T_min, yT_hi = d.log_T_solve_max;
+  const double m = d.p.m_hq;
+  out.reason = PRR_UNSET; out.resnorm = nan_();
+  const double D = c.D, Sx = c.Sx, Sy = c.Sy, E = c.E;
+  if (is_vacuum(c)) return vacuum_recovery<EOS>(c, d);
+  const int NU = NCH ? 4 : 3;
+  double x[4], F[4], J[4][4], delta[4];
+  x[1] = (NCH && isfinite_(phi0)) ? jclamp(phi0, -FV_PHI_CAP, FV_PHI_CAP) : 0.0;
+  x[0] = jclamp(yT0, yT_lo, yT_hi);
+  x[2] = jclamp(ux0, -FV_U_CAP, FV_U_CAP);
+  x[3] = jclamp(uy0, -FV_U_CAP, FV_U_CAP);
+  double Tc = fx_exp(x[0]);
+  TPart tpc;
+  tpart<EOS>(Tc, d, tpc);
+  evalF_tp<EOS, NCH>(F, x, Tc, c, d, tpc);
+  if (!finite4(F)) {
+    out.reason = PRR_NONFINITE_INITIAL;
+    double T = jclamp(fx_exp(x[0]), FV_T_MIN, FV_T_SOLVE_MAX), P, n, en;
+    eos_Pne<EOS>(T, m, d, &P, &n, &en);
+    out.T = T; out.mu = m; out.ux = 0.0; out.uy = 0.0; out.n = 0.0; out.e = jmax(en, 0.0);
+    out.P = P; out.ok = 0;
+    return out;
+  }
+  const double sD = jmax(fabs_(D), 1e-12);
+  const double sS = jmax(jmax(jmax(fabs_(Sx), fabs_(Sy)), 1e-10 * fabs_(E)), 1e-12);
+  const double sE = jmax(fabs_(E), 1e-12);
+  double rs[4];
+  rs[0] = 1.0 / sD; rs[1] = 1.0 / sS; rs[2] = 1.0 / sS; rs[3] = 1.0 / sE;
+  bool converged = false;
+  double last_nrm = nan_();
+  const int r_lo = NCH ? 0 : 1;
+
+  for (int it = 1; it <= maxit; ++it) {
+    double nrm = 0.0;
+#pragma unroll
+    for (int r = r_lo; r < 4; ++r) nrm = jmax(nrm, fabs_(F[r] * rs[r]));
+    last_nrm = nrm;
+    if (nrm < tol) { converged = true; out.reason = PRR_CONVERGED; break; }
+    if (it > budget) { *over_budget = true; return out; }
+    /* ---- Jacobian: all 2 NU evaluations, then the finiteness test of the columns */
+    const double h0 = 1e-6 * jmax(1.0, fabs_(x[0]));
+    const double Tp = fx_exp(x[0] + h0), Tn = fx_exp(x[0] - h0);
+    TPart tpp, tpn;
+    tpart<EOS>(Tp, d, tpp);
+    tpart<EOS>(Tn, d, tpn);
+    double Fp[4][4], Fm[4][4], hh[4];
+    bool ok_jac = true;
+#pragma unroll
+    for (int k = 0; k < NU; ++k) {
+      const int s = NCH ? k : (k == 0 ? 0 : k + 1);
+      const double xs = x[s];
+      const double h = 1e-6 * jmax(1.0, fabs_(xs));
+      hh[k] = h;
+      double xp[4] = {x[0], x[1], x[2], x[3]}, xm[4] = {x[0], x[1], x[2], x[3]};
+      xp[s] = xs + h;
+      xm[s] = xs - h;
+      if (s == 0) {
+        evalF_tp<EOS, NCH>(Fp[k], xp, Tp, c, d, tpp);
+        evalF_tp<EOS, NCH>(Fm[k], xm, Tn, c, d, tpn);
+      } else {
+        evalF_tp<EOS, NCH>(Fp[k], xp, Tc, c, d, tpc);
+        evalF_tp<EOS, NCH>(Fm[k], xm, Tc, c, d, tpc);
+      }
+      ok_jac = ok_jac && finite4(Fp[k]) && finite4(Fm[k]);
+    }
+    if (!ok_jac) { out.reason = PRR_NONFINITE_JACOBIAN; break; }
+#pragma unroll
+    for (int k = 0; k < NU; ++k) {
+      const double inv2h = 1.0 / (2.0 * hh[k]);
+#pragma unroll
+      for (int r = 0; r < NU; ++r) {
+        const int rr = NCH ? r : r + 1;
+        J[r][k] = ((Fp[k][rr] - Fm[k][rr]) * inv2h) * rs[rr];
+      }
+    }
+    double Fact[4];
+#pragma unroll
+    for (int r = 0; r < NU; ++r) {
+      const int rr = NCH ? r : r + 1;
+      delta[r] = 0.0;
+      Fact[r] = F[rr] * rs[rr];
+    }
+    if (!solve_gauss<NU>(delta, J, Fact)) { out.reason = PRR_LINSOLVE_FAILED; break; }
+    double alpha = 1.0;
+#pragma unroll
+    for (int k = 0; k < NU; ++k) {
+      double ad = fabs_(delta[k]);
+      if (ad > 1.0) alpha = jmin(alpha, 1.0 / ad);
+    }
+    const double xs1 = x[0], xs2 = x[1], xs3 = x[2], xs4 = x[3];
+    bool accepted = false;
+    for (int ls = 0; ls < 12; ++ls) {
+      x[0] = xs1; x[1] = xs2; x[2] = xs3; x[3] = xs4;
+      if (NCH) { x[0] += alpha * delta[0]; x[1] += alpha * delta[1]; x[2] += alpha * delta[2]; x[3] += alpha * delta[3]; }
+      else { x[0] += alpha * delta[0]; x[2] += alpha * delta[1]; x[3] += alpha * delta[2]; }
+      x[0] = jclamp(x[0], yT_lo, yT_hi);
+      if (NCH) x[1] = jclamp(x[1], -FV_PHI_CAP, FV_PHI_CAP);
+      x[2] = jclamp(x[2], -FV_U_CAP, FV_U_CAP);
+      x[3] = jclamp(x[3], -FV_U_CAP, FV_U_CAP);
+      Tc = fx_exp(x[0]);
+      tpart<EOS>(Tc, d, tpc);
+      evalF_tp<EOS, NCH>(F, x, Tc, c, d, tpc);
+      if (finite4(F)) {
+        double trial = 0.0;
+#pragma unroll
+        for (int r = r_lo; r < 4; ++r) trial = jmax(trial, fabs_(F[r] * rs[r]));
+        if (trial < nrm * (1.0 - (1e-4 * alpha))) { accepted = true; break; }
+      }
+      alpha *= 0.5;
+    }
+    if (!accepted) { out.reason = PRR_LINESEARCH_FAILED; break; }
+  }
+  out.resnorm = last_nrm;
+  double T = jclamp(fx_exp(x[0]), FV_T_MIN, FV_T_SOLVE_MAX);
+  double mu = NCH ? (m + (T * x[1])) : m;
+  double ux = x[2], uy = x[3];
+  double P, n, en;
+  {
+    TPart tpf;
+    tpart<EOS>(T, d, tpf);
+    eos_tp<EOS>(T, mu, d, tpf, &P, &n, &en);
+  }
+  if (!converged) out.reason = (out.reason == PRR_UNSET) ? PRR_MAXIT : out.reason;
+  evalF_tp<EOS, NCH>(F, x, Tc, c, d, tpc);
+  double rows[4] = {0.0, 0.0, 0.0, 0.0};
+  double resnorm = 0.0;
+#pragma unroll
+  for (int r = r_lo; r < 4; ++r) { rows[r] = fabs_(F[r] * rs[r]); resnorm = jmax(resnorm, rows[r]); }
+  out.resnorm = resnorm;
+  out.T = T; out.mu = mu; out.ux = ux; out.uy = uy;
+  if (!(isfinite_(resnorm) && resnorm < tol)) {
+    double hyd = jmax(jmax(rows[1], rows[2]), rows[3]);
+    if (NCH && isfinite_(hyd) && hyd < tol) {
+      EosMemo memo; memo.reset();
+      double phb; bool okb;
+      solve_phi_bisect<EOS>(D, T, ux, uy, c.nux, c.nuy, d, memo, &phb, &okb);
+      double xp = jclamp(phb, -FV_PHI_CAP, FV_PHI_CAP);
+      mu = m + (T * xp);
+      eos_Pne_memo<EOS>(T, mu, d, memo, &P, &n, &en);
+      out.reason = okb ? PRR_CONVERGED : PRR_RESIDUAL_TOO_LARGE;
+      out.mu = mu; out.n = jmax(n, 0.0); out.e = jmax(en, 0.0); out.P = P; out.ok = 1;
+      return out;
+    }
+    out.reason = PRR_RESIDUAL_TOO_LARGE;
+    out.n = n; out.e = jmax(en, 0.0); out.P = P; out.ok = 0;
+    return out;
+  }
+  out.reason = PRR_CONVERGED;
+  out.n = n; out.e = jmax(en, 0.0); out.P = P; out.ok = 1;
+  return out;
+}
+
 /* ==================== prim -> cons and fluxes ==================== */
 
 /* PrimIdealVisc2D without the ok flag; dissipatives in physical units */
