@@ -18,6 +18,9 @@ cells make this event's run stop (the CPU restatement stops at the same step).
 
   value  device-resident: per-step CUDA events on the library's stream, L2
          flushed (256 MB write) between steps, sum over K steps, max over ranks.
+         The per-kernel times of the roofline come from replaying the same K
+         steps (a device copy of the state taken before them) with the
+         library's kernel timing on, so the timed run has no profiling events.
   e2e    the same steps through the C ABI with the state in pinned host memory:
          every step uploads U, advances, downloads U (the drop-in usage from a
          host driver that keeps U on the host).
@@ -192,13 +195,16 @@ def run_gpu(args):
     tau = TAU0
     res = A.FivoRunResult()
 
-    def advance(n):
-        nonlocal tau
-        A.check(lib, lib.fivo_advance(w.h, tau, 1e9, CFL, CFLTAU, A.FIVO_SSPRK3, A.FIVO_BC_OUTFLOW, n,
+    def step_on(h, tau_, n):
+        A.check(lib, lib.fivo_advance(h, tau_, 1e9, CFL, CFLTAU, A.FIVO_SSPRK3, A.FIVO_BC_OUTFLOW, n,
                                       C.byref(res)), "fivo_advance")
         if not res.ok:
-            raise RuntimeError(f"step failed at tau={tau}")
-        tau = res.tau
+            raise RuntimeError(f"step failed at tau={tau_}")
+        return res.tau
+
+    def advance(n):
+        nonlocal tau
+        tau = step_on(w.h, tau, n)
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -209,12 +215,16 @@ def run_gpu(args):
     for _ in range(args.warmup):
         advance(1)
 
+    # A twin context holds the state at the start of the timed window; the same
+    # steps are replayed on it afterwards with per-kernel CUDA-event timing, so
+    # the timed run itself carries no profiling events.
+    twin = GPUWork2D(m, g, lib=lib)
+    A.check(lib, lib.fivo_ctx_set_stream(twin.h, C.c_void_p(stream.cuda_stream)), "set_stream")
+    twin.clone_state_from(w)
+
     # ---------------- device-resident timing
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    A.check(lib, lib.fivo_profile(w.h, 1), "profile")
-    kt = A.FivoKernelTimes()
-    lib.fivo_profile_read(w.h, C.byref(kt), 1)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -229,8 +239,19 @@ def run_gpu(args):
     if dist:
         dist.barrier()
     ms = sum(s.elapsed_time(e) for s, e in zip(starts, stops))
-    lib.fivo_profile_read(w.h, C.byref(kt), 1)
-    A.check(lib, lib.fivo_profile(w.h, 0), "profile")
+
+    # ---------------- the same steps again on the twin, kernel by kernel
+    A.check(lib, lib.fivo_profile(twin.h, 1), "profile")
+    kt = A.FivoKernelTimes()
+    lib.fivo_profile_read(twin.h, C.byref(kt), 1)
+    tau_r = tau_start
+    for k in range(args.steps):
+        l2_flush()
+        tau_r = step_on(twin.h, tau_r, 1)
+    lib.fivo_profile_read(twin.h, C.byref(kt), 1)
+    if tau_r != tau:
+        raise RuntimeError("the profiled replay left the timed trajectory")
+    twin.close()
     clocks = clk.summary()
     t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if dist:

@@ -591,6 +591,33 @@ int fivo_ctx_info(const fivo_ctx* c, int* nv, int64_t* ntot, double* evac) {
   return FIVO_OK;
 }
 
+int fivo_ctx_clone_state(fivo_ctx* dst, const fivo_ctx* src) {
+  if (!dst || !src) return fail(FIVO_ERR_ARG, "null context");
+  if (dst == src) return FIVO_OK;
+  const DevParams& a = dst->dp;
+  const DevParams& b = src->dp;
+  if (a.Nx != b.Nx || a.Ny != b.Ny || a.nv != b.nv || a.dx != b.dx || a.dy != b.dy ||
+      std::memcmp(&a.p, &b.p, sizeof(fivo_params)) != 0)
+    return fail(FIVO_ERR_ARG, "fivo_ctx_clone_state: contexts differ in parameters or grid");
+  if (dst->device != src->device) return fail(FIVO_ERR_ARG, "fivo_ctx_clone_state: contexts on different devices");
+  const size_t N = (size_t)a.Ntot;
+  CK(cudaStreamSynchronize(src->st));
+  CK(cudaMemcpyAsync(dst->slab, src->slab, 4 * (size_t)a.nv * N * 8, cudaMemcpyDeviceToDevice, dst->st));
+  CK(cudaMemcpyAsync(dst->pbuf, src->pbuf, 9 * N * 8 + N, cudaMemcpyDeviceToDevice, dst->st));
+  CK(cudaMemcpyAsync(dst->hbuf, src->hbuf, 8 * N * 8, cudaMemcpyDeviceToDevice, dst->st));
+  CK(cudaMemcpyAsync(dst->masks, src->masks, 3 * N, cudaMemcpyDeviceToDevice, dst->st));
+  /* the role indices and the plane permutation of the relaxation double buffer */
+  for (int s = 0; s < 4; ++s)
+    for (int k = 0; k < FV_MAXV; ++k)
+      dst->S[s].f[k] = src->S[s].f[k] ? dst->slab + (src->S[s].f[k] - src->slab) : nullptr;
+  dst->iU = src->iU; dst->iU1 = src->iU1; dst->iU2 = src->iU2; dst->iT = src->iT;
+  dst->hist_valid = src->hist_valid;
+  dst->nsteps_run = src->nsteps_run;
+  dst->cnt = src->cnt;
+  CK(ctx_sync(dst));
+  return FIVO_OK;
+}
+
 int fivo_upload_state(fivo_ctx* c, const double* U, int nv, int64_t ntot) {
   if (!c || !U) return fail(FIVO_ERR_ARG, "null argument");
   if (nv != c->dp.nv || ntot != c->dp.Ntot) return fail(FIVO_ERR_ARG, "state size mismatch");

@@ -108,6 +108,7 @@ SIGNATURES = {
                                   C.c_double, C.POINTER(C.c_void_p)]),
     "fivo_ctx_destroy": (C.c_int, [C.c_void_p]),
     "fivo_ctx_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int64), _D]),
+    "fivo_ctx_clone_state": (C.c_int, [C.c_void_p, C.c_void_p]),
     "fivo_upload_state": (C.c_int, [C.c_void_p, _D, C.c_int, _I64]),
     "fivo_download_state": (C.c_int, [C.c_void_p, _D, C.c_int, _I64]),
     "fivo_upload_history": (C.c_int, [C.c_void_p, _I64] + [_D] * 8),

@@ -163,6 +163,10 @@ class GPUWork2D:
     def sync(self):
         self._ck(self.lib.fivo_sync(self.h), "fivo_sync")
 
+    def clone_state_from(self, other: "GPUWork2D"):
+        """Make this work object's next steps bitwise those of `other` (same model and grid)."""
+        self._ck(self.lib.fivo_ctx_clone_state(self.h, other.h), "fivo_ctx_clone_state")
+
 
 def set_cells(model: IdealDiffVisc2DModel, tau, T, alpha, ux, uy, *, Pi=None, pixx=None, pixy=None,
               piyy=None, nux=None, nuy=None, U=None, lib=None):

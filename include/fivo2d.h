@@ -214,6 +214,12 @@ int  fivo_ctx_create(const fivo_params* p, int nx, int ny, int nghost,
                      double xmax, double ymax, fivo_ctx** out);
 int  fivo_ctx_destroy(fivo_ctx* ctx);
 int  fivo_ctx_info(const fivo_ctx* ctx, int* nv, int64_t* ntot, double* E_vac_cut);
+/* Copy everything that determines the next steps of src into dst (state
+ * buffers, primitives, warm starts and history, masks, the last signal speed
+ * and the run bookkeeping): dst then advances to the same bits as src. Both
+ * contexts must come from the same parameters and grid. A device-memory
+ * checkpoint; no counterpart in the reference (Julia copies the arrays). */
+int  fivo_ctx_clone_state(fivo_ctx* dst, const fivo_ctx* src);
 
 /* --- state and history transfer --- */
 int  fivo_upload_state(fivo_ctx* ctx, const double* U, int nv, int64_t ntot);

@@ -279,3 +279,26 @@ def test_failure_injection_maxit(gpu_lib):
     assert nw == no and nw > 100
     assert w.counters().primfail_reason == o1.counters().primfail_reason == 8
     _assert_same_work(w, o1, "maxit=1")
+
+
+def test_clone_state_replays_the_same_steps(gpu_lib):
+    """fivo_ctx_clone_state: a copy taken mid-run advances to the bits of the
+    original (the bench replays its timed steps this way with kernel timing)."""
+    g, m, U = _glauber_setup(40)
+    w, o = _pair(m, g, U)
+    w.rhs(0.6)
+    r = w.advance(0.6, 5.0, 0.2, 0.05, A.FIVO_SSPRK3, A.FIVO_BC_OUTFLOW, 3)
+    twin = GPUWork2D(m, g, lib=w.lib)
+    twin.clone_state_from(w)
+    ra = w.advance(r["tau"], 5.0, 0.2, 0.05, A.FIVO_SSPRK3, A.FIVO_BC_OUTFLOW, 4)
+    rb = twin.advance(r["tau"], 5.0, 0.2, 0.05, A.FIVO_SSPRK3, A.FIVO_BC_OUTFLOW, 4)
+    assert ra == rb
+    assert bits_equal(w.get_state(), twin.get_state())
+    hw, ht = w.get_history(), twin.get_history()
+    for k in hw:
+        assert bits_equal(hw[k], ht[k]), k
+    other = GPUWork2D(fivo2d.build_model_2d(eos=fivo2d.LatticeHRGEOS()), g, lib=w.lib)
+    with pytest.raises(A.FivoError):
+        other.clone_state_from(w)
+    other.close()
+    twin.close()
