@@ -626,28 +626,39 @@ __device__ void vorticity_coupling(double ux, double uy, double ut, double pxx, 
  * Every cell writes its dissipative rows: interior ok cells relaxed, the rest
  * copied. Then the shear projection of every interior cell. */
 template <int EOS>
-__global__ void __launch_bounds__(128) k_relax(DevParams d, DevState Uq, DevState Uo, DevPrims w,
-                                               DevHist h, double tau, double D, int do_relax,
-                                               int do_project, DevFlags* fl) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.Ntot) return;
-  const int nv = d.nv;
+__device__ __forceinline__ double relax_cell(const DevParams& d, const DevState& Uq, const DevState& Uo,
+                                             const DevPrims& w, const DevHist& h, double tau, double D,
+                                             int do_relax, int do_project, long long i) {
+  double rel_out = -1.0;
   const int ix = (int)(i / d.Nytot), iy = (int)(i % d.Nytot);
   const int ng = d.ng;
   const bool interior = ix >= ng && ix < ng + d.Nx && iy >= ng && iy < ng + d.Ny;
-  double u[FV_MAXV];
-  for (int a = 4; a < nv; ++a) u[a] = Uq.f[a][i];
+  /* the dissipative rows as named values (a layout-indexed array would live in
+   * local memory); rows a sector does not have stay 0 and are not stored */
+  const double* QNux = d.hasNu ? Uq.f[d.iNux] : nullptr;
+  const double* QNuy = d.hasNu ? Uq.f[d.iNuy] : nullptr;
+  const double* QPi = d.hasPi ? Uq.f[d.iPi] : nullptr;
+  const double* QPixx = d.hasShear ? Uq.f[d.iPixx] : nullptr;
+  const double* QPixy = d.hasShear ? Uq.f[d.iPixy] : nullptr;
+  const double* QPiyy = d.hasShear ? Uq.f[d.iPiyy] : nullptr;
+  const double* QPieta = d.hasShear ? Uq.f[d.iPieta] : nullptr;
+  double v_nux = d.hasNu ? QNux[i] : 0.0, v_nuy = d.hasNu ? QNuy[i] : 0.0;
+  double v_Pi = d.hasPi ? QPi[i] : 0.0;
+  double v_pixx = d.hasShear ? QPixx[i] : 0.0, v_pixy = d.hasShear ? QPixy[i] : 0.0;
+  double v_piyy = d.hasShear ? QPiyy[i] : 0.0, v_pieta = d.hasShear ? QPieta[i] : 0.0;
   const fivo_params& p = d.p;
   const double ux = w.ux[i], uy = w.uy[i];
   const double ut = utau(ux, uy);
   if (do_relax && interior && w.ok[i]) {
     const double invdx = 1.0 / d.dx, invdy = 1.0 / d.dy;
     const long long st = d.Nytot;
-    auto upw = [&](int a) {
-      const double* Q = Uq.f[a];
-      double q0 = Q[i];
-      double dqx = ux >= 0 ? (q0 - Q[i - st]) * invdx : (Q[i + st] - q0) * invdx;
-      double dqy = uy >= 0 ? (q0 - Q[i - 1]) * invdy : (Q[i + 1] - q0) * invdy;
+    /* upwind neighbours: chosen by the sign of u, loaded before any use */
+    const long long jx = ux >= 0 ? i - st : i + st;
+    const long long jy = uy >= 0 ? i - 1 : i + 1;
+    auto upw = [&](const double* Q, double q0) {
+      double qx = Q[jx], qy = Q[jy];
+      double dqx = ux >= 0 ? (q0 - qx) * invdx : (qx - q0) * invdx;
+      double dqy = uy >= 0 ? (q0 - qy) * invdy : (qy - q0) * invdy;
       return (ux * dqx) + (uy * dqy);
     };
     /* kinematics_2d, src2d/dissipation2d.jl:141-167 */
@@ -673,7 +684,7 @@ __global__ void __launch_bounds__(128) k_relax(DevParams d, DevState Uq, DevStat
     const double s_ent = eos_entropy(T, mu, n, en, P);
     /* ---- bulk ---- */
     if (p.enable_bulk && d.hasPi) {
-      double Pin = u[d.iPi];
+      double Pin = v_Pi;
       double zeta = 0.0, tPi = 0.0;
       if (p.bulk_kind != FIVO_BULK_ZERO) {
         double cs2 = eos_cs2<EOS>(T, d);
@@ -687,19 +698,19 @@ __global__ void __launch_bounds__(128) k_relax(DevParams d, DevState Uq, DevStat
       }
       double PiNS = (-zeta) * k.th;
       double A = safe_div(tPi * ut, D);
-      double adv = p.relax_advect_Pi ? (-tPi) * upw(d.iPi) : 0.0;
+      double adv = p.relax_advect_Pi ? (-tPi) * upw(QPi, v_Pi) : 0.0;
       double dPi = p.deltaPi_factor * tPi;
       if (p.lambda_Pi_pi_factor != 0.0 && p.enable_shear && d.hasShear) {
         double sxx, sxy, syy, se, ps, c1, c2, c3;
         ns_shear(ux, uy, ut, tau, k, -0.5, &sxx, &sxy, &syy, &se);
-        pi_sigma(ux, uy, u[d.iPixx], u[d.iPixy], u[d.iPiyy], u[d.iPieta], sxx, sxy, syy, se, &ps, &c1, &c2, &c3);
+        pi_sigma(ux, uy, v_pixx, v_pixy, v_piyy, v_pieta, sxx, sxy, syy, se, &ps, &c1, &c2, &c3);
         adv = adv - ((p.lambda_Pi_pi_factor * tPi) * ps);
       }
       double num = ((A * Pin) + PiNS) + adv;
       Pin = dPi == 0.0 ? num / (A + 1.0) : num / jmax((A + 1.0) + (dPi * k.th), 0.5 * (A + 1.0));
       Pin = jmax(Pin, -0.99 * jmax(P, 0.0));
       if (p.Pi_clip_factor > 0) { double cap = p.Pi_clip_factor * fabs_(P); Pin = jclamp(Pin, -cap, cap); }
-      u[d.iPi] = Pin;
+      v_Pi = Pin;
     }
     /* ---- shear ---- */
     if (p.enable_shear && d.hasShear) {
@@ -712,7 +723,7 @@ __global__ void __launch_bounds__(128) k_relax(DevParams d, DevState Uq, DevStat
       } else {
         dpi = p.deltaShear_factor * 0.0;
       }
-      double pixx = u[d.iPixx], pixy = u[d.iPixy], piyy = u[d.iPiyy], pieta = u[d.iPieta];
+      double pixx = v_pixx, pixy = v_pixy, piyy = v_piyy, pieta = v_pieta;
       double nsxx, nsxy, nsyy, nse;
       ns_shear(ux, uy, ut, tau, k, eta, &nsxx, &nsxy, &nsyy, &nse);
       PiC pc = shear_tensor(ux, uy, ut, pixx, pixy, piyy);
@@ -722,9 +733,9 @@ __global__ void __launch_bounds__(128) k_relax(DevParams d, DevState Uq, DevStat
       double den = jmax((A + 1.0) + (dpi * k.th), 0.5 * (A + 1.0));
       double pd = p.shear_projected_deriv ? tpi : 0.0;
       bool ra = p.relax_advect_pi != 0;
-      double axx = ra ? (-tpi) * upw(d.iPixx) : 0.0;
-      double axy = ra ? (-tpi) * upw(d.iPixy) : 0.0;
-      double ayy = ra ? (-tpi) * upw(d.iPiyy) : 0.0;
+      double axx = ra ? (-tpi) * upw(QPixx, v_pixx) : 0.0;
+      double axy = ra ? (-tpi) * upw(QPixy, v_pixy) : 0.0;
+      double ayy = ra ? (-tpi) * upw(QPiyy, v_piyy) : 0.0;
       if (p.terms & FIVO_TERM_SHEAR_VORTICITY) {
         double iu = safe_inv(ut);
         double dtux = ((k.ax - (ux * k.dxux)) - (uy * k.dyux)) * iu;
@@ -747,7 +758,7 @@ __global__ void __launch_bounds__(128) k_relax(DevParams d, DevState Uq, DevStat
         }
         if (p.lambda_pi_Pi_factor != 0.0 && p.enable_bulk && d.hasPi) {
           /* bulk already updated above, as in the reference (bulk runs first) */
-          double lP = (p.lambda_pi_Pi_factor * tpi) * u[d.iPi];
+          double lP = (p.lambda_pi_Pi_factor * tpi) * v_Pi;
           axx -= lP * sxx; axy -= lP * sxy; ayy -= lP * syy;
         }
       }
@@ -759,7 +770,7 @@ __global__ void __launch_bounds__(128) k_relax(DevParams d, DevState Uq, DevStat
         pixx = jclamp(pixx, -cap, cap); pixy = jclamp(pixy, -cap, cap); piyy = jclamp(piyy, -cap, cap);
       }
       double pe = project_traceless(ux, uy, ut, pixx, pixy, piyy);
-      u[d.iPixx] = pixx; u[d.iPixy] = pixy; u[d.iPiyy] = piyy; u[d.iPieta] = pe;
+      v_pixx = pixx; v_pixy = pixy; v_piyy = piyy; v_pieta = pe;
     }
     /* ---- charge ---- */
     if (p.enable_diff && d.hasNu) {
@@ -768,7 +779,7 @@ __global__ void __launch_bounds__(128) k_relax(DevParams d, DevState Uq, DevStat
         double lo = p.vacuum_n_lo, hi = p.vacuum_n_hi;
         wv = hi <= lo ? 1.0 : (n <= lo ? 0.0 : (n >= hi ? 1.0 : (n - lo) / (hi - lo)));
       }
-      if (wv <= 0.0) { u[d.iNux] = 0.0; u[d.iNuy] = 0.0; }
+      if (wv <= 0.0) { v_nux = 0.0; v_nuy = 0.0; }
       else {
         double Tm = posden(T);
         double alpha = mu / Tm;
@@ -776,7 +787,7 @@ __global__ void __launch_bounds__(128) k_relax(DevParams d, DevState Uq, DevStat
         double tn;
         diff_tauN<EOS>(d, Tm, alpha, &tn);
         double dN = p.deltaN_factor * tn;
-        double nux = u[d.iNux], nuy = u[d.iNuy];
+        double nux = v_nux, nuy = v_nuy;
         double dxa = alpha_grad(w.alpha, i, st, ix, d.Nxtot, ng, invdx);
         double dya = alpha_grad(w.alpha, i, 1, iy, d.Nytot, ng, invdy);
         double ap = h.alpha_prev[i];
@@ -794,8 +805,8 @@ __global__ void __launch_bounds__(128) k_relax(DevParams d, DevState Uq, DevStat
         double A = safe_div(tn * ut, D);
         double den = jmax((A + 1.0) + (dN * k.th), 0.5 * (A + 1.0));
         double pdn = p.diff_projected_deriv ? tn : 0.0;
-        double anx = p.relax_advect_nu ? (-tn) * upw(d.iNux) : 0.0;
-        double any_ = p.relax_advect_nu ? (-tn) * upw(d.iNuy) : 0.0;
+        double anx = p.relax_advect_nu ? (-tn) * upw(QNux, v_nux) : 0.0;
+        double any_ = p.relax_advect_nu ? (-tn) * upw(QNuy, v_nuy) : 0.0;
         nux = ((((A * nux) + nsx) + ((pdn * ux) * nua)) + anx) / den;
         nuy = ((((A * nuy) + nsy) + ((pdn * uy) * nua)) + any_) / den;
         if (p.nu_clip_factor > 0) {
@@ -803,18 +814,45 @@ __global__ void __launch_bounds__(128) k_relax(DevParams d, DevState Uq, DevStat
           double mag = fx_hypot(nux, nuy);
           if (mag > cap && mag > FV_TINY) { double sc = cap / mag; nux *= sc; nuy *= sc; }
         }
-        u[d.iNux] = nux; u[d.iNuy] = nuy;
+        v_nux = nux; v_nuy = nuy;
       }
     }
   }
   /* project_shear!: residual monitor and pieta from tracelessness, interior cells */
   if (do_project && d.hasShear && interior) {
-    double rel = shear_residual_rel(ux, uy, ut, u[d.iPixx], u[d.iPixy], u[d.iPiyy], u[d.iPieta]);
-    atomic_max_pos(&fl->shear_max_bits, rel);
-    atomicAdd(&fl->shear_sum, rel);
-    if (p.shear_constraint_project) u[d.iPieta] = project_traceless(ux, uy, ut, u[d.iPixx], u[d.iPixy], u[d.iPiyy]);
+    double rel = shear_residual_rel(ux, uy, ut, v_pixx, v_pixy, v_piyy, v_pieta);
+    rel_out = rel;
+    if (p.shear_constraint_project) v_pieta = project_traceless(ux, uy, ut, v_pixx, v_pixy, v_piyy);
   }
-  for (int a = 4; a < nv; ++a) Uo.f[a][i] = u[a];
+  if (d.hasNu) { Uo.f[d.iNux][i] = v_nux; Uo.f[d.iNuy][i] = v_nuy; }
+  if (d.hasPi) Uo.f[d.iPi][i] = v_Pi;
+  if (d.hasShear) {
+    Uo.f[d.iPixx][i] = v_pixx; Uo.f[d.iPixy][i] = v_pixy; Uo.f[d.iPiyy][i] = v_piyy; Uo.f[d.iPieta][i] = v_pieta;
+  }
+  return rel_out;
+}
+
+/* relax_dissipative_2d! + project_shear! on every cell. The shear-residual
+ * monitor (max and sum over interior cells) is reduced over the warp before
+ * its atomics: one per warp instead of one per cell on a single address. */
+template <int EOS>
+__global__ void __launch_bounds__(128) k_relax(DevParams d, DevState Uq, DevState Uo, DevPrims w,
+                                               DevHist h, double tau, double D, int do_relax,
+                                               int do_project, DevFlags* fl) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double rel = -1.0;
+  if (i < d.Ntot) rel = relax_cell<EOS>(d, Uq, Uo, w, h, tau, D, do_relax, do_project, i);
+  if (do_project && d.hasShear) {
+    double mx = rel > 0.0 ? rel : 0.0, sm = rel >= 0.0 ? rel : 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+      mx = jmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      sm += __shfl_xor_sync(0xffffffffu, sm, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomic_max_pos(&fl->shear_max_bits, mx);
+      if (sm != 0.0) atomicAdd(&fl->shear_sum, sm);
+    }
+  }
 }
 
 /* --------------------------------------------------------------- utilities */
