@@ -210,3 +210,24 @@ function run_sim_2d_gpu!(U::AbstractMatrix, g::Grid2D, model, work::GPUWork2D;
             max_shear_res = r.max_shear_res, work = work, maxu = r.maxu, dQ = r.dQ, Q0 = r.Q0, Q1 = r.Q1,
             minPtot = r.minPtot)
 end
+
+"""Device checkpoint: `dst` continues bit for bit as `src` would (same grid and model)."""
+clone_state!(dst::GPUWork2D, src::GPUWork2D) =
+    fivocheck(ccall((:fivo_ctx_clone_state, LIBFIVO2D), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), dst.h, src.h),
+              "fivo_ctx_clone_state")
+
+"""Per-kernel-class CUDA-event times (fivo_kernel_times): classes prim_fast, prim_slow,
+faces, update, adm_slow, relax, other."""
+struct FivoKernelTimes
+    launches::NTuple{8,Int64}; ms::NTuple{8,Float64}; units::NTuple{8,Int64}; total_launches::Int64
+end
+
+profile!(w::GPUWork2D, on::Bool) =
+    fivocheck(ccall((:fivo_profile, LIBFIVO2D), Cint, (Ptr{Cvoid}, Cint), w.h, Cint(on)), "fivo_profile")
+
+function kernel_times(w::GPUWork2D; reset::Bool = false)
+    kt = Ref{FivoKernelTimes}()
+    fivocheck(ccall((:fivo_profile_read, LIBFIVO2D), Cint, (Ptr{Cvoid}, Ref{FivoKernelTimes}, Cint),
+                    w.h, kt, Cint(reset)), "fivo_profile_read")
+    return kt[]
+end
