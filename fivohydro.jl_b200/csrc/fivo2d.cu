@@ -13,9 +13,11 @@
  */
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "kernels.cuh"
@@ -132,6 +134,8 @@ struct fivo_ctx {
   DevFlags* fl = nullptr;
   DevFlags* flh = nullptr;    /* pinned mirror */
   double* dU = nullptr;       /* lazily allocated RHS planes for fivo_rhs */
+  double* part = nullptr;     /* per-warp partial sums of the run diagnostics */
+  cudaEvent_t ev_sync = nullptr;   /* set: waits block the host thread (batch workers) */
   double* fh = nullptr;       /* face fluxes: x faces then y faces, nv planes each */
   unsigned int* queues = nullptr;  /* deferred recoveries | deferred admissibility tests */
   int nsm = 148;
@@ -193,7 +197,13 @@ void prof_flush(fivo_ctx* c) {
 }
 
 cudaError_t ctx_sync(fivo_ctx* c) {
-  cudaError_t e = cudaStreamSynchronize(c->st);
+  cudaError_t e;
+  if (c->ev_sync) {   /* blocking wait: the host thread sleeps instead of spinning */
+    e = cudaEventRecord(c->ev_sync, c->st);
+    if (e == cudaSuccess) e = cudaEventSynchronize(c->ev_sync);
+  } else {
+    e = cudaStreamSynchronize(c->st);
+  }
   if (e == cudaSuccess) prof_flush(c);
   return e;
 }
@@ -472,8 +482,11 @@ int diag(fivo_ctx* c, bool want_u, double* sumD, double* maxu, double* minPtot) 
   const DevParams& d = c->dp;
   int rc = reset_flags(c, 8);
   if (rc) return rc;
-  KTimer t_(c, FIVO_KCLASS_OTHER);
-  k_diag<<<nblk((long long)d.Nx * d.Ny, 256), 256, 0, c->st>>>(d, c->S[c->iU], c->w, c->fl, want_u ? 1 : 0);
+  const long long nwarps = (long long)nblk((long long)d.Nx * d.Ny, 256) * 8;
+  KTimer t_(c, FIVO_KCLASS_OTHER, 2);
+  k_diag<<<nblk((long long)d.Nx * d.Ny, 256), 256, 0, c->st>>>(d, c->S[c->iU], c->w, c->fl, want_u ? 1 : 0, c->part);
+  CKL();
+  k_sum_parts<<<1, 256, 0, c->st>>>(c->part, nwarps, &c->fl->sumD);
   CKL();
   CK(cudaMemcpyAsync(c->flh, c->fl, sizeof(DevFlags), cudaMemcpyDeviceToHost, c->st));
   CK(ctx_sync(c));
@@ -543,7 +556,8 @@ int fivo_ctx_create(const fivo_params* p, int nx, int ny, int nghost, double xma
       cudaMalloc(&c->fl, sizeof(DevFlags)) != cudaSuccess ||
       cudaMalloc(&c->stage, (size_t)d.nv * N * 8) != cudaSuccess ||
       cudaMalloc(&c->fh, 2 * (size_t)d.nv * N * 8) != cudaSuccess ||
-      cudaMalloc(&c->queues, 2 * N * sizeof(unsigned int)) != cudaSuccess)
+      cudaMalloc(&c->queues, 2 * N * sizeof(unsigned int)) != cudaSuccess ||
+      cudaMalloc(&c->part, (size_t)nblk((long long)d.Nx * d.Ny, 256) * 8 * sizeof(double)) != cudaSuccess)
     return cleanup(fail(FIVO_ERR_NOMEM, "device allocation failed"));
   if (cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess || c->nsm < 1)
     c->nsm = 148;
@@ -576,9 +590,10 @@ int fivo_ctx_destroy(fivo_ctx* c) {
   for (auto& q : c->pend) { cudaEventDestroy(q.a); cudaEventDestroy(q.b); }
   for (auto e : c->pool) cudaEventDestroy(e);
   cudaFree(c->slab); cudaFree(c->pbuf); cudaFree(c->hbuf); cudaFree(c->masks); cudaFree(c->fl);
-  cudaFree(c->dU); cudaFree(c->stage); cudaFree(c->fh); cudaFree(c->queues);
+  cudaFree(c->dU); cudaFree(c->stage); cudaFree(c->fh); cudaFree(c->queues); cudaFree(c->part);
   if (c->flh) cudaFreeHost(c->flh);
   if (c->own_st) cudaStreamDestroy(c->own_st);
+  if (c->ev_sync) cudaEventDestroy(c->ev_sync);
   delete c;
   return FIVO_OK;
 }
@@ -1112,4 +1127,107 @@ extern "C" int fivo_rhs_noalloc(const fivo_params* p, int nx, int ny, double xma
   CK(cudaStreamSynchronize(st));
   std::memcpy(amax, &bits, 8);
   return FIVO_OK;
+}
+
+/* ------------------------------------------------------------------------
+ * Batches of events (event-by-event hydro: many independent events, uneven
+ * grids). Each event is a context with its own stream; a pool of host threads
+ * drives them, so the kernels of different events run on the GPU at the same
+ * time and the latency-bound passes of one event overlap the work of others.
+ * Events share the model parameters; each has its own grid, dt and control
+ * flow, exactly as separate run_sim_2d! calls.
+ * ---------------------------------------------------------------------- */
+struct fivo_batch {
+  std::vector<fivo_ctx*> ev;
+  int nworkers = 1;
+  int device = 0;
+};
+
+int fivo_batch_create(const fivo_params* p, int nevents, const int* nx, const int* ny, const double* xmax,
+                      const double* ymax, int nghost, int nworkers, fivo_batch** out) {
+  if (!p || !nx || !ny || !xmax || !ymax || !out) return fail(FIVO_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (nevents < 1) return fail(FIVO_ERR_ARG, "fivo_batch_create: nevents must be >= 1");
+  fivo_batch* b = new fivo_batch();
+  if (cudaGetDevice(&b->device) != cudaSuccess) { delete b; return fail(FIVO_ERR_CUDA, "no CUDA device"); }
+  b->nworkers = nworkers > 0 ? std::min(nworkers, nevents) : std::min(nevents, 32);
+  for (int k = 0; k < nevents; ++k) {
+    fivo_ctx* c = nullptr;
+    int rc = fivo_ctx_create(p, nx[k], ny[k], nghost, xmax[k], ymax[k], &c);
+    if (rc == FIVO_OK && cudaEventCreateWithFlags(&c->ev_sync, cudaEventBlockingSync | cudaEventDisableTiming) !=
+                             cudaSuccess)
+      rc = fail(FIVO_ERR_CUDA, "event creation failed");
+    if (rc != FIVO_OK) {
+      std::string msg = "event " + std::to_string(k) + ": " + g_err;
+      if (c) fivo_ctx_destroy(c);
+      fivo_batch_destroy(b);
+      return fail(rc, msg);
+    }
+    b->ev.push_back(c);
+  }
+  *out = b;
+  return FIVO_OK;
+}
+
+int fivo_batch_destroy(fivo_batch* b) {
+  if (!b) return FIVO_OK;
+  for (fivo_ctx* c : b->ev) fivo_ctx_destroy(c);
+  delete b;
+  return FIVO_OK;
+}
+
+int fivo_batch_event(fivo_batch* b, int k, fivo_ctx** ctx) {
+  if (!b || !ctx) return fail(FIVO_ERR_ARG, "null argument");
+  if (k < 0 || k >= (int)b->ev.size()) return fail(FIVO_ERR_ARG, "fivo_batch_event: index out of range");
+  *ctx = b->ev[k];
+  return FIVO_OK;
+}
+
+namespace {
+/* run fn(k) for every event on the batch's worker threads; per-event status
+ * and message; returns the first failing event's status */
+template <class F>
+int batch_for_each(fivo_batch* b, int* status, F fn) {
+  const int n = (int)b->ev.size();
+  std::vector<int> st(n, FIVO_OK);
+  std::vector<std::string> msg(n);
+  std::atomic<int> next{0};
+  auto worker = [&]() {
+    if (cudaSetDevice(b->device) != cudaSuccess) return;
+    for (;;) {
+      int k = next.fetch_add(1);
+      if (k >= n) break;
+      st[k] = fn(k);
+      if (st[k] != FIVO_OK) msg[k] = g_err;
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < b->nworkers; ++t) pool.emplace_back(worker);
+  worker();
+  for (auto& t : pool) t.join();
+  int first = -1;
+  for (int k = 0; k < n; ++k) {
+    if (status) status[k] = st[k];
+    if (st[k] != FIVO_OK && first < 0) first = k;
+  }
+  if (next.load() < n) return fail(FIVO_ERR_CUDA, "fivo_batch: a worker could not select the device");
+  if (first >= 0) return fail(st[first], "event " + std::to_string(first) + ": " + msg[first]);
+  return FIVO_OK;
+}
+}  // namespace
+
+int fivo_batch_run(fivo_batch* b, double tau0, double taufinal, double cfl, double cfltau, int integrator, int bc,
+                   int64_t max_steps, int reset_hist, fivo_run_result* results, int* status) {
+  if (!b || !results) return fail(FIVO_ERR_ARG, "null argument");
+  return batch_for_each(b, status, [&](int k) {
+    return fivo_run(b->ev[k], tau0, taufinal, cfl, cfltau, integrator, bc, max_steps, reset_hist, &results[k]);
+  });
+}
+
+int fivo_batch_advance(fivo_batch* b, const double* tau, double taufinal, double cfl, double cfltau, int integrator,
+                       int bc, int64_t max_steps, fivo_run_result* results, int* status) {
+  if (!b || !tau || !results) return fail(FIVO_ERR_ARG, "null argument");
+  return batch_for_each(b, status, [&](int k) {
+    return fivo_advance(b->ev[k], tau[k], taufinal, cfl, cfltau, integrator, bc, max_steps, &results[k]);
+  });
 }

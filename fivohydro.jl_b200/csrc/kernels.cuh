@@ -907,7 +907,7 @@ __global__ void k_soa_to_aos(DevState U, double* aos, int nv, long long n) {
 }
 
 /* run_sim_2d! diagnostics over the interior (main2D.jl:421-426, 542-556) */
-__global__ void k_diag(DevParams d, DevState U, DevPrims w, DevFlags* fl, int want_u) {
+__global__ void k_diag(DevParams d, DevState U, DevPrims w, DevFlags* fl, int want_u, double* part) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double sD = 0.0, mu = 0.0, mp = inf_();
   if (t < (long long)d.Nx * d.Ny) {
@@ -925,7 +925,8 @@ __global__ void k_diag(DevParams d, DevState U, DevPrims w, DevFlags* fl, int wa
     mp = jmin(mp, __shfl_xor_sync(0xffffffffu, mp, o));
   }
   if ((threadIdx.x & 31) == 0) {
-    atomicAdd(&fl->sumD, sD);
+    /* the sum is finished by k_sum_parts in a fixed order, so it repeats exactly */
+    part[t >> 5] = sD;
     if (want_u) {
       atomic_max_pos((unsigned long long*)&fl->maxu, mu);
       /* minPtot: min over positive and negative values via a CAS loop */
@@ -938,6 +939,20 @@ __global__ void k_diag(DevParams d, DevState U, DevPrims w, DevFlags* fl, int wa
       }
     }
   }
+}
+
+/* sum of the per-warp partial sums of k_diag in a fixed order (one block) */
+__global__ void k_sum_parts(const double* part, long long n, double* out) {
+  __shared__ double red[256];
+  double acc = 0.0;
+  for (long long k = threadIdx.x; k < n; k += blockDim.x) acc += part[k];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = red[0];
 }
 
 /* one-shot helpers for the C ABI's batched entry points */

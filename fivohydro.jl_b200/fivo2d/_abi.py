@@ -109,6 +109,14 @@ SIGNATURES = {
     "fivo_ctx_destroy": (C.c_int, [C.c_void_p]),
     "fivo_ctx_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int64), _D]),
     "fivo_ctx_clone_state": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "fivo_batch_create": (C.c_int, [C.POINTER(FivoParams), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _D, _D,
+                                    C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "fivo_batch_destroy": (C.c_int, [C.c_void_p]),
+    "fivo_batch_event": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "fivo_batch_run": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
+                                 C.c_int64, C.c_int, C.POINTER(FivoRunResult), C.POINTER(C.c_int)]),
+    "fivo_batch_advance": (C.c_int, [C.c_void_p, _D, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
+                                     C.c_int64, C.POINTER(FivoRunResult), C.POINTER(C.c_int)]),
     "fivo_upload_state": (C.c_int, [C.c_void_p, _D, C.c_int, _I64]),
     "fivo_download_state": (C.c_int, [C.c_void_p, _D, C.c_int, _I64]),
     "fivo_upload_history": (C.c_int, [C.c_void_p, _I64] + [_D] * 8),

@@ -49,19 +49,23 @@ PRIMS = ("yT", "phi", "mu", "alpha", "ux", "uy", "P", "n", "e")
 class GPUWork2D:
     """A device-resident Work2D for one (grid, model) pair."""
 
-    def __init__(self, model: IdealDiffVisc2DModel, g: Grid2D, lib=None):
+    def __init__(self, model: IdealDiffVisc2DModel, g: Grid2D, lib=None, _handle=None):
         self.lib = lib or A.load_library()
         self.model, self.g = model, g
         self.nv, self.N = model.nv, g.Ntot
+        self._owned = _handle is None
+        if _handle is not None:          # an event of a GPUBatch2D: the batch owns the context
+            self.h = _handle
+            return
         h = C.c_void_p()
         A.check(self.lib, self.lib.fivo_ctx_create(C.byref(model.params), g.Nx, g.Ny, g.nghost, g.xmax,
                                                    g.ymax, C.byref(h)), "fivo_ctx_create")
         self.h = h
 
     def close(self):
-        if getattr(self, "h", None) and self.h.value:
+        if getattr(self, "h", None) and self.h.value and getattr(self, "_owned", True):
             self.lib.fivo_ctx_destroy(self.h)
-            self.h = C.c_void_p()
+        self.h = C.c_void_p()
 
     def __del__(self):
         try:
@@ -166,6 +170,68 @@ class GPUWork2D:
     def clone_state_from(self, other: "GPUWork2D"):
         """Make this work object's next steps bitwise those of `other` (same model and grid)."""
         self._ck(self.lib.fivo_ctx_clone_state(self.h, other.h), "fivo_ctx_clone_state")
+
+
+class GPUBatch2D:
+    """Many independent events (one model, uneven grids) advanced together: one
+    device context per event on its own stream, driven by `nworkers` host
+    threads inside the library (fivo_batch_*). `events[k]` is event k's
+    GPUWork2D (for its initial condition and readout); `run` and `advance` are
+    run_sim_2d! and its loop body on every event at once."""
+
+    def __init__(self, model: IdealDiffVisc2DModel, grids, nworkers=0, lib=None):
+        self.lib = lib or A.load_library()
+        self.model, self.grids = model, list(grids)
+        n = len(self.grids)
+        nx = (C.c_int * n)(*[g.Nx for g in self.grids])
+        ny = (C.c_int * n)(*[g.Ny for g in self.grids])
+        xm = (C.c_double * n)(*[g.xmax for g in self.grids])
+        ym = (C.c_double * n)(*[g.ymax for g in self.grids])
+        h = C.c_void_p()
+        A.check(self.lib, self.lib.fivo_batch_create(C.byref(model.params), n, nx, ny, xm, ym, self.grids[0].nghost,
+                                                     int(nworkers), C.byref(h)), "fivo_batch_create")
+        self.h = h
+        self.events = []
+        for k, g in enumerate(self.grids):
+            ck = C.c_void_p()
+            A.check(self.lib, self.lib.fivo_batch_event(self.h, k, C.byref(ck)), "fivo_batch_event")
+            self.events.append(GPUWork2D(model, g, lib=self.lib, _handle=ck))
+
+    def __len__(self):
+        return len(self.grids)
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            for e in self.events:
+                e.h = C.c_void_p()
+            self.lib.fivo_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _results(self, res, st):
+        return [dict(r.as_dict(), status=int(s)) for r, s in zip(res, st)]
+
+    def run(self, tau0, taufinal, cfl=0.2, cfltau=0.05, integrator=A.FIVO_SSPRK2, bc=A.FIVO_BC_OUTFLOW,
+            max_steps=10**9, reset_history=True):
+        n = len(self)
+        res, st = (A.FivoRunResult * n)(), (C.c_int * n)()
+        A.check(self.lib, self.lib.fivo_batch_run(self.h, tau0, taufinal, cfl, cfltau, integrator, bc, max_steps,
+                                                  int(reset_history), res, st), "fivo_batch_run")
+        return self._results(res, st)
+
+    def advance(self, taus, taufinal, cfl=0.2, cfltau=0.05, integrator=A.FIVO_SSPRK2, bc=A.FIVO_BC_OUTFLOW,
+                max_steps=1):
+        n = len(self)
+        t = (C.c_double * n)(*[float(x) for x in taus])
+        res, st = (A.FivoRunResult * n)(), (C.c_int * n)()
+        A.check(self.lib, self.lib.fivo_batch_advance(self.h, t, taufinal, cfl, cfltau, integrator, bc, max_steps,
+                                                      res, st), "fivo_batch_advance")
+        return self._results(res, st)
 
 
 def set_cells(model: IdealDiffVisc2DModel, tau, T, alpha, ux, uy, *, Pi=None, pixx=None, pixy=None,

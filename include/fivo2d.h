@@ -312,6 +312,28 @@ int  fivo_cons_to_prim(const fivo_params* p, int64_t n, double tau,
 int  fivo_rhs_noalloc(const fivo_params* p, int nx, int ny, double xmax, double ymax,
                       double tau, int bc, double* U, double* dU, double* amax, void* stream);
 
+/* --- batches of events (event-by-event hydro, uneven grids) ---
+ * One context per event (same model, own grid), each on its own stream, driven
+ * by nworkers host threads (<= 0: min(nevents, 32)); their waits block instead
+ * of spinning. Event k's context (fivo_batch_event) takes the usual calls:
+ * fivo_set_cells/fivo_upload_state for its IC, fivo_download_state, ... The
+ * run and advance calls are run_sim_2d! and its loop body on every event at
+ * once; results[k] and status[k] (may be NULL) are event k's. A run's outcome
+ * per event is bitwise that of a separate fivo_run on the same context.
+ * The reference has no batch driver (a Julia user loops over run_sim_2d!). */
+typedef struct fivo_batch fivo_batch;
+int  fivo_batch_create(const fivo_params* p, int nevents, const int* nx, const int* ny,
+                       const double* xmax, const double* ymax, int nghost, int nworkers,
+                       fivo_batch** out);
+int  fivo_batch_destroy(fivo_batch* b);
+int  fivo_batch_event(fivo_batch* b, int k, fivo_ctx** ctx);
+int  fivo_batch_run(fivo_batch* b, double tau0, double taufinal, double CFL, double CFLtau,
+                    int integrator, int bc, int64_t max_steps, int reset_history,
+                    fivo_run_result* results, int* status);
+int  fivo_batch_advance(fivo_batch* b, const double* tau, double taufinal, double CFL,
+                        double CFLtau, int integrator, int bc, int64_t max_steps,
+                        fivo_run_result* results, int* status);
+
 /* --- streams, synchronisation, timing --- */
 int  fivo_sync(fivo_ctx* ctx);
 /* Run the context's later calls on a caller's CUDA stream (a cudaStream_t of

@@ -1,0 +1,110 @@
+"""Batches of events (fivo_batch_*): many independent events of uneven grid
+sizes advanced together, one context and stream per event, driven by the
+library's worker threads.
+
+The batch is a scheduling layer only: every event's run must equal, to the bit,
+the same event run alone through fivo_run (and, for one of them, the oracle).
+Grid sizes follow the event-by-event workload: the box half-width scales with N
+so that dx = 30/384 fm for every event.
+"""
+import numpy as np
+import pytest
+
+import _oracle as O
+import fivo2d
+from fivo2d import _abi as A
+from fivo2d import ic
+from fivo2d.solver import GPUBatch2D, GPUWork2D, set_cells
+
+pytestmark = pytest.mark.gpu
+
+DX = 30.0 / 384.0
+
+
+def bits_equal(a, b):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    same = a.view(np.int64) == b.view(np.int64)
+    return bool(np.all(same | (np.isnan(a) & np.isnan(b))))
+
+
+def _model():
+    return fivo2d.build_model_2d(eos=fivo2d.LatticeHRGEOS(), enable_shear=True, enable_bulk=True,
+                                 enable_diff=True, eta_over_s=0.16, tauShear_coeff=0.2, zeta_over_s=0.05,
+                                 bulk_model="gaussian", bulk_T0=0.180, bulk_width=0.024, kappa_coeff=0.5)
+
+
+def _events(sizes, tau0=0.6, seed0=1001):
+    m = _model()
+    grids, states = [], []
+    for k, (nx, ny) in enumerate(sizes):
+        g = fivo2d.make_grid2d(nx, ny, xmax=nx * DX / 2, ymax=ny * DX / 2)
+        T, a, ux, uy, _ = ic.glauber_fields(g, tau0, seed0 + k)
+        U, _ = set_cells(m, tau0, T, a, ux, uy)
+        grids.append(g)
+        states.append(U)
+    return m, grids, states
+
+
+def test_batch_run_equals_single_runs(gpu_lib):
+    sizes = [(24, 24), (40, 32), (32, 48), (56, 56)]
+    m, grids, states = _events(sizes)
+    b = GPUBatch2D(m, grids, nworkers=3, lib=gpu_lib)
+    for e, U in zip(b.events, states):
+        e.set_state(U)
+        e.finalize_ic(0.6)
+    rb = b.run(0.6, 1.4, 0.2, 0.05, A.FIVO_SSPRK3, max_steps=12)
+    for k, (g, U) in enumerate(zip(grids, states)):
+        w = GPUWork2D(m, g, lib=gpu_lib)
+        w.set_state(U)
+        w.finalize_ic(0.6)
+        rw = w.run(0.6, 1.4, 0.2, 0.05, A.FIVO_SSPRK3, max_steps=12)
+        assert rb[k]["status"] == A.FIVO_OK
+        for key in ("ok", "tau", "nsteps", "nprimfail", "nvacuum", "maxu", "max_shear_res", "dQ"):
+            assert rb[k][key] == rw[key] or (np.isnan(rb[k][key]) and np.isnan(rw[key])), (k, key)
+        assert bits_equal(b.events[k].get_state(), w.get_state()), k
+        hb, hw = b.events[k].get_history(), w.get_history()
+        for name in hb:
+            assert bits_equal(hb[name], hw[name]), (k, name)
+        w.close()
+    # and one event against the oracle
+    o = O.OracleSolver(m, grids[1])
+    o.set_state(states[1])
+    o.finalize_ic(0.6)
+    ro = o.run(0.6, 1.4, 0.2, 0.05, A.FIVO_SSPRK3, max_steps=12)
+    assert ro["tau"] == rb[1]["tau"] and ro["nsteps"] == rb[1]["nsteps"]
+    assert bits_equal(o.get_state(), b.events[1].get_state())
+    b.close()
+
+
+def test_batch_advance_in_chunks(gpu_lib):
+    """fivo_batch_advance step by step (per-event tau) equals one batch run."""
+    sizes = [(24, 32), (36, 36), (28, 20)]
+    m, grids, states = _events(sizes, seed0=1101)
+    ba = GPUBatch2D(m, grids, nworkers=2, lib=gpu_lib)
+    bb = GPUBatch2D(m, grids, nworkers=2, lib=gpu_lib)
+    for bt in (ba, bb):
+        for e, U in zip(bt.events, states):
+            e.set_state(U)
+            e.finalize_ic(0.6)
+            e.rhs(0.6)
+    taus = [0.6] * len(sizes)
+    for _ in range(5):
+        r = ba.advance(taus, 10.0, 0.2, 0.05, A.FIVO_SSPRK3, max_steps=1)
+        assert all(x["ok"] and x["nsteps"] == 1 for x in r)
+        taus = [x["tau"] for x in r]
+    r5 = bb.advance([0.6] * len(sizes), 10.0, 0.2, 0.05, A.FIVO_SSPRK3, max_steps=5)
+    for k in range(len(sizes)):
+        assert r5[k]["tau"] == taus[k]
+        assert bits_equal(ba.events[k].get_state(), bb.events[k].get_state())
+    ba.close()
+    bb.close()
+
+
+def test_batch_rejects_bad_event(gpu_lib):
+    m = _model()
+    grids = [fivo2d.make_grid2d(24, 24, xmax=1.0, ymax=1.0), fivo2d.make_grid2d(24, 24, xmax=1.0, ymax=1.0)]
+    grids[1].Nx = 4                                      # make_grid2d refuses N <= 8; so must the library
+    with pytest.raises(A.FivoError) as e:
+        GPUBatch2D(m, grids, lib=gpu_lib)
+    assert "event 1" in str(e.value)
