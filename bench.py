@@ -336,6 +336,109 @@ def run_gpu(args):
     return line
 
 
+# ----------------------------------------------------------------------------- event batches
+
+def run_batch(args):
+    """The event-by-event workload: args.events seeded MC-Glauber events with N drawn
+    from {96, 128, 192, 256, 320, 400} (dx = 30/384 fm), split over the ranks by cell
+    count; each rank advances its share with the batch API (one stream per event,
+    library worker threads). Not the default line: the headline config is the single
+    384^2 event."""
+    import torch
+
+    from fivo2d import _abi as A
+    from fivo2d.events import event_grids, shard_events
+    from fivo2d.solver import GPUBatch2D, set_cells
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    lib = A.load_library()
+    _, m = model_and_grid()
+    grids = event_grids(args.events)
+    mine = shard_events([g.Nx * g.Ny for g in grids], world, rank)
+    my_grids = [grids[k] for k in mine]
+    b = GPUBatch2D(m, my_grids, nworkers=args.workers, lib=lib)
+    for e, k in zip(b.events, mine):
+        T, a, ux, uy = ic_fields(grids[k], 1000 + k)
+        U, _ = set_cells(m, TAU0, T, a, ux, uy, lib=lib)
+        e.set_state(U)
+        e.finalize_ic(TAU0)
+        e.rhs(TAU0)
+    taus = [TAU0] * len(mine)
+
+    def adv(n):
+        nonlocal taus
+        r = b.advance(taus, 1e9, CFL, CFLTAU, A.FIVO_SSPRK3, max_steps=n)
+        if not all(x["ok"] and x["nsteps"] == n for x in r):
+            raise RuntimeError("a batch event failed a step")
+        taus = [x["tau"] for x in r]
+
+    adv(args.warmup)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    adv(args.steps)          # returns when every event's stream has finished
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    cells = sum(g.Nx * g.Ny for g in my_grids)
+    t = torch.tensor([dt, float(cells)], dtype=torch.float64, device="cuda")
+    if dist:
+        tmax = t[:1].clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        csum = t[1:].clone()
+        dist.all_reduce(csum, op=dist.ReduceOp.SUM)
+        dt, cells_all = float(tmax.item()), float(csum.item())
+    else:
+        cells_all = float(cells)
+    value = args.steps * cells_all / dt
+    # end to end: the host holds every event's state; each step uploads, advances, downloads
+    hosts = [e.get_state() for e in b.events]
+    e2e_steps = max(1, min(args.steps, 5))
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for e, U in zip(b.events, hosts):
+            e.set_state(U)
+        adv(1)
+        hosts = [e.get_state() for e in b.events]
+    torch.cuda.synchronize()
+    e2e_dt = time.perf_counter() - t0
+    t = torch.tensor([e2e_dt], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e = e2e_steps * cells_all / float(t.item())
+    state_bytes = sum(g.Ntot for g in my_grids) * m.nv * 8
+    b.close()
+    if dist:
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+    sizes = sorted({g.Nx for g in grids})
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded MC-Glauber events)",
+        "config": {"workload": f"batch_{args.events}_events_N{sizes[0]}-{sizes[-1]}_dx0.078125_ssprk3_lhrg",
+                   "events": args.events, "grids": [g.Nx for g in grids], "tau0": TAU0, "integrator": "ssprk3",
+                   "cfl": CFL, "cfltau": CFLTAU, "workers": args.workers, "parallelism": f"events over {world} GPUs",
+                   "timing": "host wall clock around the synchronous batch call (one stream per event)",
+                   "l2": "inputs (all events' state) larger than L2"},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
+                "steps": e2e_steps},
+    }
+
+
 # ----------------------------------------------------------------------------- CPU legs
 
 def oracle_event():
@@ -404,11 +507,20 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=30)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="event", choices=["event", "batch"],
+                    help="event: the 384^2 viscous event (default); batch: many uneven events")
+    ap.add_argument("--events", type=int, default=32, help="batch workload: number of events")
+    ap.add_argument("--workers", type=int, default=0, help="batch workload: host threads (0: library default)")
     args = ap.parse_args()
+    if args.workload == "batch":
+        # more hardware queues for the per-event streams (read when CUDA initialises)
+        os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
     if args.impl == "reference":
         line = run_reference(args)
+    elif args.workload == "batch":
+        line = run_batch(args)
     else:
         line = run_gpu(args)
     if line is not None:
