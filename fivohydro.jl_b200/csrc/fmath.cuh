@@ -99,20 +99,24 @@ FX_HD double jsign(double x) {
 }
 
 FX_HD double scale2(double p, int k) {
-  if (k > 1023) { p = p * 8.98846567431158e307; k -= 1023; if (k > 1023) k = 1023; }
-  if (k < -1022) {
-    p = p * from_bits((uint64_t)(k + 1000 + 1023) << 52);
-    return p * from_bits((uint64_t)(1023 - 1000) << 52);
-  }
-  return p * from_bits((uint64_t)(k + 1023) << 52);
+  /* p * 2^k in two exact power-of-two factors, without branches: the second
+   * factor is 1.0 (an exact multiplication) in the normal range; above it the
+   * first is 2^1023, below it 2^(k+1000) and the second 2^-1000 */
+  const bool big = k > 1023, small = k < -1022;
+  int k1 = big ? 1023 : (small ? k + 1000 : k);
+  int k2 = big ? k - 1023 : (small ? -1000 : 0);
+  k2 = k2 > 1023 ? 1023 : k2;
+  double t = p * from_bits((uint64_t)(k1 + 1023) << 52);
+  return t * from_bits((uint64_t)(k2 + 1023) << 52);
 }
 
 FX_HD double fx_exp(double x) {
-  if (isnan_(x)) return x;
-  if (x > 709.782712893384) return inf_();
-  if (x < -745.1332191019412) return 0.0;
-  double kd = rint_(x * 1.4426950408889634);
-  double r = fma_(-kd, 0.6931471803691238, x);
+  /* the special cases are selected at the end, so the body is straight-line
+   * code that the scheduler can interleave with independent work */
+  const bool nan = isnan_(x), over = x > 709.782712893384, under = x < -745.1332191019412;
+  const double xs = (nan || over || under) ? 0.0 : x;
+  double kd = rint_(xs * 1.4426950408889634);
+  double r = fma_(-kd, 0.6931471803691238, xs);
   r = fma_(-kd, 1.9082149292705877e-10, r);
   double p = 1.6059043836821613e-10;
   p = fma_(p, r, 2.08767569878681e-09);
@@ -128,7 +132,8 @@ FX_HD double fx_exp(double x) {
   p = fma_(p, r, 0.5);
   p = fma_(p, r, 1.0);
   p = fma_(p, r, 1.0);
-  return scale2(p, (int)kd);
+  const double v = scale2(p, (int)kd);
+  return nan ? x : (over ? inf_() : (under ? 0.0 : v));
 }
 
 FX_HD double fx_log(double x) {
@@ -253,7 +258,8 @@ static const double FX_K0B_HOST[FX_CHEB_NB] = FX_CHEB_K0B;
 static const double FX_K1B_HOST[FX_CHEB_NB] = FX_CHEB_K1B;
 
 /* Clenshaw's recurrence for sum_k c_k T_k(u), two series at once:
- * b_k = (2u b_{k+1} - b_{k+2}) + c_k, sum = (u b_1 - b_2) + c_0. */
+ * b_k = fma(2u, b_{k+1}, c_k - b_{k+2}), sum = fma(u, b_1, c_0 - b_2): the
+ * subtraction runs beside the chain, which is one fused multiply-add per term. */
 template <int N>
 FX_HD void fx_clenshaw2(const double* c0, const double* c1, double u, double* s0, double* s1) {
   const double tu = 2.0 * u;
@@ -262,12 +268,25 @@ FX_HD void fx_clenshaw2(const double* c0, const double* c1, double u, double* s0
 #pragma unroll
 #endif
   for (int k = N - 1; k >= 1; --k) {
-    double p = ((tu * p1) - p2) + c0[k];
-    double q = ((tu * q1) - q2) + c1[k];
+    double p = fma_(tu, p1, c0[k] - p2);
+    double q = fma_(tu, q1, c1[k] - q2);
     p2 = p1; p1 = p; q2 = q1; q1 = q;
   }
-  *s0 = ((u * p1) - p2) + c0[0];
-  *s1 = ((u * q1) - q2) + c1[0];
+  *s0 = fma_(u, p1, c0[0] - p2);
+  *s1 = fma_(u, q1, c1[0] - q2);
+}
+
+/* e^x K0(x), e^x K1(x) for 2 <= x < 1e4 (piece B) */
+FX_HD void fx_k01x_B(double x, double* k0x, double* k1x) {
+  double g0, g1;
+#ifdef __CUDA_ARCH__
+  fx_clenshaw2<FX_CHEB_NB>(FX_K0B_DEV, FX_K1B_DEV, (4.0 / x) - 1.0, &g0, &g1);
+#else
+  fx_clenshaw2<FX_CHEB_NB>(FX_K0B_HOST, FX_K1B_HOST, (4.0 / x) - 1.0, &g0, &g1);
+#endif
+  double rs = 1.0 / sqrt_(x);
+  *k0x = g0 * rs;
+  *k1x = g1 * rs;
 }
 
 /* e^x K0(x), e^x K1(x) for 0 < x < 1e4 */
@@ -307,15 +326,7 @@ FX_HD void fx_k01x(double x, double* k0x, double* k1x) {
 #endif
     return;
   }
-  double g0, g1;
-#ifdef __CUDA_ARCH__
-  fx_clenshaw2<FX_CHEB_NB>(FX_K0B_DEV, FX_K1B_DEV, (4.0 / x) - 1.0, &g0, &g1);
-#else
-  fx_clenshaw2<FX_CHEB_NB>(FX_K0B_HOST, FX_K1B_HOST, (4.0 / x) - 1.0, &g0, &g1);
-#endif
-  double rs = 1.0 / sqrt_(x);
-  *k0x = g0 * rs;
-  *k1x = g1 * rs;
+  fx_k01x_B(x, k0x, k1x);
 }
 
 /* the reference's asymptotic series (safe_besselkx, src/eos.jl:30-33) */

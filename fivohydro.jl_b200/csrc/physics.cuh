@@ -111,7 +111,8 @@ FX_HD void light_eos(double T, const DevParams& d, double* P, double* dP, double
 /* _lhrg_assemble_2d, src2d/primrec2d.jl:134-154 */
 FX_HD void lhrg_assemble(double T, double mu, const DevParams& d, double x, double Pl, double el,
                          double K2x, double* P, double* n, double* en) {
-  if (!isfinite_(x) || x <= 0.0) { *P = Pl; *n = 0.0; *en = el; return; }
+  /* computed unconditionally and selected, so it has no branch */
+  const bool off = !isfinite_(x) || x <= 0.0;
   double m = d.p.m_hq;
   double z = (mu - m) / T;
   z = jclamp(z, -700.0, 700.0);
@@ -119,11 +120,25 @@ FX_HD void lhrg_assemble(double T, double mu, const DevParams& d, double x, doub
   double n_hq = ((d.A_lhrg * T) * Efac) * K2x;
   double P_hq = 0.0, e_hq = 0.0;
   if (d.p.hq_times_fmGeV3) { n_hq *= d.fmgev3; P_hq *= d.fmgev3; e_hq *= d.fmgev3; }
-  *P = Pl + P_hq; *n = n_hq; *en = el + e_hq;
+  *P = off ? Pl : Pl + P_hq;
+  *n = off ? 0.0 : n_hq;
+  *en = off ? el : el + e_hq;
 }
 
 FX_HD double lhrg_x(double T, const DevParams& d) { return jmin(d.p.m_hq / T, 100000.0); }
-FX_HD double lhrg_K2(double x) { return (!isfinite_(x) || x <= 0.0) ? 0.0 : fx_besselk2x(x); }
+/* e^x K2(x) as the LatticeHRG charm density uses it (0 off the domain). The
+ * usual range 2 <= x < 1e4 (0.15 < T < 750 MeV) is straight-line code on a
+ * clamped argument, so it interleaves with the light-sector EOS; the rest of
+ * the domain goes through the general function. Same bits either way. */
+FX_HD double lhrg_K2(double x) {
+  const bool common = x >= 2.0 && x < 1.0e4;
+  const double xc = common ? x : 2.0;
+  double k0, k1;
+  fx_k01x_B(xc, &k0, &k1);
+  double v = k0 + (2.0 / xc) * k1;
+  if (!common) v = (!isfinite_(x) || x <= 0.0) ? 0.0 : fx_besselk2x(x);
+  return v;
+}
 
 /* ConformalHQEOS eos_Pne, src/eos.jl:53-84. A == 0 (g_hq = 0) skips the Bessel
  * functions: the HQ terms are then 0 * (finite) or NaN when exp overflows. */
@@ -291,6 +306,25 @@ struct Recovery {
   uint8_t ok, reason;
 };
 
+/* the residual rows of evalF_2d! from the EOS values (src2d/primrec2d.jl:375-389);
+ * a non-finite EOS value makes every row inf (selected, not branched) */
+template <bool NCH>
+FX_HD void evalF_rows(double F[4], double P, double n, double en, double ux, double uy, double ut,
+                      const CellCons& c) {
+  const bool bad = !(isfinite_(P) && isfinite_(n) && isfinite_(en));
+  double weff = (en + P) + c.Pi;
+  double Ptot = P + c.Pi;
+  PiC pc = shear_tensor(ux, uy, ut, c.pixx, c.pixy, c.piyy);
+  const double f0 = NCH ? (((n * ut) + nu_tau(ux, uy, ut, c.nux, c.nuy)) - c.D) : 0.0;
+  const double f1 = (((weff * ut) * ux) + pc.tx) - c.Sx;
+  const double f2 = (((weff * ut) * uy) + pc.ty) - c.Sy;
+  const double f3 = ((((weff * ut) * ut) - Ptot) + pc.tt) - c.E;
+  F[0] = bad ? inf_() : f0;
+  F[1] = bad ? inf_() : f1;
+  F[2] = bad ? inf_() : f2;
+  F[3] = bad ? inf_() : f3;
+}
+
 /* evalF_2d!, src2d/primrec2d.jl:360-390 */
 template <int EOS, bool NCH>
 FX_HD void evalF(double F[4], const double x[4], const CellCons& c, const DevParams& d, EosMemo& memo) {
@@ -303,14 +337,7 @@ FX_HD void evalF(double F[4], const double x[4], const CellCons& c, const DevPar
   double ut = utau(ux, uy);
   double P, n, en;
   eos_Pne_memo<EOS>(T, mu, d, memo, &P, &n, &en);
-  if (!(isfinite_(P) && isfinite_(n) && isfinite_(en))) { F[0] = F[1] = F[2] = F[3] = inf_(); return; }
-  double weff = (en + P) + c.Pi;
-  double Ptot = P + c.Pi;
-  PiC pc = shear_tensor(ux, uy, ut, c.pixx, c.pixy, c.piyy);
-  F[0] = NCH ? (((n * ut) + nu_tau(ux, uy, ut, c.nux, c.nuy)) - c.D) : 0.0;
-  F[1] = (((weff * ut) * ux) + pc.tx) - c.Sx;
-  F[2] = (((weff * ut) * uy) + pc.ty) - c.Sy;
-  F[3] = ((((weff * ut) * ut) - Ptot) + pc.tt) - c.E;
+  evalF_rows<NCH>(F, P, n, en, ux, uy, ut, c);
 }
 
 FX_HD bool finite4(const double F[4]) {
@@ -647,14 +674,7 @@ FX_HD void evalF_tp(double F[4], const double x[4], double T, const CellCons& c,
   double ut = utau(ux, uy);
   double P, n, en;
   eos_tp<EOS>(T, mu, d, tp, &P, &n, &en);
-  if (!(isfinite_(P) && isfinite_(n) && isfinite_(en))) { F[0] = F[1] = F[2] = F[3] = inf_(); return; }
-  double weff = (en + P) + c.Pi;
-  double Ptot = P + c.Pi;
-  PiC pc = shear_tensor(ux, uy, ut, c.pixx, c.pixy, c.piyy);
-  F[0] = NCH ? (((n * ut) + nu_tau(ux, uy, ut, c.nux, c.nuy)) - c.D) : 0.0;
-  F[1] = (((weff * ut) * ux) + pc.tx) - c.Sx;
-  F[2] = (((weff * ut) * uy) + pc.ty) - c.Sy;
-  F[3] = ((((weff * ut) * ut) - Ptot) + pc.tt) - c.E;
+  evalF_rows<NCH>(F, P, n, en, ux, uy, ut, c);
 }
 
 /* recover_attempt from a finite warm start (x0 already clamped), with the

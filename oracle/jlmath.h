@@ -207,14 +207,15 @@ static const double O_CHEB_K1B[] = {
   -5.7567444820733025e-18};
 static const double O_EULER_GAMMA = 0.5772156649015329;
 
-/* Clenshaw: b_k = (2u b_{k+1} - b_{k+2}) + c_k for k = n-1..1; sum = (u b_1 - b_2) + c_0 */
+/* Clenshaw: b_k = fma(2u, b_{k+1}, c_k - b_{k+2}) for k = n-1..1;
+ * sum = fma(u, b_1, c_0 - b_2) (one rounding per step on the dependency chain) */
 static inline double o_clenshaw(const double* c, int n, double u) {
   double tu = 2.0 * u, b1 = 0.0, b2 = 0.0;
   for (int k = n - 1; k >= 1; --k) {
-    double b = ((tu * b1) - b2) + c[k];
+    double b = std::fma(tu, b1, c[k] - b2);
     b2 = b1; b1 = b;
   }
-  return ((u * b1) - b2) + c[0];
+  return std::fma(u, b1, c[0] - b2);
 }
 
 /* e^x K0(x), e^x K1(x) for 0 < x < 1e4 */
