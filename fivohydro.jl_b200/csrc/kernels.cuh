@@ -1061,7 +1061,7 @@ __device__ __forceinline__ void load_cons(const DevParams& d, const DevState& U,
 }
 
 template <int EOS, bool NCH>
-__global__ void __launch_bounds__(128) k_prim_fast(DevParams d, DevState U, DevPrims w, DevHist h, double tau,
+__global__ void __launch_bounds__(128, 4) k_prim_fast(DevParams d, DevState U, DevPrims w, DevHist h, double tau,
                                                    DevFlags* fl, unsigned int* queue) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   bool vac = false, defer = false;
@@ -1156,7 +1156,7 @@ __global__ void __launch_bounds__(128) k_prim_slow(DevParams d, DevState U, DevP
 
 /* one thread per face of one direction, every face of the (ghost-inclusive) grid */
 template <int EOS, bool XDIR>
-__global__ void __launch_bounds__(128) k_faces(DevParams d, DevState Ub, DevPrims w, double tau,
+__global__ void __launch_bounds__(128, 4) k_faces(DevParams d, DevState Ub, DevPrims w, double tau,
                                                const uint8_t* ffo, double* Fh, DevFlags* fl) {
   const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long nf = XDIR ? (long long)(d.Nxtot - 1) * d.Nytot : (long long)d.Nxtot * (d.Nytot - 1);
