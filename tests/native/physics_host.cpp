@@ -68,4 +68,33 @@ void ph_cons_to_prim(const fivo_params* p, long n, double tau, const double* con
     ok[i] = r.ok; reason[i] = r.reason;
   }
 }
+
+/* the fast pass's recovery (recover_fast, explicit EOS temperature parts) against the
+ * memo-based first attempt from the same finite warm start, for every cell: returns
+ * the number of cells whose results differ in any bit */
+long ph_fast_vs_attempt(const fivo_params* p, long n, double tau, const double* cons, const double* warm, int budget) {
+  DevParams d = mk(p);
+  long bad = 0;
+  for (long i = 0; i < n; ++i) {
+    const double* c = cons + 11 * i;
+    CellCons cc;
+    cc.D = c[0]; cc.Sx = c[1]; cc.Sy = c[2]; cc.E = c[3]; cc.nux = c[4]; cc.nuy = c[5]; cc.Pi = c[6];
+    cc.pixx = c[7]; cc.pixy = c[8]; cc.piyy = c[9]; cc.pieta = c[10];
+    const double* w = warm + 4 * i;
+    bool over = false;
+    Recovery a, b;
+    if (p->eos_kind == FIVO_EOS_LATTICE_HRG) {
+      a = recover_attempt<FIVO_EOS_LATTICE_HRG, true>(cc, d, w[0], w[1], w[2], w[3], p->primrec_maxit, p->primrec_tol);
+      b = recover_fast<FIVO_EOS_LATTICE_HRG, true>(cc, d, w[0], w[1], w[2], w[3], p->primrec_maxit, p->primrec_tol, budget, &over);
+    } else {
+      a = recover_attempt<FIVO_EOS_CONFORMAL_HQ, true>(cc, d, w[0], w[1], w[2], w[3], p->primrec_maxit, p->primrec_tol);
+      b = recover_fast<FIVO_EOS_CONFORMAL_HQ, true>(cc, d, w[0], w[1], w[2], w[3], p->primrec_maxit, p->primrec_tol, budget, &over);
+    }
+    if (over) continue;   /* the fast pass would defer this cell */
+    const double va[8] = {a.T, a.mu, a.ux, a.uy, a.n, a.e, a.P, a.resnorm};
+    const double vb[8] = {b.T, b.mu, b.ux, b.uy, b.n, b.e, b.P, b.resnorm};
+    if (std::memcmp(va, vb, sizeof(va)) != 0 || a.ok != b.ok || a.reason != b.reason) ++bad;
+  }
+  return bad;
+}
 }
