@@ -348,7 +348,7 @@ def run_batch(args):
 
     from fivo2d import _abi as A
     from fivo2d.events import event_grids, shard_events
-    from fivo2d.solver import GPUBatch2D, set_cells
+    from fivo2d.solver import GPUBatch2D
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -368,10 +368,7 @@ def run_batch(args):
     my_grids = [grids[k] for k in mine]
     b = GPUBatch2D(m, my_grids, nworkers=args.workers, lib=lib)
     for e, k in zip(b.events, mine):
-        T, a, ux, uy = ic_fields(grids[k], 1000 + k)
-        U, _ = set_cells(m, TAU0, T, a, ux, uy, lib=lib)
-        e.set_state(U)
-        e.finalize_ic(TAU0)
+        e.glauber_ic(TAU0, 1000 + k)      # the MC-Glauber IC built on the device
         e.rhs(TAU0)
     taus = [TAU0] * len(mine)
 

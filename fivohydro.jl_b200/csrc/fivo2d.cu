@@ -963,6 +963,71 @@ int fivo_set_cells(const fivo_params* p, int64_t ncell, double tau, const double
   return FIVO_OK;
 }
 
+int fivo_glauber_ic(fivo_ctx* c, double tau0, const double* parts, const double* weights, int64_t npart,
+                    const double* binary, int64_t nbin, double width, double Tpeak, double ncharm,
+                    double alpha_min, int bc, double* T_out, double* alpha_out) {
+  if (!c || !parts || !weights || (nbin > 0 && !binary)) return fail(FIVO_ERR_ARG, "null argument");
+  const DevParams& d = c->dp;
+  if (d.p.eos_kind != FIVO_EOS_LATTICE_HRG)
+    return fail(FIVO_ERR_CONFIG, "fivo_glauber_ic: the MC-Glauber initial condition is built for LatticeHRGEOS");
+  if (npart < 1 || nbin < 0 || !(width > 0) || !(Tpeak > 0) || !(tau0 > 0))
+    return fail(FIVO_ERR_ARG, "fivo_glauber_ic: need npart >= 1, nbin >= 0, width > 0, Tpeak > 0, tau0 > 0");
+  const long long N = d.Ntot;
+  int rc;
+  DevBuf bp, bw, bb, planes, aos, zero, okb, scal;
+  if ((rc = up(bp, parts, 2 * npart)) || (rc = up(bw, weights, npart))) return rc;
+  if (nbin > 0 && (rc = up(bb, binary, 2 * nbin))) return rc;
+  CK(cudaMalloc(&planes.p, 4 * (size_t)N * 8));
+  CK(cudaMalloc(&aos.p, (size_t)N * d.nv * 8));
+  CK(cudaMalloc(&zero.p, (size_t)N * 8));
+  CK(cudaMalloc(&okb.p, (size_t)N));
+  CK(cudaMalloc(&scal.p, 16));
+  double* s = (double*)planes.p;
+  double* nb = s + N;
+  double* T = s + 2 * N;
+  double* al = s + 3 * N;
+  unsigned long long* mx = (unsigned long long*)scal.p;
+  double* interior = (double*)scal.p + 1;
+  CK(cudaMemsetAsync(scal.p, 0, 16, c->st));
+  CK(cudaMemsetAsync(aos.p, 0, (size_t)N * d.nv * 8, c->st));
+  CK(cudaMemsetAsync(zero.p, 0, (size_t)N * 8, c->st));
+  /* e_peak: the light-sector energy density at Tpeak (the same functions on the host) */
+  double Pl, dP;
+  const double Tp = jmax(Tpeak, FV_T_MIN);
+  light_eos<3>(Tp, d, &Pl, &dP, nullptr);
+  const double e_peak = (-Pl) + (Tp * dP);
+  const long long nw = (long long)nblk(N, 256) * 8;
+  DevBuf partb;
+  CK(cudaMalloc(&partb.p, (size_t)nw * 8));
+  {
+    KTimer t_(c, FIVO_KCLASS_OTHER, 5);
+    k_glauber_deposit<<<nblk(N, 128), 128, 0, c->st>>>(d, (const double*)bp.p, (const double*)bw.p, npart, width, s);
+    CKL();
+    k_glauber_deposit<<<nblk(N, 128), 128, 0, c->st>>>(d, (const double*)bb.p, nullptr, nbin, width, nb);
+    CKL();
+    k_glauber_reduce<<<nblk(N, 256), 256, 0, c->st>>>(d, s, nb, mx, (double*)partb.p);
+    CKL();
+    k_sum_parts<<<1, 256, 0, c->st>>>((const double*)partb.p, nw, interior);
+    CKL();
+    k_glauber_fields<<<nblk(N, 128), 128, 0, c->st>>>(d, s, nb, mx, interior, e_peak, tau0, ncharm, alpha_min, T, al);
+    CKL();
+  }
+  {
+    KTimer t_(c, FIVO_KCLASS_OTHER, 2);
+    const double* z = (const double*)zero.p;
+    k_set_cells<FIVO_EOS_LATTICE_HRG><<<nblk(N, 128), 128, 0, c->st>>>(d, N, tau0, T, al, z, z, nullptr, nullptr, nullptr,
+                                                                      nullptr, nullptr, nullptr, (double*)aos.p,
+                                                                      (uint8_t*)okb.p);
+    CKL();
+    k_aos_to_soa<<<nblk(N * d.nv, 256), 256, 0, c->st>>>(c->S[c->iU], (const double*)aos.p, d.nv, N);
+    CKL();
+  }
+  if (T_out) CK(cudaMemcpyAsync(T_out, T, (size_t)N * 8, cudaMemcpyDeviceToHost, c->st));
+  if (alpha_out) CK(cudaMemcpyAsync(alpha_out, al, (size_t)N * 8, cudaMemcpyDeviceToHost, c->st));
+  CK(ctx_sync(c));
+  return fivo_finalize_ic(c, tau0, bc);
+}
+
 int fivo_eos_Pne(const fivo_params* p, int64_t n, const double* T, const double* mu, double* P, double* nq,
                  double* e) {
   if (!p || !T || !mu || !P || !nq || !e) return fail(FIVO_ERR_ARG, "null argument");

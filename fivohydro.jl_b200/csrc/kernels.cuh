@@ -941,6 +941,81 @@ __global__ void k_diag(DevParams d, DevState U, DevPrims w, DevFlags* fl, int wa
   }
 }
 
+/* ---------------------------------------------------- MC-Glauber initial condition */
+
+/* sum over point sources of w_k exp(-|x - x_k|^2 / 2 width^2) / (2 pi width^2) at every
+ * cell centre (ghosts too), in the order of the point list */
+__global__ void k_glauber_deposit(DevParams d, const double* pts, const double* wts, long long np,
+                                  double width, double* out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.Ntot) return;
+  const int ix = (int)(i / d.Nytot), iy = (int)(i % d.Nytot);
+  const double x = d.xmin + (((double)(ix + 1 - d.ng)) - 0.5) * d.dx;
+  const double y = d.ymin + (((double)(iy + 1 - d.ng)) - 0.5) * d.dy;
+  const double inv = 1.0 / ((2.0 * width) * width);
+  const double norm = 1.0 / (((2.0 * FX_PI) * width) * width);
+  double acc = 0.0;
+  for (long long k = 0; k < np; ++k) {
+    const double dxp = x - pts[2 * k], dyp = y - pts[2 * k + 1];
+    const double wk = wts ? wts[k] : 1.0;
+    acc = acc + ((wk * norm) * fx_exp((-((dxp * dxp) + (dyp * dyp))) * inv));
+  }
+  out[i] = acc;
+}
+
+/* max over every cell (into *mx, as ordered bits of a non-negative double) and the
+ * per-warp partial sums over the interior (for k_sum_parts) */
+__global__ void k_glauber_reduce(DevParams d, const double* s, const double* nb, unsigned long long* mx,
+                                 double* part) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double m = 0.0, sum = 0.0;
+  if (t < d.Ntot) {
+    m = s[t];
+    const int ix = (int)(t / d.Nytot), iy = (int)(t % d.Nytot);
+    if (ix >= d.ng && ix < d.ng + d.Nx && iy >= d.ng && iy < d.ng + d.Ny) sum = nb[t];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    m = jmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_pos(mx, m);
+    part[t >> 5] = sum;
+  }
+}
+
+/* T from e = s * (e_peak / max s) by 90-step bisection of the light-sector e(T) in
+ * log T, and alpha = log(n_target / n(T, alpha = 0)) floored at alpha_min */
+__global__ void k_glauber_fields(DevParams d, const double* s, const double* nb, const unsigned long long* mx,
+                                 const double* interior, double e_peak, double tau0, double ncharm,
+                                 double alpha_min, double* Tout, double* aout) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.Ntot) return;
+  const double smax = __longlong_as_double((long long)*mx);
+  const double e = s[i] * (e_peak / smax);
+  double lo = d.log_T_min, hi = d.log_T_solve_max;
+  for (int it = 0; it < 90; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    const double Tm = jmax(fx_exp(mid), FV_T_MIN);
+    double Pl, dP;
+    light_eos<3>(Tm, d, &Pl, &dP, nullptr);
+    const double em = (-Pl) + (Tm * dP);
+    if (em > e) hi = mid; else lo = mid;
+  }
+  const double T = jmax(fx_exp(0.5 * (lo + hi)), FV_T_MIN);
+  const double I = ((*interior) * d.dx) * d.dy;   /* the interior sum of nb times dx dy */
+  const double ntgt = I > 0.0 ? nb[i] * (ncharm / (tau0 * I)) : 0.0;
+  const double x = lhrg_x(T, d);
+  double Pl, dP;
+  light_eos<3>(T, d, &Pl, &dP, nullptr);
+  double P0, n0, e0;
+  lhrg_assemble(T, 0.0, d, x, Pl, (-Pl) + (T * dP), lhrg_K2(x), &P0, &n0, &e0);
+  double a = fx_log(ntgt / n0);
+  a = isfinite_(a) ? jmax(a, alpha_min) : alpha_min;
+  Tout[i] = T;
+  aout[i] = a;
+}
+
 /* sum of the per-warp partial sums of k_diag in a fixed order (one block) */
 __global__ void k_sum_parts(const double* part, long long n, double* out) {
   __shared__ double red[256];

@@ -167,6 +167,23 @@ class GPUWork2D:
     def sync(self):
         self._ck(self.lib.fivo_sync(self.h), "fivo_sync")
 
+    def glauber_ic(self, tau0, seed, *, Tpeak=0.450, ncharm=10.0, bmax=8.0, alpha_min=-20.0,
+                   bc=A.FIVO_BC_OUTFLOW, fields=False):
+        """The seeded MC-Glauber initial condition built on the device into this
+        context's state (fivo_glauber_ic); the nucleon sampling is ic.glauber_event's.
+        Returns (T, alpha) planes when fields=True."""
+        from .ic import SRC_WIDTH, glauber_event
+        ev = glauber_event(seed, bmax)
+        pts = np.ascontiguousarray(ev["participants"], dtype=np.float64)
+        w = np.ascontiguousarray(ev["weights"], dtype=np.float64)
+        bi = np.ascontiguousarray(ev["binary"], dtype=np.float64)
+        T = np.empty(self.N) if fields else None
+        a = np.empty(self.N) if fields else None
+        self._ck(self.lib.fivo_glauber_ic(self.h, tau0, _ptr(pts), _ptr(w), len(w), _ptr(bi) if len(bi) else None,
+                                          len(bi), SRC_WIDTH, Tpeak, ncharm, alpha_min, bc, _ptr(T), _ptr(a)),
+                 "fivo_glauber_ic")
+        return (T, a) if fields else None
+
     def clone_state_from(self, other: "GPUWork2D"):
         """Make this work object's next steps bitwise those of `other` (same model and grid)."""
         self._ck(self.lib.fivo_ctx_clone_state(self.h, other.h), "fivo_ctx_clone_state")

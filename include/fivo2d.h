@@ -287,6 +287,20 @@ int  fivo_set_cells(const fivo_params* p, int64_t ncell, double tau,
 
 /* --- equation of state (for IC builders and tests) --- */
 /* eos_Pne (src/eos.jl:53-84, 483-519) for n points. */
+/* The MC-Glauber initial condition of the event-by-event workload, built on the
+ * device into the context's state (the reference's IC builder is not public; the
+ * same construction runs on the host in fivo2d.ic.glauber_fields): Gaussian
+ * deposits of width `width` of npart participants (x, y pairs, with weights) and
+ * nbin binary collisions (x, y pairs) at every cell centre; energy density scaled
+ * so its maximum is the light-sector e(Tpeak); T by 90-step bisection of e(T);
+ * charm density proportional to the binary density with tau0 * sum(n) dx dy =
+ * ncharm over the interior; alpha = log(n / n(T, alpha = 0)) floored at alpha_min;
+ * u = 0 and no dissipative parts; then set_cell! and finalize_ic! (main2D.jl:142-171)
+ * with boundary bc. T_out, alpha_out (Ntot each, may be NULL) receive the fields.
+ * LatticeHRGEOS only. No counterpart in the reference. */
+int  fivo_glauber_ic(fivo_ctx* ctx, double tau0, const double* parts, const double* weights,
+                     int64_t npart, const double* binary, int64_t nbin, double width, double Tpeak,
+                     double ncharm, double alpha_min, int bc, double* T_out, double* alpha_out);
 int  fivo_eos_Pne(const fivo_params* p, int64_t n, const double* T, const double* mu,
                   double* P, double* nq, double* e);
 
