@@ -264,9 +264,9 @@ int launch_stage_t(fivo_ctx* c, const StageArgs& a) {
   {
     long long nfx = (long long)(d.Nxtot - 1) * d.Nytot, nfy = (long long)d.Nxtot * (d.Nytot - 1);
     KTimer t_(c, FIVO_KCLASS_FACES, 2, nfx + nfy);
-    k_faces<EOS, true><<<nblk(nfx, 128), 128, 0, c->st>>>(d, a.Ub, a.w, a.tau, a.ffo, fhx, c->fl);
+    k_faces<EOS, true><<<nblk(2 * nfx, 128), 128, 0, c->st>>>(d, a.Ub, a.w, a.tau, a.ffo, fhx, c->fl);
     CKL();
-    k_faces<EOS, false><<<nblk(nfy, 128), 128, 0, c->st>>>(d, a.Ub, a.w, a.tau, a.ffo, fhy, c->fl);
+    k_faces<EOS, false><<<nblk(2 * nfy, 128), 128, 0, c->st>>>(d, a.Ub, a.w, a.tau, a.ffo, fhy, c->fl);
     CKL();
   }
   unsigned int* aq = c->queues + d.Ntot;

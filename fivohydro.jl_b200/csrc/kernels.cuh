@@ -1229,26 +1229,120 @@ __global__ void __launch_bounds__(128) k_prim_slow(DevParams d, DevState U, DevP
   }
 }
 
-/* one thread per face of one direction, every face of the (ghost-inclusive) grid */
+/* One face, computed by a pair of lanes: lane side 0 owns the left state (cell
+ * i), side 1 the right state (cell i + st). Each lane reconstructs, maps to
+ * conserved variables (EOS with c_s^2), applies the fallbacks and evaluates the
+ * physical flux and wave speeds of its own state; the pair then exchanges them
+ * by shuffle and both lanes form the HLLE flux. The operations on each state are
+ * those of face_flux (the same expressions, the same order), so the fluxes have
+ * its bits; a lane does half the EOS work, which halves the dependent chain of a
+ * face and the registers it needs. All lanes of the warp must call it.
+ * Returns max(|sL|, |sR|); writes the flux of every row into out[]. */
 template <int EOS, bool XDIR>
-__global__ void __launch_bounds__(128, 4) k_faces(DevParams d, DevState Ub, DevPrims w, double tau,
-                                               const uint8_t* ffo, double* Fh, DevFlags* fl) {
-  const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long nf = XDIR ? (long long)(d.Nxtot - 1) * d.Nytot : (long long)d.Nxtot * (d.Nytot - 1);
-  double amax = 0.0;
-  if (f < nf) {
-    long long i;
-    int k, kmax;
-    if (XDIR) { i = f; k = (int)(f / d.Nytot); kmax = d.Nxtot; }
-    else {
-      int ix = (int)(f / (d.Nytot - 1)), iy = (int)(f % (d.Nytot - 1));
-      i = (long long)ix * d.Nytot + iy; k = iy; kmax = d.Nytot;
+__device__ __forceinline__ double face_flux_pair(const DevParams& d, const DevState& U, const DevPrims& w,
+                                                 long long i, long long st, int k, int kmax, double tau,
+                                                 const uint8_t* ffo, int side, double out[FV_MAXV]) {
+  const long long ip = i + st;
+  const long long c0 = side ? ip : i;
+  /* the two lanes of this pair; every branch below is taken by both or neither */
+  const unsigned pm = 3u << (threadIdx.x & 30);
+  const int ng = d.ng;
+  double dis[7];
+  load_dis(d, U, c0, dis);
+  const bool forced = ffo != nullptr && (ffo[i] || ffo[ip]);
+  Prim p;
+  double uc[4];
+  bool good = false, floored = false;
+  if (!forced) {
+    double v[4];
+    const double* fld[4] = {w.yT, w.phi, w.ux, w.uy};
+    const bool first = (k + 1 <= ng) || (k + 1 >= kmax - ng);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double* f = fld[q];
+      /* left: (vm, vi, vp) around vi; right: (vi, vp, vpp) around vp */
+      const double c = f[c0];
+      if (first) { v[q] = c; continue; }
+      const double a = side ? f[i] : f[i - st];
+      const double b = side ? f[ip + st] : f[ip];
+      const double sl = mc_limiter(c - a, b - c);
+      const double h = 0.5 * sl;
+      const double val = side ? c - h : c + h;
+      v[q] = jclamp(val, jmin(jmin(a, c), b), jmax(jmax(a, c), b));
     }
-    double out[FV_MAXV];
-    double a = face_flux<EOS, XDIR>(d, Ub, w, i, XDIR ? d.Nytot : 1, k, kmax, tau, ffo, out);
-    if (a > amax) amax = a;
-    for (int q = 0; q < d.nv; ++q) Fh[(size_t)q * d.Ntot + i] = out[q];
+    const double T = fx_exp(v[0]);
+    const double mu = d.p.m_hq + (T * v[1]);
+    const bool ok = prim_to_cons<EOS>(uc, p, T, mu, v[2], v[3], dis, tau, d);
+    const bool mine = ok && uc[0] >= 0.0 && uc[3] >= FV_E_FLOOR;
+    const int theirs = __shfl_xor_sync(pm, (int)mine, 1);
+    good = mine && theirs;
   }
+  if (!good) {
+    const double Tc = fx_exp(w.yT[c0]), muc = w.mu[c0];
+    const bool ok = prim_to_cons<EOS>(uc, p, Tc, muc, w.ux[c0], w.uy[c0], dis, tau, d);
+    const int theirs = __shfl_xor_sync(pm, (int)ok, 1);
+    const bool both = ok && theirs;
+    if (!both && !ok) {
+      /* _floor_prim_2d!, src2d/rhs2d.jl:259-268 */
+      floored = true;
+      uc[0] = 0.0; uc[1] = 0.0; uc[2] = 0.0; uc[3] = FV_E_FLOOR;
+      p.T = FV_T_MIN; p.mu = 0.0; p.ux = 0.0; p.uy = 0.0; p.n = 0.0; p.e = FV_E_FLOOR; p.P = 0.0;
+      p.nux = p.nuy = p.Pi = p.pixx = p.pixy = p.piyy = p.pieta = 0.0;
+    }
+  }
+  if (floored) p.cs2 = eos_cs2<EOS>(FV_T_MIN, d);
+  double F[11];
+  flux_cell<XDIR>(F, p, tau, d);
+  double lm, lp;
+  wavespeeds<XDIR>(p, XDIR ? p.pixx : p.piyy, &lm, &lp);
+  const double lmo = __shfl_xor_sync(pm, lm, 1), lpo = __shfl_xor_sync(pm, lp, 1);
+  const double lmL = side ? lmo : lm, lmR = side ? lm : lmo;
+  const double lpL = side ? lpo : lp, lpR = side ? lp : lpo;
+  const double sL = jmin(lmL, lmR), sR = jmax(lpL, lpR);
+  /* conserved column of this state incl. its stored dissipatives (zero when floored) */
+  double cv[11];
+  cv[0] = uc[0]; cv[1] = uc[1]; cv[2] = uc[2]; cv[3] = uc[3];
+#pragma unroll
+  for (int q = 0; q < 7; ++q) cv[4 + q] = floored ? 0.0 : dis[q];
+  const double inv = 1.0 / ((sR - sL) + FV_TINY);
+#pragma unroll
+  for (int s = 0; s < 11; ++s) {
+    const double Fo = __shfl_xor_sync(pm, F[s], 1);
+    const double co = __shfl_xor_sync(pm, cv[s], 1);
+    const double FLs = side ? Fo : F[s], FRs = side ? F[s] : Fo;
+    const double cls = side ? co : cv[s], crs = side ? cv[s] : co;
+    double h;
+    if (sL >= 0) h = FLs;
+    else if (sR <= 0) h = FRs;
+    else h = (((sR * FLs) - (sL * FRs)) + ((sR * sL) * (crs - cls))) * inv;
+    F[s] = h;
+  }
+  for (int a = 0; a < d.nv; ++a) out[a] = F[slot_of(d, a)];
+  return jmax(fabs_(sL), fabs_(sR));
+}
+
+/* two lanes per face of one direction, every face of the (ghost-inclusive) grid;
+ * the lane of the left state stores the even rows, its partner the odd ones */
+template <int EOS, bool XDIR>
+__global__ void __launch_bounds__(128, 8) k_faces(DevParams d, DevState Ub, DevPrims w, double tau,
+                                               const uint8_t* ffo, double* Fh, DevFlags* fl) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nf = XDIR ? (long long)(d.Nxtot - 1) * d.Nytot : (long long)d.Nxtot * (d.Nytot - 1);
+  const int side = (int)(t & 1);
+  long long f = t >> 1;
+  const bool valid = f < nf;
+  if (!valid) f = nf - 1;          /* a spare pair repeats the last face and stores nothing */
+  long long i;
+  int k, kmax;
+  if (XDIR) { i = f; k = (int)(f / d.Nytot); kmax = d.Nxtot; }
+  else {
+    int ix = (int)(f / (d.Nytot - 1)), iy = (int)(f % (d.Nytot - 1));
+    i = (long long)ix * d.Nytot + iy; k = iy; kmax = d.Nytot;
+  }
+  double out[FV_MAXV];
+  double amax = face_flux_pair<EOS, XDIR>(d, Ub, w, i, XDIR ? d.Nytot : 1, k, kmax, tau, ffo, side, out);
+  if (valid)
+    for (int q = side; q < d.nv; q += 2) Fh[(size_t)q * d.Ntot + i] = out[q];
   for (int o = 16; o > 0; o >>= 1) amax = jmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
   __shared__ double red[4];
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = amax;
