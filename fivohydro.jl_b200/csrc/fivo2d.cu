@@ -49,8 +49,11 @@ inline unsigned nblk(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 
 /* reject_unwired_knobs_2d + check_terms (src2d/primitives2d.jl:246-272, src/terms.jl) */
 int validate(const fivo_params* p) {
-  if (p->consistent_fm || p->consistent_m2)
-    return fail(FIVO_ERR_CONFIG, "consistent_fm / consistent_m2 (the charm closures) are not built");
+  if (p->consistent_m2)
+    return fail(FIVO_ERR_CONFIG, "consistent_m2 (the charm second moment) is not built");
+  if (p->consistent_fm && p->tauN_coeff != 1.0)   /* reject_unwired_knobs_2d, src2d/primitives2d.jl:263-269 */
+    return fail(FIVO_ERR_CONFIG, "tauN_coeff cannot be combined with consistent_fm = true (the closure ties "
+                                 "tau_n = D_s h / T with h in closed form)");
   if (p->eos_kind != FIVO_EOS_CONFORMAL_HQ && p->eos_kind != FIVO_EOS_LATTICE_HRG)
     return fail(FIVO_ERR_CONFIG, "unknown eos_kind");
   if (p->enable_shear && p->shear_kind != FIVO_SHEAR_QGP && p->shear_kind != FIVO_SHEAR_ZERO)
@@ -68,8 +71,10 @@ int validate(const fivo_params* p) {
     return fail(FIVO_ERR_CONFIG, "Terms: nu_gradalpha switched but enable_diff is off");
   if ((diff & FIVO_TERM_SHEAR_VORTICITY) && !p->enable_shear)
     return fail(FIVO_ERR_CONFIG, "Terms: shear_vorticity switched but enable_shear is off");
-  if ((diff & fm) || (diff & m2))
-    return fail(FIVO_ERR_CONFIG, "Terms: a charm-closure term is switched but its sector is not built");
+  if ((diff & fm) && !p->consistent_fm)
+    return fail(FIVO_ERR_CONFIG, "Terms: a consistent-first-moment term is switched but consistent_fm is off");
+  if (diff & m2)
+    return fail(FIVO_ERR_CONFIG, "Terms: a second-moment term is switched but its sector is not built");
   if (p->primrec_maxit < 1 || !(p->primrec_tol > 0))
     return fail(FIVO_ERR_CONFIG, "primrec_maxit must be >= 1 and primrec_tol > 0");
   return FIVO_OK;

@@ -588,6 +588,56 @@ __device__ void pi_sigma(double ux, double uy, double pxx, double pxy, double py
 
 struct Kin { double th, ax, ay, at, dxux, dxuy, dyux, dyuy; };
 
+/* ---- the consistent charm first moment (src2d/hq_consistent_firstmoment2d.jl) ---- */
+
+/* hq_h_hprime_2d, :145-160: dh/dT of the enthalpy per particle h = m K3/K2 */
+__device__ __forceinline__ double hq_hprime(double T, const DevParams& d) {
+  const double Tm = jmax(T, FV_T_MIN);
+  const double m = d.p.m_hq;
+  const double z = m / Tm;
+  if (z <= 0.0) return 0.0;
+  const double K1 = fx_besselkx(1, z), K2 = fx_besselkx(2, z), K3 = fx_besselkx(3, z), K4 = fx_besselkx(4, z);
+  if (fabs_(K2) <= FV_TINY) return 0.0;
+  const double hpv = ((m * z) / Tm) * ((((K2 + K4) * K2) - ((K1 + K3) * K3))) / ((2.0 * K2) * K2);
+  return isfinite_(hpv) ? hpv : 0.0;
+}
+
+/* hq_dn_dT_2d, :172-182: dn/dT at fixed alpha = (n/T)(3 + z K1/K2) */
+__device__ __forceinline__ double hq_dn_dT(double T, double n, const DevParams& d) {
+  const double Tm = jmax(T, FV_T_MIN);
+  const double z = d.p.m_hq / Tm;
+  if (z <= 0.0) return 0.0;
+  const double K1 = fx_besselkx(1, z), K2 = fx_besselkx(2, z);
+  if (fabs_(K2) <= FV_TINY) return 0.0;
+  const double v = (n / Tm) * (3.0 + ((z * K1) / K2));
+  return isfinite_(v) ? v : 0.0;
+}
+
+/* consistent_fm_source_2d, :218-282: the sources s^i (written on the left-hand side
+ * of the charge row, so the relaxation subtracts them), each behind its Terms switch */
+__device__ __forceinline__ void consistent_fm_source(double ux, double uy, double ut, double T, double dxT,
+                                                     double dyT, double dtT, double nux, double nuy, double n,
+                                                     double dn_dT, double tn, double Ds, double hp, const Kin& k,
+                                                     uint32_t terms, double* sx, double* sy) {
+  const double Tm = jmax(T, FV_T_MIN);
+  const double DT = ((ut * dtT) + (ux * dxT)) + (uy * dyT);
+  const double gTx = dxT + (ux * DT);
+  const double gTy = dyT + (uy * DT);
+  const double nut = nu_tau(ux, uy, ut, nux, nuy);
+  const double dtux = ((k.ax - (ux * k.dxux)) - (uy * k.dyux)) * safe_inv(ut);
+  const double dtuy = ((k.ay - (ux * k.dxuy)) - (uy * k.dyuy)) * safe_inv(ut);
+  const double ngux = ((nut * dtux) + (nux * k.dxux)) + (nuy * k.dyux);
+  const double nguy = ((nut * dtuy) + (nux * k.dxuy)) + (nuy * k.dyuy);
+  const double expansion = (terms & FIVO_TERM_FM_EXPANSION) ? tn * k.th : 0.0;
+  const double dlnh = (terms & FIVO_TERM_FM_DLNH) ? ((Ds / Tm) * hp) * DT : 0.0;
+  const double br = expansion + dlnh;
+  const double pref = (Ds / Tm) * (n + (Tm * dn_dT));
+  *sx = ((((terms & FIVO_TERM_FM_GRADT) ? pref * gTx : 0.0) + ((terms & FIVO_TERM_FM_INERTIAL) ? (tn * n) * k.ax : 0.0)) +
+         ((terms & FIVO_TERM_FM_NU_GRADU) ? tn * ngux : 0.0)) + (nux * br);
+  *sy = ((((terms & FIVO_TERM_FM_GRADT) ? pref * gTy : 0.0) + ((terms & FIVO_TERM_FM_INERTIAL) ? (tn * n) * k.ay : 0.0)) +
+         ((terms & FIVO_TERM_FM_NU_GRADU) ? tn * nguy : 0.0)) + (nuy * br);
+}
+
 /* ns_shear_target_2d, src2d/dissipation2d.jl:181-192 */
 __device__ __forceinline__ void ns_shear(double ux, double uy, double ut, double tau, const Kin& k,
                                          double eta, double* xx, double* xy, double* yy, double* et) {
@@ -797,6 +847,19 @@ __device__ __forceinline__ double relax_cell(const DevParams& d, const DevState&
           double Da = ((ut * dta) + (ux * dxa)) + (uy * dya);
           nsx = (-kappa) * (dxa + (ux * Da));
           nsy = (-kappa) * (dya + (uy * Da));
+        }
+        /* the consistent first moment (src2d/dissipation2d.jl:589-623), subtracted */
+        if (p.consistent_fm) {
+          const double Tp = h.T_prev[i];
+          const double dtT = isfinite_(Tp) ? (T - Tp) / D : 0.0;
+          const double dxT = (fx_exp(w.yT[i + st]) - fx_exp(w.yT[i - st])) / (2.0 * d.dx);
+          const double dyT = (fx_exp(w.yT[i + 1]) - fx_exp(w.yT[i - 1])) / (2.0 * d.dy);
+          const double hp = hq_hprime(T, d);
+          const double dn_dT = hq_dn_dT(T, n, d);
+          const double Ds = safe_div(p.kappa_coeff, T) / FV_FMGEV;
+          double csx, csy;
+          consistent_fm_source(ux, uy, ut, T, dxT, dyT, dtT, nux, nuy, n, dn_dT, tn, Ds, hp, k, p.terms, &csx, &csy);
+          nsx -= csx; nsy -= csy;
         }
         nsx *= wv; nsy *= wv;
         if (p.vacuum_ramp_relax) { tn = wv * tn; dN = wv * dN; }

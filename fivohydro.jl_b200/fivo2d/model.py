@@ -258,8 +258,8 @@ def build_model_2d(*, eos=None, r_domain: float = math.inf, enable_shear: bool =
                              f"2-D solver; use the default ({default}).")
     if knobs["consistent_fm"] and knobs["tauN_coeff"] != 1.0:
         raise ValueError("IdealDiffVisc2DModel: `tauN_coeff` cannot be combined with `consistent_fm = true`.")
-    if knobs["consistent_fm"] or knobs["consistent_m2"]:
-        raise NotImplementedError("consistent_fm / consistent_m2 (the charm closures) are not built")
+    if knobs["consistent_m2"]:
+        raise NotImplementedError("consistent_m2 (the charm second moment) is not built")
     if knobs["shear_constraint"] not in ("project", "monitor"):
         raise ValueError("shear_constraint must be 'project' or 'monitor'")
 
@@ -291,7 +291,7 @@ def build_model_2d(*, eos=None, r_domain: float = math.inf, enable_shear: bool =
         setattr(p, name, int(bool(knobs[name])))
     p.shear_constraint_project = int(knobs["shear_constraint"] == "project")
     p.primrec_maxit, p.primrec_tol = int(primrec_maxit), float(primrec_tol)
-    sectors = dict(enable_diff=enable_diff, enable_shear=enable_shear, consistent_fm=False,
+    sectors = dict(enable_diff=enable_diff, enable_shear=enable_shear, consistent_fm=bool(knobs["consistent_fm"]),
                    consistent_m2=False)
     p.terms = _resolve_terms(terms, lambda s: sectors[s])
     return IdealDiffVisc2DModel(eos=eos, layout=L, params=p, knobs=knobs)

@@ -229,4 +229,18 @@ void oracle_hypot(int64_t n, const double* x, const double* y, double* out) {
   for (int64_t i = 0; i < n; ++i) out[i] = o_hypot(x[i], y[i]);
 }
 
+/* the consistent first moment's closed forms; in[] = ux, uy, ut, T, dxT, dyT, dtT, nux, nuy, n,
+ * dn_dT, tau_n, Ds, hp, theta, ax, ay, dxux, dxuy, dyux, dyuy (21 values) */
+void oracle_cfm_source(const double* in, uint32_t terms, double* sx, double* sy) {
+  const double* v = in;
+  cfm_source(v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7], v[8], v[9], v[10], v[11], v[12], v[13], v[14],
+             v[15], v[16], v[17], v[18], v[19], v[20], terms, sx, sy);
+}
+void oracle_cfm_h_hprime(const fivo_params* p, double T, double* h, double* hp) { cfm_h_hprime(T, *p, h, hp); }
+double oracle_cfm_dn_dT(const fivo_params* p, double T, double n) { return cfm_dn_dT(T, n, *p); }
+void oracle_diff_coeffs(const fivo_params* p, double T, double mu, double n, double* kappa, double* taun,
+                        double* dN) {
+  cfm_diff_coeffs(T, mu, n, *p, kappa, taun, dN);
+}
+
 }  /* extern "C" */

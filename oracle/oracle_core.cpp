@@ -574,7 +574,12 @@ bool make_model(const fivo_params& p, Model& m, const char** err) {
   L.iPixx = L.hasShear ? k++ : -1; L.iPixy = L.hasShear ? k++ : -1;
   L.iPiyy = L.hasShear ? k++ : -1; L.iPieta = L.hasShear ? k++ : -1;
   L.nv = k;
-  if (p.consistent_fm || p.consistent_m2) { if (err) *err = "consistent_fm/consistent_m2 are not built"; return false; }
+  if (p.consistent_m2) { if (err) *err = "consistent_m2 is not built"; return false; }
+  /* reject_unwired_knobs_2d, src2d/primitives2d.jl:263-269 */
+  if (p.consistent_fm && p.tauN_coeff != 1.0) {
+    if (err) *err = "tauN_coeff cannot be combined with consistent_fm = true";
+    return false;
+  }
   /* build_model_2d, main2D.jl:102-108 */
   if (p.E_vac_cut > 0.0) m.E_vac_cut = p.E_vac_cut;
   else { double P, n, en; eos_Pne(p.T_vac_cut, 0.0, p, &P, &n, &en); m.E_vac_cut = en; }
@@ -1447,6 +1452,72 @@ static void compute_alpha_grad(Work& w, const Grid& g) {
   }
 }
 
+/* ---- the consistent charm first moment, src2d/hq_consistent_firstmoment2d.jl ---- */
+
+/* hq_h_hprime_2d, :145-160: h = m K3/K2 and dh/dT (scaled Bessel functions) */
+static void hq_h_hprime(double T, const fivo_params& p, double* h, double* hp) {
+  double Tm = o_max(T, T_MIN);
+  double m = p.m_hq;
+  double z = m / Tm;
+  *h = 0.0; *hp = 0.0;
+  if (z <= 0.0) return;
+  double K1 = o_besselkx(1, z), K2 = o_besselkx(2, z), K3 = o_besselkx(3, z), K4 = o_besselkx(4, z);
+  if (std::fabs(K2) <= TINY) return;
+  double hv = (m * K3) / K2;
+  double hpv = ((m * z) / Tm) * ((((K2 + K4) * K2) - ((K1 + K3) * K3))) / ((2.0 * K2) * K2);
+  *h = o_isfinite(hv) ? hv : 0.0;
+  *hp = o_isfinite(hpv) ? hpv : 0.0;
+}
+
+/* hq_dn_dT_2d, :172-182: dn/dT at fixed alpha = (n/T)(3 + z K1/K2) */
+static double hq_dn_dT(double T, double n, const fivo_params& p) {
+  double Tm = o_max(T, T_MIN);
+  double z = p.m_hq / Tm;
+  if (z <= 0.0) return 0.0;
+  double K1 = o_besselkx(1, z), K2 = o_besselkx(2, z);
+  if (std::fabs(K2) <= TINY) return 0.0;
+  double v = (n / Tm) * (3.0 + ((z * K1) / K2));
+  return o_isfinite(v) ? v : 0.0;
+}
+
+/* consistent_fm_source_2d, :218-282: the sources s^i, SOURCE-ON-THE-LHS */
+static void consistent_fm_source(double ux, double uy, double ut, double T, double dxT, double dyT, double dtT,
+                                 double nux, double nuy, double n, double dn_dT, double tn, double Ds, double hp,
+                                 const Kin& k, uint32_t terms, double* sx, double* sy) {
+  double Tm = o_max(T, T_MIN);
+  double DT = ((ut * dtT) + (ux * dxT)) + (uy * dyT);
+  double gTx = dxT + (ux * DT);
+  double gTy = dyT + (uy * DT);
+  double nut = nu_tau(ux, uy, ut, nux, nuy);
+  double dtux = ((k.ax - (ux * k.dxux)) - (uy * k.dyux)) * safe_inv(ut);
+  double dtuy = ((k.ay - (ux * k.dxuy)) - (uy * k.dyuy)) * safe_inv(ut);
+  double ngux = ((nut * dtux) + (nux * k.dxux)) + (nuy * k.dyux);
+  double nguy = ((nut * dtuy) + (nux * k.dxuy)) + (nuy * k.dyuy);
+  double expansion = (terms & FIVO_TERM_FM_EXPANSION) ? tn * k.th : 0.0;
+  double dlnh = (terms & FIVO_TERM_FM_DLNH) ? ((Ds / Tm) * hp) * DT : 0.0;
+  double br = expansion + dlnh;
+  double pref = (Ds / Tm) * (n + (Tm * dn_dT));
+  *sx = ((((terms & FIVO_TERM_FM_GRADT) ? pref * gTx : 0.0) + ((terms & FIVO_TERM_FM_INERTIAL) ? (tn * n) * k.ax : 0.0)) +
+         ((terms & FIVO_TERM_FM_NU_GRADU) ? tn * ngux : 0.0)) + (nux * br);
+  *sy = ((((terms & FIVO_TERM_FM_GRADT) ? pref * gTy : 0.0) + ((terms & FIVO_TERM_FM_INERTIAL) ? (tn * n) * k.ay : 0.0)) +
+         ((terms & FIVO_TERM_FM_NU_GRADU) ? tn * nguy : 0.0)) + (nuy * br);
+}
+
+/* the closure's pieces with plain arguments, for the gate tests */
+void cfm_h_hprime(double T, const fivo_params& p, double* h, double* hp) { hq_h_hprime(T, p, h, hp); }
+double cfm_dn_dT(double T, double n, const fivo_params& p) { return hq_dn_dT(T, n, p); }
+void cfm_diff_coeffs(double T, double mu, double n, const fivo_params& p, double* kappa, double* taun,
+                     double* dN) {
+  diff_coeffs(T, mu, n, p, kappa, taun, dN);
+}
+void cfm_source(double ux, double uy, double ut, double T, double dxT, double dyT, double dtT, double nux,
+                double nuy, double n, double dn_dT, double tn, double Ds, double hp, double th, double ax,
+                double ay, double dxux, double dxuy, double dyux, double dyuy, uint32_t terms, double* sx,
+                double* sy) {
+  const Kin k{th, ax, ay, 0.0, dxux, dxuy, dyux, dyuy};
+  consistent_fm_source(ux, uy, ut, T, dxT, dyT, dtT, nux, nuy, n, dn_dT, tn, Ds, hp, k, terms, sx, sy);
+}
+
 /* relax_dissipative_2d! and the per-cell sector updates, src2d/dissipation2d.jl:293-705 */
 int64_t relax_dissipative_2d(double* U, const Grid& g, double tau, double D, const Model& m, Work& w) {
   const Layout& L = m.L;
@@ -1562,6 +1633,21 @@ int64_t relax_dissipative_2d(double* U, const Grid& g, double tau, double D, con
           double Da = ((ut * dta) + (ux * dxa)) + (uy * dya);
           nsx = (-kappa) * (dxa + (ux * Da));
           nsy = (-kappa) * (dya + (uy * Da));
+        }
+        /* the consistent first moment, src2d/dissipation2d.jl:589-623: subtracted
+         * (the source is written on the left-hand side of the row) */
+        if (p.consistent_fm) {
+          double Tp = w.T_prev[i];
+          double dtT = o_isfinite(Tp) ? (T - Tp) / D : 0.0;
+          double dxT = (o_exp(w.yT[i + g.Nytot]) - o_exp(w.yT[i - g.Nytot])) / (2.0 * g.dx);
+          double dyT = (o_exp(w.yT[i + 1]) - o_exp(w.yT[i - 1])) / (2.0 * g.dy);
+          double hh, hp;
+          hq_h_hprime(T, p, &hh, &hp);
+          double dn_dT = hq_dn_dT(T, n, p);
+          double Ds = safe_div(p.kappa_coeff, T) / FMGEV;
+          double csx, csy;
+          consistent_fm_source(ux, uy, ut, T, dxT, dyT, dtT, nux, nuy, n, dn_dT, tn, Ds, hp, k, p.terms, &csx, &csy);
+          nsx -= csx; nsy -= csy;
         }
         nsx *= wv; nsy *= wv;
         if (p.vacuum_ramp_relax) { tn = wv * tn; dN = wv * dN; }

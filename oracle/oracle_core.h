@@ -138,5 +138,15 @@ void run_sim_2d(double* U, const Grid& g, const Model& m, Work& w, double tau0, 
                 double CFL, double CFLtau, int integrator, int bc, bool reset_history,
                 int64_t max_steps, fivo_run_result* res);
 
+/* the consistent charm first moment (src2d/hq_consistent_firstmoment2d.jl) */
+void cfm_h_hprime(double T, const fivo_params& p, double* h, double* hp);
+double cfm_dn_dT(double T, double n, const fivo_params& p);
+void cfm_diff_coeffs(double T, double mu, double n, const fivo_params& p, double* kappa, double* taun,
+                     double* dN);
+void cfm_source(double ux, double uy, double ut, double T, double dxT, double dyT, double dtT, double nux,
+                double nuy, double n, double dn_dT, double tn, double Ds, double hp, double th, double ax,
+                double ay, double dxux, double dxuy, double dyux, double dyuy, uint32_t terms, double* sx,
+                double* sy);
+
 }  // namespace orc
 #endif

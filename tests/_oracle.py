@@ -77,6 +77,10 @@ def lib():
             "oracle_log": (None, [C.c_int64, _D, _D]),
             "oracle_pow4": (None, [C.c_int64, _D, _D]),
             "oracle_hypot": (None, [C.c_int64, _D, _D, _D]),
+            "oracle_cfm_source": (None, [_D, C.c_uint32, _D, _D]),
+            "oracle_cfm_h_hprime": (None, [P, C.c_double, _D, _D]),
+            "oracle_cfm_dn_dT": (C.c_double, [P, C.c_double, C.c_double]),
+            "oracle_diff_coeffs": (None, [P, C.c_double, C.c_double, C.c_double, _D, _D, _D]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

@@ -78,7 +78,9 @@ def test_config_refusals_are_status_codes(lib):
     g = fivo2d.make_grid2d(16, 16)
     base = fivo2d.build_model_2d(eos=fivo2d.LatticeHRGEOS()).params
     cases = []
-    p = A.FivoParams.from_buffer_copy(base); p.consistent_fm = 1; cases.append(p)
+    p = A.FivoParams.from_buffer_copy(base); p.consistent_fm = 1; p.tauN_coeff = 1.5; cases.append(p)
+    p = A.FivoParams.from_buffer_copy(base); p.consistent_m2 = 1; cases.append(p)
+    p = A.FivoParams.from_buffer_copy(base); p.terms = A.FIVO_TERMS_DEFAULT & ~A.TERM_BIT["fm_dlnh"]; cases.append(p)
     p = A.FivoParams.from_buffer_copy(base); p.terms = A.FIVO_TERMS_DEFAULT | A.TERM_BIT["shear_vorticity"]; cases.append(p)
     p = A.FivoParams.from_buffer_copy(base); p.terms = A.FIVO_TERMS_DEFAULT & ~A.TERM_BIT["nu_gradalpha"]; cases.append(p)
     p = A.FivoParams.from_buffer_copy(base); p.primrec_maxit = 0; cases.append(p)

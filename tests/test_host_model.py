@@ -73,8 +73,13 @@ def test_conformal_eos_without_charge_is_three_unknowns():
 def test_refusals_follow_the_reference():
     with pytest.raises(TypeError):
         fivo2d.build_model_2d(no_such_knob=1)
-    with pytest.raises((ValueError, NotImplementedError)):
-        fivo2d.build_model_2d(consistent_fm=True)
+    assert fivo2d.build_model_2d(consistent_fm=True).params.consistent_fm == 1
+    with pytest.raises(ValueError):
+        fivo2d.build_model_2d(consistent_fm=True, tauN_coeff=1.5)
+    with pytest.raises(ValueError):
+        fivo2d.build_model_2d(terms={"fm_dlnh": False})           # its sector (consistent_fm) is off
+    assert fivo2d.build_model_2d(consistent_fm=True, terms={"fm_dlnh": False}).params.terms & \
+        A.TERM_BIT["fm_dlnh"] == 0
     with pytest.raises((ValueError, NotImplementedError)):
         fivo2d.build_model_2d(consistent_m2=True)
     with pytest.raises(ValueError):
