@@ -13,7 +13,9 @@
  */
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -156,6 +158,10 @@ struct fivo_ctx {
   std::vector<cudaEvent_t> pool;
   fivo_kernel_times kt;
   int64_t tot_base_p = 0, tot_base_a = 0;   /* device deferred-cell totals at the last reset */
+  /* the learned recovery guess (fivo_ctx_set_guess): k_prim_learned replaces k_prim_fast */
+  bool learned = false;
+  guess::Net gnet{};
+  int64_t stats_base_p = 0;                 /* deferred-cell total at the last Newton-statistics reset */
 };
 
 namespace {
@@ -233,11 +239,25 @@ int reset_flags(fivo_ctx* c, int what) {
   return FIVO_OK;
 }
 
+/* shared memory a block of the learned pass holds, static and reserved: with one
+ * KB per block reserved by the hardware, 5 blocks (255 KB) do not fit in the 228 KB
+ * of an SM and 4 (204 KB) do */
+constexpr int LEARNED_SMEM = 50 * 1024;
+
 template <int EOS, bool NCH>
 int launch_primitive_t(fivo_ctx* c, const DevState& U, double tau) {
   const DevParams& d = c->dp;
   unsigned int* q = c->queues;
-  {
+  if (c->learned) {
+    /* at most 4 blocks per SM (4 x 128 tensor-memory columns): the launch reserves
+     * shared memory up to LEARNED_SMEM per block */
+    CK(cudaFuncSetAttribute(k_prim_learned<EOS, NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            LEARNED_SMEM - (int)sizeof(guess::FwdSmem)));
+    KTimer t_(c, FIVO_KCLASS_PRIM_FAST, 1, d.Ntot);
+    k_prim_learned<EOS, NCH><<<nblk(d.Ntot, 128), 128, LEARNED_SMEM - sizeof(guess::FwdSmem), c->st>>>(
+        d, U, c->w, c->h, tau, c->fl, q, c->gnet);
+    CKL();
+  } else {
     KTimer t_(c, FIVO_KCLASS_PRIM_FAST, 1, d.Ntot);
     k_prim_fast<EOS, NCH><<<nblk(d.Ntot, 128), 128, 0, c->st>>>(d, U, c->w, c->h, tau, c->fl, q);
     CKL();
@@ -298,6 +318,7 @@ int sync_flags(fivo_ctx* c, bool read_amax) {
   CK(cudaMemcpyAsync(c->flh, c->fl, sizeof(DevFlags), cudaMemcpyDeviceToHost, c->st));
   CK(ctx_sync(c));
   const DevFlags& f = *c->flh;
+  if (f.status == 3) return fail(FIVO_ERR_DEVICE, "learned recovery guess: a tensor-core wait gave up");
   c->cnt.nprimfail = f.nprimfail;
   c->cnt.nvacuum = f.nvacuum;
   if (f.rep != (unsigned long long)REP_NONE) {
@@ -583,7 +604,7 @@ int fivo_ctx_create(const fivo_params* p, int nx, int ny, int nghost, double xma
       cudaMemsetAsync(c->masks, 0, 3 * N, c->st) != cudaSuccess)
     return cleanup(fail(FIVO_ERR_CUDA, "memset failed"));
   if ((rc = reset_history(c))) return cleanup(rc);
-  if ((rc = reset_flags(c, 1 | 2 | 4 | 8 | 16))) return cleanup(rc);
+  if ((rc = reset_flags(c, 1 | 2 | 4 | 8 | 16 | 32))) return cleanup(rc);
   if (ctx_sync(c) != cudaSuccess) return cleanup(fail(FIVO_ERR_CUDA, "sync failed"));
   *out = c;
   return FIVO_OK;
@@ -1300,4 +1321,341 @@ int fivo_batch_advance(fivo_batch* b, const double* tau, double taufinal, double
   return batch_for_each(b, status, [&](int k) {
     return fivo_advance(b->ev[k], tau[k], taufinal, cfl, cfltau, integrator, bc, max_steps, &results[k]);
   });
+}
+
+/* ------------------------------------------------ the learned recovery guess */
+
+struct fivo_guess {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  float* params = nullptr;          /* NPARAM FP32 master weights */
+  float* adam = nullptr;            /* m | v */
+  uint8_t* img = nullptr;           /* BF16 operand images */
+  guess::Norm norm{};
+  int64_t adam_t = 0;
+  float* samples = nullptr;         /* the sample store, cap x NSAMP floats */
+  int64_t cap = 0;
+  unsigned long long* count = nullptr;
+  float* part = nullptr;            /* per-CTA partial gradients of a step */
+  int part_ctas = 0;
+  float* loss_part = nullptr;
+  float* grad = nullptr;
+  int* err = nullptr;
+};
+
+namespace {
+
+guess::Net net_of(const fivo_guess* g) { return guess::Net{g->img, g->params, g->norm}; }
+
+int guess_pack(fivo_guess* g) {
+  guess::k_pack<<<(guess::PACK_ELEMS + 255) / 256, 256, 0, g->st>>>(g->params, g->img);
+  CKL();
+  return FIVO_OK;
+}
+
+int guess_parts(fivo_guess* g, int ctas) {
+  if (ctas <= g->part_ctas) return FIVO_OK;
+  cudaFree(g->part); cudaFree(g->loss_part);
+  g->part = nullptr; g->loss_part = nullptr; g->part_ctas = 0;
+  CK(cudaMalloc(&g->part, (size_t)ctas * guess::NPARAM * sizeof(float)));
+  CK(cudaMalloc(&g->loss_part, (size_t)ctas * sizeof(float)));
+  g->part_ctas = ctas;
+  return FIVO_OK;
+}
+
+/* one forward + backward over ctas x 128 samples, the partials summed by k_adam
+ * (lr = 0: the summed gradient only, into grad_out) */
+int guess_step(fivo_guess* g, const float* smp, long long n, unsigned long long seed, int ctas, float lr,
+               float* grad_out) {
+  int rc = guess_parts(g, ctas);
+  if (rc) return rc;
+  CK(cudaFuncSetAttribute(guess::k_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)sizeof(guess::TrainSmem)));
+  guess::k_train<<<ctas, 128, sizeof(guess::TrainSmem), g->st>>>(net_of(g), smp, n, seed, 0,
+                                                                 1.0f / (128.0f * (float)ctas), g->part,
+                                                                 g->loss_part, g->err);
+  CKL();
+  float c1 = 1.0f, c2 = 1.0f;
+  if (lr != 0.0f) {
+    g->adam_t += 1;
+    c1 = 1.0f - std::pow(0.9f, (float)g->adam_t);
+    c2 = 1.0f - std::pow(0.999f, (float)g->adam_t);
+  }
+  guess::k_adam<<<(guess::NPARAM + 255) / 256, 256, 0, g->st>>>(g->params, g->adam, g->adam + guess::NPARAM,
+                                                               g->part, ctas, lr, 0.9f, 0.999f, 1e-8f, c1, c2,
+                                                               grad_out);
+  CKL();
+  if (lr != 0.0f) return guess_pack(g);
+  return FIVO_OK;
+}
+
+int guess_loss(fivo_guess* g, int ctas, double* loss) {
+  std::vector<float> lp(ctas);
+  CK(cudaMemcpyAsync(lp.data(), g->loss_part, ctas * sizeof(float), cudaMemcpyDeviceToHost, g->st));
+  CK(cudaStreamSynchronize(g->st));
+  int e = 0;
+  CK(cudaMemcpy(&e, g->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) return fail(FIVO_ERR_DEVICE, "guess training: a tensor-core wait gave up");
+  double s = 0.0;
+  for (int b = 0; b < ctas; ++b) s += lp[b];
+  *loss = s / (128.0 * ctas);
+  return FIVO_OK;
+}
+
+}  // namespace
+
+int fivo_guess_create(fivo_ctx* c, uint64_t seed, fivo_guess** out) {
+  if (!out) return fail(FIVO_ERR_ARG, "null argument");
+  *out = nullptr;
+  fivo_guess* g = new fivo_guess();
+  g->device = c ? c->device : 0;
+  if (!c) cudaGetDevice(&g->device);
+  auto bad = [&](int rc) { fivo_guess_destroy(g); return rc; };
+  if (cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&g->params, guess::NPARAM * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&g->adam, 2 * guess::NPARAM * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&g->img, guess::IMG_BYTES) != cudaSuccess || cudaMalloc(&g->err, sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&g->count, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&g->grad, guess::NPARAM * sizeof(float)) != cudaSuccess)
+    return bad(fail(FIVO_ERR_NOMEM, "fivo_guess_create: device allocation failed"));
+  /* uniform(-1/sqrt(fan_in), 1/sqrt(fan_in)) weights from a splitmix64 stream, zero biases */
+  std::vector<float> P(guess::NPARAM, 0.0f);
+  uint64_t st = seed;
+  auto uni = [&]() { st += 1; return (double)(guess::mix64(st) >> 11) * (1.0 / 9007199254740992.0); };
+  for (int j = 0; j < guess::NH; ++j)
+    for (int k = 0; k < guess::NIN; ++k) P[guess::P_W1 + j * guess::K0 + k] = (float)((2 * uni() - 1) / std::sqrt(8.0));
+  for (int j = 0; j < guess::NH; ++j)
+    for (int k = 0; k < guess::NH; ++k) P[guess::P_W2 + j * guess::NH + k] = (float)((2 * uni() - 1) / 8.0);
+  for (int o = 0; o < guess::NOUT; ++o)
+    for (int k = 0; k < guess::NH; ++k) P[guess::P_W3 + o * guess::NH + k] = (float)((2 * uni() - 1) / 8.0);
+  float nm[FIVO_GUESS_NNORM];
+  for (int q = 0; q < 8; ++q) { nm[q] = 0.0f; nm[8 + q] = 1.0f; }
+  for (int o = 0; o < 3; ++o) { nm[16 + o] = 0.0f; nm[19 + o] = 1.0f; }
+  int rc = fivo_guess_set_params(g, P.data(), nm);
+  if (rc) return bad(rc);
+  *out = g;
+  return FIVO_OK;
+}
+
+int fivo_guess_destroy(fivo_guess* g) {
+  if (!g) return FIVO_OK;
+  if (g->st) cudaStreamSynchronize(g->st);
+  cudaFree(g->params); cudaFree(g->adam); cudaFree(g->img); cudaFree(g->samples); cudaFree(g->count);
+  cudaFree(g->part); cudaFree(g->loss_part); cudaFree(g->grad); cudaFree(g->err);
+  if (g->st) cudaStreamDestroy(g->st);
+  delete g;
+  return FIVO_OK;
+}
+
+int fivo_guess_set_params(fivo_guess* g, const float* params, const float* norm) {
+  if (!g) return fail(FIVO_ERR_ARG, "null guess");
+  if (params) {
+    CK(cudaMemcpyAsync(g->params, params, guess::NPARAM * sizeof(float), cudaMemcpyHostToDevice, g->st));
+    CK(cudaMemsetAsync(g->adam, 0, 2 * guess::NPARAM * sizeof(float), g->st));
+    g->adam_t = 0;
+    int rc = guess_pack(g);
+    if (rc) return rc;
+  }
+  if (norm) {
+    for (int q = 0; q < 8; ++q) { g->norm.in_mean[q] = norm[q]; g->norm.in_istd[q] = norm[8 + q]; }
+    for (int o = 0; o < 3; ++o) { g->norm.out_mean[o] = norm[16 + o]; g->norm.out_std[o] = norm[19 + o]; }
+  }
+  CK(cudaMemsetAsync(g->err, 0, sizeof(int), g->st));
+  CK(cudaStreamSynchronize(g->st));
+  return FIVO_OK;
+}
+
+int fivo_guess_get_params(fivo_guess* g, float* params, float* norm) {
+  if (!g) return fail(FIVO_ERR_ARG, "null guess");
+  if (params) {
+    CK(cudaMemcpyAsync(params, g->params, guess::NPARAM * sizeof(float), cudaMemcpyDeviceToHost, g->st));
+    CK(cudaStreamSynchronize(g->st));
+  }
+  if (norm) {
+    for (int q = 0; q < 8; ++q) { norm[q] = g->norm.in_mean[q]; norm[8 + q] = g->norm.in_istd[q]; }
+    for (int o = 0; o < 3; ++o) { norm[16 + o] = g->norm.out_mean[o]; norm[19 + o] = g->norm.out_std[o]; }
+  }
+  return FIVO_OK;
+}
+
+int fivo_guess_reserve(fivo_guess* g, int64_t capacity) {
+  if (!g || capacity < 0) return fail(FIVO_ERR_ARG, "bad argument");
+  CK(cudaStreamSynchronize(g->st));
+  cudaFree(g->samples);
+  g->samples = nullptr;
+  g->cap = 0;
+  if (capacity > 0 && cudaMalloc(&g->samples, (size_t)capacity * guess::NSAMP * sizeof(float)) != cudaSuccess)
+    return fail(FIVO_ERR_NOMEM, "fivo_guess_reserve: device allocation failed");
+  g->cap = capacity;
+  CK(cudaMemset(g->count, 0, sizeof(unsigned long long)));
+  return FIVO_OK;
+}
+
+int fivo_guess_nsamples(fivo_guess* g, int64_t* n) {
+  if (!g || !n) return fail(FIVO_ERR_ARG, "null argument");
+  unsigned long long k = 0;
+  CK(cudaStreamSynchronize(g->st));
+  CK(cudaMemcpy(&k, g->count, sizeof(k), cudaMemcpyDeviceToHost));
+  *n = (int64_t)std::min<unsigned long long>(k, (unsigned long long)g->cap);
+  return FIVO_OK;
+}
+
+int fivo_guess_set_samples(fivo_guess* g, const float* samples, int64_t n) {
+  if (!g || (!samples && n > 0) || n < 0) return fail(FIVO_ERR_ARG, "bad argument");
+  if (n > g->cap) { int rc = fivo_guess_reserve(g, n); if (rc) return rc; }
+  if (n > 0) CK(cudaMemcpy(g->samples, samples, (size_t)n * guess::NSAMP * sizeof(float), cudaMemcpyHostToDevice));
+  unsigned long long k = (unsigned long long)n;
+  CK(cudaMemcpy(g->count, &k, sizeof(k), cudaMemcpyHostToDevice));
+  return FIVO_OK;
+}
+
+int fivo_guess_get_samples(fivo_guess* g, float* samples, int64_t n) {
+  int64_t have = 0;
+  int rc = fivo_guess_nsamples(g, &have);
+  if (rc) return rc;
+  if (!samples || n < 0 || n > have) return fail(FIVO_ERR_ARG, "bad argument");
+  if (n > 0) CK(cudaMemcpy(samples, g->samples, (size_t)n * guess::NSAMP * sizeof(float), cudaMemcpyDeviceToHost));
+  return FIVO_OK;
+}
+
+int fivo_guess_harvest(fivo_ctx* c, fivo_guess* g, double tau, int stride, int phase) {
+  if (!c || !g || stride < 1 || phase < 0) return fail(FIVO_ERR_ARG, "bad argument");
+  if (g->cap <= 0) return fail(FIVO_ERR_ARG, "fivo_guess_harvest: no sample store (fivo_guess_reserve)");
+  CK(ctx_sync(c));
+  const DevParams& d = c->dp;
+  if (d.p.eos_kind == FIVO_EOS_LATTICE_HRG)
+    k_guess_harvest<FIVO_EOS_LATTICE_HRG><<<nblk(d.Ntot, 256), 256, 0, c->st>>>(
+        d, c->S[c->iU], c->w, tau, g->samples, (unsigned long long)g->cap, g->count, stride, phase);
+  else
+    k_guess_harvest<FIVO_EOS_CONFORMAL_HQ><<<nblk(d.Ntot, 256), 256, 0, c->st>>>(
+        d, c->S[c->iU], c->w, tau, g->samples, (unsigned long long)g->cap, g->count, stride, phase);
+  CKL();
+  CK(ctx_sync(c));
+  return FIVO_OK;
+}
+
+int fivo_guess_fit_norm(fivo_guess* g) {
+  int64_t n = 0;
+  int rc = fivo_guess_nsamples(g, &n);
+  if (rc) return rc;
+  if (n < 2) return fail(FIVO_ERR_ARG, "fivo_guess_fit_norm: fewer than 2 samples");
+  const int nb = 256;
+  double* part = nullptr;
+  CK(cudaMalloc(&part, (size_t)nb * 2 * guess::NSAMP * sizeof(double)));
+  guess::k_moments<<<nb, 256, 0, g->st>>>(g->samples, n, part);
+  std::vector<double> hp((size_t)nb * 2 * guess::NSAMP);
+  cudaError_t e1 = cudaGetLastError();
+  cudaError_t e2 = cudaMemcpyAsync(hp.data(), part, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, g->st);
+  cudaError_t e3 = cudaStreamSynchronize(g->st);
+  cudaFree(part);
+  if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+    return fail(FIVO_ERR_CUDA, "fivo_guess_fit_norm: moments failed");
+  double sum[guess::NSAMP] = {}, sq[guess::NSAMP] = {};
+  for (int b = 0; b < nb; ++b)
+    for (int q = 0; q < guess::NSAMP; ++q) {
+      sum[q] += hp[(size_t)b * 2 * guess::NSAMP + q];
+      sq[q] += hp[(size_t)b * 2 * guess::NSAMP + guess::NSAMP + q];
+    }
+  for (int q = 0; q < guess::NSAMP; ++q) {
+    const double m = sum[q] / n;
+    const double sd = std::sqrt(std::max(sq[q] / n - m * m, 0.0));
+    const double s = std::max(sd, 1e-6);
+    if (q < guess::NIN) { g->norm.in_mean[q] = (float)m; g->norm.in_istd[q] = (float)(1.0 / s); }
+    else { g->norm.out_mean[q - guess::NIN] = (float)m; g->norm.out_std[q - guess::NIN] = (float)s; }
+  }
+  return FIVO_OK;
+}
+
+int fivo_guess_train(fivo_guess* g, int steps, int ctas, float lr, uint64_t seed, double* loss_out) {
+  if (!g || steps < 1 || ctas < 1 || !(lr > 0.0f)) return fail(FIVO_ERR_ARG, "bad argument");
+  int64_t n = 0;
+  int rc = fivo_guess_nsamples(g, &n);
+  if (rc) return rc;
+  if (n < 1) return fail(FIVO_ERR_ARG, "fivo_guess_train: no samples");
+  CK(cudaMemsetAsync(g->err, 0, sizeof(int), g->st));
+  for (int s = 0; s < steps; ++s) {
+    const unsigned long long sd = guess::mix64(seed + (uint64_t)s) | 1ULL;
+    if ((rc = guess_step(g, g->samples, n, sd, ctas, lr, nullptr))) return rc;
+    if (loss_out && (s == 0 || s == steps - 1)) {
+      double l = 0.0;
+      if ((rc = guess_loss(g, ctas, &l))) return rc;
+      loss_out[s == 0 ? 0 : 1] = l;
+      if (steps == 1) loss_out[1] = l;
+    }
+  }
+  CK(cudaStreamSynchronize(g->st));
+  return FIVO_OK;
+}
+
+int fivo_guess_grad(fivo_guess* g, const float* samples, int64_t n, float* grad, double* loss) {
+  if (!g || !samples || !grad || n < 128 || n % 128) return fail(FIVO_ERR_ARG, "bad argument");
+  float* ds = nullptr;
+  CK(cudaMalloc(&ds, (size_t)n * guess::NSAMP * sizeof(float)));
+  int rc = FIVO_OK;
+  if (cudaMemcpy(ds, samples, (size_t)n * guess::NSAMP * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = fail(FIVO_ERR_CUDA, "fivo_guess_grad: upload failed");
+  if (!rc) { cudaMemsetAsync(g->err, 0, sizeof(int), g->st); rc = guess_step(g, ds, n, 0ULL, (int)(n / 128), 0.0f, g->grad); }
+  double l = 0.0;
+  if (!rc) rc = guess_loss(g, (int)(n / 128), &l);
+  if (!rc && cudaMemcpy(grad, g->grad, guess::NPARAM * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = fail(FIVO_ERR_CUDA, "fivo_guess_grad: download failed");
+  cudaFree(ds);
+  if (!rc && loss) *loss = l;
+  return rc;
+}
+
+int fivo_guess_forward(fivo_guess* g, const float* raw, int64_t n, float* out) {
+  if (!g || !raw || !out || n < 1) return fail(FIVO_ERR_ARG, "bad argument");
+  float *dr = nullptr, *dout = nullptr;
+  CK(cudaMalloc(&dr, (size_t)n * guess::NIN * sizeof(float)));
+  if (cudaMalloc(&dout, (size_t)n * guess::NOUT * sizeof(float)) != cudaSuccess) {
+    cudaFree(dr);
+    return fail(FIVO_ERR_NOMEM, "fivo_guess_forward: device allocation failed");
+  }
+  int rc = FIVO_OK;
+  const int dyn = LEARNED_SMEM - (int)sizeof(guess::FwdSmem);
+  if (cudaMemcpy(dr, raw, (size_t)n * guess::NIN * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemset(g->err, 0, sizeof(int)) != cudaSuccess ||
+      cudaFuncSetAttribute(guess::k_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) != cudaSuccess)
+    rc = fail(FIVO_ERR_CUDA, "fivo_guess_forward: setup failed");
+  if (!rc) {
+    guess::k_infer<<<(unsigned)((n + 127) / 128), 128, dyn, g->st>>>(net_of(g), dr, n, dout, g->err);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(g->st) != cudaSuccess)
+      rc = fail(FIVO_ERR_CUDA, "fivo_guess_forward: kernel failed");
+  }
+  int e = 0;
+  if (!rc && cudaMemcpy(&e, g->err, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess && e)
+    rc = fail(FIVO_ERR_DEVICE, "fivo_guess_forward: a tensor-core wait gave up");
+  if (!rc && cudaMemcpy(out, dout, (size_t)n * guess::NOUT * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = fail(FIVO_ERR_CUDA, "fivo_guess_forward: download failed");
+  cudaFree(dr);
+  cudaFree(dout);
+  return rc;
+}
+
+int fivo_ctx_set_guess(fivo_ctx* c, fivo_guess* g) {
+  if (!c) return fail(FIVO_ERR_ARG, "null context");
+  if (g && g->device != c->device) return fail(FIVO_ERR_ARG, "fivo_ctx_set_guess: the guess lives on another device");
+  CK(ctx_sync(c));
+  if (g) CK(cudaStreamSynchronize(g->st));
+  c->learned = g != nullptr;
+  c->gnet = g ? net_of(g) : guess::Net{};
+  return FIVO_OK;
+}
+
+int fivo_newton_stats_read(fivo_ctx* c, fivo_newton_stats* out, int reset) {
+  if (!c || !out) return fail(FIVO_ERR_ARG, "null argument");
+  CK(cudaMemcpyAsync(c->flh, c->fl, sizeof(DevFlags), cudaMemcpyDeviceToHost, c->st));
+  CK(ctx_sync(c));
+  const DevFlags& f = *c->flh;
+  out->it_fast = f.it_fast; out->n_fast = f.n_fast; out->it_learn = f.it_learn; out->n_learn = f.n_learn;
+  out->ok_learn = f.ok_learn; out->it_fb = f.it_fb; out->n_fb = f.n_fb;
+  out->deferred = f.tot_p - (uint64_t)c->stats_base_p;
+  if (reset) {
+    k_reset_flags<<<1, 32, 0, c->st>>>(c->fl, 32, 0ULL);
+    CKL();
+    c->stats_base_p = (int64_t)f.tot_p;
+    CK(ctx_sync(c));
+  }
+  return FIVO_OK;
 }

@@ -23,6 +23,7 @@
 
 #include "physics.cuh"
 #include "coop.cuh"
+#include "guess.cuh"
 
 namespace fv {
 
@@ -51,6 +52,10 @@ struct DevFlags {
   unsigned int qcount_p, qnext_p; /* deferred recoveries of the current pass           */
   unsigned int qcount_a, qnext_a; /* deferred admissibility inversions of the stage     */
   unsigned long long tot_p, tot_a;/* deferred cells summed over passes (kernel timing)   */
+  /* Newton statistics, cumulative until reset (what & 32): updates and attempts of
+   * the warm-started fast pass; of the learned guess (attempts, accepted); of the
+   * warm attempts that follow a rejected learned guess */
+  unsigned long long it_fast, n_fast, it_learn, n_learn, ok_learn, it_fb, n_fb;
 };
 
 __device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) {
@@ -933,6 +938,7 @@ __global__ void k_reset_flags(DevFlags* fl, int what, unsigned long long amax_bi
   if (what & 4) { fl->shear_max_bits = 0; fl->shear_sum = 0.0; }
   if (what & 8) { fl->sumD = 0.0; fl->maxu = 0.0; fl->minPtot = inf_(); }
   if (what & 16) { fl->tot_p = 0; fl->tot_a = 0; }
+  if (what & 32) { fl->it_fast = fl->n_fast = fl->it_learn = fl->n_learn = fl->ok_learn = fl->it_fb = fl->n_fb = 0; }
   fl->status = 0;
 }
 
@@ -1203,6 +1209,7 @@ __global__ void __launch_bounds__(128, 4) k_prim_fast(DevParams d, DevState U, D
                                                    DevFlags* fl, unsigned int* queue) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   bool vac = false, defer = false;
+  unsigned nit = 0, natt = 0;
   if (i < d.Ntot) {
     CellCons c;
     load_cons(d, U, i, tau, c);
@@ -1214,14 +1221,20 @@ __global__ void __launch_bounds__(128, 4) k_prim_fast(DevParams d, DevState U, D
       defer = true;
     } else {
       bool over = false;
+      int it = 0;
       Recovery r = recover_fast<EOS, NCH>(c, d, yT0, h.x0_phi[i], ux0, uy0, d.p.primrec_maxit,
-                                          d.p.primrec_tol, FAST_BUDGET, &over);
+                                          d.p.primrec_tol, FAST_BUDGET, &over, 0x7fffffff, 0.0, &it);
+      nit = (unsigned)it; natt = 1;
       if (over || !r.ok) defer = true;
       else store_recovery<EOS>(d, w, h, i, r);
     }
   }
   /* warp-aggregated counters and queue appends (the grid holds whole warps) */
   const unsigned lane = threadIdx.x & 31;
+  {
+    const unsigned si = __reduce_add_sync(0xffffffffu, nit), sa = __reduce_add_sync(0xffffffffu, natt);
+    if (lane == 0 && sa) { atomicAdd(&fl->it_fast, (unsigned long long)si); atomicAdd(&fl->n_fast, (unsigned long long)sa); }
+  }
   unsigned mv = __ballot_sync(0xffffffffu, vac);
   if (lane == 0 && mv) atomicAdd((unsigned long long*)&fl->nvacuum, (unsigned long long)__popc(mv));
   unsigned md = __ballot_sync(0xffffffffu, defer);
@@ -1231,6 +1244,132 @@ __global__ void __launch_bounds__(128, 4) k_prim_fast(DevParams d, DevState U, D
     base = __shfl_sync(0xffffffffu, base, 0);
     if (defer) queue[base + __popc(md & ((1u << lane) - 1u))] = (unsigned)i;
   }
+}
+
+/* The warm pass with the learned guess in front of it. Every cell of a block of
+ * 128 (one tensor-core tile) gets the MLP's (log T, u^x, u^y); the charm
+ * chemical potential follows in closed form from N^tau = n u^tau + nu^tau with
+ * the LatticeHRG charm density n = A T e^phi e^x K2(x) (x = m/T); for another
+ * EOS it is the warm start's. Newton from that guess must reach residual 1e-10
+ * within GUESS_CHECK_IT updates and then converge as usual; a cell that does not
+ * falls back to the plain warm-started attempt (the FAST_BUDGET pass), and a
+ * cell that fails that too is deferred to k_prim_slow like any other. */
+#define GUESS_CHECK_IT 3
+#define GUESS_CHECK_TOL 1e-10
+template <int EOS, bool NCH>
+__global__ void __launch_bounds__(128, 4) k_prim_learned(DevParams d, DevState U, DevPrims w, DevHist h,
+                                                       double tau, DevFlags* fl, unsigned int* queue,
+                                                       guess::Net net) {
+  __shared__ __align__(128) guess::FwdSmem s;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = i < d.Ntot;
+  CellCons c;
+  bool vac = false;
+  float xn[guess::NIN];
+#pragma unroll
+  for (int q = 0; q < guess::NIN; ++q) xn[q] = 0.0f;
+  if (live) {
+    load_cons(d, U, i, tau, c);
+    vac = is_vacuum(c);
+    if (!vac && c.E > 0.0) {
+      float r[guess::NIN];
+      guess::features(c.E, c.Sx, c.Sy, c.Pi, c.pixx, c.pixy, c.piyy, r);
+#pragma unroll
+      for (int q = 0; q < guess::NIN; ++q) xn[q] = guess::nrm_in(net.norm, q, r[q]);
+    }
+  }
+  float y[guess::NOUT] = {0.0f, 0.0f, 0.0f};
+  const bool net_ok = guess::forward_tile(s, net, xn, y);
+  bool defer = false;
+  unsigned it_l = 0, n_l = 0, ok_l = 0, it_f = 0, n_f = 0;
+  if (live) {
+    const double yTw = h.x0_yT[i], phw = h.x0_phi[i], uxw = h.x0_ux[i], uyw = h.x0_uy[i];
+    const bool warm = isfinite_(yTw) && isfinite_(uxw) && isfinite_(uyw);
+    if (vac) {
+      store_recovery<EOS>(d, w, h, i, vacuum_recovery<EOS>(c, d));
+    } else {
+      double g[4];
+      bool have_guess = net_ok && c.E > 0.0;
+      if (have_guess) {
+        g[0] = ((double)y[0] * (double)net.norm.out_std[0] + (double)net.norm.out_mean[0]) + 0.25 * log(c.E);
+        g[2] = (double)y[1] * (double)net.norm.out_std[1] + (double)net.norm.out_mean[1];
+        g[3] = (double)y[2] * (double)net.norm.out_std[2] + (double)net.norm.out_mean[2];
+        g[1] = isfinite_(phw) ? phw : 0.0;
+        if (NCH && EOS == FIVO_EOS_LATTICE_HRG) {
+          const double T0 = jclamp(exp(g[0]), FV_T_MIN, FV_T_SOLVE_MAX);
+          const double K2 = lhrg_K2(lhrg_x(T0, d));
+          double Cn = (d.A_lhrg * T0) * K2;
+          if (d.p.hq_times_fmGeV3) Cn *= d.fmgev3;
+          const double ut = utau(g[2], g[3]);
+          const double nt = (c.D - nu_tau(g[2], g[3], ut, c.nux, c.nuy)) / ut;
+          if (nt > 0.0 && Cn > 0.0) g[1] = log(nt / Cn);
+        }
+        have_guess = isfinite_(g[0]) && isfinite_(g[1]) && isfinite_(g[2]) && isfinite_(g[3]);
+      }
+      /* pass 0: the learned guess; pass 1: the warm start (one call site) */
+      bool done = false;
+      for (int pass = have_guess ? 0 : 1; pass < 2 && !done; ++pass) {
+        if (pass == 1 && !warm) break;
+        const double a0 = pass == 0 ? g[0] : yTw, a1 = pass == 0 ? g[1] : phw;
+        const double a2 = pass == 0 ? g[2] : uxw, a3 = pass == 0 ? g[3] : uyw;
+        bool over = false;
+        int it = 0;
+        Recovery r = recover_fast<EOS, NCH>(c, d, a0, a1, a2, a3, d.p.primrec_maxit, d.p.primrec_tol,
+                                            pass == 0 ? d.p.primrec_maxit : FAST_BUDGET, &over,
+                                            pass == 0 ? GUESS_CHECK_IT : 0x7fffffff, GUESS_CHECK_TOL, &it);
+        if (pass == 0) { it_l += (unsigned)it; n_l = 1; } else { it_f += (unsigned)it; n_f = 1; }
+        if (!over && r.ok) {
+          store_recovery<EOS>(d, w, h, i, r);
+          done = true;
+          if (pass == 0) ok_l = 1;
+        }
+      }
+      defer = !done;
+    }
+  }
+  const unsigned lane = threadIdx.x & 31;
+  {
+    const unsigned a = __reduce_add_sync(0xffffffffu, it_l), b = __reduce_add_sync(0xffffffffu, n_l);
+    const unsigned e = __reduce_add_sync(0xffffffffu, ok_l), f = __reduce_add_sync(0xffffffffu, it_f);
+    const unsigned g2 = __reduce_add_sync(0xffffffffu, n_f);
+    if (lane == 0 && (b || g2)) {
+      atomicAdd(&fl->it_learn, (unsigned long long)a); atomicAdd(&fl->n_learn, (unsigned long long)b);
+      atomicAdd(&fl->ok_learn, (unsigned long long)e); atomicAdd(&fl->it_fb, (unsigned long long)f);
+      atomicAdd(&fl->n_fb, (unsigned long long)g2);
+    }
+  }
+  unsigned mv = __ballot_sync(0xffffffffu, live && vac);
+  if (lane == 0 && mv) atomicAdd((unsigned long long*)&fl->nvacuum, (unsigned long long)__popc(mv));
+  unsigned md = __ballot_sync(0xffffffffu, defer);
+  if (md) {
+    unsigned base = 0;
+    if (lane == 0) base = atomicAdd(&fl->qcount_p, (unsigned)__popc(md));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (defer) queue[base + __popc(md & ((1u << lane) - 1u))] = (unsigned)i;
+  }
+  if (!net_ok && threadIdx.x == 0) atomicExch(&fl->status, 3);
+}
+
+/* (features, targets) pairs of the interior cells whose recovery succeeded, every
+ * stride-th cell from phase on: out[k][11], k < cap, *count counts every offered
+ * pair (it may pass cap) */
+template <int EOS>
+__global__ void k_guess_harvest(DevParams d, DevState U, DevPrims w, double tau, float* out, unsigned long long cap,
+                                unsigned long long* count, int stride, int phase) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.Ntot || ((i + phase) % stride) != 0) return;
+  const int ix = (int)(i / d.Nytot), iy = (int)(i % d.Nytot);
+  if (!(ix >= d.ng && ix < d.ng + d.Nx && iy >= d.ng && iy < d.ng + d.Ny) || !w.ok[i]) return;
+  CellCons c;
+  load_cons(d, U, i, tau, c);
+  if (is_vacuum(c) || !(c.E > 0.0)) return;
+  float f[guess::NSAMP];
+  guess::features(c.E, c.Sx, c.Sy, c.Pi, c.pixx, c.pixy, c.piyy, f);
+  guess::targets(w.yT[i], w.ux[i], w.uy[i], c.E, f + guess::NIN);
+  for (int q = 0; q < guess::NSAMP; ++q) if (!isfinite(f[q])) return;
+  const unsigned long long k = atomicAdd(count, 1ULL);
+  if (k < cap)
+    for (int q = 0; q < guess::NSAMP; ++q) out[k * guess::NSAMP + q] = f[q];
 }
 
 /* Barrier of the two warps of pair p of a block (named barrier 1 + p, 64 threads). */

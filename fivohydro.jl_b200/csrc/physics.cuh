@@ -681,7 +681,8 @@ FX_HD void evalF_tp(double F[4], const double x[4], double T, const CellCons& c,
  * iteration budget of the fast pass; the same arithmetic, rounded the same way */
 template <int EOS, bool NCH>
 FX_HD Recovery recover_fast(const CellCons& c, const DevParams& d, double yT0, double phi0, double ux0,
-                            double uy0, int maxit, double tol, int budget, bool* over_budget) {
+                            double uy0, int maxit, double tol, int budget, bool* over_budget,
+                            int check_it = 0x7fffffff, double check_tol = 0.0, int* iters = nullptr) {
   Recovery out;
   const double yT_lo = d.log_T_min, yT_hi = d.log_T_solve_max;
   const double m = d.p.m_hq;
@@ -715,13 +716,20 @@ FX_HD Recovery recover_fast(const CellCons& c, const DevParams& d, double yT0, d
   double last_nrm = nan_();
   const int r_lo = NCH ? 0 : 1;
 
+  int nupd = 0;
   for (int it = 1; it <= maxit; ++it) {
+    nupd = it - 1;
     double nrm = 0.0;
 #pragma unroll
     for (int r = r_lo; r < 4; ++r) nrm = jmax(nrm, fabs_(F[r] * rs[r]));
     last_nrm = nrm;
     if (nrm < tol) { converged = true; out.reason = PRR_CONVERGED; break; }
-    if (it > budget) { *over_budget = true; return out; }
+    /* the budget of the fast pass, and the learned guess's test after check_it updates */
+    if (it > budget || (it == check_it + 1 && !(nrm <= check_tol))) {
+      *over_budget = true;
+      if (iters) *iters = nupd;
+      return out;
+    }
     /* ---- Jacobian: all 2 NU evaluations, then the finiteness test of the columns */
     const double h0 = 1e-6 * jmax(1.0, fabs_(x[0]));
     const double Tp = fx_exp(x[0] + h0), Tn = fx_exp(x[0] - h0);
@@ -795,6 +803,7 @@ FX_HD Recovery recover_fast(const CellCons& c, const DevParams& d, double yT0, d
     }
     if (!accepted) { out.reason = PRR_LINESEARCH_FAILED; break; }
   }
+  if (iters) *iters = nupd;
   out.resnorm = last_nrm;
   double T = jclamp(fx_exp(x[0]), FV_T_MIN, FV_T_SOLVE_MAX);
   double mu = NCH ? (m + (T * x[1])) : m;

@@ -88,6 +88,17 @@ KERNEL_CLASSES = ("prim_fast", "prim_slow", "faces", "update", "adm_slow", "rela
  FIVO_KCLASS_RELAX, FIVO_KCLASS_OTHER) = range(7)
 
 
+FIVO_GUESS_NPARAM, FIVO_GUESS_NNORM, FIVO_GUESS_NSAMP = 6288, 22, 11
+
+
+class FivoNewtonStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("it_fast", "n_fast", "it_learn", "n_learn", "ok_learn", "it_fb", "n_fb",
+                                          "deferred")]
+
+    def as_dict(self):
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+
+
 class FivoKernelTimes(C.Structure):
     _fields_ = [("launches", C.c_int64 * FIVO_KCLASS_N), ("ms", C.c_double * FIVO_KCLASS_N),
                 ("units", C.c_int64 * FIVO_KCLASS_N), ("total_launches", C.c_int64)]
@@ -96,6 +107,7 @@ PKG_DIR = pathlib.Path(__file__).resolve().parent
 LIB_PATH = PKG_DIR.parent / "csrc" / "libfivo2d.so"
 
 _D = C.POINTER(C.c_double)
+_F = C.POINTER(C.c_float)
 _U8 = C.POINTER(C.c_uint8)
 _I64 = C.c_int64
 
@@ -147,6 +159,21 @@ SIGNATURES = {
     "fivo_ctx_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "fivo_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "fivo_profile_read": (C.c_int, [C.c_void_p, C.POINTER(FivoKernelTimes), C.c_int]),
+    "fivo_guess_create": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_void_p)]),
+    "fivo_guess_destroy": (C.c_int, [C.c_void_p]),
+    "fivo_guess_set_params": (C.c_int, [C.c_void_p, _F, _F]),
+    "fivo_guess_get_params": (C.c_int, [C.c_void_p, _F, _F]),
+    "fivo_guess_reserve": (C.c_int, [C.c_void_p, _I64]),
+    "fivo_guess_set_samples": (C.c_int, [C.c_void_p, _F, _I64]),
+    "fivo_guess_get_samples": (C.c_int, [C.c_void_p, _F, _I64]),
+    "fivo_guess_nsamples": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "fivo_guess_harvest": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_int]),
+    "fivo_guess_fit_norm": (C.c_int, [C.c_void_p]),
+    "fivo_guess_train": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_uint64, _D]),
+    "fivo_guess_grad": (C.c_int, [C.c_void_p, _F, _I64, _F, _D]),
+    "fivo_guess_forward": (C.c_int, [C.c_void_p, _F, _I64, _F]),
+    "fivo_ctx_set_guess": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "fivo_newton_stats_read": (C.c_int, [C.c_void_p, C.POINTER(FivoNewtonStats), C.c_int]),
 }
 
 _LIB = None

@@ -348,6 +348,65 @@ int  fivo_batch_advance(fivo_batch* b, const double* tau, double taufinal, doubl
                         double CFLtau, int integrator, int bc, int64_t max_steps,
                         fivo_run_result* results, int* status);
 
+/* --- the learned starting guess of the primitive recovery (no counterpart in
+ * the reference: its Newton starts from the previous step's primitives or the
+ * closed-form seed, src2d/primrec2d.jl:300-347,465-486) ---
+ * An MLP 8 -> 64 -> 64 -> 3 (GELU; BF16 weights, FP32 accumulation on the
+ * tensor cores) maps a cell's normalised (log E, S^x/E, S^y/E, Pi/E, pi^xx/E,
+ * pi^xy/E, pi^yy/E, |S|/E) to (log T - log(E)/4, u^x, u^y); the charm chemical
+ * potential of the guess follows in closed form from N^tau. A context with a
+ * guess attached starts each cell's Newton there; a cell whose residual is above
+ * 1e-10 after 3 updates falls back to the plain warm-started recovery. Results
+ * then agree with the plain path to the recovery tolerance, not bitwise.
+ * Parameters: FIVO_GUESS_NPARAM floats, W1[64][16] b1[64] W2[64][64] b2[64]
+ * W3[16][64] b3[16] (W[out][in]; columns 8..15 of W1, rows 3..15 of W3 and
+ * b3[3..15] are padding and stay 0). Normalisation: FIVO_GUESS_NNORM floats,
+ * in_mean[8] in_istd[8] out_mean[3] out_std[3]. A sample is 11 floats: the 8
+ * raw features and the 3 raw targets. */
+#define FIVO_GUESS_NPARAM 6288
+#define FIVO_GUESS_NNORM 22
+#define FIVO_GUESS_NSAMP 11
+typedef struct fivo_guess fivo_guess;
+typedef struct {
+  uint64_t it_fast, n_fast;      /* Newton updates / attempts of the warm-started pass   */
+  uint64_t it_learn, n_learn;    /* ... of the attempts from the learned guess           */
+  uint64_t ok_learn;             /* learned attempts accepted                             */
+  uint64_t it_fb, n_fb;          /* warm attempts after a rejected learned guess          */
+  uint64_t deferred;             /* cells deferred to the slow pass                       */
+} fivo_newton_stats;
+/* on the device of `ctx_or_null` (the current device when NULL); weights drawn
+ * from a seeded uniform(-1/sqrt(fan_in), 1/sqrt(fan_in)), identity normalisation */
+int  fivo_guess_create(fivo_ctx* ctx_or_null, uint64_t seed, fivo_guess** out);
+int  fivo_guess_destroy(fivo_guess* g);
+int  fivo_guess_set_params(fivo_guess* g, const float* params, const float* norm);
+int  fivo_guess_get_params(fivo_guess* g, float* params, float* norm);
+/* the device sample store: capacity in samples; set/get copy host samples in/out */
+int  fivo_guess_reserve(fivo_guess* g, int64_t capacity);
+int  fivo_guess_set_samples(fivo_guess* g, const float* samples, int64_t n);
+int  fivo_guess_get_samples(fivo_guess* g, float* samples, int64_t n);
+int  fivo_guess_nsamples(fivo_guess* g, int64_t* n);
+/* append the (features, targets) pairs of ctx's interior cells: the features
+ * from its current state, the targets from its last primitive pass, so that
+ * pass must be of the current state (fivo_update_primitives after a step, whose
+ * relaxation moved the dissipative rows); every stride-th cell from phase;
+ * stops at capacity */
+int  fivo_guess_harvest(fivo_ctx* ctx, fivo_guess* g, double tau, int stride, int phase);
+/* normalisation = the mean and standard deviation of the stored samples */
+int  fivo_guess_fit_norm(fivo_guess* g);
+/* steps of Adam (beta 0.9, 0.999, eps 1e-8) on the mean-squared error of the
+ * normalised outputs, batch = 128 * ctas_per_step samples drawn with a seeded
+ * hash; loss_out[0] = the loss of the first step, loss_out[1] = of the last */
+int  fivo_guess_train(fivo_guess* g, int steps, int ctas_per_step, float lr, uint64_t seed,
+                      double* loss_out);
+/* the gradient of the mean-squared error over n samples (n % 128 == 0, taken in
+ * order) with respect to every parameter, and that loss; no update */
+int  fivo_guess_grad(fivo_guess* g, const float* samples, int64_t n, float* grad, double* loss);
+/* normalised outputs out[k*3 + o] for raw features raw[k*8 + q] */
+int  fivo_guess_forward(fivo_guess* g, const float* raw, int64_t n, float* out);
+/* attach (g) or detach (NULL) the guess; the context keeps no ownership */
+int  fivo_ctx_set_guess(fivo_ctx* ctx, fivo_guess* g);
+int  fivo_newton_stats_read(fivo_ctx* ctx, fivo_newton_stats* out, int reset);
+
 /* --- streams, synchronisation, timing --- */
 int  fivo_sync(fivo_ctx* ctx);
 /* Run the context's later calls on a caller's CUDA stream (a cudaStream_t of
