@@ -70,6 +70,57 @@ def ic_fields(g, seed):
     return T, a, ux, uy
 
 
+# ----------------------------------------------------------------------------- the learned guess
+
+GUESS_SEEDS = (3001, 3002, 3003)     # training events: never the timed ones (1001 + rank, 1000 + k)
+GUESS_TRAIN_STEPS = 220              # per training event (the timed window ends near step 210)
+
+
+def train_guess(lib, m, g, seeds=GUESS_SEEDS, nsteps=GUESS_TRAIN_STEPS, train_steps=3000):
+    """Harvest (features, primitives) pairs from plain runs of seeded training events
+    on grid g (every 4th step, every 8th cell), fit the normalisation and train the
+    guess network on the GPU. Returns (guess, info)."""
+    from fivo2d import _abi as A
+    from fivo2d.guess import RecoveryGuess
+    from fivo2d.solver import GPUWork2D, set_cells
+
+    t0 = time.perf_counter()
+    guess = RecoveryGuess(lib=lib, seed=17)
+    guess.reserve(8_000_000)
+    harvested_steps = 0
+    for s in seeds:
+        T, a, ux, uy = ic_fields(g, s)
+        U, _ = set_cells(m, TAU0, T, a, ux, uy, lib=lib)
+        wt = GPUWork2D(m, g, lib=lib)
+        wt.set_state(U)
+        wt.finalize_ic(TAU0)
+        wt.rhs(TAU0)
+        tau = TAU0
+        for k in range(nsteps):
+            r = wt.advance(tau, 1e9, CFL, CFLTAU, A.FIVO_SSPRK3, max_steps=1)
+            if not r["ok"]:
+                break
+            tau = r["tau"]
+            if k % 4 == 0:
+                wt.update_primitives(tau)
+                guess.harvest(wt, tau, stride=8, phase=(k // 4) % 8)
+                harvested_steps += 1
+        wt.close()
+    t1 = time.perf_counter()
+    guess.fit_norm()
+    l0, l1 = guess.train(train_steps, ctas_per_step=148, lr=2e-3, seed=5)
+    t2 = time.perf_counter()
+    return guess, {"samples": guess.nsamples(), "training_events": list(seeds),
+                   "harvested_steps": harvested_steps, "train_steps": train_steps,
+                   "batch": 148 * 128, "loss_first": l0, "loss_last": l1,
+                   "harvest_s": t1 - t0, "train_s": t2 - t1}
+
+
+def l2_rel(a, b):
+    import numpy as np
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
 # ----------------------------------------------------------------------------- clocks
 
 class ClockSampler:
@@ -181,9 +232,12 @@ def run_gpu(args):
 
     lib = A.load_library()
     g, m = model_and_grid()
+    guess, ginfo = (train_guess(lib, m, g) if args.guess else (None, None))
     T, a, ux, uy = ic_fields(g, SEED + rank)
     U0, ok = set_cells(m, TAU0, T, a, ux, uy, lib=lib)
     w = GPUWork2D(m, g, lib=lib)
+    if guess is not None:
+        guess.attach(w)
     stream = torch.cuda.Stream()
     A.check(lib, lib.fivo_ctx_set_stream(w.h, C.c_void_p(stream.cuda_stream)), "set_stream")
     w.set_state(U0)
@@ -221,6 +275,12 @@ def run_gpu(args):
     twin = GPUWork2D(m, g, lib=lib)
     A.check(lib, lib.fivo_ctx_set_stream(twin.h, C.c_void_p(stream.cuda_stream)), "set_stream")
     twin.clone_state_from(w)
+    if guess is not None:
+        from fivo2d.guess import newton_stats
+        guess.attach(twin)
+        plain = GPUWork2D(m, g, lib=lib)          # the plain FP64 path over the same steps
+        plain.clone_state_from(w)
+        newton_stats(w, reset=True)
 
     # ---------------- device-resident timing
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -249,9 +309,34 @@ def run_gpu(args):
         l2_flush()
         tau_r = step_on(twin.h, tau_r, 1)
     lib.fivo_profile_read(twin.h, C.byref(kt), 1)
-    if tau_r != tau:
+    if guess is None and tau_r != tau:
         raise RuntimeError("the profiled replay left the timed trajectory")
     twin.close()
+    learned = None
+    if guess is not None:
+        import numpy as np
+        st = newton_stats(w)
+        pw = w.primitives()
+        tau_p = tau_start
+        for k in range(args.steps):
+            tau_p = step_on(plain.h, tau_p, 1)
+        pp = plain.primitives()
+        sx, sy = g.interior()
+        okm = ((pw["ok"] == 1) & (pp["ok"] == 1)).reshape(g.Nxtot, g.Nytot)[sx, sy]
+
+        def inner(p, key):
+            return p[key].reshape(g.Nxtot, g.Nytot)[sx, sy][okm]
+        learned = dict(ginfo)
+        learned.update({
+            "accept_rate": st["ok_learn"] / max(1, st["n_learn"]),
+            "fallback_rate": 1.0 - st["ok_learn"] / max(1, st["n_learn"]),
+            "updates_per_cell": (st["it_learn"] + st["it_fb"]) / max(1, st["n_learn"]),
+            "slow_pass_cells_per_step": st["deferred"] / args.steps,
+            "vs_plain_fp64": {"steps": args.steps, "tau_learned": tau, "tau_plain": tau_p,
+                              "L2_T": l2_rel(np.exp(inner(pw, "yT")), np.exp(inner(pp, "yT"))),
+                              "L2_ux": l2_rel(inner(pw, "ux"), inner(pp, "ux")),
+                              "L2_uy": l2_rel(inner(pw, "uy"), inner(pp, "uy"))}})
+        plain.close()
     clocks = clk.summary()
     t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if dist:
@@ -331,6 +416,11 @@ def run_gpu(args):
         "roofline": roof,
         "clocks": clocks,
     }
+    if learned is not None:
+        line["learned_guess"] = learned
+        line["config"]["workload"] = WORKLOAD + "_learned_guess"
+        line["config"]["recovery"] = ("learned MLP guess (BF16 tcgen05, FP32 accumulate), fallback to the "
+                                      "plain warm start; trained on seeds " + str(list(GUESS_SEEDS)))
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.cpu_steps)
     return line
@@ -366,10 +456,16 @@ def run_batch(args):
     grids = event_grids(args.events)
     mine = shard_events([g.Nx * g.Ny for g in grids], world, rank)
     my_grids = [grids[k] for k in mine]
+    guess, ginfo = (None, None)
+    if args.guess:
+        g384, _ = model_and_grid()
+        guess, ginfo = train_guess(lib, m, g384)
     b = GPUBatch2D(m, my_grids, nworkers=args.workers, lib=lib)
     for e, k in zip(b.events, mine):
         e.glauber_ic(TAU0, 1000 + k)      # the MC-Glauber IC built on the device
         e.rhs(TAU0)
+        if guess is not None:
+            guess.attach(e)
     taus = [TAU0] * len(mine)
 
     def adv(n):
@@ -380,6 +476,10 @@ def run_batch(args):
         taus = [x["tau"] for x in r]
 
     adv(args.warmup)
+    if guess is not None:
+        from fivo2d.guess import newton_stats
+        for e in b.events:
+            newton_stats(e, reset=True)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -398,6 +498,16 @@ def run_batch(args):
     else:
         cells_all = float(cells)
     value = args.steps * cells_all / dt
+    learned = None
+    if guess is not None:
+        tot = {}
+        for e in b.events:
+            for key, v in newton_stats(e).items():
+                tot[key] = tot.get(key, 0) + v
+        learned = dict(ginfo)
+        learned.update({"accept_rate": tot["ok_learn"] / max(1, tot["n_learn"]),
+                        "updates_per_cell": (tot["it_learn"] + tot["it_fb"]) / max(1, tot["n_learn"]),
+                        "slow_pass_cells_per_step": tot["deferred"] / args.steps})
     # end to end: the host holds every event's state; each step uploads, advances, downloads
     hosts = [e.get_state() for e in b.events]
     e2e_steps = max(1, min(args.steps, 5))
@@ -422,7 +532,7 @@ def run_batch(args):
     if rank != 0:
         return None
     sizes = sorted({g.Nx for g in grids})
-    return {
+    line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded MC-Glauber events)",
@@ -434,6 +544,10 @@ def run_batch(args):
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
                 "steps": e2e_steps},
     }
+    if learned is not None:
+        line["learned_guess"] = learned
+        line["config"]["workload"] += "_learned_guess"
+    return line
 
 
 # ----------------------------------------------------------------------------- CPU legs
@@ -508,6 +622,8 @@ def main():
                     help="event: the 384^2 viscous event (default); batch: many uneven events")
     ap.add_argument("--events", type=int, default=32, help="batch workload: number of events")
     ap.add_argument("--workers", type=int, default=0, help="batch workload: host threads (0: library default)")
+    ap.add_argument("--guess", action="store_true",
+                    help="train the learned recovery guess on other seeded events and time with it attached")
     args = ap.parse_args()
     if args.workload == "batch":
         # more hardware queues for the per-event streams (read when CUDA initialises)

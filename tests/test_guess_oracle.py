@@ -80,3 +80,29 @@ def test_device_rounded_gradient_tracks_float64():
     rel = np.linalg.norm(g - g64) / np.linalg.norm(g64)
     assert rel < 3e-2, rel
     assert abs(loss - G.loss64(P, G.normalise(norm, samples), G.norm_targets(norm, samples))) < 3e-2 * loss
+
+
+def _cutlass_include():
+    import site
+    for sp in site.getsitepackages():
+        p = pathlib.Path(sp) / "flashinfer" / "data" / "cutlass" / "include"
+        if (p / "cute" / "arch" / "mma_sm100_desc.hpp").exists():
+            return p
+    return None
+
+
+def test_tc05_descriptors_match_cutlass(tmp_path):
+    """the tensor-core descriptor encoders (csrc/tc05.cuh) against CUTLASS's own
+    bitfield definitions of the sm_100 UMMA descriptors, on the CPU"""
+    import shutil
+    import subprocess
+    inc = _cutlass_include()
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if inc is None or not pathlib.Path(nvcc).exists():
+        pytest.skip("CUTLASS headers or nvcc not available")
+    src = pathlib.Path(__file__).resolve().parent / "native" / "tc05_desc_check.cu"
+    exe = tmp_path / "tc05_desc_check"
+    subprocess.run([nvcc, "-std=c++17", "-Wno-deprecated-gpu-targets", f"-I{inc}", "-o", str(exe), str(src)],
+                   check=True, capture_output=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0 and out.stdout.strip() == "ok", out.stdout
