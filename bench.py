@@ -550,6 +550,60 @@ def run_batch(args):
     return line
 
 
+# ----------------------------------------------------------------------------- freeze-out
+
+def run_freezeout(args):
+    """The axisymmetric control of freezeout2d.jl: the calibrated radial profile on
+    200^2 cells over [-18, 18] fm, evolved from tau 0.4 to 16 in chunks of 0.02 with
+    the freeze_surface model, the T = 0.156 surface recorded after every chunk, then
+    the Cooper-Frye pion yield over it. The 1-D calibration it should reproduce is
+    N_pi = 1339.63 (freezeout2d.jl:7-10, 73-75)."""
+    import numpy as np
+    import torch
+
+    import fivo2d
+    from fivo2d import _abi as A
+    from fivo2d.freezeout import axisym_fields, cf_params, freeze_model, freeze_surface
+    from fivo2d.solver import GPUWork2D, set_cells
+
+    lib = A.load_library()
+    g = fivo2d.make_grid2d(200, 200, xmax=18.0, ymax=18.0)
+    m = freeze_model()
+    T, a, ux, uy = axisym_fields(g, ROOT / "tests" / "golden" / "initial_profiles_physical.csv")
+    U, _ = set_cells(m, 0.4, T, a, ux, uy, lib=lib)
+    w = GPUWork2D(m, g, lib=lib)
+    w.set_state(U)
+    w.finalize_ic(0.4)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    fo, chunks = freeze_surface(w, 0.4, 16.0, dtau=0.02)
+    t1 = time.perf_counter()
+    s = fo.surface()
+    p = cf_params()
+    fo.pion_yield(p)                       # warm-up
+    reps = 5
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    for _ in range(reps):
+        NB, Nb, negf = fo.pion_yield(p)
+    t3 = time.perf_counter()
+    ncells = int(np.sum(~np.isnan(s["tau_fo"])))
+    evals = ncells * p.n_pt * p.n_phi * p.n_eta
+    cf_s = (t3 - t2) / reps
+    return {
+        "metric": "Cooper-Frye integrand evaluations/s (freeze-out surface of the axisymmetric control)",
+        "value": evals / cf_s, "unit": "evaluations/s", "n_gpus": 1, "higher_is_better": True,
+        "dtype": "f64", "data": "the reference's calibrated radial profile (data/initial_profiles_physical.csv)",
+        "config": {"workload": "freezeout_axisym_200x200_box18_tau0.4-16_dtau0.02_Tfo0.156",
+                   "grid": [200, 200], "cf_grid": [p.n_pt, p.n_phi, p.n_eta],
+                   "timing": "host wall clock around synchronous calls"},
+        "freezeout": {"dNdy_boltzmann": NB, "dNdy_bose": Nb, "negative_dsigma_fraction": negf,
+                      "calibration_1d": 1339.63, "chunks": chunks, "surface_run_s": t1 - t0,
+                      "cooper_frye_ms": 1e3 * cf_s, "cells_hot": s["nhot"], "cells_frozen": s["nfroze"],
+                      "reheated_after_freezing": s["refroze"]},
+    }
+
+
 # ----------------------------------------------------------------------------- CPU legs
 
 def oracle_event():
@@ -618,7 +672,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=30)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="event", choices=["event", "batch"],
+    ap.add_argument("--workload", default="event", choices=["event", "batch", "freezeout"],
                     help="event: the 384^2 viscous event (default); batch: many uneven events")
     ap.add_argument("--events", type=int, default=32, help="batch workload: number of events")
     ap.add_argument("--workers", type=int, default=0, help="batch workload: host threads (0: library default)")
@@ -634,6 +688,8 @@ def main():
         line = run_reference(args)
     elif args.workload == "batch":
         line = run_batch(args)
+    elif args.workload == "freezeout":
+        line = run_freezeout(args)
     else:
         line = run_gpu(args)
     if line is not None:

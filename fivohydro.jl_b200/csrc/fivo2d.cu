@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "freezeout.cuh"
 
 using namespace fv;
 
@@ -1657,5 +1658,151 @@ int fivo_newton_stats_read(fivo_ctx* c, fivo_newton_stats* out, int reset) {
     c->stats_base_p = (int64_t)f.tot_p;
     CK(ctx_sync(c));
   }
+  return FIVO_OK;
+}
+
+/* ------------------------------------------------ freeze-out surface and Cooper-Frye */
+
+struct fivo_fo {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  int nx = 0, ny = 0;
+  double dx = 0.0, T_fo = 0.0;
+  double tau_prev = 0.0;
+  bool have_prev = false;
+  double* planes = nullptr;               /* tau_fo | uxf | uyf | Tprev */
+  uint8_t* above = nullptr;
+  unsigned long long* refroze = nullptr;
+  double* part = nullptr;
+  long long part_n = 0;
+};
+
+namespace {
+fo::Surf surf_of(fivo_fo* f) {
+  const size_t n = (size_t)f->nx * f->ny;
+  return fo::Surf{f->planes, f->planes + n, f->planes + 2 * n, f->planes + 3 * n, f->above, f->refroze, f->nx, f->ny};
+}
+}  // namespace
+
+void fivo_cf_params_default(fivo_cf_params* p) {
+  if (!p) return;
+  p->T_fo = 0.156; p->m = 0.138; p->pt_lo = 0.1; p->pt_hi = 5.0; p->eta_max = 6.0; p->f_yield = 2.0 * 2.5;
+  p->n_eta = 40; p->n_pt = 40; p->n_phi = 24; p->pad = 0;
+}
+
+int fivo_fo_create(fivo_ctx* c, double T_fo, fivo_fo** out) {
+  if (!c || !out || !(T_fo > 0.0)) return fail(FIVO_ERR_ARG, "bad argument");
+  *out = nullptr;
+  fivo_fo* f = new fivo_fo();
+  f->device = c->device; f->nx = c->dp.Nx; f->ny = c->dp.Ny; f->dx = c->dp.dx; f->T_fo = T_fo;
+  if (c->dp.dx != c->dp.dy) { delete f; return fail(FIVO_ERR_ARG, "fivo_fo_create: the surface needs dx == dy"); }
+  const size_t n = (size_t)f->nx * f->ny;
+  if (cudaStreamCreateWithFlags(&f->st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&f->planes, 4 * n * sizeof(double)) != cudaSuccess || cudaMalloc(&f->above, n) != cudaSuccess ||
+      cudaMalloc(&f->refroze, sizeof(unsigned long long)) != cudaSuccess) {
+    fivo_fo_destroy(f);
+    return fail(FIVO_ERR_NOMEM, "fivo_fo_create: device allocation failed");
+  }
+  int rc = fivo_fo_reset(f);
+  if (rc) { fivo_fo_destroy(f); return rc; }
+  *out = f;
+  return FIVO_OK;
+}
+
+int fivo_fo_reset(fivo_fo* f) {
+  if (!f) return fail(FIVO_ERR_ARG, "null surface");
+  const size_t n = (size_t)f->nx * f->ny;
+  k_fill_nan<<<nblk((long long)n, 256), 256, 0, f->st>>>(f->planes, (long long)n);             /* tau_fo */
+  CKL();
+  CK(cudaMemsetAsync(f->planes + n, 0, 2 * n * sizeof(double), f->st));                     /* uxf, uyf */
+  k_fill_nan<<<nblk((long long)n, 256), 256, 0, f->st>>>(f->planes + 3 * n, (long long)n);  /* Tprev */
+  CKL();
+  CK(cudaMemsetAsync(f->above, 0, n, f->st));
+  CK(cudaMemsetAsync(f->refroze, 0, sizeof(unsigned long long), f->st));
+  CK(cudaStreamSynchronize(f->st));
+  f->have_prev = false;
+  return FIVO_OK;
+}
+
+int fivo_fo_destroy(fivo_fo* f) {
+  if (!f) return FIVO_OK;
+  if (f->st) cudaStreamSynchronize(f->st);
+  cudaFree(f->planes); cudaFree(f->above); cudaFree(f->refroze); cudaFree(f->part);
+  if (f->st) cudaStreamDestroy(f->st);
+  delete f;
+  return FIVO_OK;
+}
+
+int fivo_fo_record(fivo_fo* f, fivo_ctx* c, double tau) {
+  if (!f || !c) return fail(FIVO_ERR_ARG, "null argument");
+  if (c->dp.Nx != f->nx || c->dp.Ny != f->ny) return fail(FIVO_ERR_ARG, "fivo_fo_record: grid mismatch");
+  const double tp = f->have_prev ? f->tau_prev : tau;
+  const long long n = (long long)f->nx * f->ny;
+  fo::k_record<<<nblk(n, 256), 256, 0, c->st>>>(c->dp, c->w, tau, tp, f->T_fo, surf_of(f));
+  CKL();
+  CK(ctx_sync(c));
+  f->tau_prev = tau;
+  f->have_prev = true;
+  return FIVO_OK;
+}
+
+int fivo_fo_surface(fivo_fo* f, double* tau_fo, double* uxf, double* uyf, int64_t* counts) {
+  if (!f) return fail(FIVO_ERR_ARG, "null surface");
+  const size_t n = (size_t)f->nx * f->ny;
+  std::vector<double> t(n);
+  std::vector<uint8_t> ab(n);
+  unsigned long long rf = 0;
+  CK(cudaMemcpyAsync(t.data(), f->planes, n * sizeof(double), cudaMemcpyDeviceToHost, f->st));
+  if (uxf) CK(cudaMemcpyAsync(uxf, f->planes + n, n * sizeof(double), cudaMemcpyDeviceToHost, f->st));
+  if (uyf) CK(cudaMemcpyAsync(uyf, f->planes + 2 * n, n * sizeof(double), cudaMemcpyDeviceToHost, f->st));
+  CK(cudaMemcpyAsync(ab.data(), f->above, n, cudaMemcpyDeviceToHost, f->st));
+  CK(cudaMemcpyAsync(&rf, f->refroze, sizeof(rf), cudaMemcpyDeviceToHost, f->st));
+  CK(cudaStreamSynchronize(f->st));
+  if (tau_fo) std::memcpy(tau_fo, t.data(), n * sizeof(double));
+  if (counts) {
+    int64_t hot = 0, froze = 0;
+    for (size_t k = 0; k < n; ++k) { hot += ab[k] != 0; froze += !std::isnan(t[k]); }
+    counts[0] = hot; counts[1] = froze; counts[2] = (int64_t)rf;
+  }
+  return FIVO_OK;
+}
+
+int fivo_fo_set_surface(fivo_fo* f, const double* tau_fo, const double* uxf, const double* uyf) {
+  if (!f || !tau_fo || !uxf || !uyf) return fail(FIVO_ERR_ARG, "null argument");
+  const size_t n = (size_t)f->nx * f->ny;
+  CK(cudaMemcpyAsync(f->planes, tau_fo, n * sizeof(double), cudaMemcpyHostToDevice, f->st));
+  CK(cudaMemcpyAsync(f->planes + n, uxf, n * sizeof(double), cudaMemcpyHostToDevice, f->st));
+  CK(cudaMemcpyAsync(f->planes + 2 * n, uyf, n * sizeof(double), cudaMemcpyHostToDevice, f->st));
+  CK(cudaStreamSynchronize(f->st));
+  return FIVO_OK;
+}
+
+int fivo_cooper_frye(fivo_fo* f, const fivo_cf_params* p, double* out) {
+  if (!f || !p || !out) return fail(FIVO_ERR_ARG, "null argument");
+  if (p->n_eta < 2 || p->n_pt < 2 || p->n_phi < 1 || !(p->T_fo > 0.0))
+    return fail(FIVO_ERR_ARG, "fivo_cooper_frye: bad grid");
+  const long long total = (long long)f->nx * f->ny * p->n_pt * p->n_phi;
+  const long long nb = nblk(total, 256);
+  if (nb > f->part_n) {
+    cudaFree(f->part);
+    f->part = nullptr;
+    f->part_n = 0;
+    CK(cudaMalloc(&f->part, (size_t)nb * 4 * sizeof(double)));
+    f->part_n = nb;
+  }
+  const fo::CF cf{p->T_fo, p->m, p->pt_lo, p->pt_hi, p->eta_max, p->n_eta, p->n_pt, p->n_phi};
+  fo::k_cooper_frye<<<(unsigned)nb, 256, 0, f->st>>>(surf_of(f), f->dx, cf, f->part);
+  CKL();
+  std::vector<double> h((size_t)nb * 4);
+  CK(cudaMemcpyAsync(h.data(), f->part, h.size() * sizeof(double), cudaMemcpyDeviceToHost, f->st));
+  CK(cudaStreamSynchronize(f->st));
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  for (long long b = 0; b < nb; ++b)
+    for (int q = 0; q < 4; ++q) s[q] += h[(size_t)b * 4 + q];
+  const double hc = 0.1973269804;
+  const double pref = p->f_yield / std::pow((2.0 * M_PI) * hc, 3);
+  out[0] = pref * s[0];
+  out[1] = pref * s[1];
+  out[2] = s[2] / std::max(s[3] + s[2], 1e-30);
   return FIVO_OK;
 }

@@ -99,6 +99,12 @@ class FivoNewtonStats(C.Structure):
         return {n: int(getattr(self, n)) for n, _ in self._fields_}
 
 
+class FivoCFParams(C.Structure):
+    _fields_ = [("T_fo", C.c_double), ("m", C.c_double), ("pt_lo", C.c_double), ("pt_hi", C.c_double),
+                ("eta_max", C.c_double), ("f_yield", C.c_double), ("n_eta", C.c_int32), ("n_pt", C.c_int32),
+                ("n_phi", C.c_int32), ("pad", C.c_int32)]
+
+
 class FivoKernelTimes(C.Structure):
     _fields_ = [("launches", C.c_int64 * FIVO_KCLASS_N), ("ms", C.c_double * FIVO_KCLASS_N),
                 ("units", C.c_int64 * FIVO_KCLASS_N), ("total_launches", C.c_int64)]
@@ -174,6 +180,14 @@ SIGNATURES = {
     "fivo_guess_forward": (C.c_int, [C.c_void_p, _F, _I64, _F]),
     "fivo_ctx_set_guess": (C.c_int, [C.c_void_p, C.c_void_p]),
     "fivo_newton_stats_read": (C.c_int, [C.c_void_p, C.POINTER(FivoNewtonStats), C.c_int]),
+    "fivo_cf_params_default": (None, [C.POINTER(FivoCFParams)]),
+    "fivo_fo_create": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_void_p)]),
+    "fivo_fo_destroy": (C.c_int, [C.c_void_p]),
+    "fivo_fo_reset": (C.c_int, [C.c_void_p]),
+    "fivo_fo_record": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double]),
+    "fivo_fo_surface": (C.c_int, [C.c_void_p, _D, _D, _D, C.POINTER(C.c_int64)]),
+    "fivo_fo_set_surface": (C.c_int, [C.c_void_p, _D, _D, _D]),
+    "fivo_cooper_frye": (C.c_int, [C.c_void_p, C.POINTER(FivoCFParams), _D]),
 }
 
 _LIB = None

@@ -407,6 +407,35 @@ int  fivo_guess_forward(fivo_guess* g, const float* raw, int64_t n, float* out);
 int  fivo_ctx_set_guess(fivo_ctx* ctx, fivo_guess* g);
 int  fivo_newton_stats_read(fivo_ctx* ctx, fivo_newton_stats* out, int reset);
 
+/* --- the freeze-out surface and its Cooper-Frye pion yield (freezeout2d.jl) ---
+ * The surface tau = tau_fo(x, y) over ctx's interior cells: each record takes the
+ * primitives of ctx's last primitive pass (fivo_update_primitives first, as
+ * freeze_surface does after each chunk of the run) and, per cell, keeps the last
+ * downward crossing of T_fo, interpolated linearly between records, with the flow
+ * at that record (freezeout2d.jl:94-115). Arrays are Nx x Ny, cell (a, b) at
+ * a * Ny + b; tau_fo is NaN where the cell has not frozen. counts = (cells ever
+ * above T_fo, cells frozen, re-heatings after freezing). */
+typedef struct fivo_fo fivo_fo;
+typedef struct {
+  double T_fo;       /* GeV (0.156)                                    */
+  double m;          /* particle mass, GeV (pion: 0.138)               */
+  double pt_lo, pt_hi;  /* p_T range, GeV (0.1, 5.0)                   */
+  double eta_max;    /* |eta| <= eta_max (6)                           */
+  double f_yield;    /* overall factor (2 charge states x 2.5 feed-down) */
+  int32_t n_eta, n_pt, n_phi, pad;   /* grid (40, 40, 24)              */
+} fivo_cf_params;
+void fivo_cf_params_default(fivo_cf_params* p);
+int  fivo_fo_create(fivo_ctx* ctx, double T_fo, fivo_fo** out);
+int  fivo_fo_destroy(fivo_fo* f);
+int  fivo_fo_reset(fivo_fo* f);
+int  fivo_fo_record(fivo_fo* f, fivo_ctx* ctx, double tau);
+int  fivo_fo_surface(fivo_fo* f, double* tau_fo, double* uxf, double* uyf, int64_t* counts);
+int  fivo_fo_set_surface(fivo_fo* f, const double* tau_fo, const double* uxf, const double* uyf);
+/* pion_yield (freezeout2d.jl:144-190): out = (dN/dy Boltzmann, dN/dy Bose,
+ * negative-dSigma fraction of the Boltzmann integrand); one-sided tau_fo gradients
+ * at the rim of the frozen region, cells without a gradient skipped */
+int  fivo_cooper_frye(fivo_fo* f, const fivo_cf_params* p, double* out);
+
 /* --- streams, synchronisation, timing --- */
 int  fivo_sync(fivo_ctx* ctx);
 /* Run the context's later calls on a caller's CUDA stream (a cudaStream_t of

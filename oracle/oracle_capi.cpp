@@ -4,6 +4,8 @@
  * Signatures mirror include/fivo2d.h with an `oracle_` prefix; the state is
  * the reference's AoS U[a, i] (cell i, field a at U[i*nv + a]).
  */
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <string>
 #include "oracle_core.h"
@@ -241,6 +243,92 @@ double oracle_cfm_dn_dT(const fivo_params* p, double T, double n) { return cfm_d
 void oracle_diff_coeffs(const fivo_params* p, double T, double mu, double n, double* kappa, double* taun,
                         double* dN) {
   cfm_diff_coeffs(T, mu, n, *p, kappa, taun, dN);
+}
+
+/* record!(tau) of freeze_surface, freezeout2d.jl:94-115, on the context's last
+ * primitives; arrays nx x ny (cell (a, b) at a*ny + b); *refroze accumulates */
+void oracle_fo_record(void* h, double tau, double tau_prev, double T_fo, double* tau_fo, double* uxf,
+                      double* uyf, double* Tprev, uint8_t* above, int64_t* refroze) {
+  OCtx* c = (OCtx*)h;
+  const Grid& g = c->g;
+  for (int a = 0; a < g.Nx; ++a)
+    for (int b = 0; b < g.Ny; ++b) {
+      const int64_t k = (int64_t)a * g.Ny + b;
+      const int64_t i = (int64_t)(g.ng + a) * g.Nytot + (g.ng + b);
+      const double T = o_exp(c->w.yT[i]);
+      if (T > T_fo) {
+        if (!std::isnan(tau_fo[k])) *refroze += 1;
+        above[k] = 1;
+        tau_fo[k] = O_NAN;
+      } else if (above[k] && std::isnan(tau_fo[k])) {
+        const double Tp = Tprev[k];
+        tau_fo[k] = (std::isnan(Tp) || Tp <= T_fo) ? tau : tau_prev + ((tau - tau_prev) * (Tp - T_fo)) / (Tp - T);
+        uxf[k] = c->w.ux[i];
+        uyf[k] = c->w.uy[i];
+      }
+      Tprev[k] = T;
+    }
+}
+
+/* grad1, freezeout2d.jl:132-141 */
+static double fo_grad1(const double* A, int ny, int a, int b, int dir, double dx) {
+  const double lo = dir == 1 ? A[(a - 1) * ny + b] : A[a * ny + b - 1];
+  const double hi = dir == 1 ? A[(a + 1) * ny + b] : A[a * ny + b + 1];
+  const double cc = A[a * ny + b];
+  if (!std::isnan(lo) && !std::isnan(hi)) return (hi - lo) / (2.0 * dx);
+  if (!std::isnan(hi)) return (hi - cc) / dx;
+  if (!std::isnan(lo)) return (cc - lo) / dx;
+  return O_NAN;
+}
+
+/* pion_yield, freezeout2d.jl:144-190, in its loop order (a outer, summed in order);
+ * prm = (T_fo, m, pt_lo, pt_hi, eta_max, f_yield), ngrid = (n_eta, n_pt, n_phi);
+ * out = (N_boltzmann, N_bose, negative fraction) */
+void oracle_pion_yield(int nx, int ny, double dx, const double* tau_fo, const double* uxf, const double* uyf,
+                       const double* prm, const int* ngrid, double* out) {
+  const double T_fo = prm[0], m = prm[1], pt_lo = prm[2], pt_hi = prm[3], eta_max = prm[4], fy = prm[5];
+  const int n_eta = ngrid[0], n_pt = ngrid[1], n_phi = ngrid[2];
+  const double dpt = (pt_hi - pt_lo) / (double)(n_pt - 1);
+  const double dphi = (2.0 * M_PI) / (double)n_phi;
+  const double deta = (2.0 * eta_max) / (double)(n_eta - 1);
+  double tot = 0.0, totB = 0.0, negc = 0.0, posc = 0.0;
+  for (int a = 1; a <= nx - 2; ++a) {
+    double acc = 0.0, accB = 0.0, neg = 0.0, pos = 0.0;
+    for (int b = 1; b <= ny - 2; ++b) {
+      const int64_t k = (int64_t)a * ny + b;
+      if (std::isnan(tau_fo[k])) continue;
+      const double gx = fo_grad1(tau_fo, ny, a, b, 1, dx), gy = fo_grad1(tau_fo, ny, a, b, 2, dx);
+      if (std::isnan(gx) || std::isnan(gy)) continue;
+      const double tau = tau_fo[k], ux = uxf[k], uy = uyf[k];
+      const double ut = std::sqrt((1.0 + (ux * ux)) + (uy * uy));
+      for (int ipt = 0; ipt < n_pt; ++ipt) {
+        const double pt = pt_lo + (double)ipt * dpt;
+        const double mT = std::sqrt((pt * pt) + (m * m));
+        for (int iphi = 0; iphi < n_phi; ++iphi) {
+          const double phi = (double)iphi * dphi;
+          const double px = pt * std::cos(phi), py = pt * std::sin(phi);
+          for (int ie = 0; ie < n_eta; ++ie) {
+            const double eta = -eta_max + (double)ie * deta;
+            const double ch = std::cosh(eta);
+            const double dSp = tau * (((mT * ch) - (gx * px)) - (gy * py));
+            const double Es = (((ut * mT) * ch) - (ux * px)) - (uy * py);
+            const double x = Es / T_fo;
+            const double fB = std::exp(-x);
+            const double fb = x > 1e-8 ? 1.0 / (std::exp(x) - 1.0) : 0.0;
+            const double w = (((((dSp * pt) * dpt) * dphi) * deta) * dx) * dx;
+            acc += w * fB;
+            accB += w * fb;
+            if (dSp < 0.0) neg += -(w * fB); else pos += w * fB;
+          }
+        }
+      }
+    }
+    tot += acc; totB += accB; negc += neg; posc += pos;
+  }
+  const double pref = fy / std::pow((2.0 * M_PI) * 0.1973269804, 3);
+  out[0] = pref * tot;
+  out[1] = pref * totB;
+  out[2] = negc / std::max(posc + negc, 1e-30);
 }
 
 }  /* extern "C" */

@@ -81,6 +81,9 @@ def lib():
             "oracle_cfm_h_hprime": (None, [P, C.c_double, _D, _D]),
             "oracle_cfm_dn_dT": (C.c_double, [P, C.c_double, C.c_double]),
             "oracle_diff_coeffs": (None, [P, C.c_double, C.c_double, C.c_double, _D, _D, _D]),
+            "oracle_fo_record": (None, [C.c_void_p, C.c_double, C.c_double, C.c_double, _D, _D, _D, _D, _U8,
+                                        C.POINTER(C.c_int64)]),
+            "oracle_pion_yield": (None, [C.c_int, C.c_int, C.c_double, _D, _D, _D, _D, C.POINTER(C.c_int), _D]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
