@@ -231,3 +231,91 @@ function kernel_times(w::GPUWork2D; reset::Bool = false)
                     w.h, kt, Cint(reset)), "fivo_profile_read")
     return kt[]
 end
+
+# ----------------------------------------------------------------------------- freeze-out
+
+"""Cooper-Frye grid and constants of pion_yield (freezeout2d.jl:144-190)."""
+mutable struct FivoCFParams
+    T_fo::Float64; m::Float64; pt_lo::Float64; pt_hi::Float64; eta_max::Float64; f_yield::Float64
+    n_eta::Int32; n_pt::Int32; n_phi::Int32; pad::Int32
+end
+function FivoCFParams(; kw...)
+    p = FivoCFParams(0, 0, 0, 0, 0, 0, 0, 0, 0, 0)
+    ccall((:fivo_cf_params_default, LIBFIVO2D), Cvoid, (Ref{FivoCFParams},), p)
+    for (k, v) in kw; setfield!(p, k, convert(fieldtype(FivoCFParams, k), v)); end
+    return p
+end
+
+"""The device freeze-out surface tau_fo(x, y) of a GPUWork2D (freeze_surface's record!)."""
+mutable struct GPUFreezeOut
+    h::Ptr{Cvoid}
+    nx::Int
+    ny::Int
+    function GPUFreezeOut(w::GPUWork2D, g::Grid2D; T_fo::Float64 = 0.156)
+        h = Ref{Ptr{Cvoid}}(C_NULL)
+        fivocheck(ccall((:fivo_fo_create, LIBFIVO2D), Cint, (Ptr{Cvoid}, Cdouble, Ref{Ptr{Cvoid}}), w.h, T_fo, h),
+                  "fivo_fo_create")
+        f = new(h[], g.Nx, g.Ny)
+        finalizer(f -> ccall((:fivo_fo_destroy, LIBFIVO2D), Cint, (Ptr{Cvoid},), f.h), f)
+        return f
+    end
+end
+
+"""record!(τ) after update_primitives_2d! (freezeout2d.jl:94-115)."""
+record!(f::GPUFreezeOut, w::GPUWork2D, τ::Float64) =
+    fivocheck(ccall((:fivo_fo_record, LIBFIVO2D), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Cdouble), f.h, w.h, τ),
+              "fivo_fo_record")
+
+"""(; τfo, uxf, uyf, nhot, nfroze, refroze) as freeze_surface returns them (row-major a*ny + b
+on the device, returned as nx x ny Julia matrices)."""
+function surface(f::GPUFreezeOut)
+    n = f.nx * f.ny
+    t = Vector{Float64}(undef, n); ux = similar(t); uy = similar(t); c = zeros(Int64, 3)
+    fivocheck(ccall((:fivo_fo_surface, LIBFIVO2D), Cint,
+                    (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Int64}), f.h, t, ux, uy, c),
+              "fivo_fo_surface")
+    m(v) = permutedims(reshape(v, f.ny, f.nx))
+    return (; τfo = m(t), uxf = m(ux), uyf = m(uy), nhot = c[1], nfroze = c[2], refroze = c[3])
+end
+
+"""pion_yield on the device: (N_boltzmann, N_bose, negative-dSigma fraction)."""
+function pion_yield(f::GPUFreezeOut; kw...)
+    p = FivoCFParams(; kw...)
+    out = zeros(3)
+    fivocheck(ccall((:fivo_cooper_frye, LIBFIVO2D), Cint, (Ptr{Cvoid}, Ref{FivoCFParams}, Ptr{Float64}),
+                    f.h, p, out), "fivo_cooper_frye")
+    return (out[1], out[2], out[3])
+end
+
+# ----------------------------------------------------------------------------- learned recovery guess
+
+"""The learned Newton starting guess (fivo_guess_*): harvest pairs from plain runs,
+train on the GPU, attach to a GPUWork2D."""
+mutable struct GPURecoveryGuess
+    h::Ptr{Cvoid}
+    function GPURecoveryGuess(w::GPUWork2D; seed::Integer = 1)
+        h = Ref{Ptr{Cvoid}}(C_NULL)
+        fivocheck(ccall((:fivo_guess_create, LIBFIVO2D), Cint, (Ptr{Cvoid}, UInt64, Ref{Ptr{Cvoid}}),
+                        w.h, UInt64(seed), h), "fivo_guess_create")
+        gg = new(h[])
+        finalizer(gg -> ccall((:fivo_guess_destroy, LIBFIVO2D), Cint, (Ptr{Cvoid},), gg.h), gg)
+        return gg
+    end
+end
+
+reserve!(gg::GPURecoveryGuess, n::Integer) =
+    fivocheck(ccall((:fivo_guess_reserve, LIBFIVO2D), Cint, (Ptr{Cvoid}, Int64), gg.h, n), "fivo_guess_reserve")
+harvest!(gg::GPURecoveryGuess, w::GPUWork2D, τ::Float64; stride::Integer = 1, phase::Integer = 0) =
+    fivocheck(ccall((:fivo_guess_harvest, LIBFIVO2D), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Cdouble, Cint, Cint),
+                    w.h, gg.h, τ, stride, phase), "fivo_guess_harvest")
+function train!(gg::GPURecoveryGuess; steps::Integer = 3000, ctas::Integer = 148, lr::Float32 = 2f-3,
+                seed::Integer = 5)
+    fivocheck(ccall((:fivo_guess_fit_norm, LIBFIVO2D), Cint, (Ptr{Cvoid},), gg.h), "fivo_guess_fit_norm")
+    loss = zeros(2)
+    fivocheck(ccall((:fivo_guess_train, LIBFIVO2D), Cint, (Ptr{Cvoid}, Cint, Cint, Cfloat, UInt64, Ptr{Float64}),
+                    gg.h, steps, ctas, lr, UInt64(seed), loss), "fivo_guess_train")
+    return (first = loss[1], last = loss[2])
+end
+attach!(w::GPUWork2D, gg::Union{GPURecoveryGuess,Nothing}) =
+    fivocheck(ccall((:fivo_ctx_set_guess, LIBFIVO2D), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), w.h,
+                    gg === nothing ? C_NULL : gg.h), "fivo_ctx_set_guess")
