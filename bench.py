@@ -238,6 +238,8 @@ def run_gpu(args):
     w = GPUWork2D(m, g, lib=lib)
     if guess is not None:
         guess.attach(w)
+    if args.fp32_faces:
+        w.set_precision(A.FIVO_PRECISION_FP32_FACES)
     stream = torch.cuda.Stream()
     A.check(lib, lib.fivo_ctx_set_stream(w.h, C.c_void_p(stream.cuda_stream)), "set_stream")
     w.set_state(U0)
@@ -275,11 +277,15 @@ def run_gpu(args):
     twin = GPUWork2D(m, g, lib=lib)
     A.check(lib, lib.fivo_ctx_set_stream(twin.h, C.c_void_p(stream.cuda_stream)), "set_stream")
     twin.clone_state_from(w)
+    plain = None
+    if guess is not None or args.fp32_faces:
+        plain = GPUWork2D(m, g, lib=lib)          # the plain FP64 path over the same steps
+        plain.clone_state_from(w)
+    if args.fp32_faces:
+        twin.set_precision(A.FIVO_PRECISION_FP32_FACES)
     if guess is not None:
         from fivo2d.guess import newton_stats
         guess.attach(twin)
-        plain = GPUWork2D(m, g, lib=lib)          # the plain FP64 path over the same steps
-        plain.clone_state_from(w)
         newton_stats(w, reset=True)
 
     # ---------------- device-resident timing
@@ -309,34 +315,45 @@ def run_gpu(args):
         l2_flush()
         tau_r = step_on(twin.h, tau_r, 1)
     lib.fivo_profile_read(twin.h, C.byref(kt), 1)
-    if guess is None and tau_r != tau:
+    if plain is None and tau_r != tau:
         raise RuntimeError("the profiled replay left the timed trajectory")
     twin.close()
     learned = None
-    if guess is not None:
+    vs_plain = None
+    if plain is not None:
         import numpy as np
-        st = newton_stats(w)
         pw = w.primitives()
+        Uw = w.get_state()
         tau_p = tau_start
         for k in range(args.steps):
             tau_p = step_on(plain.h, tau_p, 1)
         pp = plain.primitives()
+        Up = plain.get_state()
         sx, sy = g.interior()
         okm = ((pw["ok"] == 1) & (pp["ok"] == 1)).reshape(g.Nxtot, g.Nytot)[sx, sy]
 
         def inner(p, key):
             return p[key].reshape(g.Nxtot, g.Nytot)[sx, sy][okm]
+        iP = m.layout.idx("pixx")
+        piw = Uw.reshape(g.Nxtot, g.Nytot, m.nv)[sx, sy, iP:iP + 3][okm]
+        pip = Up.reshape(g.Nxtot, g.Nytot, m.nv)[sx, sy, iP:iP + 3][okm]
+        iN = m.layout.idx("nux")
+        vs_plain = {"steps": args.steps, "tau": tau, "tau_plain": tau_p,
+                    "L2_T": l2_rel(np.exp(inner(pw, "yT")), np.exp(inner(pp, "yT"))),
+                    "Linf_T": float(np.max(np.abs(np.exp(inner(pw, "yT")) - np.exp(inner(pp, "yT"))) /
+                                           np.exp(inner(pp, "yT")))),
+                    "L2_ux": l2_rel(inner(pw, "ux"), inner(pp, "ux")),
+                    "L2_uy": l2_rel(inner(pw, "uy"), inner(pp, "uy")),
+                    "L2_pi": l2_rel(piw, pip), "L2_n": l2_rel(inner(pw, "n"), inner(pp, "n"))}
+        plain.close()
+    if guess is not None:
+        st = newton_stats(w)
         learned = dict(ginfo)
         learned.update({
             "accept_rate": st["ok_learn"] / max(1, st["n_learn"]),
             "fallback_rate": 1.0 - st["ok_learn"] / max(1, st["n_learn"]),
             "updates_per_cell": (st["it_learn"] + st["it_fb"]) / max(1, st["n_learn"]),
-            "slow_pass_cells_per_step": st["deferred"] / args.steps,
-            "vs_plain_fp64": {"steps": args.steps, "tau_learned": tau, "tau_plain": tau_p,
-                              "L2_T": l2_rel(np.exp(inner(pw, "yT")), np.exp(inner(pp, "yT"))),
-                              "L2_ux": l2_rel(inner(pw, "ux"), inner(pp, "ux")),
-                              "L2_uy": l2_rel(inner(pw, "uy"), inner(pp, "uy"))}})
-        plain.close()
+            "slow_pass_cells_per_step": st["deferred"] / args.steps})
     clocks = clk.summary()
     t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if dist:
@@ -416,9 +433,14 @@ def run_gpu(args):
         "roofline": roof,
         "clocks": clocks,
     }
+    if vs_plain is not None:
+        line["vs_plain_fp64"] = vs_plain
+    if args.fp32_faces:
+        line["config"]["workload"] += "_fp32_faces"
+        line["dtype"] = "f64 (faces f32)"
     if learned is not None:
         line["learned_guess"] = learned
-        line["config"]["workload"] = WORKLOAD + "_learned_guess"
+        line["config"]["workload"] += "_learned_guess"
         line["config"]["recovery"] = ("learned MLP guess (BF16 tcgen05, FP32 accumulate), fallback to the "
                                       "plain warm start; trained on seeds " + str(list(GUESS_SEEDS)))
     if world == 1 and not args.no_cpu_baseline:
@@ -466,6 +488,8 @@ def run_batch(args):
         e.rhs(TAU0)
         if guess is not None:
             guess.attach(e)
+        if args.fp32_faces:
+            e.set_precision(A.FIVO_PRECISION_FP32_FACES)
     taus = [TAU0] * len(mine)
 
     def adv(n):
@@ -544,6 +568,9 @@ def run_batch(args):
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
                 "steps": e2e_steps},
     }
+    if args.fp32_faces:
+        line["config"]["workload"] += "_fp32_faces"
+        line["dtype"] = "f64 (faces f32)"
     if learned is not None:
         line["learned_guess"] = learned
         line["config"]["workload"] += "_learned_guess"
@@ -676,6 +703,8 @@ def main():
                     help="event: the 384^2 viscous event (default); batch: many uneven events")
     ap.add_argument("--events", type=int, default=32, help="batch workload: number of events")
     ap.add_argument("--workers", type=int, default=0, help="batch workload: host threads (0: library default)")
+    ap.add_argument("--fp32-faces", action="store_true",
+                    help="the mixed-precision form: the face pass in FP32 (fivo_ctx_set_precision)")
     ap.add_argument("--guess", action="store_true",
                     help="train the learned recovery guess on other seeded events and time with it attached")
     args = ap.parse_args()

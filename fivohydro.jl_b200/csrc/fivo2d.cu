@@ -24,6 +24,7 @@
 
 #include "kernels.cuh"
 #include "freezeout.cuh"
+#include "face32.cuh"
 
 using namespace fv;
 
@@ -163,6 +164,9 @@ struct fivo_ctx {
   bool learned = false;
   guess::Net gnet{};
   int64_t stats_base_p = 0;                 /* deferred-cell total at the last Newton-statistics reset */
+  /* the mixed-precision face pass (fivo_ctx_set_precision): FP32 face fluxes */
+  int precision = FIVO_PRECISION_FP64;
+  float* fh32 = nullptr;                    /* x faces then y faces, nv FP32 planes each */
 };
 
 namespace {
@@ -287,18 +291,31 @@ int launch_stage_t(fivo_ctx* c, const StageArgs& a) {
   const DevParams& d = c->dp;
   double* fhx = c->fh;
   double* fhy = c->fh + (size_t)d.nv * d.Ntot;
+  float* fhx32 = c->fh32;
+  float* fhy32 = c->fh32 ? c->fh32 + (size_t)d.nv * d.Ntot : nullptr;
+  const bool f32 = c->precision == FIVO_PRECISION_FP32_FACES;
   {
     long long nfx = (long long)(d.Nxtot - 1) * d.Nytot, nfy = (long long)d.Nxtot * (d.Nytot - 1);
     KTimer t_(c, FIVO_KCLASS_FACES, 2, nfx + nfy);
-    k_faces<EOS, true><<<nblk(2 * nfx, 128), 128, 0, c->st>>>(d, a.Ub, a.w, a.tau, a.ffo, fhx, c->fl);
-    CKL();
-    k_faces<EOS, false><<<nblk(2 * nfy, 128), 128, 0, c->st>>>(d, a.Ub, a.w, a.tau, a.ffo, fhy, c->fl);
-    CKL();
+    if (f32) {
+      f32::k_faces32<EOS, true><<<nblk(2 * nfx, 128), 128, 0, c->st>>>(d, a.Ub, a.w, a.tau, a.ffo, fhx32, c->fl);
+      CKL();
+      f32::k_faces32<EOS, false><<<nblk(2 * nfy, 128), 128, 0, c->st>>>(d, a.Ub, a.w, a.tau, a.ffo, fhy32, c->fl);
+      CKL();
+    } else {
+      k_faces<EOS, true><<<nblk(2 * nfx, 128), 128, 0, c->st>>>(d, a.Ub, a.w, a.tau, a.ffo, fhx, c->fl);
+      CKL();
+      k_faces<EOS, false><<<nblk(2 * nfy, 128), 128, 0, c->st>>>(d, a.Ub, a.w, a.tau, a.ffo, fhy, c->fl);
+      CKL();
+    }
   }
   unsigned int* aq = c->queues + d.Ntot;
   {
     KTimer t_(c, FIVO_KCLASS_UPDATE, 1, (long long)d.Nx * d.Ny);
-    k_update<EOS, NCH><<<nblk((long long)d.Nx * d.Ny, 128), 128, 0, c->st>>>(d, a, fhx, fhy, aq);
+    if (f32)
+      k_update<EOS, NCH, float><<<nblk((long long)d.Nx * d.Ny, 128), 128, 0, c->st>>>(d, a, fhx32, fhy32, aq);
+    else
+      k_update<EOS, NCH><<<nblk((long long)d.Nx * d.Ny, 128), 128, 0, c->st>>>(d, a, fhx, fhy, aq);
     CKL();
   }
   if (a.mode != COMB_RHS_ONLY) {
@@ -618,6 +635,7 @@ int fivo_ctx_destroy(fivo_ctx* c) {
   for (auto e : c->pool) cudaEventDestroy(e);
   cudaFree(c->slab); cudaFree(c->pbuf); cudaFree(c->hbuf); cudaFree(c->masks); cudaFree(c->fl);
   cudaFree(c->dU); cudaFree(c->stage); cudaFree(c->fh); cudaFree(c->queues); cudaFree(c->part);
+  cudaFree(c->fh32);
   if (c->flh) cudaFreeHost(c->flh);
   if (c->own_st) cudaStreamDestroy(c->own_st);
   if (c->ev_sync) cudaEventDestroy(c->ev_sync);
@@ -1804,5 +1822,22 @@ int fivo_cooper_frye(fivo_fo* f, const fivo_cf_params* p, double* out) {
   out[0] = pref * s[0];
   out[1] = pref * s[1];
   out[2] = s[2] / std::max(s[3] + s[2], 1e-30);
+  return FIVO_OK;
+}
+
+/* ------------------------------------------------ mixed precision */
+
+int fivo_ctx_set_precision(fivo_ctx* c, int mode) {
+  if (!c) return fail(FIVO_ERR_ARG, "null context");
+  if (mode != FIVO_PRECISION_FP64 && mode != FIVO_PRECISION_FP32_FACES)
+    return fail(FIVO_ERR_ARG, "fivo_ctx_set_precision: unknown mode");
+  CK(ctx_sync(c));
+  if (mode == FIVO_PRECISION_FP32_FACES && !c->fh32) {
+    if (cudaMalloc(&c->fh32, 2 * (size_t)c->dp.nv * c->dp.Ntot * sizeof(float)) != cudaSuccess) {
+      c->fh32 = nullptr;
+      return fail(FIVO_ERR_NOMEM, "fivo_ctx_set_precision: device allocation failed");
+    }
+  }
+  c->precision = mode;
   return FIVO_OK;
 }

@@ -1582,8 +1582,9 @@ __device__ __forceinline__ int adm_prefilter(const DevParams& d, const double u[
 /* per interior cell: flux divergence + source (rhs_2d! assembly), the stage
  * combination, sanitize_stage_2d!'s floors and bounds, and the admissibility
  * test up to the inversion */
-template <int EOS, bool NCH>
-__global__ void __launch_bounds__(128) k_update(DevParams d, StageArgs s, const double* Fhx, const double* Fhy,
+/* FT: the type of the face-flux planes (double; float for the mixed-precision face pass) */
+template <int EOS, bool NCH, typename FT = double>
+__global__ void __launch_bounds__(128) k_update(DevParams d, StageArgs s, const FT* Fhx, const FT* Fhy,
                                                 unsigned int* aqueue) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int verdict = 1;
@@ -1625,9 +1626,10 @@ __global__ void __launch_bounds__(128) k_update(DevParams d, StageArgs s, const 
     }
     double u[FV_MAXV];
     for (int a = 0; a < nv; ++a) {
-      const double* fx = Fhx + (size_t)a * N;
-      const double* fy = Fhy + (size_t)a * N;
-      double k = (((-(fx[i] - fx[i - d.Nytot])) * invdx) - ((fy[i] - fy[i - 1]) * invdy)) + Sr[a];
+      const FT* fx = Fhx + (size_t)a * N;
+      const FT* fy = Fhy + (size_t)a * N;
+      double k = (((-((double)fx[i] - (double)fx[i - d.Nytot])) * invdx) -
+                  (((double)fy[i] - (double)fy[i - 1]) * invdy)) + Sr[a];
       if (s.dU) s.dU[(size_t)a * N + i] = k;
       if (s.mode == COMB_EULER) u[a] = ub[a] + (s.dt * k);
       else if (s.mode == COMB_BLEND) u[a] = (s.wold * s.Uold.f[a][i]) + (s.wnew * (ub[a] + (s.dt * k)));

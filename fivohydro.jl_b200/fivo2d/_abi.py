@@ -89,6 +89,7 @@ KERNEL_CLASSES = ("prim_fast", "prim_slow", "faces", "update", "adm_slow", "rela
 
 
 FIVO_GUESS_NPARAM, FIVO_GUESS_NNORM, FIVO_GUESS_NSAMP = 6288, 22, 11
+FIVO_PRECISION_FP64, FIVO_PRECISION_FP32_FACES = 0, 1
 
 
 class FivoNewtonStats(C.Structure):
@@ -180,6 +181,7 @@ SIGNATURES = {
     "fivo_guess_forward": (C.c_int, [C.c_void_p, _F, _I64, _F]),
     "fivo_ctx_set_guess": (C.c_int, [C.c_void_p, C.c_void_p]),
     "fivo_newton_stats_read": (C.c_int, [C.c_void_p, C.POINTER(FivoNewtonStats), C.c_int]),
+    "fivo_ctx_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
     "fivo_cf_params_default": (None, [C.POINTER(FivoCFParams)]),
     "fivo_fo_create": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_void_p)]),
     "fivo_fo_destroy": (C.c_int, [C.c_void_p]),

@@ -164,6 +164,11 @@ class GPUWork2D:
     def finalize_ic(self, tau0, bc=A.FIVO_BC_OUTFLOW):
         self._ck(self.lib.fivo_finalize_ic(self.h, tau0, bc), "fivo_finalize_ic")
 
+    def set_precision(self, mode):
+        """FIVO_PRECISION_FP64 (the reference's arithmetic) or FIVO_PRECISION_FP32_FACES
+        (the face pass of rhs_2d! in FP32, everything else FP64)"""
+        self._ck(self.lib.fivo_ctx_set_precision(self.h, int(mode)), "fivo_ctx_set_precision")
+
     def sync(self):
         self._ck(self.lib.fivo_sync(self.h), "fivo_sync")
 

@@ -407,6 +407,16 @@ int  fivo_guess_forward(fivo_guess* g, const float* raw, int64_t n, float* out);
 int  fivo_ctx_set_guess(fivo_ctx* ctx, fivo_guess* g);
 int  fivo_newton_stats_read(fivo_ctx* ctx, fivo_newton_stats* out, int reset);
 
+/* --- mixed precision (no counterpart in the reference, which is FP64 throughout) ---
+ * FIVO_PRECISION_FP32_FACES runs the face pass of rhs_2d! (MUSCL reconstruction,
+ * the EOS at the faces, physical fluxes, wave speeds, HLLE) in FP32 and stores FP32
+ * face fluxes; the recovery, the divergence and sources, the SSPRK combination,
+ * the floors and the relaxation stay FP64. Results then differ from the FP64 path
+ * at the FP32 rounding level of the fluxes (not bitwise). */
+#define FIVO_PRECISION_FP64        0
+#define FIVO_PRECISION_FP32_FACES  1
+int  fivo_ctx_set_precision(fivo_ctx* ctx, int mode);
+
 /* --- the freeze-out surface and its Cooper-Frye pion yield (freezeout2d.jl) ---
  * The surface tau = tau_fo(x, y) over ctx's interior cells: each record takes the
  * primitives of ctx's last primitive pass (fivo_update_primitives first, as

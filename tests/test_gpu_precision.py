@@ -1,0 +1,133 @@
+"""The mixed-precision form (fivo_ctx_set_precision: the face pass of rhs_2d! in
+FP32, everything else FP64) against the FP64 path and the reference's gates:
+
+  - the Gubser gate G1 (test/test_gubser2d.jl:97-246): L2(T) and L2(u) against the
+    exact solution stay at the published values (the FP32 fluxes move them by far
+    less than the scheme's own error), and the run differs from the FP64 one at the
+    FP32 level;
+  - the Bjorken gate G0 (test/test_bjorken2d.jl:133-169): convergence orders 2.00 /
+    2.99 for SSPRK2 / SSPRK3 (a uniform state has equal fluxes on both faces of a
+    cell in any precision, so the FP32 form must reproduce the FP64 run exactly);
+  - the viscous MC-Glauber event: L2(T) <= 1e-6 and L2(pi) <= 1e-4 against the FP64
+    path over a window that ends before the charge-free edge forms.
+"""
+import json
+import math
+import pathlib
+
+import numpy as np
+import pytest
+
+import fivo2d
+from fivo2d import _abi as A
+from fivo2d import ic
+from fivo2d.solver import GPUWork2D, set_cells
+
+import test_oracle_gates as G
+
+pytestmark = pytest.mark.gpu
+GATES = json.loads((pathlib.Path(__file__).resolve().parent / "golden" / "gates.json").read_text())
+
+
+def _gubser(lib, N, mode):
+    s = GATES["gubser"]["settings"]
+    g = fivo2d.make_grid2d(N, N, xmax=s["box"], ymax=s["box"])
+    m = fivo2d.build_model_2d(eos=fivo2d.ConformalHQEOS())
+    Tsc = ic.gubser_Tscale_from_center_T(s["tau0"], s["q"], s["Tc0"])
+    T, a, ux, uy = ic.gubser_fields(g, s["tau0"], q=s["q"], Tscale=Tsc, alpha=s["alpha"])
+    U, ok = set_cells(m, s["tau0"], T, a, ux, uy, lib=lib)
+    w = GPUWork2D(m, g, lib=lib)
+    w.set_precision(mode)
+    w.set_state(U)
+    r = w.run(s["tau0"], s["tauf"], s["CFL"], s["CFLtau"], A.FIVO_SSPRK2)
+    assert r["ok"]
+    w.update_primitives(r["tau"])
+    pr = w.primitives()
+    Te, uxe, uye, rr = ic.gubser_exact(g, r["tau"], q=s["q"], Tscale=Tsc)
+    sl = g.interior()
+    Tn = np.exp(pr["yT"]).reshape(g.Nxtot, g.Nytot)[sl]
+    uxn = pr["ux"].reshape(g.Nxtot, g.Nytot)[sl]
+    uyn = pr["uy"].reshape(g.Nxtot, g.Nytot)[sl]
+    msk = rr[sl] <= s["rcmp"]
+    L2T = math.sqrt(((Tn - Te[sl])[msk] ** 2).sum() / (Te[sl][msk] ** 2).sum())
+    L2U = math.sqrt((((uxn - uxe[sl]) ** 2 + (uyn - uye[sl]) ** 2)[msk]).sum() /
+                    ((uxe[sl] ** 2 + uye[sl] ** 2)[msk]).sum())
+    w.close()
+    return L2T, L2U, Tn
+
+
+def test_gubser_gate_in_fp32_faces(gpu_lib):
+    pub = GATES["gubser"]
+    for N, key in ((100, 0), (200, 1)):
+        l2t, l2u, T32 = _gubser(gpu_lib, N, A.FIVO_PRECISION_FP32_FACES)
+        l2t64, l2u64, T64 = _gubser(gpu_lib, N, A.FIVO_PRECISION_FP64)
+        assert abs(l2t - l2t64) <= 1e-3 * l2t64 and abs(l2u - l2u64) <= 1e-3 * l2u64, (l2t, l2t64, l2u, l2u64)
+        assert abs(l2t - pub["L2T"][key]) <= 0.01 * pub["L2T"][key]
+        d = np.linalg.norm(T32 - T64) / np.linalg.norm(T64)
+        assert 0 < d < 1e-6, d                      # FP32-level, and really different arithmetic
+
+
+def _bjorken_err(lib, cfltau, integrator, mode):
+    s = GATES["bjorken"]["settings"]
+    g = fivo2d.make_grid2d(s["N"], s["N"], xmax=s["box"], ymax=s["box"])
+    m = fivo2d.build_model_2d(eos=fivo2d.LatticeHRGEOS())
+    T, a, ux, uy = ic.uniform_fields(g, T0=s["T0"], alpha0=s["alpha0"])
+    U, _ = set_cells(m, s["tau0"], T, a, ux, uy, lib=lib)
+    w = GPUWork2D(m, g, lib=lib)
+    w.set_precision(mode)
+    w.set_state(U)
+    w.finalize_ic(s["tau0"])
+    r = w.run(s["tau0"], s["tauf"], s["CFL"], cfltau, integrator)
+    assert r["ok"]
+    U1 = w.get_state()
+    w.close()
+    Tx, mux, nx_, ex, Px = G.bjorken_exact(m.params, s["T0"], s["alpha0"] * s["T0"], s["tau0"], r["tau"])
+    ic_ = g.lin(g.nghost + g.Nx // 2 - 1, g.nghost + g.Ny // 2 - 1)
+    return abs(U1[ic_, 3] - ex) / ex, U1
+
+
+@pytest.mark.parametrize("integrator,expect", [(A.FIVO_SSPRK2, "ssprk2"), (A.FIVO_SSPRK3, "ssprk3")])
+def test_bjorken_order_in_fp32_faces(gpu_lib, integrator, expect):
+    errs = []
+    for c in (0.02, 0.01, 0.005):
+        e32, U32 = _bjorken_err(gpu_lib, c, integrator, A.FIVO_PRECISION_FP32_FACES)
+        e64, U64 = _bjorken_err(gpu_lib, c, integrator, A.FIVO_PRECISION_FP64)
+        assert np.array_equal(U32, U64)
+        errs.append(e32)
+    p2 = math.log2(errs[1] / errs[2])
+    assert abs(p2 - GATES["bjorken"]["order"][expect]) < 0.15, (errs, p2)
+
+
+def test_viscous_event_error_against_fp64(gpu_lib):
+    """the bench workload's physics on a 192^2 event (dx = 30/384 fm), 30 SSPRK3 steps
+    from tau0 = 0.6"""
+    m = fivo2d.build_model_2d(eos=fivo2d.LatticeHRGEOS(), enable_shear=True, enable_bulk=True,
+                              enable_diff=True, eta_over_s=0.16, tauShear_coeff=0.2, deltaShear_factor=4 / 3,
+                              zeta_over_s=0.05, bulk_model="gaussian", bulk_T0=0.180, bulk_width=0.024,
+                              kappa_coeff=0.5)
+    n = 192
+    g = fivo2d.make_grid2d(n, n, xmax=n * 15.0 / 384, ymax=n * 15.0 / 384)
+    T, a, ux, uy, _ = ic.glauber_fields(g, 0.6, 1001)
+    U, _ = set_cells(m, 0.6, T, a, ux, uy, lib=gpu_lib)
+    out = {}
+    for mode in (A.FIVO_PRECISION_FP64, A.FIVO_PRECISION_FP32_FACES):
+        w = GPUWork2D(m, g, lib=gpu_lib)
+        w.set_precision(mode)
+        w.set_state(U)
+        w.finalize_ic(0.6)
+        r = w.run(0.6, 10.0, 0.2, 0.05, A.FIVO_SSPRK3, max_steps=30)
+        assert r["ok"] and r["nsteps"] == 30
+        out[mode] = (w.primitives(), w.get_state())
+        w.close()
+    (p64, U64), (p32, U32) = out[A.FIVO_PRECISION_FP64], out[A.FIVO_PRECISION_FP32_FACES]
+    sx, sy = g.interior()
+    ok = ((p64["ok"] == 1) & (p32["ok"] == 1)).reshape(g.Nxtot, g.Nytot)[sx, sy]
+    T64 = np.exp(p64["yT"]).reshape(g.Nxtot, g.Nytot)[sx, sy][ok]
+    T32 = np.exp(p32["yT"]).reshape(g.Nxtot, g.Nytot)[sx, sy][ok]
+    l2T = np.linalg.norm(T32 - T64) / np.linalg.norm(T64)
+    iP = m.layout.idx("pixx")
+    pi64 = U64.reshape(g.Nxtot, g.Nytot, m.nv)[sx, sy, iP:iP + 3][ok]
+    pi32 = U32.reshape(g.Nxtot, g.Nytot, m.nv)[sx, sy, iP:iP + 3][ok]
+    l2pi = np.linalg.norm(pi32 - pi64) / np.linalg.norm(pi64)
+    print(f"FP32 faces vs FP64 after 30 steps: L2(T) {l2T:.3e}, L2(pi) {l2pi:.3e}")
+    assert 0 < l2T <= 1e-6 and l2pi <= 1e-4, (l2T, l2pi)
