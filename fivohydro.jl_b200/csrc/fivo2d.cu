@@ -167,6 +167,7 @@ struct fivo_ctx {
   /* the mixed-precision face pass (fivo_ctx_set_precision): FP32 face fluxes */
   int precision = FIVO_PRECISION_FP64;
   float* fh32 = nullptr;                    /* x faces then y faces, nv FP32 planes each */
+  double* x0save = nullptr;                 /* the warm starts before an optimistic step */
 };
 
 namespace {
@@ -357,12 +358,16 @@ int sync_flags(fivo_ctx* c, bool read_amax) {
 
 /* rhs_2d! + combination + sanitize + admissibility on the given roles.
  * ub = base (and combination input), uo = output, uold = blend partner.
- * Returns FIVO_OK; *nbad = inadmissible interior cells. */
+ * Returns FIVO_OK; *nbad = inadmissible interior cells. With sync = false the
+ * host does not wait (nbad is not read), and with first = false the device's
+ * count of inadmissible cells carries on from the previous stage, so a chain of
+ * stages can be checked once at its end. */
 int run_stage(fivo_ctx* c, int ub, int uo, int uold, double tau, double tau_state, double dt, double wold,
-              double wnew, int mode, const uint8_t* mask, int bc, long long* nbad, double* dU) {
+              double wnew, int mode, const uint8_t* mask, int bc, long long* nbad, double* dU,
+              bool sync = true, bool first = true) {
   int rc;
   if ((rc = launch_bc(c, c->S[ub], bc))) return rc;
-  if ((rc = reset_flags(c, 1 | 2))) return rc;
+  if ((rc = reset_flags(c, first ? (1 | 2 | 64) : (1 | 2)))) return rc;
   if ((rc = launch_primitive(c, c->S[ub], tau))) return rc;
   StageArgs a;
   a.Ub = c->S[ub]; a.Uold = c->S[uold]; a.Uout = c->S[uo]; a.w = c->w; a.ffo = mask;
@@ -371,6 +376,7 @@ int run_stage(fivo_ctx* c, int ub, int uo, int uold, double tau, double tau_stat
   if ((rc = launch_stage(c, a))) return rc;
   if (mode != COMB_RHS_ONLY)
     if ((rc = launch_bc(c, c->S[uo], bc))) return rc;
+  if (!sync) return FIVO_OK;
   if ((rc = sync_flags(c, true))) return rc;
   if (nbad) *nbad = c->flh->nbad;
   return FIVO_OK;
@@ -408,6 +414,24 @@ int stage_mood(fivo_ctx* c, int ub, int uo, int uold, double tau, double tau_sta
   return FIVO_OK;
 }
 
+/* The warm starts x0_* (four contiguous planes of the history block) are updated by
+ * every recovery pass, so an optimistic step that is thrown away must leave them as
+ * they were for the stage-by-stage procedure to take the reference's path. */
+int save_warm(fivo_ctx* c) {
+  const size_t bytes = 4 * (size_t)c->dp.Ntot * sizeof(double);
+  if (!c->x0save && cudaMalloc(&c->x0save, bytes) != cudaSuccess) {
+    c->x0save = nullptr;
+    return fail(FIVO_ERR_NOMEM, "device allocation failed");
+  }
+  CK(cudaMemcpyAsync(c->x0save, c->h.x0_yT, bytes, cudaMemcpyDeviceToDevice, c->st));
+  return FIVO_OK;
+}
+int restore_warm(fivo_ctx* c) {
+  const size_t bytes = 4 * (size_t)c->dp.Ntot * sizeof(double);
+  CK(cudaMemcpyAsync(c->h.x0_yT, c->x0save, bytes, cudaMemcpyDeviceToDevice, c->st));
+  return FIVO_OK;
+}
+
 int copy_state(fivo_ctx* c, int dst, int src) {
   const DevParams& d = c->dp;
   KTimer t_(c, FIVO_KCLASS_OTHER);
@@ -420,6 +444,22 @@ int copy_state(fivo_ctx* c, int dst, int src) {
 int step2(fivo_ctx* c, double tau, double dtau, int max_halve, int max_mood, int bc, double* used, int* okout) {
   double D = dtau;
   c->cnt.nmood = 0; c->cnt.nhalve = 0;
+  /* Optimistic first pass: both stages at the full step without a host read in
+   * between, their inadmissible cells counted together. Nothing inadmissible: the
+   * step is the one the stage-by-stage procedure below takes (same kernels on the
+   * same inputs). Otherwise the state is restored and that procedure runs. */
+  {
+    int rc;
+    long long nbad = 0;
+    if ((rc = save_warm(c))) return rc;
+    if ((rc = copy_state(c, c->iU2, c->iU))) return rc;
+    if ((rc = run_stage(c, c->iU, c->iU1, c->iU2, tau, tau + D, D, 1.0, 0.0, COMB_EULER, nullptr, bc, nullptr,
+                        nullptr, false, true))) return rc;
+    if ((rc = run_stage(c, c->iU1, c->iT, c->iU2, tau + D, tau + D, D, 0.5, 0.5, COMB_BLEND, nullptr, bc, &nbad,
+                        nullptr, true, false))) return rc;
+    if (nbad == 0) { std::swap(c->iU, c->iT); *used = D; *okout = 1; return FIVO_OK; }
+    if ((rc = restore_warm(c))) return rc;
+  }
   for (int h = 0; h <= max_halve; ++h) {
     int rc;
     if ((rc = copy_state(c, c->iU2, c->iU))) return rc;
@@ -441,6 +481,26 @@ int step2(fivo_ctx* c, double tau, double dtau, int max_halve, int max_mood, int
 int step3(fivo_ctx* c, double tau, double dtau, int max_halve, int bc, double* used, int* okout) {
   double D = dtau;
   c->cnt.nmood = 0; c->cnt.nhalve = 0;
+  /* Optimistic first pass (as in step2): the three stages at the full step, one
+   * host read at the end; any inadmissible cell restores the state and the
+   * stage-by-stage procedure below takes the step. */
+  {
+    int rc;
+    long long nbad = 0;
+    if ((rc = save_warm(c))) return rc;
+    if ((rc = copy_state(c, c->iU2, c->iU))) return rc;
+    if ((rc = run_stage(c, c->iU, c->iU1, c->iU2, tau, tau + D, D, 1.0, 0.0, COMB_EULER, nullptr, bc, nullptr,
+                        nullptr, false, true))) return rc;
+    if ((rc = run_stage(c, c->iU1, c->iT, c->iU2, tau + D, tau + D, D, 0.75, 0.25, COMB_BLEND, nullptr, bc, nullptr,
+                        nullptr, false, false))) return rc;
+    std::swap(c->iU1, c->iT);
+    if ((rc = run_stage(c, c->iU1, c->iT, c->iU2, tau + (0.5 * D), tau + D, D, 0.0, 0.0, COMB_THIRD, nullptr, bc,
+                        &nbad, nullptr, true, false))) return rc;
+    std::swap(c->iU, c->iT);
+    if (nbad == 0) { *used = D; *okout = 1; return FIVO_OK; }
+    std::swap(c->iU, c->iU2);    /* the state before the step */
+    if ((rc = restore_warm(c))) return rc;
+  }
   for (int h = 0; h <= max_halve; ++h) {
     int rc;
     long long nbad = 0;
@@ -465,7 +525,7 @@ int step3(fivo_ctx* c, double tau, double dtau, int max_halve, int bc, double* u
 int update_prims(fivo_ctx* c, double tau, int bc) {
   int rc;
   if ((rc = launch_bc(c, c->S[c->iU], bc))) return rc;
-  if ((rc = reset_flags(c, 1))) return rc;
+  if ((rc = reset_flags(c, 1 | 64))) return rc;
   if ((rc = launch_primitive(c, c->S[c->iU], tau))) return rc;
   return FIVO_OK;
 }
@@ -622,7 +682,7 @@ int fivo_ctx_create(const fivo_params* p, int nx, int ny, int nghost, double xma
       cudaMemsetAsync(c->masks, 0, 3 * N, c->st) != cudaSuccess)
     return cleanup(fail(FIVO_ERR_CUDA, "memset failed"));
   if ((rc = reset_history(c))) return cleanup(rc);
-  if ((rc = reset_flags(c, 1 | 2 | 4 | 8 | 16 | 32))) return cleanup(rc);
+  if ((rc = reset_flags(c, 1 | 2 | 4 | 8 | 16 | 32 | 64))) return cleanup(rc);
   if (ctx_sync(c) != cudaSuccess) return cleanup(fail(FIVO_ERR_CUDA, "sync failed"));
   *out = c;
   return FIVO_OK;
@@ -635,7 +695,7 @@ int fivo_ctx_destroy(fivo_ctx* c) {
   for (auto e : c->pool) cudaEventDestroy(e);
   cudaFree(c->slab); cudaFree(c->pbuf); cudaFree(c->hbuf); cudaFree(c->masks); cudaFree(c->fl);
   cudaFree(c->dU); cudaFree(c->stage); cudaFree(c->fh); cudaFree(c->queues); cudaFree(c->part);
-  cudaFree(c->fh32);
+  cudaFree(c->fh32); cudaFree(c->x0save);
   if (c->flh) cudaFreeHost(c->flh);
   if (c->own_st) cudaStreamDestroy(c->own_st);
   if (c->ev_sync) cudaEventDestroy(c->ev_sync);
@@ -1201,7 +1261,7 @@ extern "C" int fivo_rhs_noalloc(const fivo_params* p, int nx, int ny, double xma
   /* clear what the pass must start from: NaN warm starts (a cold start), the flags */
   k_fill_nan<<<nblk(4 * (long long)N, 256), 256, 0, st>>>(h.x0_yT, 4 * (long long)N);
   CKL();
-  k_reset_flags<<<1, 32, 0, st>>>(fl, 1 | 2 | 4 | 8, 0ULL);
+  k_reset_flags<<<1, 32, 0, st>>>(fl, 1 | 2 | 4 | 8 | 64, 0ULL);
   CKL();
   CK(cudaMemsetAsync(dU, 0, (size_t)d.nv * N * 8, st));
   /* rhs_2d!: BCs, primitive pass, faces + sources (src2d/rhs2d.jl:169-249) */

@@ -931,9 +931,10 @@ __global__ void __launch_bounds__(128) k_relax(DevParams d, DevState Uq, DevStat
 __global__ void k_reset_flags(DevFlags* fl, int what, unsigned long long amax_bits) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   if (what & 1) {
-    fl->nprimfail = 0; fl->nvacuum = 0; fl->rep = 0x7fffffffffffffffULL; fl->nbad = 0;
+    fl->nprimfail = 0; fl->nvacuum = 0; fl->rep = 0x7fffffffffffffffULL;
     fl->qcount_p = 0; fl->qnext_p = 0; fl->qcount_a = 0; fl->qnext_a = 0;
   }
+  if (what & 64) fl->nbad = 0;      /* inadmissible cells: accumulate over a step's stages otherwise */
   if (what & 2) fl->amax_bits = amax_bits;
   if (what & 4) { fl->shear_max_bits = 0; fl->shear_sum = 0.0; }
   if (what & 8) { fl->sumD = 0.0; fl->maxu = 0.0; fl->minPtot = inf_(); }
