@@ -1600,6 +1600,7 @@ int fivo_guess_get_samples(fivo_guess* g, float* samples, int64_t n) {
 int fivo_guess_harvest(fivo_ctx* c, fivo_guess* g, double tau, int stride, int phase) {
   if (!c || !g || stride < 1 || phase < 0) return fail(FIVO_ERR_ARG, "bad argument");
   if (g->cap <= 0) return fail(FIVO_ERR_ARG, "fivo_guess_harvest: no sample store (fivo_guess_reserve)");
+  if (g->device != c->device) return fail(FIVO_ERR_ARG, "fivo_guess_harvest: the guess lives on another device");
   CK(ctx_sync(c));
   const DevParams& d = c->dp;
   if (d.p.eos_kind == FIVO_EOS_LATTICE_HRG)
@@ -1814,6 +1815,7 @@ int fivo_fo_destroy(fivo_fo* f) {
 int fivo_fo_record(fivo_fo* f, fivo_ctx* c, double tau) {
   if (!f || !c) return fail(FIVO_ERR_ARG, "null argument");
   if (c->dp.Nx != f->nx || c->dp.Ny != f->ny) return fail(FIVO_ERR_ARG, "fivo_fo_record: grid mismatch");
+  if (c->device != f->device) return fail(FIVO_ERR_ARG, "fivo_fo_record: the surface lives on another device");
   const double tp = f->have_prev ? f->tau_prev : tau;
   const long long n = (long long)f->nx * f->ny;
   fo::k_record<<<nblk(n, 256), 256, 0, c->st>>>(c->dp, c->w, tau, tp, f->T_fo, surf_of(f));
