@@ -232,7 +232,6 @@ struct TrainSmem {
   float lossw[4];                   /* per-warp sums of the squared error */
   uint64_t mbar;
   uint32_t tbase;
-  int err;
 };
 
 /* TMEM columns of the training kernel (512 allocated; one CTA per SM) */
@@ -256,16 +255,16 @@ __global__ void __launch_bounds__(128, 1) k_train(Net net, const float* __restri
   TrainSmem& s = *reinterpret_cast<TrainSmem*>(smem_raw);
   const int t = threadIdx.x, warp = t >> 5;
   if (warp == 0) { tc05::tmem_alloc(&s.tbase, 512); tc05::tmem_relinquish(); }
-  if (t == 0) { tc05::mbar_init(&s.mbar, 1); s.err = 0; }
+  if (t == 0) tc05::mbar_init(&s.mbar, 1);
   copy16(s.W1, net.img + I_W1, NH * K0 * 2, t, 128);
   copy16(s.W2, net.img + I_W2, NH * NH * 2, t, 128);
   copy16(s.W3, net.img + I_W3, N3 * NH * 2, t, 128);
   copy16(s.W3T, net.img + I_W3T, NH * N3 * 2, t, 128);
   copy16(s.W2T, net.img + I_W2T, NH * NH * 2, t, 128);
   const long long gi = start + (long long)blockIdx.x * 128 + t;
-  const unsigned long long k = seed == 0 ? (unsigned long long)gi % (unsigned long long)n
-                                          : mix64(seed ^ (unsigned long long)gi) % (unsigned long long)n;
-  const float* smp = samples + (size_t)k * NSAMP;
+  const unsigned long long ks = seed == 0 ? (unsigned long long)gi % (unsigned long long)n
+                                           : mix64(seed ^ (unsigned long long)gi) % (unsigned long long)n;
+  const float* smp = samples + (size_t)ks * NSAMP;
   float xn[8], tn[NOUT];
 #pragma unroll
   for (int q = 0; q < NIN; ++q) xn[q] = nrm_in(net.norm, q, smp[q]);
