@@ -277,6 +277,13 @@ def run_gpu(args):
     twin = GPUWork2D(m, g, lib=lib)
     A.check(lib, lib.fivo_ctx_set_stream(twin.h, C.c_void_p(stream.cuda_stream)), "set_stream")
     twin.clone_state_from(w)
+    # the mixed-precision form over the same window, from a device clone (default line only)
+    form32 = None
+    if guess is None and not args.fp32_faces and not args.no_forms:
+        form32 = GPUWork2D(m, g, lib=lib)
+        A.check(lib, lib.fivo_ctx_set_stream(form32.h, C.c_void_p(stream.cuda_stream)), "set_stream")
+        form32.clone_state_from(w)
+        form32.set_precision(A.FIVO_PRECISION_FP32_FACES)
     plain = None
     if guess is not None or args.fp32_faces:
         plain = GPUWork2D(m, g, lib=lib)          # the plain FP64 path over the same steps
@@ -318,6 +325,30 @@ def run_gpu(args):
     if plain is None and tau_r != tau:
         raise RuntimeError("the profiled replay left the timed trajectory")
     twin.close()
+    forms = None
+    if form32 is not None:
+        import numpy as np
+        e0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        e1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        tau_f = tau_start
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            l2_flush()
+            e0[k].record(stream)
+            tau_f = step_on(form32.h, tau_f, 1)
+            e1[k].record(stream)
+        torch.cuda.synchronize()
+        ms32 = sum(a_.elapsed_time(b_) for a_, b_ in zip(e0, e1))
+        pw, pf = w.primitives(), form32.primitives()
+        sx, sy = g.interior()
+        okm = ((pw["ok"] == 1) & (pf["ok"] == 1)).reshape(g.Nxtot, g.Nytot)[sx, sy]
+        Tw = np.exp(pw["yT"]).reshape(g.Nxtot, g.Nytot)[sx, sy][okm]
+        Tf = np.exp(pf["yT"]).reshape(g.Nxtot, g.Nytot)[sx, sy][okm]
+        forms = {"fp32_faces": {"value": args.steps * nint / (ms32 / 1e3), "ms_per_step": ms32 / args.steps,
+                                "L2_T_vs_fp64_after_window": l2_rel(Tf, Tw),
+                                "note": "the same window replayed from a device clone with the face pass in "
+                                        "FP32 (fivo_ctx_set_precision); --fp32-faces makes it the headline"}}
+        form32.close()
     learned = None
     vs_plain = None
     if plain is not None:
@@ -435,6 +466,8 @@ def run_gpu(args):
     }
     if vs_plain is not None:
         line["vs_plain_fp64"] = vs_plain
+    if forms is not None:
+        line["forms"] = forms
     if args.fp32_faces:
         line["config"]["workload"] += "_fp32_faces"
         line["dtype"] = "f64 (faces f32)"
@@ -703,6 +736,8 @@ def main():
                     help="event: the 384^2 viscous event (default); batch: many uneven events")
     ap.add_argument("--events", type=int, default=32, help="batch workload: number of events")
     ap.add_argument("--workers", type=int, default=0, help="batch workload: host threads (0: library default)")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the FP32-faces replay of the window that the default line carries")
     ap.add_argument("--fp32-faces", action="store_true",
                     help="the mixed-precision form: the face pass in FP32 (fivo_ctx_set_precision)")
     ap.add_argument("--guess", action="store_true",
