@@ -89,7 +89,7 @@ def uniform_fields(g: Grid2D, *, T0: float = 0.5, alpha0: float = -4.2):
 
 # ----------------------------------------------------------------------------- MC-Glauber
 
-# Pb-208 Woods-Saxon (BASELINE event description)
+# Pb-208 Woods-Saxon nuclei of the event-by-event workload
 WS_R, WS_A, WS_N = 6.62, 0.546, 208
 SIGMA_NN = 6.8          # fm^2
 SRC_WIDTH = 0.5         # fm, Gaussian width per participant

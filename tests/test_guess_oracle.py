@@ -1,5 +1,5 @@
 """The learned recovery guess's CPU oracle (oracle/guess_oracle.py), pinned on
-the CPU before it judges the device: its backward pass against central finite
+the CPU before it checks the device: its backward pass against central finite
 differences of its loss, its BF16 rounding against the format's definition, and
 its device-rounded gradient against the float64 one."""
 import sys
