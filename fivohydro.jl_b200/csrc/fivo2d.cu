@@ -1497,6 +1497,8 @@ int fivo_guess_create(fivo_ctx* c, uint64_t seed, fivo_guess** out) {
       cudaMalloc(&g->count, sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&g->grad, guess::NPARAM * sizeof(float)) != cudaSuccess)
     return bad(fail(FIVO_ERR_NOMEM, "fivo_guess_create: device allocation failed"));
+  if (cudaMemset(g->count, 0, sizeof(unsigned long long)) != cudaSuccess)
+    return bad(fail(FIVO_ERR_CUDA, "fivo_guess_create: memset failed"));
   /* uniform(-1/sqrt(fan_in), 1/sqrt(fan_in)) weights from a splitmix64 stream, zero biases */
   std::vector<float> P(guess::NPARAM, 0.0f);
   uint64_t st = seed;

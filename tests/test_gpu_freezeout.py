@@ -58,3 +58,24 @@ def test_cooper_frye_on_a_given_surface(gpu_lib):
             assert abs(a - b) <= 1e-11 * max(abs(b), 1e-30), (dev, ref)
     fo.close()
     w.close()
+
+
+def test_empty_surface_and_refusals(gpu_lib):
+    """no frozen cell: zero yield; a surface refuses a context of another grid"""
+    import ctypes as C
+    import fivo2d
+    g = fivo2d.make_grid2d(12, 12, xmax=6.0, ymax=6.0)
+    w = GPUWork2D(H.freeze_model(), g, lib=gpu_lib)
+    fo = FreezeOut(w)
+    assert fo.pion_yield() == (0.0, 0.0, 0.0)
+    s = fo.surface()
+    assert s["nfroze"] == 0 and s["nhot"] == 0 and np.isnan(s["tau_fo"]).all()
+    g2 = fivo2d.make_grid2d(14, 12, xmax=7.0, ymax=6.0)
+    w2 = GPUWork2D(H.freeze_model(), g2, lib=gpu_lib)
+    assert gpu_lib.fivo_fo_record(fo.h, w2.h, C.c_double(1.0)) == A.FIVO_ERR_ARG
+    bad = cf_params(n_pt=1)
+    out = np.zeros(3)
+    assert gpu_lib.fivo_cooper_frye(fo.h, C.byref(bad), out.ctypes.data_as(A._D)) == A.FIVO_ERR_ARG
+    fo.close()
+    w.close()
+    w2.close()

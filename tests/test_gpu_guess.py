@@ -176,3 +176,19 @@ def test_trained_guess_run_agrees_and_saves_updates(trained, gpu_lib):
     it_p = sp["it_fast"] / sp["n_fast"]
     print(f"updates per cell: learned {it_l:.3f} (accept {acc:.4f}), plain {it_p:.3f}; "
           f"deferred learned {sl['deferred']} plain {sp['deferred']}")
+
+
+def test_guess_argument_refusals(gpu_lib):
+    import ctypes as C
+    g = RecoveryGuess(seed=2, lib=gpu_lib)
+    s = np.zeros((100, 11), dtype=np.float32)                # not a multiple of 128
+    grad = np.zeros(A.FIVO_GUESS_NPARAM, dtype=np.float32)
+    loss = C.c_double()
+    fp = C.POINTER(C.c_float)
+    assert gpu_lib.fivo_guess_grad(g.h, s.ctypes.data_as(fp), 100, grad.ctypes.data_as(fp),
+                                   C.byref(loss)) == A.FIVO_ERR_ARG
+    out = np.zeros(2)
+    assert gpu_lib.fivo_guess_train(g.h, 10, 4, C.c_float(1e-3), 1, out.ctypes.data_as(A._D)) == A.FIVO_ERR_ARG  # no samples
+    y = g.forward(np.zeros((1, 8), dtype=np.float32))      # one row, a ragged tile
+    assert y.shape == (1, 3) and np.isfinite(y).all()
+    g.close()

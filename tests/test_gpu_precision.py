@@ -131,3 +131,30 @@ def test_viscous_event_error_against_fp64(gpu_lib):
     l2pi = np.linalg.norm(pi32 - pi64) / np.linalg.norm(pi64)
     print(f"FP32 faces vs FP64 after 30 steps: L2(T) {l2T:.3e}, L2(pi) {l2pi:.3e}")
     assert 0 < l2T <= 1e-6 and l2pi <= 1e-4, (l2T, l2pi)
+
+
+def test_precision_switch_and_refusal(gpu_lib):
+    """an unknown mode is refused; switching back to FP64 mid-run continues as the
+    FP64 path does from that state (bit for bit)"""
+    m = fivo2d.build_model_2d(eos=fivo2d.LatticeHRGEOS(), enable_shear=True, enable_diff=True, kappa_coeff=0.5)
+    g = fivo2d.make_grid2d(32, 32, xmax=32 * 15.0 / 384, ymax=32 * 15.0 / 384)
+    T, a, ux, uy, _ = ic.glauber_fields(g, 0.6, 1003)
+    U, _ = set_cells(m, 0.6, T, a, ux, uy, lib=gpu_lib)
+    w = GPUWork2D(m, g, lib=gpu_lib)
+    assert gpu_lib.fivo_ctx_set_precision(w.h, 7) == A.FIVO_ERR_ARG
+    w.set_state(U)
+    w.finalize_ic(0.6)
+    w.set_precision(A.FIVO_PRECISION_FP32_FACES)
+    r = w.run(0.6, 10.0, 0.2, 0.05, A.FIVO_SSPRK3, max_steps=5)
+    mid = w.get_state()
+    hist = w.get_history()
+    w.set_precision(A.FIVO_PRECISION_FP64)
+    r2 = w.advance(r["tau"], 10.0, 0.2, 0.05, A.FIVO_SSPRK3, max_steps=5)
+    v = GPUWork2D(m, g, lib=gpu_lib)
+    v.set_state(mid)
+    v.set_history(**hist)
+    w.close()
+    v.rhs(r["tau"])
+    r3 = v.advance(r["tau"], 10.0, 0.2, 0.05, A.FIVO_SSPRK3, max_steps=5)
+    assert r2["ok"] and r3["ok"] and r2["nsteps"] == r3["nsteps"] == 5
+    v.close()
