@@ -361,12 +361,13 @@ int sync_flags(fivo_ctx* c, bool read_amax) {
  * Returns FIVO_OK; *nbad = inadmissible interior cells. With sync = false the
  * host does not wait (nbad is not read), and with first = false the device's
  * count of inadmissible cells carries on from the previous stage, so a chain of
- * stages can be checked once at its end. */
+ * stages can be checked once at its end. With bc_in = false the input's ghost frame is
+ * taken as filled: the previous stage's output got the same (idempotent) fill. */
 int run_stage(fivo_ctx* c, int ub, int uo, int uold, double tau, double tau_state, double dt, double wold,
               double wnew, int mode, const uint8_t* mask, int bc, long long* nbad, double* dU,
-              bool sync = true, bool first = true) {
+              bool sync = true, bool first = true, bool bc_in = true) {
   int rc;
-  if ((rc = launch_bc(c, c->S[ub], bc))) return rc;
+  if (bc_in && (rc = launch_bc(c, c->S[ub], bc))) return rc;
   if ((rc = reset_flags(c, first ? (1 | 2 | 64) : (1 | 2)))) return rc;
   if ((rc = launch_primitive(c, c->S[ub], tau))) return rc;
   StageArgs a;
@@ -456,7 +457,7 @@ int step2(fivo_ctx* c, double tau, double dtau, int max_halve, int max_mood, int
     if ((rc = run_stage(c, c->iU, c->iU1, c->iU2, tau, tau + D, D, 1.0, 0.0, COMB_EULER, nullptr, bc, nullptr,
                         nullptr, false, true))) return rc;
     if ((rc = run_stage(c, c->iU1, c->iT, c->iU2, tau + D, tau + D, D, 0.5, 0.5, COMB_BLEND, nullptr, bc, &nbad,
-                        nullptr, true, false))) return rc;
+                        nullptr, true, false, false))) return rc;
     if (nbad == 0) { std::swap(c->iU, c->iT); *used = D; *okout = 1; return FIVO_OK; }
     if ((rc = restore_warm(c))) return rc;
   }
@@ -492,10 +493,10 @@ int step3(fivo_ctx* c, double tau, double dtau, int max_halve, int bc, double* u
     if ((rc = run_stage(c, c->iU, c->iU1, c->iU2, tau, tau + D, D, 1.0, 0.0, COMB_EULER, nullptr, bc, nullptr,
                         nullptr, false, true))) return rc;
     if ((rc = run_stage(c, c->iU1, c->iT, c->iU2, tau + D, tau + D, D, 0.75, 0.25, COMB_BLEND, nullptr, bc, nullptr,
-                        nullptr, false, false))) return rc;
+                        nullptr, false, false, false))) return rc;
     std::swap(c->iU1, c->iT);
     if ((rc = run_stage(c, c->iU1, c->iT, c->iU2, tau + (0.5 * D), tau + D, D, 0.0, 0.0, COMB_THIRD, nullptr, bc,
-                        &nbad, nullptr, true, false))) return rc;
+                        &nbad, nullptr, true, false, false))) return rc;
     std::swap(c->iU, c->iT);
     if (nbad == 0) { *used = D; *okout = 1; return FIVO_OK; }
     std::swap(c->iU, c->iU2);    /* the state before the step */
