@@ -522,10 +522,11 @@ int step3(fivo_ctx* c, double tau, double dtau, int max_halve, int bc, double* u
   return FIVO_OK;
 }
 
-/* update_primitives_2d!, src2d/rhs2d.jl:57-65 */
-int update_prims(fivo_ctx* c, double tau, int bc) {
+/* update_primitives_2d!, src2d/rhs2d.jl:57-65. bc_in = false: the state's ghost
+ * frame is already filled (a step's last stage filled it). */
+int update_prims(fivo_ctx* c, double tau, int bc, bool bc_in = true) {
   int rc;
-  if ((rc = launch_bc(c, c->S[c->iU], bc))) return rc;
+  if (bc_in && (rc = launch_bc(c, c->S[c->iU], bc))) return rc;
   if ((rc = reset_flags(c, 1 | 64))) return rc;
   if ((rc = launch_primitive(c, c->S[c->iU], tau))) return rc;
   return FIVO_OK;
@@ -921,7 +922,7 @@ int advance_loop(fivo_ctx* c, double tau, double taufinal, double cfl, double cf
     nsteps += 1;
     c->nsteps_run += 1;
     if (any_sector) {
-      if ((rc = update_prims(c, tau, bc))) return rc;
+      if ((rc = update_prims(c, tau, bc, false))) return rc;
       if ((rc = relax_project(c, tau, used, 1, d.hasShear))) return rc;
       if ((rc = sync_flags(c, false))) return rc;
       if (d.hasShear) {
