@@ -319,3 +319,14 @@ end
 attach!(w::GPUWork2D, gg::Union{GPURecoveryGuess,Nothing}) =
     fivocheck(ccall((:fivo_ctx_set_guess, LIBFIVO2D), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), w.h,
                     gg === nothing ? C_NULL : gg.h), "fivo_ctx_set_guess")
+
+# ----------------------------------------------------------------------------- mixed precision
+
+"""The face pass of rhs_2d! in FP32 (`:fp32_faces`) or the reference's FP64 (`:fp64`);
+recovery, SSPRK combination, floors and relaxation stay FP64 either way."""
+function set_precision!(w::GPUWork2D, mode::Symbol)
+    m = mode === :fp32_faces ? Cint(1) : mode === :fp64 ? Cint(0) :
+        throw(ArgumentError("precision must be :fp64 or :fp32_faces"))
+    fivocheck(ccall((:fivo_ctx_set_precision, LIBFIVO2D), Cint, (Ptr{Cvoid}, Cint), w.h, m),
+              "fivo_ctx_set_precision")
+end
