@@ -158,3 +158,38 @@ def test_precision_switch_and_refusal(gpu_lib):
     r3 = v.advance(r["tau"], 10.0, 0.2, 0.05, A.FIVO_SSPRK3, max_steps=5)
     assert r2["ok"] and r3["ok"] and r2["nsteps"] == r3["nsteps"] == 5
     v.close()
+
+
+@pytest.mark.parametrize("case", ["ideal_conformal", "viscous_lhrg"])
+def test_rhs_fp32_faces_against_fp64(gpu_lib, case):
+    """one rhs_2d! on the same state: the FP32 face pass moves every row of dU by no more
+    than FP32 rounding of the face fluxes allows (relative to the row's scale), and the
+    signal speed by less than 1e-6"""
+    if case == "ideal_conformal":
+        g = fivo2d.make_grid2d(48, 48, xmax=10.0, ymax=10.0)
+        m = fivo2d.build_model_2d(eos=fivo2d.ConformalHQEOS(g_eff=47.5, g_hq=0.0), with_charge=False)
+        T, a, ux, uy = ic.gubser_fields(g, 1.0, q=1.0, Tscale=5.55 * fivo2d.model.HBARC, alpha=0.0)
+        tau = 1.0
+    else:
+        m = fivo2d.build_model_2d(eos=fivo2d.LatticeHRGEOS(), enable_shear=True, enable_bulk=True,
+                                  enable_diff=True, eta_over_s=0.16, kappa_coeff=0.5)
+        g = fivo2d.make_grid2d(64, 64, xmax=64 * 15.0 / 384, ymax=64 * 15.0 / 384)
+        T, a, ux, uy, _ = ic.glauber_fields(g, 0.6, 1004)
+        tau = 0.6
+    U, _ = set_cells(m, tau, T, a, ux, uy, lib=gpu_lib)
+    out = {}
+    for mode in (A.FIVO_PRECISION_FP64, A.FIVO_PRECISION_FP32_FACES):
+        w = GPUWork2D(m, g, lib=gpu_lib)
+        w.set_precision(mode)
+        w.set_state(U)
+        out[mode] = (w.rhs(tau), w.counters().amax)
+        w.close()
+    (d64, a64), (d32, a32) = out[A.FIVO_PRECISION_FP64], out[A.FIVO_PRECISION_FP32_FACES]
+    sx, sy = g.interior()
+    for k in range(m.nv):
+        x64 = d64.reshape(g.Nxtot, g.Nytot, m.nv)[sx, sy, k]
+        x32 = d32.reshape(g.Nxtot, g.Nytot, m.nv)[sx, sy, k]
+        scale = max(np.abs(x64).max(), 1e-300)
+        assert np.abs(x32 - x64).max() <= 1e-3 * scale, (k, np.abs(x32 - x64).max() / scale)
+    assert abs(a32 - a64) <= 1e-6 * a64
+    assert not np.array_equal(d32, d64)               # really the FP32 arithmetic
