@@ -261,12 +261,18 @@ __device__ __forceinline__ Recovery attempt_warp(const CellCons& c, const DevPar
       jac_ok = __all_sync(FV_FULL, fin);
     }
     if (!jac_ok) { out.reason = PRR_NONFINITE_JACOBIAN; break; }
+    /* 1 / (2h) of column k on lane k: independent IEEE divisions do not overlap
+     * within a lane, across lanes they cost one */
+    double inv2h_l;
+    {
+      const int k = lane & 3;
+      const int s = NCH ? k : (k == 0 ? 0 : k + 1);
+      double h = 1e-6 * jmax(1.0, fabs_(pick4(x, s)));
+      inv2h_l = 1.0 / (2.0 * h);
+    }
 #pragma unroll
     for (int k = 0; k < NU; ++k) {
-      const int s = NCH ? k : (k == 0 ? 0 : k + 1);
-      double xs = x[s];
-      double h = 1e-6 * jmax(1.0, fabs_(xs));
-      double inv2h = 1.0 / (2.0 * h);
+      const double inv2h = shfl_d(inv2h_l, k);
 #pragma unroll
       for (int r = 0; r < NU; ++r) {
         const int rr = NCH ? r : r + 1;
@@ -282,24 +288,35 @@ __device__ __forceinline__ Recovery attempt_warp(const CellCons& c, const DevPar
       Fact[r] = F[rr] * rs[rr];
     }
     if (!solve_gauss<NU>(delta, J, Fact)) { out.reason = PRR_LINSOLVE_FAILED; break; }
-    double alpha = 1.0;
+    /* alpha = min(1, min over |delta_k| > 1 of 1 / |delta_k|) as the reference
+     * takes it; a correctly rounded reciprocal is monotone, so the minimum of the
+     * reciprocals is the reciprocal of the maximum: one division, same bits
+     * (a NaN |delta_k| fails `> 1` in both forms, an infinite one gives 0) */
+    double amax = 0.0;
 #pragma unroll
     for (int k = 0; k < NU; ++k) {
       double ad = fabs_(delta[k]);
-      if (ad > 1.0) alpha = jmin(alpha, 1.0 / ad);
+      if (ad > 1.0 && !(ad <= amax)) amax = ad;
     }
+    const double alpha = amax > 1.0 ? 1.0 / amax : 1.0;
     /* ---- one round: lane l < 12 tries alpha * 2^-l (the line search); lanes
      * 12 .. 12 + 2 NU - 1 evaluate the Jacobian at the first trial point, which
-     * the next iteration uses when that trial is the one accepted */
+     * the next iteration uses when that trial is the one accepted. The l
+     * halvings of the sequential loop are exact while the result is normal,
+     * which alpha >= 2^-1011 guarantees for l <= 11; below that the halvings are
+     * repeated as written (warp-uniform). */
+    double al = alpha * (lane < 12 ? from_bits((uint64_t)(1023 - lane) << 52) : 1.0);
+    if (!(alpha >= 0x1p-1011)) {
+      al = alpha;
+      if (lane < 12)
+        for (int q = 0; q < lane; ++q) al *= 0.5;
+    }
     double xt[4];
-    double al = alpha;
-    if (lane < 12) {
-      for (int q = 0; q < lane; ++q) al *= 0.5;
-      trial_point<NCH>(x, delta, al, yT_lo, yT_hi, xt);
-    } else {
-      double x0[4];
-      trial_point<NCH>(x, delta, alpha, yT_lo, yT_hi, x0);
-      jac_point<NCH>(x0, (lane - 12) & 7, xt);
+    trial_point<NCH>(x, delta, al, yT_lo, yT_hi, xt);
+    if (lane >= 12) {
+      double xj[4];
+      jac_point<NCH>(xt, (lane - 12) & 7, xj);
+      xt[0] = xj[0]; xt[1] = xj[1]; xt[2] = xj[2]; xt[3] = xj[3];
     }
     double Ft[4] = {0.0, 0.0, 0.0, 0.0};
     bool acc = false, fspec = true;
