@@ -690,7 +690,7 @@ FX_HD Recovery recover_fast(const CellCons& c, const DevParams& d, double yT0, d
   const double D = c.D, Sx = c.Sx, Sy = c.Sy, E = c.E;
   if (is_vacuum(c)) return vacuum_recovery<EOS>(c, d);
   const int NU = NCH ? 4 : 3;
-  double x[4], F[4], J[4][4], delta[4];
+  double x[4], F[4], J[4][4] = {}, delta[4];
   x[1] = (NCH && isfinite_(phi0)) ? jclamp(phi0, -FV_PHI_CAP, FV_PHI_CAP) : 0.0;
   x[0] = jclamp(yT0, yT_lo, yT_hi);
   x[2] = jclamp(ux0, -FV_U_CAP, FV_U_CAP);
@@ -732,40 +732,49 @@ FX_HD Recovery recover_fast(const CellCons& c, const DevParams& d, double yT0, d
     }
     /* ---- Jacobian: all 2 NU evaluations, then the finiteness test of the columns */
     const double h0 = 1e-6 * jmax(1.0, fabs_(x[0]));
-    const double Tp = fx_exp(x[0] + h0), Tn = fx_exp(x[0] - h0);
+    double Tp = 0.0, Tn = 0.0;
     TPart tpp, tpn;
-    tpart<EOS>(Tp, d, tpp);
-    tpart<EOS>(Tn, d, tpn);
-    double Fp[4][4], Fm[4][4], hh[4];
+#pragma unroll 1
+    for (int sg = 0; sg < 2; ++sg) {   /* T e^{+h}, then T e^{-h}: one inlined copy */
+      const double Tq = fx_exp(sg ? x[0] - h0 : x[0] + h0);
+      TPart t;
+      tpart<EOS>(Tq, d, t);
+      if (sg) { Tn = Tq; tpn = t; } else { Tp = Tq; tpp = t; }
+    }
+    /* one column per trip of a loop that is not unrolled: two evaluation sites
+     * instead of 2 NU keep the kernel's code small (instruction fetch, not the
+     * FP64 pipe, is what its warps wait on most). The column enters J from the
+     * right and the earlier ones shift left, so J keeps static indices. */
     bool ok_jac = true;
-#pragma unroll
+#pragma unroll 1
     for (int k = 0; k < NU; ++k) {
       const int s = NCH ? k : (k == 0 ? 0 : k + 1);
-      const double xs = x[s];
+      const double xs = s == 0 ? x[0] : (s == 1 ? x[1] : (s == 2 ? x[2] : x[3]));
       const double h = 1e-6 * jmax(1.0, fabs_(xs));
-      hh[k] = h;
-      double xp[4] = {x[0], x[1], x[2], x[3]}, xm[4] = {x[0], x[1], x[2], x[3]};
-      xp[s] = xs + h;
-      xm[s] = xs - h;
-      if (s == 0) {
-        evalF_tp<EOS, NCH>(Fp[k], xp, Tp, c, d, tpp);
-        evalF_tp<EOS, NCH>(Fm[k], xm, Tn, c, d, tpn);
-      } else {
-        evalF_tp<EOS, NCH>(Fp[k], xp, Tc, c, d, tpc);
-        evalF_tp<EOS, NCH>(Fm[k], xm, Tc, c, d, tpc);
-      }
-      ok_jac = ok_jac && finite4(Fp[k]) && finite4(Fm[k]);
-    }
-    if (!ok_jac) { out.reason = PRR_NONFINITE_JACOBIAN; break; }
-#pragma unroll
-    for (int k = 0; k < NU; ++k) {
-      const double inv2h = 1.0 / (2.0 * hh[k]);
+      const double xsp = xs + h, xsm = xs - h;
+      double xp[4], xm[4];
+      xp[0] = s == 0 ? xsp : x[0]; xm[0] = s == 0 ? xsm : x[0];
+      xp[1] = s == 1 ? xsp : x[1]; xm[1] = s == 1 ? xsm : x[1];
+      xp[2] = s == 2 ? xsp : x[2]; xm[2] = s == 2 ? xsm : x[2];
+      xp[3] = s == 3 ? xsp : x[3]; xm[3] = s == 3 ? xsm : x[3];
+      const bool ts = s == 0;
+      TPart ap, am;
+      ap.x = ts ? tpp.x : tpc.x; ap.Pl = ts ? tpp.Pl : tpc.Pl; ap.el = ts ? tpp.el : tpc.el; ap.K2 = ts ? tpp.K2 : tpc.K2;
+      am.x = ts ? tpn.x : tpc.x; am.Pl = ts ? tpn.Pl : tpc.Pl; am.el = ts ? tpn.el : tpc.el; am.K2 = ts ? tpn.K2 : tpc.K2;
+      double fp[4], fm[4];
+      evalF_tp<EOS, NCH>(fp, xp, ts ? Tp : Tc, c, d, ap);
+      evalF_tp<EOS, NCH>(fm, xm, ts ? Tn : Tc, c, d, am);
+      ok_jac = ok_jac && finite4(fp) && finite4(fm);
+      const double inv2h = 1.0 / (2.0 * h);
 #pragma unroll
       for (int r = 0; r < NU; ++r) {
         const int rr = NCH ? r : r + 1;
-        J[r][k] = ((Fp[k][rr] - Fm[k][rr]) * inv2h) * rs[rr];
+#pragma unroll
+        for (int q = 0; q + 1 < NU; ++q) J[r][q] = J[r][q + 1];
+        J[r][NU - 1] = ((fp[rr] - fm[rr]) * inv2h) * rs[rr];
       }
     }
+    if (!ok_jac) { out.reason = PRR_NONFINITE_JACOBIAN; break; }
     double Fact[4];
 #pragma unroll
     for (int r = 0; r < NU; ++r) {
