@@ -25,6 +25,15 @@
 #include "coop.cuh"
 #include "guess.cuh"
 
+/* resident blocks of 128 threads per SM the recovery and face kernels are
+ * compiled for (their register budget): measured optima, overridable */
+#ifndef FV_FAST_MINB
+#define FV_FAST_MINB 4
+#endif
+#ifndef FV_FACE_MINB
+#define FV_FACE_MINB 8
+#endif
+
 namespace fv {
 
 #define FV_MAXV 11
@@ -1206,7 +1215,7 @@ __device__ __forceinline__ void load_cons(const DevParams& d, const DevState& U,
 }
 
 template <int EOS, bool NCH>
-__global__ void __launch_bounds__(128, 4) k_prim_fast(DevParams d, DevState U, DevPrims w, DevHist h, double tau,
+__global__ void __launch_bounds__(128, FV_FAST_MINB) k_prim_fast(DevParams d, DevState U, DevPrims w, DevHist h, double tau,
                                                    DevFlags* fl, unsigned int* queue) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   bool vac = false, defer = false;
@@ -1527,7 +1536,7 @@ __device__ __forceinline__ double face_flux_pair(const DevParams& d, const DevSt
 /* two lanes per face of one direction, every face of the (ghost-inclusive) grid;
  * the lane of the left state stores the even rows, its partner the odd ones */
 template <int EOS, bool XDIR>
-__global__ void __launch_bounds__(128, 8) k_faces(DevParams d, DevState Ub, DevPrims w, double tau,
+__global__ void __launch_bounds__(128, FV_FACE_MINB) k_faces(DevParams d, DevState Ub, DevPrims w, double tau,
                                                const uint8_t* ffo, double* Fh, DevFlags* fl) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long nf = XDIR ? (long long)(d.Nxtot - 1) * d.Nytot : (long long)d.Nxtot * (d.Nytot - 1);

@@ -814,17 +814,20 @@ FX_HD Recovery recover_fast(const CellCons& c, const DevParams& d, double yT0, d
   }
   if (iters) *iters = nupd;
   out.resnorm = last_nrm;
-  double T = jclamp(fx_exp(x[0]), FV_T_MIN, FV_T_SOLVE_MAX);
+  /* Here Tc = exp(x[0]), tpc is its temperature part and F the residual at x:
+   * every exit of the loop leaves the three from the last evaluation at x. The
+   * closing EOS call reuses tpc unless the clamp moved T, and the closing
+   * residual is F itself (the same pure function of the same arguments). */
+  double T = jclamp(Tc, FV_T_MIN, FV_T_SOLVE_MAX);
   double mu = NCH ? (m + (T * x[1])) : m;
   double ux = x[2], uy = x[3];
   double P, n, en;
   {
-    TPart tpf;
-    tpart<EOS>(T, d, tpf);
+    TPart tpf = tpc;
+    if (!(T == Tc)) tpart<EOS>(T, d, tpf);
     eos_tp<EOS>(T, mu, d, tpf, &P, &n, &en);
   }
   if (!converged) out.reason = (out.reason == PRR_UNSET) ? PRR_MAXIT : out.reason;
-  evalF_tp<EOS, NCH>(F, x, Tc, c, d, tpc);
   double rows[4] = {0.0, 0.0, 0.0, 0.0};
   double resnorm = 0.0;
 #pragma unroll
