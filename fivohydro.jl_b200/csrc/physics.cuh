@@ -662,10 +662,12 @@ FX_HD void eos_tp(double T, double mu, const DevParams& d, const TPart& tp, doub
   lhrg_assemble(Tm, mu, d, tp.x, tp.Pl, tp.el, tp.K2, P, n, en);
 }
 
-/* evalF_2d! (src2d/primrec2d.jl:360-390) with tp the T-part of exp(x[0]) */
+/* evalF_2d! (src2d/primrec2d.jl:360-390) with tp the T-part of exp(x[0]);
+ * *eo receives the EOS values at x when given */
+struct EosAt { double P, n, en; };
 template <int EOS, bool NCH>
 FX_HD void evalF_tp(double F[4], const double x[4], double T, const CellCons& c, const DevParams& d,
-                    const TPart& tp) {
+                    const TPart& tp, EosAt* eo = nullptr) {
   double yT = x[0], phi = x[1], ux = x[2], uy = x[3];
   if (!(isfinite_(yT) && isfinite_(phi) && isfinite_(ux) && isfinite_(uy))) {
     F[0] = F[1] = F[2] = F[3] = inf_(); return;
@@ -674,6 +676,7 @@ FX_HD void evalF_tp(double F[4], const double x[4], double T, const CellCons& c,
   double ut = utau(ux, uy);
   double P, n, en;
   eos_tp<EOS>(T, mu, d, tp, &P, &n, &en);
+  if (eo) { eo->P = P; eo->n = n; eo->en = en; }
   evalF_rows<NCH>(F, P, n, en, ux, uy, ut, c);
 }
 
@@ -697,8 +700,9 @@ FX_HD Recovery recover_fast(const CellCons& c, const DevParams& d, double yT0, d
   x[3] = jclamp(uy0, -FV_U_CAP, FV_U_CAP);
   double Tc = fx_exp(x[0]);
   TPart tpc;
+  EosAt ec;    /* the EOS values of the last evaluation at x */
   tpart<EOS>(Tc, d, tpc);
-  evalF_tp<EOS, NCH>(F, x, Tc, c, d, tpc);
+  evalF_tp<EOS, NCH>(F, x, Tc, c, d, tpc, &ec);
   if (!finite4(F)) {
     out.reason = PRR_NONFINITE_INITIAL;
     double T = jclamp(fx_exp(x[0]), FV_T_MIN, FV_T_SOLVE_MAX), P, n, en;
@@ -762,8 +766,16 @@ FX_HD Recovery recover_fast(const CellCons& c, const DevParams& d, double yT0, d
       ap.x = ts ? tpp.x : tpc.x; ap.Pl = ts ? tpp.Pl : tpc.Pl; ap.el = ts ? tpp.el : tpc.el; ap.K2 = ts ? tpp.K2 : tpc.K2;
       am.x = ts ? tpn.x : tpc.x; am.Pl = ts ? tpn.Pl : tpc.Pl; am.el = ts ? tpn.el : tpc.el; am.K2 = ts ? tpn.K2 : tpc.K2;
       double fp[4], fm[4];
-      evalF_tp<EOS, NCH>(fp, xp, ts ? Tp : Tc, c, d, ap);
-      evalF_tp<EOS, NCH>(fm, xm, ts ? Tn : Tc, c, d, am);
+      if (s <= 1) {
+        evalF_tp<EOS, NCH>(fp, xp, ts ? Tp : Tc, c, d, ap);
+        evalF_tp<EOS, NCH>(fm, xm, ts ? Tn : Tc, c, d, am);
+      } else {
+        /* a velocity column keeps x's T and phi, so mu and the EOS values are
+         * those at x (the same pure function of the same arguments); the
+         * shifted points are finite, x being finite and clamped */
+        evalF_rows<NCH>(fp, ec.P, ec.n, ec.en, xp[2], xp[3], utau(xp[2], xp[3]), c);
+        evalF_rows<NCH>(fm, ec.P, ec.n, ec.en, xm[2], xm[3], utau(xm[2], xm[3]), c);
+      }
       ok_jac = ok_jac && finite4(fp) && finite4(fm);
       const double inv2h = 1.0 / (2.0 * h);
 #pragma unroll
@@ -801,7 +813,7 @@ FX_HD Recovery recover_fast(const CellCons& c, const DevParams& d, double yT0, d
       x[3] = jclamp(x[3], -FV_U_CAP, FV_U_CAP);
       Tc = fx_exp(x[0]);
       tpart<EOS>(Tc, d, tpc);
-      evalF_tp<EOS, NCH>(F, x, Tc, c, d, tpc);
+      evalF_tp<EOS, NCH>(F, x, Tc, c, d, tpc, &ec);
       if (finite4(F)) {
         double trial = 0.0;
 #pragma unroll
