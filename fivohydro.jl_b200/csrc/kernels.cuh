@@ -84,6 +84,12 @@ __device__ __forceinline__ int slot_of(const DevParams& d, int a) {
   return 10;
 }
 
+/* the plane of flux slot s (slot_of inverted; -1 when the model has no such plane) */
+__device__ __forceinline__ int plane_of(const DevParams& d, int s) {
+  return s < 4 ? s : (s == 4 ? d.iNux : (s == 5 ? d.iNuy : (s == 6 ? d.iPi : (s == 7 ? d.iPixx :
+         (s == 8 ? d.iPixy : (s == 9 ? d.iPiyy : d.iPieta))))));
+}
+
 __device__ __forceinline__ void load_dis(const DevParams& d, const DevState& U, long long i, double dis[7]) {
   dis[0] = d.hasNu ? U.f[d.iNux][i] : 0.0;
   dis[1] = d.hasNu ? U.f[d.iNuy][i] : 0.0;
@@ -1449,11 +1455,12 @@ __global__ void __launch_bounds__(128) k_prim_slow(DevParams d, DevState U, DevP
  * those of face_flux (the same expressions, the same order), so the fluxes have
  * its bits; a lane does half the EOS work, which halves the dependent chain of a
  * face and the registers it needs. All lanes of the warp must call it.
- * Returns max(|sL|, |sR|); writes the flux of every row into out[]. */
+ * Returns max(|sL|, |sR|); stores each row of the HLLE flux into its plane of
+ * Fh (the lane of side a % 2 stores plane a) unless Fh is null. */
 template <int EOS, bool XDIR>
 __device__ __forceinline__ double face_flux_pair(const DevParams& d, const DevState& U, const DevPrims& w,
                                                  long long i, long long st, int k, int kmax, double tau,
-                                                 const uint8_t* ffo, int side, double out[FV_MAXV]) {
+                                                 const uint8_t* ffo, int side, double* Fh) {
   const long long ip = i + st;
   const long long c0 = side ? ip : i;
   /* the two lanes of this pair; every branch below is taken by both or neither */
@@ -1503,33 +1510,39 @@ __device__ __forceinline__ double face_flux_pair(const DevParams& d, const DevSt
     }
   }
   if (floored) p.cs2 = eos_cs2<EOS>(FV_T_MIN, d);
-  double F[11];
-  flux_cell<XDIR>(F, p, tau, d);
+  double F4[4], v;
+  flux_cons4<XDIR>(F4, p, tau, &v);
   double lm, lp;
   wavespeeds<XDIR>(p, XDIR ? p.pixx : p.piyy, &lm, &lp);
   const double lmo = __shfl_xor_sync(pm, lm, 1), lpo = __shfl_xor_sync(pm, lp, 1);
   const double lmL = side ? lmo : lm, lmR = side ? lm : lmo;
   const double lpL = side ? lpo : lp, lpR = side ? lp : lpo;
   const double sL = jmin(lmL, lmR), sR = jmax(lpL, lpR);
-  /* conserved column of this state incl. its stored dissipatives (zero when floored) */
-  double cv[11];
-  cv[0] = uc[0]; cv[1] = uc[1]; cv[2] = uc[2]; cv[3] = uc[3];
-#pragma unroll
-  for (int q = 0; q < 7; ++q) cv[4 + q] = floored ? 0.0 : dis[q];
+  const bool an = d.hasNu && d.p.advect_nu, aP = d.hasPi && d.p.advect_Pi, ap = d.hasShear && d.p.advect_pi;
   const double inv = 1.0 / ((sR - sL) + FV_TINY);
 #pragma unroll
   for (int s = 0; s < 11; ++s) {
-    const double Fo = __shfl_xor_sync(pm, F[s], 1);
-    const double co = __shfl_xor_sync(pm, cv[s], 1);
-    const double FLs = side ? Fo : F[s], FRs = side ? F[s] : Fo;
-    const double cls = side ? co : cv[s], crs = side ? cv[s] : co;
+    /* row s of this state: the conserved column (its stored dissipatives, zero
+     * when floored) and the flux of flux_cell_2d!, whose advected rows are that
+     * same dissipative times v */
+    double cs, Fs;
+    if (s < 4) { cs = uc[s]; Fs = F4[s]; }
+    else {
+      cs = floored ? 0.0 : dis[s - 4];
+      const bool adv = s < 6 ? an : (s == 6 ? aP : ap);
+      Fs = adv ? cs * v : 0.0;
+    }
+    const double Fo = __shfl_xor_sync(pm, Fs, 1);
+    const double co = __shfl_xor_sync(pm, cs, 1);
+    const double FLs = side ? Fo : Fs, FRs = side ? Fs : Fo;
+    const double cls = side ? co : cs, crs = side ? cs : co;
     double h;
     if (sL >= 0) h = FLs;
     else if (sR <= 0) h = FRs;
     else h = (((sR * FLs) - (sL * FRs)) + ((sR * sL) * (crs - cls))) * inv;
-    F[s] = h;
+    const int a = plane_of(d, s);
+    if (Fh && a >= 0 && (a & 1) == side) Fh[(size_t)a * d.Ntot + i] = h;
   }
-  for (int a = 0; a < d.nv; ++a) out[a] = F[slot_of(d, a)];
   return jmax(fabs_(sL), fabs_(sR));
 }
 
@@ -1551,10 +1564,8 @@ __global__ void __launch_bounds__(128, FV_FACE_MINB) k_faces(DevParams d, DevSta
     int ix = (int)(f / (d.Nytot - 1)), iy = (int)(f % (d.Nytot - 1));
     i = (long long)ix * d.Nytot + iy; k = iy; kmax = d.Nytot;
   }
-  double out[FV_MAXV];
-  double amax = face_flux_pair<EOS, XDIR>(d, Ub, w, i, XDIR ? d.Nytot : 1, k, kmax, tau, ffo, side, out);
-  if (valid)
-    for (int q = side; q < d.nv; q += 2) Fh[(size_t)q * d.Ntot + i] = out[q];
+  double amax = face_flux_pair<EOS, XDIR>(d, Ub, w, i, XDIR ? d.Nytot : 1, k, kmax, tau, ffo, side,
+                                          valid ? Fh : nullptr);
   for (int o = 16; o > 0; o >>= 1) amax = jmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
   __shared__ double red[4];
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = amax;

@@ -924,11 +924,10 @@ FX_HD void wavespeeds(const Prim& p, double pinn, double* lm, double* lp) {
   *lp = jclamp(b, -1.0, 1.0);
 }
 
-/* flux_cell_2d!, src2d/fluxes2d.jl:24-69: conserved four into F[0..3], the
- * advected dissipatives (only with advect_*) into F[4..10] by field order
- * nux, nuy, Pi, pixx, pixy, piyy, pieta. */
+/* the conserved four rows of flux_cell_2d! (src2d/fluxes2d.jl:24-69) and the
+ * normal velocity v that the advected rows multiply */
 template <bool XDIR>
-FX_HD void flux_cell(double F[11], const Prim& p, double tau, const DevParams& d) {
+FX_HD void flux_cons4(double F[4], const Prim& p, double tau, double* vn) {
   double ux = p.ux, uy = p.uy;
   double ut = utau(ux, uy);
   double iu = safe_inv(ut);
@@ -937,20 +936,28 @@ FX_HD void flux_cell(double F[11], const Prim& p, double tau, const DevParams& d
   double weff = (p.e + p.P) + p.Pi;
   PiC pc = shear_tensor(ux, uy, ut, p.pixx, p.pixy, p.piyy);
   double Jx = (p.n * ux) + p.nux, Jy = (p.n * uy) + p.nuy;
-  double v;
   if (XDIR) {
     F[0] = tau * Jx;
     F[1] = (((weff * ux) * ux) + Ptot) + pc.xx;
     F[2] = ((weff * ux) * uy) + pc.xy;
     F[3] = ((weff * ut) * ux) + pc.tx;
-    v = vx;
+    *vn = vx;
   } else {
     F[0] = tau * Jy;
     F[1] = ((weff * ux) * uy) + pc.xy;
     F[2] = (((weff * uy) * uy) + Ptot) + pc.yy;
     F[3] = ((weff * ut) * uy) + pc.ty;
-    v = vy;
+    *vn = vy;
   }
+}
+
+/* flux_cell_2d!, src2d/fluxes2d.jl:24-69: conserved four into F[0..3], the
+ * advected dissipatives (only with advect_*) into F[4..10] by field order
+ * nux, nuy, Pi, pixx, pixy, piyy, pieta. */
+template <bool XDIR>
+FX_HD void flux_cell(double F[11], const Prim& p, double tau, const DevParams& d) {
+  double v;
+  flux_cons4<XDIR>(F, p, tau, &v);
   bool an = d.hasNu && d.p.advect_nu, aP = d.hasPi && d.p.advect_Pi, ap = d.hasShear && d.p.advect_pi;
   F[4] = an ? p.nux * v : 0.0;
   F[5] = an ? p.nuy * v : 0.0;
