@@ -166,8 +166,9 @@ __device__ __forceinline__ void wavespeeds_f(const PrimF& p, float pinn, float* 
   *lp = jclampf(((vn * (1.0f - cs2)) + disc) / den, -1.0f, 1.0f);
 }
 
+/* the conserved four rows of flux_cell_2d! and the normal velocity */
 template <bool XDIR>
-__device__ __forceinline__ void flux_cell_f(float F[11], const PrimF& p, float tau, const fv::DevParams& d) {
+__device__ __forceinline__ void flux_cons4_f(float F[4], const PrimF& p, float tau, float* vn) {
   const float ux = p.ux, uy = p.uy, ut = utauf(ux, uy), iu = safe_invf(ut);
   const float vx = ux * iu, vy = uy * iu;
   const float Ptot = p.P + p.Pi, weff = (p.e + p.P) + p.Pi;
@@ -181,17 +182,14 @@ __device__ __forceinline__ void flux_cell_f(float F[11], const PrimF& p, float t
     F[0] = tau * Jy; F[1] = ((weff * ux) * uy) + pc.xy; F[2] = (((weff * uy) * uy) + Ptot) + pc.yy;
     F[3] = ((weff * ut) * uy) + pc.ty; v = vy;
   }
-  const bool an = d.hasNu && d.p.advect_nu, aP = d.hasPi && d.p.advect_Pi, ap = d.hasShear && d.p.advect_pi;
-  F[4] = an ? p.nux * v : 0.0f; F[5] = an ? p.nuy * v : 0.0f; F[6] = aP ? p.Pi * v : 0.0f;
-  F[7] = ap ? p.pixx * v : 0.0f; F[8] = ap ? p.pixy * v : 0.0f; F[9] = ap ? p.piyy * v : 0.0f;
-  F[10] = ap ? p.pieta * v : 0.0f;
+  *vn = v;
 }
 
 /* face_flux_pair in FP32 (two lanes per face; see kernels.cuh) */
 template <int EOS, bool XDIR>
 __device__ __forceinline__ float face_flux_pair_f(const fv::DevParams& d, const fv::DevState& U, const fv::DevPrims& w,
                                                   long long i, long long st, int k, int kmax, double tau_d,
-                                                  const uint8_t* ffo, int side, float out[FV_MAXV]) {
+                                                  const uint8_t* ffo, int side, float* Fh) {
   const long long ip = i + st;
   const long long c0 = side ? ip : i;
   const unsigned pm = 3u << (threadIdx.x & 30);
@@ -240,32 +238,37 @@ __device__ __forceinline__ float face_flux_pair_f(const fv::DevParams& d, const 
     }
   }
   if (floored) p.cs2 = (float)fv::eos_cs2<EOS>(FV_T_MIN, d);
-  float F[11];
-  flux_cell_f<XDIR>(F, p, tau, d);
+  float F4[4], v;
+  flux_cons4_f<XDIR>(F4, p, tau, &v);
   float lm, lp;
   wavespeeds_f<XDIR>(p, XDIR ? p.pixx : p.piyy, &lm, &lp);
   const float lmo = __shfl_xor_sync(pm, lm, 1), lpo = __shfl_xor_sync(pm, lp, 1);
   const float lmL = side ? lmo : lm, lmR = side ? lm : lmo;
   const float lpL = side ? lpo : lp, lpR = side ? lp : lpo;
   const float sL = jminf(lmL, lmR), sR = jmaxf(lpL, lpR);
-  float cv[11];
-  cv[0] = uc[0]; cv[1] = uc[1]; cv[2] = uc[2]; cv[3] = uc[3];
-#pragma unroll
-  for (int q = 0; q < 7; ++q) cv[4 + q] = floored ? 0.0f : dis[q];
+  const bool an = d.hasNu && d.p.advect_nu, aP = d.hasPi && d.p.advect_Pi, ap = d.hasShear && d.p.advect_pi;
   const float inv = 1.0f / ((sR - sL) + TINY_F);
 #pragma unroll
   for (int s = 0; s < 11; ++s) {
-    const float Fo = __shfl_xor_sync(pm, F[s], 1);
-    const float co = __shfl_xor_sync(pm, cv[s], 1);
-    const float FLs = side ? Fo : F[s], FRs = side ? F[s] : Fo;
-    const float cls = side ? co : cv[s], crs = side ? cv[s] : co;
+    /* row s: conserved column and flux (advected rows = stored dissipative * v) */
+    float cs, Fs;
+    if (s < 4) { cs = uc[s]; Fs = F4[s]; }
+    else {
+      cs = floored ? 0.0f : dis[s - 4];
+      const bool adv = s < 6 ? an : (s == 6 ? aP : ap);
+      Fs = adv ? cs * v : 0.0f;
+    }
+    const float Fo = __shfl_xor_sync(pm, Fs, 1);
+    const float co = __shfl_xor_sync(pm, cs, 1);
+    const float FLs = side ? Fo : Fs, FRs = side ? Fs : Fo;
+    const float cls = side ? co : cs, crs = side ? cs : co;
     float h;
     if (sL >= 0.0f) h = FLs;
     else if (sR <= 0.0f) h = FRs;
     else h = (((sR * FLs) - (sL * FRs)) + ((sR * sL) * (crs - cls))) * inv;
-    F[s] = h;
+    const int a = fv::plane_of(d, s);
+    if (Fh && a >= 0 && (a & 1) == side) Fh[(size_t)a * d.Ntot + i] = h;
   }
-  for (int a = 0; a < d.nv; ++a) out[a] = F[fv::slot_of(d, a)];
   return jmaxf(fabsf(sL), fabsf(sR));
 }
 
@@ -285,10 +288,8 @@ __global__ void __launch_bounds__(128, 8) k_faces32(fv::DevParams d, fv::DevStat
     const int ix = (int)(f / (d.Nytot - 1)), iy = (int)(f % (d.Nytot - 1));
     i = (long long)ix * d.Nytot + iy; k = iy; kmax = d.Nytot;
   }
-  float out[FV_MAXV];
-  float amax = face_flux_pair_f<EOS, XDIR>(d, Ub, w, i, XDIR ? d.Nytot : 1, k, kmax, tau, ffo, side, out);
-  if (valid)
-    for (int q = side; q < d.nv; q += 2) Fh[(size_t)q * d.Ntot + i] = out[q];
+  float amax = face_flux_pair_f<EOS, XDIR>(d, Ub, w, i, XDIR ? d.Nytot : 1, k, kmax, tau, ffo, side,
+                                            valid ? Fh : nullptr);
   for (int o = 16; o > 0; o >>= 1) amax = jmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
   __shared__ float red[4];
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = amax;
