@@ -1189,9 +1189,8 @@ int fivo_cons_to_prim(const fivo_params* p, int64_t n, double tau, const double*
 /* ======================================================== rhs without allocation
  *
  * Some hosts cannot call cudaMalloc: a Julia driver whose device memory is owned
- * by CUDA.jl's pool allocator, a caller inside a captured or replayed CUDA
- * graph, or a long-running service that forbids device allocation after start-up
- * so its memory footprint stays fixed. fivo_rhs_noalloc serves them: its work
+ * by CUDA.jl's pool allocator, or a long-running service that forbids device
+ * allocation after start-up so its memory footprint stays fixed. fivo_rhs_noalloc serves them: its work
  * memory (the cell primitives, the warm-start planes it starts cold from, and
  * the flag block) is the file-scope array below, sized for
  * FIVO_NOALLOC_MAX_CELLS cells (about 17 MB). The array exists on every GPU

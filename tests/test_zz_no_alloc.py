@@ -1,9 +1,8 @@
 """fivo_rhs_noalloc: the right-hand side for callers that cannot allocate device memory.
 
 Hosts whose device memory belongs to someone else's allocator (a Julia driver
-on CUDA.jl's pool), code running inside a captured CUDA graph, or services that
-forbid device allocation after start-up cannot use the context-based entry
-points, which cudaMalloc their work arrays. fivo_rhs_noalloc keeps its work
+on CUDA.jl's pool), or services that forbid device allocation after start-up,
+cannot use the context-based entry points, which cudaMalloc their work arrays. fivo_rhs_noalloc keeps its work
 memory in a fixed file-scope device array instead; the caller passes the state
 and the output buffer. This test calls it twice in a row through the C ABI and
 checks each result against the context-based fivo_rhs on the same state, to the
