@@ -270,14 +270,21 @@ __device__ __forceinline__ Recovery attempt_warp(const CellCons& c, const DevPar
       double h = 1e-6 * jmax(1.0, fabs_(pick4(x, s)));
       inv2h_l = 1.0 / (2.0 * h);
     }
+    /* lane 2k holds F(x + h e_k), lane 2k + 1 F(x - h e_k): the even lane forms
+     * the difference from its partner's rows, then each entry is broadcast once */
+    double dF[4];
+#pragma unroll
+    for (int r = 0; r < NU; ++r) {
+      const int rr = NCH ? r : r + 1;
+      dF[r] = Fj[rr] - __shfl_xor_sync(FV_FULL, Fj[rr], 1);
+    }
 #pragma unroll
     for (int k = 0; k < NU; ++k) {
       const double inv2h = shfl_d(inv2h_l, k);
 #pragma unroll
       for (int r = 0; r < NU; ++r) {
         const int rr = NCH ? r : r + 1;
-        double fp = shfl_d(Fj[rr], 2 * k), fm = shfl_d(Fj[rr], 2 * k + 1);
-        J[r][k] = ((fp - fm) * inv2h) * rs[rr];
+        J[r][k] = (shfl_d(dF[r], 2 * k) * inv2h) * rs[rr];
       }
     }
     double Fact[4];
