@@ -678,7 +678,7 @@ int fivo_ctx_create(const fivo_params* p, int nx, int ny, int nghost, double xma
   q = c->hbuf;
   c->h.x0_yT = q; q += N; c->h.x0_phi = q; q += N; c->h.x0_ux = q; q += N; c->h.x0_uy = q; q += N;
   c->h.ux_prev = q; q += N; c->h.uy_prev = q; q += N; c->h.alpha_prev = q; q += N; c->h.T_prev = q;
-  /* Work2D(): zeros, NaN history (src2d/work2d.jl:387-411) */
+  /* Work2D(): zeros, NaN history (src2d/work2d.jl:115-139) */
   if (cudaMemsetAsync(c->slab, 0, 4 * (size_t)d.nv * N * 8, c->st) != cudaSuccess ||
       cudaMemsetAsync(c->pbuf, 0, 9 * N * 8 + N, c->st) != cudaSuccess ||
       cudaMemsetAsync(c->masks, 0, 3 * N, c->st) != cudaSuccess)
@@ -981,6 +981,11 @@ int fivo_advance(fivo_ctx* c, double tau, double taufinal, double cfl, double cf
   return advance_loop(c, tau, taufinal, cfl, cfltau, integrator, bc, max_steps, out);
 }
 
+int fivo_run_diagnostics(fivo_ctx* c, double* Q, double* maxu, double* minPtot) {
+  if (!c || !Q || !maxu || !minPtot) return fail(FIVO_ERR_ARG, "null argument");
+  return diag(c, true, Q, maxu, minPtot);
+}
+
 int fivo_finalize_ic(fivo_ctx* c, double tau0, int bc) {
   if (!c) return fail(FIVO_ERR_ARG, "null context");
   const DevParams& d = c->dp;
@@ -1195,10 +1200,13 @@ int fivo_cons_to_prim(const fivo_params* p, int64_t n, double tau, const double*
  * the flag block) is the file-scope array below, sized for
  * FIVO_NOALLOC_MAX_CELLS cells (about 17 MB). The array exists on every GPU
  * that loads this library until the process exits. The first call on a device
- * looks up its device address (cudaGetSymbolAddress), so make that first call
- * before any stream capture. Every call shares the array and it keeps the last
- * call's contents, so each call clears what must start cleared (flags, warm
- * starts); calls whose work overlaps on the GPU race on it.
+ * looks up its device address (cudaGetSymbolAddress) and keeps it for the life of
+ * the process, so make that first call before any stream capture, and do not use
+ * the library across a cudaDeviceReset (the kept address would be stale). Every
+ * call shares the array and it keeps the last call's contents, so each call clears
+ * what must start cleared (flags, warm starts); calls whose work overlaps on the
+ * GPU race on it. A call is synchronous: it waits for its stream to read back the
+ * signal speed and the recovery counters.
  */
 #include <mutex>
 
@@ -1231,7 +1239,8 @@ int noalloc_scratch(unsigned char** out) {
 }  // namespace
 
 extern "C" int fivo_rhs_noalloc(const fivo_params* p, int nx, int ny, double xmax, double ymax, double tau,
-                                int bc, double* U, double* dU, double* amax, void* stream) {
+                                int bc, double* U, double* dU, double* amax, fivo_counters* counters,
+                                void* stream) {
   if (!p || !U || !dU || !amax) return fail(FIVO_ERR_ARG, "null argument");
   if (nx <= 8 || ny <= 8) return fail(FIVO_ERR_ARG, "make_grid2d: Nx and Ny must exceed 8");
   if (!(xmax > 0) || !(ymax > 0)) return fail(FIVO_ERR_ARG, "xmax and ymax must be positive");
@@ -1293,10 +1302,25 @@ extern "C" int fivo_rhs_noalloc(const fivo_params* p, int nx, int ny, double xma
     k_stage<FIVO_EOS_CONFORMAL_HQ, false><<<grid, 256, smem, st>>>(d, a);
   }
   CKL();
-  unsigned long long bits = 0;
-  CK(cudaMemcpyAsync(&bits, &fl->amax_bits, sizeof(bits), cudaMemcpyDeviceToHost, st));
+  /* the whole flag block: the signal speed and the primitive pass's failure bookkeeping */
+  DevFlags f;
+  CK(cudaMemcpyAsync(&f, fl, sizeof(DevFlags), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  uint64_t bits = f.amax_bits;
   std::memcpy(amax, &bits, 8);
+  if (counters) {
+    std::memset(counters, 0, sizeof(*counters));
+    counters->nprimfail = f.nprimfail;
+    counters->nvacuum = f.nvacuum;
+    if (f.rep != (unsigned long long)REP_NONE) {
+      counters->primfail_index = (int64_t)(f.rep >> 8);
+      counters->primfail_reason = (int32_t)(f.rep & 0xff);
+    } else {
+      counters->primfail_index = -1;
+    }
+    counters->primfail_resnorm = fx::nan_();
+    counters->amax = *amax;
+  }
   return FIVO_OK;
 }
 

@@ -534,7 +534,7 @@ __device__ __forceinline__ double alpha_grad(const double* a, long long i, long 
   return (fi - fm) * invd;
 }
 
-/* transport coefficients at one cell (src/primitives.jl:357-409,
+/* transport coefficients at one cell (src/primitives.jl:56-108,
  * src2d/transport2d.jl:19-155) */
 template <int EOS>
 __device__ void diff_tauN(const DevParams& d, double Tm, double alpha, double* taun) {

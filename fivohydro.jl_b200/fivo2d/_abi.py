@@ -156,13 +156,15 @@ SIGNATURES = {
                            C.c_int, _I64, C.c_int, C.POINTER(FivoRunResult)]),
     "fivo_advance": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
                                C.c_int, _I64, C.POINTER(FivoRunResult)]),
+    "fivo_run_diagnostics": (C.c_int, [C.c_void_p, _D, _D, _D]),
     "fivo_finalize_ic": (C.c_int, [C.c_void_p, C.c_double, C.c_int]),
     "fivo_set_cells": (C.c_int, [C.POINTER(FivoParams), _I64, C.c_double] + [_D] * 10 + [_D, _U8]),
     "fivo_eos_Pne": (C.c_int, [C.POINTER(FivoParams), _I64, _D, _D, _D, _D, _D]),
     "fivo_cons_to_prim": (C.c_int, [C.POINTER(FivoParams), _I64, C.c_double, _D, _D, _D, _U8, _U8]),
     "fivo_sync": (C.c_int, [C.c_void_p]),
     "fivo_rhs_noalloc": (C.c_int, [C.POINTER(FivoParams), C.c_int, C.c_int, C.c_double, C.c_double,
-                                   C.c_double, C.c_int, C.c_void_p, C.c_void_p, _D, C.c_void_p]),
+                                   C.c_double, C.c_int, C.c_void_p, C.c_void_p, _D, C.POINTER(FivoCounters),
+                                   C.c_void_p]),
     "fivo_ctx_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "fivo_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "fivo_profile_read": (C.c_int, [C.c_void_p, C.POINTER(FivoKernelTimes), C.c_int]),

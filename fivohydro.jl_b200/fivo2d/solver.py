@@ -161,6 +161,14 @@ class GPUWork2D:
                                        C.byref(r)), "fivo_advance")
         return r.as_dict()
 
+    def run_diagnostics(self):
+        """run_sim_2d!'s end-of-run interior pass (main2D.jl:532-556) on the resident
+        state: (Q = sum of Dtau, maxu, minPtot)."""
+        q, mu, mp = C.c_double(0.0), C.c_double(0.0), C.c_double(0.0)
+        self._ck(self.lib.fivo_run_diagnostics(self.h, C.byref(q), C.byref(mu), C.byref(mp)),
+                 "fivo_run_diagnostics")
+        return q.value, mu.value, mp.value
+
     def finalize_ic(self, tau0, bc=A.FIVO_BC_OUTFLOW):
         self._ck(self.lib.fivo_finalize_ic(self.h, tau0, bc), "fivo_finalize_ic")
 

@@ -4,8 +4,8 @@
 #
 #     include(joinpath(@__DIR__, "..", "fivohydro.jl_b200", "julia", "FivoGPU.jl"))
 #
-# and pass `work = GPUWork2D(g, model)` to run_sim_2d! (see INTEGRATION.md for the
-# one-line hook). The stage then runs on the GPU with the reference's own driver
+# and pass `work = GPUWork2D(g, model)` to run_sim_2d! (the one-line hook is the
+# integrator selection of run_sim_2d!). The stage then runs on the GPU with the reference's own driver
 # semantics: the same keywords, the same (ok, Δ) step convention, the same
 # NamedTuple result, dumps through on_dump.
 # ==============================================================================
@@ -190,21 +190,34 @@ function run_sim_2d_gpu!(U::AbstractMatrix, g::Grid2D, model, work::GPUWork2D;
                         (Ptr{Cvoid}, Cdouble, Cdouble, Cdouble, Cdouble, Cint, Cint, Int64, Cint, Ref{FivoRunResult}),
                         work.h, τ0, τ0, CFL, CFLτ, integ, _bc(bc), 0, Cint(reset_history), res), "fivo_run")
         download!(U, work); on_dump(τ0, U, work)
+        Q0 = res[].Q0
         τ = τ0; next = τ0 + dump_dt; nsteps = 0; ok = true
+        nprimfail = 0; nvacuum = 0; max_shear_res = 0.0
         while τ < τfinal && nsteps < max_steps
             fivocheck(ccall((:fivo_advance, LIBFIVO2D), Cint,
                             (Ptr{Cvoid}, Cdouble, Cdouble, Cdouble, Cdouble, Cint, Cint, Int64, Ref{FivoRunResult}),
                             work.h, τ, min(τfinal, next), CFL, CFLτ, integ, _bc(bc), max_steps - nsteps, res),
                       "fivo_advance")
             τ = res[].tau; nsteps += res[].nsteps
+            nprimfail += res[].nprimfail; nvacuum += res[].nvacuum
+            max_shear_res = max(max_shear_res, res[].max_shear_res)
             res[].ok == 0 && (ok = false; break)
             if τ >= next - 1e-12
                 download!(U, work); on_dump(τ, U, work); next += dump_dt
             end
         end
         download!(U, work); on_dump(τ, U, work)
-        r = res[]
-        return (ok = ok, τ = τ, nsteps = nsteps, work = work)
+        # the end-of-run diagnostics of run_sim_2d! (main2D.jl:532-556); NaN after a failed step
+        Q1 = Ref{Float64}(NaN); maxu = Ref{Float64}(NaN); minPtot = Ref{Float64}(NaN)
+        if ok
+            fivocheck(ccall((:fivo_run_diagnostics, LIBFIVO2D), Cint,
+                            (Ptr{Cvoid}, Ref{Float64}, Ref{Float64}, Ref{Float64}), work.h, Q1, maxu, minPtot),
+                      "fivo_run_diagnostics")
+        end
+        dQ = ok ? (abs(Q0) > 0 ? abs(Q1[] - Q0)/abs(Q0) : 0.0) : NaN
+        return (ok = ok, τ = τ, nsteps = nsteps, nprimfail = nprimfail, nvacuum = nvacuum,
+                max_shear_res = max_shear_res, work = work, maxu = maxu[], dQ = dQ, Q0 = Q0, Q1 = Q1[],
+                minPtot = minPtot[])
     end
     return (ok = r.ok != 0, τ = r.tau, nsteps = r.nsteps, nprimfail = r.nprimfail, nvacuum = r.nvacuum,
             max_shear_res = r.max_shear_res, work = work, maxu = r.maxu, dQ = r.dQ, Q0 = r.Q0, Q1 = r.Q1,

@@ -50,7 +50,7 @@ extern "C" {
 #define FIVO_EOS_CONFORMAL_HQ  0
 #define FIVO_EOS_LATTICE_HRG   1
 
-/* shear / bulk transport models: src/primitives.jl:347-409 */
+/* shear / bulk transport models: src/primitives.jl:47-108 */
 #define FIVO_SHEAR_ZERO        0   /* ZeroViscosity                             */
 #define FIVO_SHEAR_QGP         1   /* QGPViscosity(eta/s, C_s)                  */
 #define FIVO_BULK_ZERO         0   /* ZeroBulkViscosity                         */
@@ -145,7 +145,7 @@ typedef struct fivo_params {
   int32_t vacuum_ramp_relax;
   int32_t shear_projected_deriv, diff_projected_deriv;
   int32_t shear_constraint_project; /* 1 = :project, 0 = :monitor                */
-  int32_t consistent_fm, consistent_m2; /* charm closures: not built, must be 0  */
+  int32_t consistent_fm, consistent_m2; /* charm closures (first, second moment) */
   int32_t primrec_maxit;    /* Newton iteration cap (80)                         */
   uint32_t terms;           /* FIVO_TERM_* bitmask                               */
 } fivo_params;
@@ -209,7 +209,7 @@ int         fivo_abi_version(void);
 const char* fivo_last_error(void);
 void        fivo_params_default(fivo_params* p);
 
-/* --- context (Grid2D + Work2D mirror), src2d/grid2d.jl:52-71, src2d/work2d.jl:387-411 --- */
+/* --- context (Grid2D + Work2D mirror), src2d/grid2d.jl:52-71, src2d/work2d.jl:15-139 --- */
 int  fivo_ctx_create(const fivo_params* p, int nx, int ny, int nghost,
                      double xmax, double ymax, fivo_ctx** out);
 int  fivo_ctx_destroy(fivo_ctx* ctx);
@@ -270,6 +270,11 @@ int  fivo_run(fivo_ctx* ctx, double tau0, double taufinal, double cfl, double cf
  * A host that calls on_dump between chunks uses this instead of fivo_run. */
 int  fivo_advance(fivo_ctx* ctx, double tau, double taufinal, double cfl, double cfltau,
                   int integrator, int bc, int64_t max_steps, fivo_run_result* out);
+/* The end-of-run diagnostics of run_sim_2d! (main2D.jl:532-556) on the resident
+ * state and primitives: *Q = sum of Dtau over the interior, *maxu = max |u|
+ * over the interior, *minPtot = min(P + Pi) over interior cells with P > 0.
+ * A host that ran fivo_advance chunks forms dQ from this Q and fivo_run's Q0. */
+int  fivo_run_diagnostics(fivo_ctx* ctx, double* Q, double* maxu, double* minPtot);
 
 /* --- initial conditions --- */
 /* finalize_ic! (main2D.jl:164-171) on the resident state. */
@@ -319,12 +324,18 @@ int  fivo_cons_to_prim(const fivo_params* p, int64_t n, double tau,
  * state U and writing the right-hand side dU, both caller-owned device buffers of
  * nv planes x Ntot doubles (plane a at ptr + a*Ntot). The ghost frame of U is
  * refilled in place, as rhs_2d! does. *amax (host) receives the largest HLLE
- * signal speed. stream may be NULL (the default stream). Work memory is a
- * fixed file-scope device array, so Ntot = (nx+6)*(ny+6) must not exceed
- * FIVO_NOALLOC_MAX_CELLS; concurrent calls on overlapping streams race on it. */
+ * signal speed. counters (host, may be NULL) receives the primitive pass's
+ * bookkeeping as fivo_get_counters reports it after fivo_rhs: nprimfail,
+ * nvacuum, one failing cell and its reason, amax (failed cells are floored to
+ * the cold vacuum state and the call still returns FIVO_OK, as rhs_2d! does).
+ * stream may be NULL (the default stream); the call waits for it before
+ * returning. Work memory is a fixed file-scope device array, so Ntot =
+ * (nx+6)*(ny+6) must not exceed FIVO_NOALLOC_MAX_CELLS; concurrent calls on
+ * overlapping streams race on it. */
 #define FIVO_NOALLOC_MAX_CELLS 160000
 int  fivo_rhs_noalloc(const fivo_params* p, int nx, int ny, double xmax, double ymax,
-                      double tau, int bc, double* U, double* dU, double* amax, void* stream);
+                      double tau, int bc, double* U, double* dU, double* amax,
+                      fivo_counters* counters, void* stream);
 
 /* --- batches of events (event-by-event hydro, uneven grids) ---
  * One context per event (same model, own grid), each on its own stream, driven

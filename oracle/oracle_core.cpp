@@ -1276,7 +1276,7 @@ static double diff_tauN(double Tm, double alpha, const fivo_params& e, double Ds
   return (tg / FMGEV) * tauD;
 }
 
-/* viscosity / τ_shear (QGPViscosity), src/primitives.jl:357-366 */
+/* viscosity / τ_shear (QGPViscosity), src/primitives.jl:56-65 */
 static void shear_coeffs(double T, double mu, double n, double en, double P, const fivo_params& p,
                          double* eta, double* taupi, double* dpi) {
   if (!p.enable_shear) { *eta = 0; *taupi = 0; *dpi = 0; return; }
@@ -1288,7 +1288,7 @@ static void shear_coeffs(double T, double mu, double n, double en, double P, con
   *eta = h; *taupi = tp; *dpi = p.deltaShear_factor * tp;
 }
 
-/* bulk_viscosity / τ_bulk, src/primitives.jl:399-409 (+ the Gaussian subtype) */
+/* bulk_viscosity / τ_bulk, src/primitives.jl:98-108 (+ the Gaussian subtype) */
 static void bulk_coeffs(double T, double mu, double n, double en, double P, const fivo_params& p,
                         double* zeta, double* tauPi) {
   if (!p.enable_bulk) { *zeta = 0.0; *tauPi = 0.0; return; }
@@ -1368,6 +1368,15 @@ static void ns_shear_target(double ux, double uy, double ut, double tau, const K
   double seta = (ut * safe_inv(tau)) - third;
   double m2 = -2.0 * eta;
   *xx = m2 * sxx; *xy = m2 * sxy; *yy = m2 * syy; *et = m2 * seta;
+}
+
+/* ns_diffusion_target_2d, src2d/dissipation2d.jl:204-209:
+ * nu_NS^i = -kappa (d_i alpha + u^i D alpha), D alpha = u^tau d_tau alpha + u^k d_k alpha */
+static inline void ns_diffusion_target(double ux, double uy, double ut, double dxa, double dya, double dta,
+                                       double kappa, double* nsx, double* nsy) {
+  double Da = ((ut * dta) + (ux * dxa)) + (uy * dya);
+  *nsx = (-kappa) * (dxa + (ux * Da));
+  *nsy = (-kappa) * (dya + (uy * Da));
 }
 
 /* pi_sigma_contractions_2d, src2d/hq_consistent_m2_2d.jl:201-210 */
@@ -1629,11 +1638,7 @@ int64_t relax_dissipative_2d(double* U, const Grid& g, double tau, double D, con
         double ap = w.alpha_prev[i];
         double dta = o_isfinite(ap) ? (w.alpha[i] - ap) / D : 0.0;
         double nsx = 0.0, nsy = 0.0;
-        if (p.terms & FIVO_TERM_NU_GRADALPHA) {
-          double Da = ((ut * dta) + (ux * dxa)) + (uy * dya);
-          nsx = (-kappa) * (dxa + (ux * Da));
-          nsy = (-kappa) * (dya + (uy * Da));
-        }
+        if (p.terms & FIVO_TERM_NU_GRADALPHA) ns_diffusion_target(ux, uy, ut, dxa, dya, dta, kappa, &nsx, &nsy);
         /* the consistent first moment, src2d/dissipation2d.jl:589-623: subtracted
          * (the source is written on the left-hand side of the row) */
         if (p.consistent_fm) {
@@ -1783,6 +1788,45 @@ void run_sim_2d(double* U, const Grid& g, const Model& m, Work& w, double tau0, 
   res->dQ = std::fabs(Qin) > 0 ? std::fabs(Qout - Qin) / std::fabs(Qin) : 0.0;
   res->Q1 = Qout;
   res->minPtot = minPtot;
+}
+
+/* ---- cell-level functions for the gate tests (same code the solver runs) ---- */
+void cell_shear_coeffs(double T, double mu, double n, double en, double P, const fivo_params& p, double* out3) {
+  shear_coeffs(T, mu, n, en, P, p, &out3[0], &out3[1], &out3[2]);
+}
+void cell_bulk_coeffs(double T, double mu, double n, double en, double P, const fivo_params& p, double* out2) {
+  bulk_coeffs(T, mu, n, en, P, p, &out2[0], &out2[1]);
+}
+void cell_diff_tauN(double T, double alpha, const fivo_params& p, double DsT, double tauD, double* taun,
+                    double* norm) {
+  *taun = diff_tauN(o_max(T, T_MIN), alpha, p, DsT, tauD);
+  *norm = fluidum_norm(T, alpha, p);
+}
+double cell_vacuum_weight(double n, const fivo_params& p) { return vacuum_weight(n, p); }
+double cell_entropy(double T, double mu, double n, double en, double P) { return eos_entropy(T, mu, n, en, P); }
+void cell_ns_shear_target(const double* kin12, double* out4) {
+  /* kin12 = (ux, uy, ut, tau, theta, ax, ay, dxux, dxuy, dyux, dyuy, eta) */
+  Kin k;
+  k.th = kin12[4]; k.ax = kin12[5]; k.ay = kin12[6]; k.at = 0.0;
+  k.dxux = kin12[7]; k.dxuy = kin12[8]; k.dyux = kin12[9]; k.dyuy = kin12[10];
+  ns_shear_target(kin12[0], kin12[1], kin12[2], kin12[3], k, kin12[11], &out4[0], &out4[1], &out4[2], &out4[3]);
+}
+double cell_project_traceless(double ux, double uy, double ut, double pixx, double pixy, double piyy) {
+  return project_traceless(ux, uy, ut, pixx, pixy, piyy);
+}
+void cell_ns_diffusion_target(double ux, double uy, double ut, double dxa, double dya, double dta, double kappa,
+                              double* out2) {
+  ns_diffusion_target(ux, uy, ut, dxa, dya, dta, kappa, &out2[0], &out2[1]);
+}
+void cell_pi_sigma(const double* in10, double* out4) {
+  pi_sigma(in10[0], in10[1], in10[2], in10[3], in10[4], in10[5], in10[6], in10[7], in10[8], in10[9],
+           &out4[0], &out4[1], &out4[2], &out4[3]);
+}
+void cell_shear_tensor(double ux, double uy, double ut, double tau, double pixx, double pixy, double piyy,
+                       double pieta, double* out7) {
+  PiC c = shear_tensor(ux, uy, ut, tau, pixx, pixy, piyy, pieta);
+  out7[0] = c.tt; out7[1] = c.tx; out7[2] = c.ty; out7[3] = c.xx; out7[4] = c.xy; out7[5] = c.yy;
+  out7[6] = c.etaeta;
 }
 
 }  // namespace orc

@@ -148,5 +148,20 @@ void cfm_source(double ux, double uy, double ut, double T, double dxT, double dy
                 double ay, double dxux, double dxuy, double dyux, double dyuy, uint32_t terms, double* sx,
                 double* sy);
 
+/* cell-level functions of the relaxation, for the gate tests */
+void cell_shear_coeffs(double T, double mu, double n, double en, double P, const fivo_params& p, double* out3);
+void cell_bulk_coeffs(double T, double mu, double n, double en, double P, const fivo_params& p, double* out2);
+void cell_diff_tauN(double T, double alpha, const fivo_params& p, double DsT, double tauD, double* taun,
+                    double* norm);
+double cell_vacuum_weight(double n, const fivo_params& p);
+double cell_entropy(double T, double mu, double n, double en, double P);
+void cell_ns_shear_target(const double* kin12, double* out4);
+double cell_project_traceless(double ux, double uy, double ut, double pixx, double pixy, double piyy);
+void cell_ns_diffusion_target(double ux, double uy, double ut, double dxa, double dya, double dta, double kappa,
+                              double* out2);
+void cell_pi_sigma(const double* in10, double* out4);
+void cell_shear_tensor(double ux, double uy, double ut, double tau, double pixx, double pixy, double piyy,
+                       double pieta, double* out7);
+
 }  // namespace orc
 #endif

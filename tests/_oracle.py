@@ -84,6 +84,22 @@ def lib():
             "oracle_fo_record": (None, [C.c_void_p, C.c_double, C.c_double, C.c_double, _D, _D, _D, _D, _U8,
                                         C.POINTER(C.c_int64)]),
             "oracle_pion_yield": (None, [C.c_int, C.c_int, C.c_double, _D, _D, _D, _D, C.POINTER(C.c_int), _D]),
+            "oracle_ref_bjorken_bulk": (None, [P, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int64, _D]),
+            "oracle_ref_bjorken_shear": (None, [P, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int64, _D]),
+            "oracle_ref_bjorken_dnmr": (None, [P, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int64, _D,
+                                               _D]),
+            "oracle_ref_gubser_viscous": (None, [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int64,
+                                                 C.c_int, _D, _D]),
+            "oracle_shear_coeffs": (None, [P, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, _D]),
+            "oracle_bulk_coeffs": (None, [P, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, _D]),
+            "oracle_diff_tauN": (None, [P, C.c_double, C.c_double, C.c_double, C.c_double, _D]),
+            "oracle_vacuum_weight": (C.c_double, [P, C.c_double]),
+            "oracle_entropy": (C.c_double, [C.c_double] * 5),
+            "oracle_ns_shear_target": (None, [C.c_int64, _D, _D]),
+            "oracle_project_traceless": (None, [C.c_int64, _D, _D]),
+            "oracle_ns_diffusion_target": (None, [C.c_int64, _D, _D]),
+            "oracle_pi_sigma": (None, [C.c_int64, _D, _D]),
+            "oracle_shear_tensor": (None, [C.c_int64, _D, _D]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -125,6 +141,14 @@ def eos_Pne(params, T, mu):
     P, n, e = np.empty_like(T), np.empty_like(T), np.empty_like(T)
     lib().oracle_eos_Pne(C.byref(params), T.size, _ptr(T), _ptr(mu), _ptr(P), _ptr(n), _ptr(e))
     return P, n, e
+
+
+def eos_cs2(params, T, mu):
+    T = np.ascontiguousarray(T, dtype=np.float64)
+    mu = np.ascontiguousarray(mu, dtype=np.float64)
+    out = np.empty_like(T)
+    lib().oracle_eos_cs2(C.byref(params), T.size, _ptr(T), _ptr(mu), _ptr(out))
+    return out
 
 
 def cons_to_prim(params, tau, cons, warm=None):
@@ -235,3 +259,89 @@ class OracleSolver:
 
     def finalize_ic(self, tau0, bc=0):
         lib().oracle_finalize_ic(self.h, tau0, bc)
+
+
+# ----------------------------------------------------------------- cell-level functions and referees
+
+
+def _rows(fn, rows, width_out):
+    rows = np.ascontiguousarray(rows, dtype=np.float64)
+    k = rows.shape[0]
+    out = np.empty((k, width_out)) if width_out > 1 else np.empty(k)
+    fn(k, _ptr(rows), _ptr(out))
+    return out
+
+
+def ns_shear_target(rows12):
+    """rows of (ux, uy, ut, tau, theta, ax, ay, dxux, dxuy, dyux, dyuy, eta) -> (xx, xy, yy, eta)"""
+    return _rows(lib().oracle_ns_shear_target, rows12, 4)
+
+
+def project_traceless(rows6):
+    return _rows(lib().oracle_project_traceless, rows6, 1)
+
+
+def ns_diffusion_target(rows7):
+    return _rows(lib().oracle_ns_diffusion_target, rows7, 2)
+
+
+def pi_sigma(rows10):
+    return _rows(lib().oracle_pi_sigma, rows10, 4)
+
+
+def shear_tensor(rows8):
+    return _rows(lib().oracle_shear_tensor, rows8, 7)
+
+
+def shear_coeffs(params, T, mu, n, e, P):
+    out = np.empty(3)
+    lib().oracle_shear_coeffs(C.byref(params), T, mu, n, e, P, _ptr(out))
+    return out
+
+
+def bulk_coeffs(params, T, mu, n, e, P):
+    out = np.empty(2)
+    lib().oracle_bulk_coeffs(C.byref(params), T, mu, n, e, P, _ptr(out))
+    return out
+
+
+def diff_coeffs(params, T, mu, n):
+    k, t, d = C.c_double(), C.c_double(), C.c_double()
+    lib().oracle_diff_coeffs(C.byref(params), T, mu, n, C.byref(k), C.byref(t), C.byref(d))
+    return k.value, t.value, d.value
+
+
+def diff_tauN(params, T, alpha, DsT, tauD):
+    out = np.empty(2)
+    lib().oracle_diff_tauN(C.byref(params), T, alpha, DsT, tauD, _ptr(out))
+    return out[0]
+
+
+def vacuum_weight(params, n):
+    return lib().oracle_vacuum_weight(C.byref(params), n)
+
+
+def ref_bjorken_bulk(params, T0, alpha, tau0, tauf, n=40_000):
+    out = np.empty(3)
+    lib().oracle_ref_bjorken_bulk(C.byref(params), T0, alpha, tau0, tauf, n, _ptr(out))
+    return out
+
+
+def ref_bjorken_shear(params, T0, alpha, tau0, tauf, nsub=20_000):
+    out = np.empty(3)
+    lib().oracle_ref_bjorken_shear(C.byref(params), T0, alpha, tau0, tauf, nsub, _ptr(out))
+    return out
+
+
+def ref_bjorken_dnmr(params, T0, alpha, tau0, tau1, ratios=(0.0, 0.0, 0.0, 0.0, 0.0), n=20_000):
+    r = np.ascontiguousarray(ratios, dtype=np.float64)
+    out = np.empty(3)
+    lib().oracle_ref_bjorken_dnmr(C.byref(params), T0, alpha, tau0, tau1, n, _ptr(r), _ptr(out))
+    return out
+
+
+def ref_gubser_viscous(etas, TH0=0.6, rhomin=-6.0, rhomax=2.0, n=400_000, seed_ns=True):
+    Th = np.empty(n + 1)
+    pb = np.empty(n + 1)
+    lib().oracle_ref_gubser_viscous(etas, TH0, rhomin, rhomax, n, int(seed_ns), _ptr(Th), _ptr(pb))
+    return np.linspace(rhomin, rhomax, n + 1), Th, pb
