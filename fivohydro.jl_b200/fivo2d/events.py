@@ -42,3 +42,31 @@ def shard_events(cells, world: int, rank: int | None = None):
         load[r] += cells[k]
     parts = [sorted(p) for p in parts]
     return parts if rank is None else parts[rank]
+
+
+def event_record(k: int, result: dict, U=None) -> dict:
+    """The per-event bulk results of one run_sim_2d! (main2D.jl:558-560) that a
+    multi-GPU batch gathers: ok, tau, nsteps, failure counts and the end-of-run
+    diagnostics, plus a digest of the final state when U is given."""
+    rec = {"event": int(k)}
+    for key in ("ok", "tau", "nsteps", "nprimfail", "nvacuum", "maxu", "dQ", "Q0", "Q1", "minPtot"):
+        rec[key] = result[key]
+    if U is not None:
+        import hashlib
+        rec["state_sha1"] = hashlib.sha1(np.ascontiguousarray(U, dtype=np.float64).tobytes()).hexdigest()
+    return rec
+
+
+def gather_event_results(local_records: list, nevents: int) -> list:
+    """All-gather the per-event records of every rank over the default process
+    group (the one collective of an event-sharded run, after the data path) and
+    return them ordered by event index, on every rank. Raises when an event is
+    missing or was run twice."""
+    import torch.distributed as dist
+    world = dist.get_world_size()
+    parts = [None] * world
+    dist.all_gather_object(parts, list(local_records))
+    merged = sorted((rec for part in parts for rec in part), key=lambda r: r["event"])
+    if [r["event"] for r in merged] != list(range(nevents)):
+        raise RuntimeError("gather_event_results: an event is missing or was run on two ranks")
+    return merged

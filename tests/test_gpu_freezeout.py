@@ -79,3 +79,31 @@ def test_empty_surface_and_refusals(gpu_lib):
     fo.close()
     w.close()
     w2.close()
+
+
+@pytest.mark.parametrize("N,published", [(200, 1171.3), (300, 1183.9)])
+def test_axisymmetric_control_yield_matches_reference(gpu_lib, N, published):
+    """The axisymmetric control of freezeout2d.jl (the calibrated radial profile on
+    N^2 cells over [-18, 18] fm, tau 0.4 -> 16 in chunks of 0.02, the T = 0.156
+    surface, then Cooper-Frye) against the reference's own post-fix yields: 1171.3
+    at N = 200 and 1183.9 at N = 300 (TWOD_PROGRAM.md:1845-1847, the one-sided rim
+    differences of freezeout2d.jl:156-163). The runs differ from the reference's in
+    the exp/log/Bessel implementations only; the tolerance is 0.5 %."""
+    import pathlib
+
+    import fivo2d
+    from fivo2d.freezeout import axisym_fields, freeze_model
+    from fivo2d.solver import set_cells
+    g = fivo2d.make_grid2d(N, N, xmax=18.0, ymax=18.0)
+    m = freeze_model()
+    prof = pathlib.Path(__file__).resolve().parent / "golden" / "initial_profiles_physical.csv"
+    T, a, ux, uy = axisym_fields(g, prof)
+    U, _ = set_cells(m, 0.4, T, a, ux, uy, lib=gpu_lib)
+    w = GPUWork2D(m, g, lib=gpu_lib)
+    w.set_state(U)
+    w.finalize_ic(0.4)
+    fo, chunks = freeze_surface(w, 0.4, 16.0, dtau=0.02)
+    NB, Nb, negf = fo.pion_yield(cf_params())
+    assert abs(Nb / published - 1) < 5e-3, (N, NB, Nb)
+    fo.close()
+    w.close()
