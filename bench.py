@@ -11,19 +11,27 @@ A step is one iteration of run_sim_2d!'s loop (main2D.jl:436-513): the CFL dt,
 the three SSPRK3 stages (each: BCs, primitive recovery on every cell, MUSCL +
 HLLE + sources, combination, floors/bounds/admissibility), the primitive
 refresh, the IS/DNMR relaxation and the shear projection. A zone-update is one
-interior cell advanced through one accepted step. The default window (10
-warm-up + 200 timed + 10 end-to-end steps, tau0 = 0.6 to about 4 fm/c) ends
-before tau ~ 5 fm/c, where recovery failures in the dilute, charge-free edge
-cells make this event's run stop (the CPU restatement stops at the same step).
+interior cell advanced through one accepted step. The event is laid on the edge
+state of the reference's production profile (T = 0.12786 GeV, alpha = 1.8878),
+so it runs to the configured tau = 10 fm/c.
 
-  value  device-resident: per-step CUDA events on the library's stream, L2
-         flushed (256 MB write) between steps, sum over K steps, max over ranks.
-         The per-kernel times of the roofline come from replaying the same K
-         steps (a device copy of the state taken before them) with the
-         library's kernel timing on, so the timed run has no profiling events.
-  e2e    the same steps through the C ABI with the state in pinned host memory:
-         every step uploads U, advances, downloads U (the drop-in usage from a
-         host driver that keeps U on the host).
+  value     device-resident: K steps after W warm-up steps, per-step CUDA events on
+            the library's stream, L2 flushed (256 MB write) between steps, sum over
+            the K steps, max over ranks. The per-kernel times of the roofline come
+            from replaying the same K steps (a device copy of the state taken before
+            them) with the library's kernel timing on, so the timed run has no
+            profiling events.
+  full_run  the whole configured run, tau0 = 0.6 -> 10 fm/c, timed the same way
+            from a device copy of the initial state: the figure that does not
+            depend on the window.
+  e2e       the same steps through the C ABI with the state in pinned host memory:
+            every step uploads U, advances, downloads U (the drop-in usage from a
+            host driver that keeps U on the host).
+  metric_comparison  the metric's own comparison: 256 events of the event-by-event
+            sizes (N in {96..400}, dx = 30/384 fm, one stream per event) advanced in
+            plain FP64, with the FP32 face pass, and with the learned recovery guess
+            plus FP32 faces, on the same events; each form's L2(T) and L2(pibar) against
+            the plain run after the window.
 
 `--impl reference` times the reference's CPU path (the C++ restatement in
 oracle/, all host threads) on the same workload.
@@ -47,6 +55,7 @@ sys.path.insert(0, str(ROOT / "fivohydro.jl_b200"))
 N_CELLS = 384
 BOX = 15.0
 TAU0 = 0.6
+TAU_END = 10.0          # the configured end of the viscous event's run
 CFL, CFLTAU = 0.2, 0.05
 SEED = 1001
 WORKLOAD = "viscous_event_384x384_ssprk3_lhrg_shear_bulk_diffusion"
@@ -250,6 +259,11 @@ def run_gpu(args):
     w.rhs(TAU0)
     tau = TAU0
     res = A.FivoRunResult()
+    init = None
+    if not args.no_full_run:
+        init = GPUWork2D(m, g, lib=lib)          # the state at tau0, for the full-run figure
+        A.check(lib, lib.fivo_ctx_set_stream(init.h, C.c_void_p(stream.cuda_stream)), "set_stream")
+        init.clone_state_from(w)
 
     def step_on(h, tau_, n):
         A.check(lib, lib.fivo_advance(h, tau_, 1e9, CFL, CFLTAU, A.FIVO_SSPRK3, A.FIVO_BC_OUTFLOW, n,
@@ -418,6 +432,35 @@ def run_gpu(args):
     e2e_value = e2e_steps * nint * world / (float(t.item()) / 1e3)
     state_bytes = g.Ntot * m.nv * 8
 
+    # ---------------- the whole configured run, tau0 -> TAU_END, from the initial state
+    full_run = None
+    if init is not None:
+        ev = []
+        tau_f = TAU0
+        torch.cuda.synchronize()
+        while tau_f < TAU_END - 1e-12:
+            l2_flush()
+            e0_, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0_.record(stream)
+            A.check(lib, lib.fivo_advance(init.h, tau_f, TAU_END, CFL, CFLTAU, A.FIVO_SSPRK3, A.FIVO_BC_OUTFLOW, 1,
+                                          C.byref(res)), "fivo_advance")
+            e1_.record(stream)
+            if not res.ok:
+                raise RuntimeError(f"the full run failed a step at tau={tau_f}")
+            tau_f = res.tau
+            ev.append((e0_, e1_))
+        torch.cuda.synchronize()
+        fms = sum(a_.elapsed_time(b_) for a_, b_ in ev)
+        t = torch.tensor([fms], dtype=torch.float64, device="cuda")
+        if dist:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        fms = float(t.item())
+        full_run = {"value": len(ev) * nint * world / (fms / 1e3), "unit": UNIT, "steps": len(ev),
+                    "tau": [TAU0, tau_f], "ms_per_step": fms / len(ev),
+                    "note": "the configured run tau0 -> 10 fm/c from a device copy of the initial state, "
+                            "per-step CUDA events, L2 flushed between steps"}
+        init.close()
+
     # ---------------- roofline of the dominant kernel class
     classes = A.KERNEL_CLASSES
     timed = [c for c in classes if c not in ("other", "unused")]
@@ -460,6 +503,7 @@ def run_gpu(args):
                    "parallelism": f"replicas{world}"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes, "steps": e2e_steps},
+        "full_run": full_run,
         "gpu_launches": int(kt.total_launches),
         "roofline": roof,
         "clocks": clocks,
@@ -476,9 +520,104 @@ def run_gpu(args):
         line["config"]["workload"] += "_learned_guess"
         line["config"]["recovery"] = ("learned MLP guess (BF16 tcgen05, FP32 accumulate), fallback to the "
                                       "plain warm start; trained on seeds " + str(list(GUESS_SEEDS)))
+    if world == 1 and not args.no_forms and guess is None and not args.fp32_faces and args.batch_events > 0:
+        line["metric_comparison"] = batch_forms(lib, m, args.batch_events, args.batch_steps, value)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.cpu_steps)
     return line
+
+
+# ----------------------------------------------------------------------------- the metric's comparison
+
+def _batch_fields(b, m):
+    """T, pibar = pi^eta_eta/(e+P) and the shear rows of every event's interior, and
+    the recovered-cell mask, concatenated in event order"""
+    import numpy as np
+    out = {"T": [], "pibar": [], "pi": [], "ok": []}
+    iP, iE = m.layout.idx("pixx"), m.layout.idx("pieta")
+    for e, g in zip(b.events, b.grids):
+        p = e.primitives()
+        U = e.get_state()
+        sx, sy = g.interior()
+        out["ok"].append((p["ok"] == 1).reshape(g.Nxtot, g.Nytot)[sx, sy].ravel())
+        out["T"].append(np.exp(p["yT"]).reshape(g.Nxtot, g.Nytot)[sx, sy].ravel())
+        wpl = (p["e"] + p["P"]).reshape(g.Nxtot, g.Nytot)[sx, sy].ravel()
+        Ur = U.reshape(g.Nxtot, g.Nytot, m.nv)[sx, sy]
+        out["pibar"].append(Ur[..., iE].ravel() / wpl)
+        out["pi"].append(Ur[..., iP:iP + 3].reshape(-1, 3))
+    return {k: np.concatenate(v) for k, v in out.items()}
+
+
+def batch_forms(lib, m, nevents, steps, single_value, warmup=3):
+    """The metric's comparison on one GPU: the same nevents seeded events (the
+    event-by-event sizes, device IC, seed 1000 + k) advanced in plain FP64, with
+    the FP32 face pass, and with the learned guess plus FP32 faces; zone-updates/s
+    of each (host wall clock around the synchronous batch call, one stream per
+    event) and each form's L2(T), L2(pibar) and L2(pi) against the plain run."""
+    import numpy as np
+    import torch
+
+    from fivo2d import _abi as A
+    from fivo2d.events import event_grids
+    from fivo2d.guess import newton_stats
+    from fivo2d.solver import GPUBatch2D
+
+    grids = event_grids(nevents)
+    cells = sum(g.Nx * g.Ny for g in grids)
+    g384, _ = model_and_grid()
+    guess, ginfo = train_guess(lib, m, g384)
+    out = {"events": nevents, "steps": steps, "warmup": warmup, "grids": sorted({g.Nx for g in grids}),
+           "zone_updates_per_step": cells, "single_event_plain_fp64": single_value,
+           "timing": "host wall clock around the synchronous batch call (one stream per event)"}
+    ref = None
+    for form in ("plain_fp64", "fp32_faces", "learned_fp32"):
+        b = GPUBatch2D(m, grids, lib=lib)
+        for k, e in enumerate(b.events):
+            e.glauber_ic(TAU0, 1000 + k)
+            e.rhs(TAU0)
+            if form != "plain_fp64":
+                e.set_precision(A.FIVO_PRECISION_FP32_FACES)
+            if form == "learned_fp32":
+                guess.attach(e)
+        taus = [TAU0] * len(grids)
+
+        def adv(n):
+            nonlocal taus
+            r = b.advance(taus, 1e9, CFL, CFLTAU, A.FIVO_SSPRK3, max_steps=n)
+            if not all(x["ok"] and x["nsteps"] == n for x in r):
+                raise RuntimeError(f"a batch event failed a step ({form})")
+            taus = [x["tau"] for x in r]
+
+        adv(warmup)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        adv(steps)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        row = {"value": steps * cells / dt, "unit": UNIT, "ms_per_step": 1e3 * dt / steps}
+        f = _batch_fields(b, m)
+        if ref is None:
+            ref = f
+        else:
+            ok = ref["ok"] & f["ok"]
+            row["L2_T"] = l2_rel(f["T"][ok], ref["T"][ok])
+            row["Linf_T"] = float(np.max(np.abs(f["T"][ok] - ref["T"][ok]) / ref["T"][ok]))
+            row["L2_pibar"] = l2_rel(f["pibar"][ok], ref["pibar"][ok])
+            row["L2_pi"] = l2_rel(f["pi"][ok], ref["pi"][ok])
+            row["speedup_vs_plain_batch"] = row["value"] / out["plain_fp64"]["value"]
+            row["meets_L2T_1e-6"] = bool(row["L2_T"] <= 1e-6)
+        if form == "learned_fp32":
+            st = {}
+            for e in b.events:
+                for key, v in newton_stats(e).items():
+                    st[key] = st.get(key, 0) + v
+            row["guess"] = dict(ginfo, accept_rate=st["ok_learn"] / max(1, st["n_learn"]),
+                                updates_per_cell=(st["it_learn"] + st["it_fb"]) / max(1, st["n_learn"]))
+        out[form] = row
+        b.close()
+    guess.close()
+    out["plain_batch_vs_single_event"] = out["plain_fp64"]["value"] / single_value
+    return out
 
 
 # ----------------------------------------------------------------------------- event batches
@@ -737,7 +876,10 @@ def main():
     ap.add_argument("--events", type=int, default=32, help="batch workload: number of events")
     ap.add_argument("--workers", type=int, default=0, help="batch workload: host threads (0: library default)")
     ap.add_argument("--no-forms", action="store_true",
-                    help="skip the FP32-faces replay of the window that the default line carries")
+                    help="skip the FP32-faces replay and the batched forms comparison of the default line")
+    ap.add_argument("--no-full-run", action="store_true", help="skip the full tau0 -> 10 fm/c figure")
+    ap.add_argument("--batch-events", type=int, default=256, help="events of the metric's batched comparison")
+    ap.add_argument("--batch-steps", type=int, default=30, help="timed steps of the batched comparison")
     ap.add_argument("--fp32-faces", action="store_true",
                     help="the mixed-precision form: the face pass in FP32 (fivo_ctx_set_precision)")
     ap.add_argument("--guess", action="store_true",

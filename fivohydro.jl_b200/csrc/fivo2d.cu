@@ -1077,7 +1077,8 @@ int fivo_set_cells(const fivo_params* p, int64_t ncell, double tau, const double
 
 int fivo_glauber_ic(fivo_ctx* c, double tau0, const double* parts, const double* weights, int64_t npart,
                     const double* binary, int64_t nbin, double width, double Tpeak, double ncharm,
-                    double alpha_min, int bc, double* T_out, double* alpha_out) {
+                    double alpha_min, double T_edge, double alpha_edge, int bc, double* T_out,
+                    double* alpha_out) {
   if (!c || !parts || !weights || (nbin > 0 && !binary)) return fail(FIVO_ERR_ARG, "null argument");
   const DevParams& d = c->dp;
   if (d.p.eos_kind != FIVO_EOS_LATTICE_HRG)
@@ -1108,6 +1109,17 @@ int fivo_glauber_ic(fivo_ctx* c, double tau0, const double* parts, const double*
   const double Tp = jmax(Tpeak, FV_T_MIN);
   light_eos<3>(Tp, d, &Pl, &dP, nullptr);
   const double e_peak = (-Pl) + (Tp * dP);
+  /* the edge state: its light-sector energy density and charm density n(T_edge, alpha_edge) */
+  double e_edge = 0.0, n_edge = 0.0;
+  if (T_edge > 0) {
+    double Pe, dPe;
+    light_eos<3>(T_edge, d, &Pe, &dPe, nullptr);
+    e_edge = (-Pe) + (T_edge * dPe);
+    const double x = lhrg_x(T_edge, d);
+    double P0, n0, e0;
+    lhrg_assemble(T_edge, 0.0, d, x, Pe, e_edge, lhrg_K2(x), &P0, &n0, &e0);
+    n_edge = n0 * fx_exp(alpha_edge);
+  }
   const long long nw = (long long)nblk(N, 256) * 8;
   DevBuf partb;
   CK(cudaMalloc(&partb.p, (size_t)nw * 8));
@@ -1121,7 +1133,8 @@ int fivo_glauber_ic(fivo_ctx* c, double tau0, const double* parts, const double*
     CKL();
     k_sum_parts<<<1, 256, 0, c->st>>>((const double*)partb.p, nw, interior);
     CKL();
-    k_glauber_fields<<<nblk(N, 128), 128, 0, c->st>>>(d, s, nb, mx, interior, e_peak, tau0, ncharm, alpha_min, T, al);
+    k_glauber_fields<<<nblk(N, 128), 128, 0, c->st>>>(d, s, nb, mx, interior, e_peak, e_edge, n_edge, tau0, ncharm,
+                                                      alpha_min, T, al);
     CKL();
   }
   {

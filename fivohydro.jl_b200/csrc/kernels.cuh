@@ -1069,15 +1069,16 @@ __global__ void k_glauber_reduce(DevParams d, const double* s, const double* nb,
   }
 }
 
-/* T from e = s * (e_peak / max s) by 90-step bisection of the light-sector e(T) in
- * log T, and alpha = log(n_target / n(T, alpha = 0)) floored at alpha_min */
+/* T from e = s * ((e_peak - e_edge) / max s) + e_edge by 90-step bisection of the
+ * light-sector e(T) in log T, and alpha = log(n_target / n(T, alpha = 0)) with
+ * n_target = the binary part + n_edge, floored at alpha_min where not finite */
 __global__ void k_glauber_fields(DevParams d, const double* s, const double* nb, const unsigned long long* mx,
-                                 const double* interior, double e_peak, double tau0, double ncharm,
-                                 double alpha_min, double* Tout, double* aout) {
+                                 const double* interior, double e_peak, double e_edge, double n_edge,
+                                 double tau0, double ncharm, double alpha_min, double* Tout, double* aout) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.Ntot) return;
   const double smax = __longlong_as_double((long long)*mx);
-  const double e = s[i] * (e_peak / smax);
+  const double e = (s[i] * ((e_peak - e_edge) / smax)) + e_edge;
   double lo = d.log_T_min, hi = d.log_T_solve_max;
   for (int it = 0; it < 90; ++it) {
     const double mid = 0.5 * (lo + hi);
@@ -1089,7 +1090,7 @@ __global__ void k_glauber_fields(DevParams d, const double* s, const double* nb,
   }
   const double T = jmax(fx_exp(0.5 * (lo + hi)), FV_T_MIN);
   const double I = ((*interior) * d.dx) * d.dy;   /* the interior sum of nb times dx dy */
-  const double ntgt = I > 0.0 ? nb[i] * (ncharm / (tau0 * I)) : 0.0;
+  const double ntgt = (I > 0.0 ? nb[i] * (ncharm / (tau0 * I)) : 0.0) + n_edge;
   const double x = lhrg_x(T, d);
   double Pl, dP;
   light_eos<3>(T, d, &Pl, &dP, nullptr);

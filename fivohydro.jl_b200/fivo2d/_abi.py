@@ -129,7 +129,7 @@ SIGNATURES = {
     "fivo_ctx_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int64), _D]),
     "fivo_ctx_clone_state": (C.c_int, [C.c_void_p, C.c_void_p]),
     "fivo_glauber_ic": (C.c_int, [C.c_void_p, C.c_double, _D, _D, C.c_int64, _D, C.c_int64, C.c_double, C.c_double,
-                                  C.c_double, C.c_double, C.c_int, _D, _D]),
+                                  C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _D, _D]),
     "fivo_batch_create": (C.c_int, [C.POINTER(FivoParams), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _D, _D,
                                     C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "fivo_batch_destroy": (C.c_int, [C.c_void_p]),

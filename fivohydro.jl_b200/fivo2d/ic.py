@@ -188,24 +188,39 @@ def invert_e_for_T(e, eos: LatticeHRGEOS, iters: int = 90):
     return np.exp(0.5 * (lo + hi))
 
 
+# The edge state of the reference's production radial profile (the last row of
+# data/initial_profiles_physical.csv: T0 = 0.1278551418360245 GeV, alpha0 =
+# 1.8877972332059278). The reference's floors and vacuum cut were tuned against a
+# profile that carries this edge (examples2d/04_fluctuating_event.jl:16-31), so the
+# event is laid on it: the medium never reaches vacuum and every cell carries charm.
+EDGE_T = 0.1278551418360245
+EDGE_ALPHA = 1.8877972332059278
+
+
 def glauber_fields(g: Grid2D, tau0: float, seed: int, *, eos: LatticeHRGEOS | None = None,
                    Tpeak: float = 0.450, ncharm: float = 10.0, bmax: float = 8.0,
-                   alpha_min: float = -20.0):
-    """MC-Glauber-like IC on every cell: energy density from participants scaled to
-    peak T = Tpeak via the EOS inverse; charm density proportional to the
-    binary-collision density with tau0 * sum(n u^tau) dx dy = ncharm; alpha =
-    log(n / n(T, alpha=0)), floored at alpha_min where there is no charm; u = 0."""
+                   alpha_min: float = -20.0, T_edge: float = EDGE_T, alpha_edge: float = EDGE_ALPHA):
+    """MC-Glauber-like IC on every cell: energy density from the participants, on top
+    of the edge state's energy density e(T_edge) and scaled so the peak is T = Tpeak,
+    T from the EOS inverse; charm density = n(T_edge, alpha_edge) + a part
+    proportional to the binary-collision density with tau0 * sum(n u^tau) dx dy =
+    ncharm; alpha = log(n / n(T, alpha=0)); u = 0. T_edge <= 0 builds the event on
+    vacuum instead (no edge state; alpha floored at alpha_min where there is no charm)."""
     eos = eos or LatticeHRGEOS()
     ev = glauber_event(seed, bmax)
     X, Y = np.meshgrid(g.xC, g.yC, indexing="ij")
     s = _deposit(X, Y, ev["participants"], ev["weights"], SRC_WIDTH)
     e_peak = float(_lhrg_e_of_T(np.array([Tpeak]), eos)[0])
-    e = s * (e_peak / s.max())
+    edge = T_edge > 0
+    e_edge = float(_lhrg_e_of_T(np.array([T_edge]), eos)[0]) if edge else 0.0
+    e = s * ((e_peak - e_edge) / s.max()) + e_edge
     T = np.maximum(invert_e_for_T(e, eos), T_MIN)
     nb = _deposit(X, Y, ev["binary"], np.ones(len(ev["binary"])), SRC_WIDTH)
     ng = g.nghost
     interior = nb[ng:ng + g.Nx, ng:ng + g.Ny].sum() * g.dx * g.dy
     n_tgt = nb * (ncharm / (tau0 * interior)) if interior > 0 else nb * 0.0
+    if edge:
+        n_tgt = n_tgt + float(_lhrg_n_alpha0(np.array([T_edge]), eos)[0]) * math.exp(alpha_edge)
     with np.errstate(divide="ignore", invalid="ignore"):
         n0 = _lhrg_n_alpha0(T, eos)
         a = np.log(n_tgt / n0)

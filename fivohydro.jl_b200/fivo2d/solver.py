@@ -181,11 +181,14 @@ class GPUWork2D:
         self._ck(self.lib.fivo_sync(self.h), "fivo_sync")
 
     def glauber_ic(self, tau0, seed, *, Tpeak=0.450, ncharm=10.0, bmax=8.0, alpha_min=-20.0,
-                   bc=A.FIVO_BC_OUTFLOW, fields=False):
+                   T_edge=None, alpha_edge=None, bc=A.FIVO_BC_OUTFLOW, fields=False):
         """The seeded MC-Glauber initial condition built on the device into this
-        context's state (fivo_glauber_ic); the nucleon sampling is ic.glauber_event's.
+        context's state (fivo_glauber_ic); the nucleon sampling is ic.glauber_event's
+        and the edge state is ic.glauber_fields' (T_edge <= 0: on vacuum).
         Returns (T, alpha) planes when fields=True."""
-        from .ic import SRC_WIDTH, glauber_event
+        from .ic import EDGE_ALPHA, EDGE_T, SRC_WIDTH, glauber_event
+        T_edge = EDGE_T if T_edge is None else T_edge
+        alpha_edge = EDGE_ALPHA if alpha_edge is None else alpha_edge
         ev = glauber_event(seed, bmax)
         pts = np.ascontiguousarray(ev["participants"], dtype=np.float64)
         w = np.ascontiguousarray(ev["weights"], dtype=np.float64)
@@ -193,7 +196,8 @@ class GPUWork2D:
         T = np.empty(self.N) if fields else None
         a = np.empty(self.N) if fields else None
         self._ck(self.lib.fivo_glauber_ic(self.h, tau0, _ptr(pts), _ptr(w), len(w), _ptr(bi) if len(bi) else None,
-                                          len(bi), SRC_WIDTH, Tpeak, ncharm, alpha_min, bc, _ptr(T), _ptr(a)),
+                                          len(bi), SRC_WIDTH, Tpeak, ncharm, alpha_min, T_edge, alpha_edge, bc,
+                                          _ptr(T), _ptr(a)),
                  "fivo_glauber_ic")
         return (T, a) if fields else None
 

@@ -296,16 +296,22 @@ int  fivo_set_cells(const fivo_params* p, int64_t ncell, double tau,
  * device into the context's state (the reference's IC builder is not public; the
  * same construction runs on the host in fivo2d.ic.glauber_fields): Gaussian
  * deposits of width `width` of npart participants (x, y pairs, with weights) and
- * nbin binary collisions (x, y pairs) at every cell centre; energy density scaled
- * so its maximum is the light-sector e(Tpeak); T by 90-step bisection of e(T);
- * charm density proportional to the binary density with tau0 * sum(n) dx dy =
- * ncharm over the interior; alpha = log(n / n(T, alpha = 0)) floored at alpha_min;
- * u = 0 and no dissipative parts; then set_cell! and finalize_ic! (main2D.jl:142-171)
- * with boundary bc. T_out, alpha_out (Ntot each, may be NULL) receive the fields.
+ * nbin binary collisions (x, y pairs) at every cell centre; energy density
+ * e = e_edge + (e(Tpeak) - e_edge) s / max s over the light-sector e(T), with
+ * e_edge = e(T_edge); T by 90-step bisection of e(T); charm density
+ * n = n(T_edge, alpha_edge) + a part proportional to the binary density with
+ * tau0 * sum dx dy = ncharm over the interior; alpha = log(n / n(T, alpha = 0)),
+ * floored at alpha_min where it is not finite; u = 0 and no dissipative parts;
+ * then set_cell! and finalize_ic! (main2D.jl:142-171) with boundary bc.
+ * (T_edge, alpha_edge) is the edge state the event is laid on (the reference's
+ * production profile carries T = 0.12786 GeV, alpha = 1.8878 at its edge,
+ * data/initial_profiles_physical.csv); T_edge <= 0 builds it on vacuum instead.
+ * T_out, alpha_out (Ntot each, may be NULL) receive the fields.
  * LatticeHRGEOS only. No counterpart in the reference. */
 int  fivo_glauber_ic(fivo_ctx* ctx, double tau0, const double* parts, const double* weights,
                      int64_t npart, const double* binary, int64_t nbin, double width, double Tpeak,
-                     double ncharm, double alpha_min, int bc, double* T_out, double* alpha_out);
+                     double ncharm, double alpha_min, double T_edge, double alpha_edge, int bc,
+                     double* T_out, double* alpha_out);
 int  fivo_eos_Pne(const fivo_params* p, int64_t n, const double* T, const double* mu,
                   double* P, double* nq, double* e);
 

@@ -22,13 +22,14 @@ def _model():
                                  bulk_T0=0.18, bulk_width=0.024, kappa_coeff=0.5)
 
 
-@pytest.mark.parametrize("n,seed", [(48, 1001), (64, 1005)])
-def test_device_ic_matches_host_construction(gpu_lib, n, seed):
+@pytest.mark.parametrize("n,seed,T_edge", [(48, 1001, ic.EDGE_T), (64, 1005, ic.EDGE_T), (48, 1001, 0.0)],
+                         ids=["edge-48", "edge-64", "vacuum-48"])
+def test_device_ic_matches_host_construction(gpu_lib, n, seed, T_edge):
     g = fivo2d.make_grid2d(n, n, xmax=15.0, ymax=15.0)
     m = _model()
     w = GPUWork2D(m, g, lib=gpu_lib)
-    Td, ad = w.glauber_ic(0.6, seed, fields=True)
-    Th, ah, ux, uy, _ = ic.glauber_fields(g, 0.6, seed)
+    Td, ad = w.glauber_ic(0.6, seed, T_edge=T_edge, fields=True)
+    Th, ah, ux, uy, _ = ic.glauber_fields(g, 0.6, seed, T_edge=T_edge)
     assert np.allclose(Td, Th, rtol=1e-12, atol=0.0)
     assert np.max(np.abs(ad - ah)) < 1e-9
     # the state: set_cell! + finalize_ic! of the host fields

@@ -76,20 +76,29 @@ def test_rhs_noalloc_matches_context_rhs_twice(gpu_lib):
 
 
 def test_rhs_noalloc_reports_recovery_failures(gpu_lib):
-    """With the Newton capped at one iteration (primrec_maxit = 1) the recoveries of
-    the matter cells fail and are floored to the cold vacuum state; the call still
-    returns FIVO_OK, and its counters say so exactly as the context path's do."""
+    """On an evolved state (flow everywhere), with the Newton capped at one iteration
+    (primrec_maxit = 1), the recoveries of the matter cells fail and are floored to
+    the cold vacuum state; the call still returns FIVO_OK, and its counters say so
+    exactly as the context path's do."""
     import torch
     lib = gpu_lib
     g = fivo2d.make_grid2d(40, 36, xmax=15.0, ymax=12.0)
-    m = fivo2d.build_model_2d(eos=fivo2d.LatticeHRGEOS(), enable_shear=True, enable_bulk=True,
-                              enable_diff=True, eta_over_s=0.16, zeta_over_s=0.05, bulk_model="gaussian",
-                              bulk_T0=0.18, bulk_width=0.024, kappa_coeff=0.5, primrec_maxit=1)
+    kw = dict(eos=fivo2d.LatticeHRGEOS(), enable_shear=True, enable_bulk=True, enable_diff=True, eta_over_s=0.16,
+              zeta_over_s=0.05, bulk_model="gaussian", bulk_T0=0.18, bulk_width=0.024, kappa_coeff=0.5)
+    m0 = fivo2d.build_model_2d(**kw)
     T, a, ux, uy, _ = ic.glauber_fields(g, 0.6, 1002)
-    U, _ = set_cells(m, 0.6, T, a, ux, uy)
+    U, _ = set_cells(m0, 0.6, T, a, ux, uy)
+    w0 = GPUWork2D(m0, g, lib=lib)
+    w0.set_state(U)
+    w0.finalize_ic(0.6)
+    r = w0.run(0.6, 1.2, 0.2, 0.05, A.FIVO_SSPRK3)
+    assert r["ok"]
+    U = w0.get_state()
+    w0.close()
+    m = fivo2d.build_model_2d(**kw, primrec_maxit=1)
     w = GPUWork2D(m, g, lib=lib)
     w.set_state(U)
-    dU_ref = w.rhs(0.6)
+    dU_ref = w.rhs(1.2)
     c_ref = w.counters()
     w.close()
     assert c_ref.nprimfail > 0
@@ -98,7 +107,7 @@ def test_rhs_noalloc_reports_recovery_failures(gpu_lib):
     amax = C.c_double(-1.0)
     cnt = A.FivoCounters()
     for _ in range(2):                       # the second call must not see the first one's counts
-        st = lib.fivo_rhs_noalloc(C.byref(m.params), g.Nx, g.Ny, g.xmax, g.ymax, 0.6, A.FIVO_BC_OUTFLOW,
+        st = lib.fivo_rhs_noalloc(C.byref(m.params), g.Nx, g.Ny, g.xmax, g.ymax, 1.2, A.FIVO_BC_OUTFLOW,
                                   C.c_void_p(planes.data_ptr()), C.c_void_p(dU.data_ptr()), C.byref(amax),
                                   C.byref(cnt), None)
         assert st == A.FIVO_OK, lib.fivo_last_error()
