@@ -146,7 +146,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
@@ -316,13 +316,15 @@ def run_gpu(args):
         dist.barrier()
     torch.cuda.synchronize()
     tau_start = tau
-    with ClockSampler(local) as clk:
-        for k in range(args.steps):
-            l2_flush()
-            starts[k].record(stream)
-            advance(1)
-            stops[k].record(stream)
-        torch.cuda.synchronize()
+    # the clock samples span the timed steps and their profiled replay (the same work):
+    # a window of a few tens of milliseconds alone is shorter than one sampling period
+    clk = ClockSampler(local).__enter__()
+    for k in range(args.steps):
+        l2_flush()
+        starts[k].record(stream)
+        advance(1)
+        stops[k].record(stream)
+    torch.cuda.synchronize()
     if dist:
         dist.barrier()
     ms = sum(s.elapsed_time(e) for s, e in zip(starts, stops))
@@ -336,6 +338,7 @@ def run_gpu(args):
         l2_flush()
         tau_r = step_on(twin.h, tau_r, 1)
     lib.fivo_profile_read(twin.h, C.byref(kt), 1)
+    clk.__exit__(None, None, None)
     if plain is None and tau_r != tau:
         raise RuntimeError("the profiled replay left the timed trajectory")
     twin.close()
