@@ -255,8 +255,11 @@ def run_gpu(args):
     w.finalize_ic(TAU0)
     nint = g.Nx * g.Ny
 
-    # prime primitives and signal speeds (run_sim_2d!, main2D.jl:418)
+    # prime primitives and signal speeds (run_sim_2d!, main2D.jl:418); the first stage
+    # also picks the face-pass kernel by timing the candidates (fivo_ctx_set_face_pass)
     w.rhs(TAU0)
+    face_pass = [("global" if k == A.FIVO_FACES_GLOBAL else "tile %dx%d" % A.FACE_TILE_SHAPES[k])
+                 for k in w.face_pass()]
     tau = TAU0
     res = A.FivoRunResult()
     init = None
@@ -503,7 +506,7 @@ def run_gpu(args):
         "config": {"workload": WORKLOAD, "grid": [N_CELLS, N_CELLS], "box_fm": BOX, "tau0": TAU0,
                    "tau_window": [tau_start, tau], "integrator": "ssprk3", "cfl": CFL, "cfltau": CFLTAU,
                    "events_per_gpu": 1, "seed": SEED, "l2": "flushed (256 MB write) between timed steps",
-                   "parallelism": f"replicas{world}"},
+                   "parallelism": f"replicas{world}", "face_pass_xy": face_pass},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes, "steps": e2e_steps},
         "full_run": full_run,

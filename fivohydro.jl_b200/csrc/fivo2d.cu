@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -25,6 +26,7 @@
 #include "kernels.cuh"
 #include "freezeout.cuh"
 #include "face32.cuh"
+#include "facetile.cuh"
 
 using namespace fv;
 
@@ -168,6 +170,13 @@ struct fivo_ctx {
   int precision = FIVO_PRECISION_FP64;
   float* fh32 = nullptr;                    /* x faces then y faces, nv FP32 planes each */
   double* x0save = nullptr;                 /* the warm starts before an optimistic step */
+  /* the face pass (x, y): -2 not chosen yet, -1 k_faces, k >= 0 k_faces_tile of FT_SHAPES[k];
+   * the tensor maps of the chosen shape: the primitive planes, and the dissipative
+   * planes of each of the four state buffers */
+  int ft_cfg[2] = {-2, -2};
+  CUtensorMap ft_prim[2][5];
+  CUtensorMap ft_slab[2][4 * FV_MAXV];   /* every plane of the state slab: the relaxation swaps
+                                           the dissipative planes between state buffers */
 };
 
 namespace {
@@ -285,7 +294,175 @@ int launch_primitive(fivo_ctx* c, const DevState& U, double tau) {
   return launch_primitive_t<FIVO_EOS_CONFORMAL_HQ, false>(c, U, tau);
 }
 
-/* rhs_2d! + combination + sanitiser + admissibility: k_faces (x, y), k_update,
+/* ------------------------------------------------------------ the face pass
+ * Two implementations with the same arithmetic (face_flux_pair): k_faces, whose
+ * lanes read their stencils from global memory, and k_faces_tile, which stages
+ * a halo tile of every plane it reads in shared memory by TMA first. The tile
+ * path needs 16-byte row pitches (Nytot even). Which one runs, and with which
+ * tile shape, is chosen per grid and layout by timing every candidate on the
+ * context's first stage (tune_faces); the choice is shared by contexts of the
+ * same shape. */
+struct FtShape { int tx, ty; };
+constexpr FtShape FT_SHAPES[] = {{4, 32}, {2, 64}, {8, 16}, {8, 32}};
+constexpr int FT_NSHAPES = (int)(sizeof(FT_SHAPES) / sizeof(FT_SHAPES[0]));
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+/* the tensor map of one Nxtot x Nytot plane (y contiguous) with the box of a tile
+ * of shape sh in direction dir (0 = x faces) */
+bool encode_plane(CUtensorMap* m, const double* plane, const DevParams& d, FtShape sh, int dir) {
+  EncodeTiledFn fn = encode_tiled_fn();
+  if (!fn) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)d.Nytot, (cuuint64_t)d.Nxtot};
+  const cuuint64_t strides[1] = {(cuuint64_t)d.Nytot * 8};
+  const cuuint32_t box[2] = {(cuuint32_t)(dir == 0 ? sh.ty : sh.ty + 4), (cuuint32_t)(dir == 0 ? sh.tx + 3 : sh.tx)};
+  const cuuint32_t es[2] = {1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(plane), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+/* the dissipative planes of a state, in face_flux_pair's slot order */
+void dis_planes(const DevParams& d, const DevState& U, const double* out[7]) {
+  out[0] = d.hasNu ? U.f[d.iNux] : nullptr;
+  out[1] = d.hasNu ? U.f[d.iNuy] : nullptr;
+  out[2] = d.hasPi ? U.f[d.iPi] : nullptr;
+  out[3] = d.hasShear ? U.f[d.iPixx] : nullptr;
+  out[4] = d.hasShear ? U.f[d.iPixy] : nullptr;
+  out[5] = d.hasShear ? U.f[d.iPiyy] : nullptr;
+  out[6] = d.hasShear ? U.f[d.iPieta] : nullptr;
+}
+
+/* encode the maps of shape index k for direction dir into the context: the primitive
+ * planes and every plane of the state slab */
+bool ft_encode(fivo_ctx* c, int dir, int k) {
+  const DevParams& d = c->dp;
+  const FtShape sh = FT_SHAPES[k];
+  const double* prim[5] = {c->w.yT, c->w.phi, c->w.ux, c->w.uy, c->w.mu};
+  for (int q = 0; q < 5; ++q)
+    if (!encode_plane(&c->ft_prim[dir][q], prim[q], d, sh, dir)) return false;
+  for (int p = 0; p < 4 * d.nv; ++p)
+    if (!encode_plane(&c->ft_slab[dir][p], c->slab + (size_t)p * d.Ntot, d, sh, dir)) return false;
+  return true;
+}
+
+/* the launch's maps: the primitives, then the dissipative rows of U that exist (found by
+ * their place in the slab); false when a plane is not in the slab */
+bool ft_maps(const fivo_ctx* c, int dir, const DevState& U, FaceTileMaps* m) {
+  const DevParams& d = c->dp;
+  for (int q = 0; q < 5; ++q) m->map[q] = c->ft_prim[dir][q];
+  const double* dp[7];
+  dis_planes(d, U, dp);
+  int np = 5;
+  for (int j = 0; j < 7; ++j) {
+    if (!dp[j]) { m->dis_plane[j] = -1; continue; }
+    const long long off = dp[j] - c->slab;
+    if (off < 0 || off % d.Ntot != 0 || off / d.Ntot >= 4LL * d.nv) return false;
+    m->map[np] = c->ft_slab[dir][off / d.Ntot];
+    m->dis_plane[j] = np;
+    ++np;
+  }
+  m->nplanes = np;
+  return true;
+}
+
+template <int EOS, bool XDIR, int TX, int TY>
+int launch_tile(fivo_ctx* c, const StageArgs& a, const FaceTileMaps& m, double* Fh) {
+  const DevParams& d = c->dp;
+  const int smem = ft_smem_bytes(XDIR, TX, TY, m.nplanes);
+  CK(cudaFuncSetAttribute(k_faces_tile<EOS, XDIR, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  const dim3 grid(XDIR ? (d.Nytot + TY - 1) / TY : (d.Nytot - 1 + TY - 1) / TY,
+                  XDIR ? (d.Nxtot - 1 + TX - 1) / TX : (d.Nxtot + TX - 1) / TX);
+  k_faces_tile<EOS, XDIR, TX, TY><<<grid, 2 * TX * TY, smem, c->st>>>(d, m, a.tau, a.ffo, Fh, c->fl);
+  CKL();
+  return FIVO_OK;
+}
+
+/* one direction of the face pass with configuration cfg (-1: k_faces) */
+template <int EOS, bool XDIR>
+int launch_faces_dir(fivo_ctx* c, const StageArgs& a, int cfg, double* Fh) {
+  const DevParams& d = c->dp;
+  FaceTileMaps m;
+  if (cfg < 0 || !ft_maps(c, XDIR ? 0 : 1, a.Ub, &m)) {
+    const long long nf = XDIR ? (long long)(d.Nxtot - 1) * d.Nytot : (long long)d.Nxtot * (d.Nytot - 1);
+    k_faces<EOS, XDIR><<<nblk(2 * nf, 128), 128, 0, c->st>>>(d, a.Ub, a.w, a.tau, a.ffo, Fh, c->fl);
+    CKL();
+    return FIVO_OK;
+  }
+  switch (cfg) {
+    case 0: return launch_tile<EOS, XDIR, 4, 32>(c, a, m, Fh);
+    case 1: return launch_tile<EOS, XDIR, 2, 64>(c, a, m, Fh);
+    case 2: return launch_tile<EOS, XDIR, 8, 16>(c, a, m, Fh);
+    default: return launch_tile<EOS, XDIR, 8, 32>(c, a, m, Fh);
+  }
+}
+
+std::mutex g_ft_mu;
+std::vector<std::pair<std::vector<long long>, std::pair<int, int>>> g_ft_choice;
+
+/* the choice of the face pass for this context: cached per (grid, EOS, layout),
+ * else timed here: each candidate once to warm up, then the best of three */
+template <int EOS>
+int tune_faces(fivo_ctx* c, const StageArgs& a, double* fhx, double* fhy) {
+  const DevParams& d = c->dp;
+  const std::vector<long long> key = {d.Nxtot, d.Nytot, EOS, d.nv, d.hasNu, d.hasPi, d.hasShear, c->device};
+  {
+    std::lock_guard<std::mutex> lk(g_ft_mu);
+    for (auto& e : g_ft_choice)
+      if (e.first == key) { c->ft_cfg[0] = e.second.first; c->ft_cfg[1] = e.second.second; break; }
+  }
+  const bool tile_ok = (d.Nytot % 2 == 0) && encode_tiled_fn() != nullptr;
+  if (c->ft_cfg[0] == -2) {
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    for (int dir = 0; dir < 2; ++dir) {
+      double* Fh = dir == 0 ? fhx : fhy;
+      int best = -1;
+      float best_ms = 1e30f;
+      for (int cfg = -1; cfg < (tile_ok ? FT_NSHAPES : 0); ++cfg) {
+        if (cfg >= 0 && !ft_encode(c, dir, cfg)) continue;
+        float tmin = 1e30f;
+        for (int rep = 0; rep < 4; ++rep) {
+          CK(cudaEventRecord(e0, c->st));
+          int rc = dir == 0 ? launch_faces_dir<EOS, true>(c, a, cfg, Fh) : launch_faces_dir<EOS, false>(c, a, cfg, Fh);
+          if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
+          CK(cudaEventRecord(e1, c->st));
+          CK(cudaEventSynchronize(e1));
+          float ms = 0.f;
+          CK(cudaEventElapsedTime(&ms, e0, e1));
+          if (rep > 0) tmin = std::min(tmin, ms);
+        }
+        if (tmin < best_ms) { best_ms = tmin; best = cfg; }
+      }
+      c->ft_cfg[dir] = best;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::lock_guard<std::mutex> lk(g_ft_mu);
+    g_ft_choice.push_back({key, {c->ft_cfg[0], c->ft_cfg[1]}});
+  }
+  for (int dir = 0; dir < 2; ++dir)
+    if (c->ft_cfg[dir] >= 0 && !(tile_ok && ft_encode(c, dir, c->ft_cfg[dir]))) c->ft_cfg[dir] = -1;
+  return FIVO_OK;
+}
+
+/* rhs_2d! + combination + sanitiser + admissibility: the face pass (x, y), k_update,
  * and k_adm_slow for the cells whose admissibility needs an inversion. */
 template <int EOS, bool NCH>
 int launch_stage_t(fivo_ctx* c, const StageArgs& a) {
@@ -304,10 +481,10 @@ int launch_stage_t(fivo_ctx* c, const StageArgs& a) {
       f32::k_faces32<EOS, false><<<nblk(2 * nfy, 128), 128, 0, c->st>>>(d, a.Ub, a.w, a.tau, a.ffo, fhy32, c->fl);
       CKL();
     } else {
-      k_faces<EOS, true><<<nblk(2 * nfx, 128), 128, 0, c->st>>>(d, a.Ub, a.w, a.tau, a.ffo, fhx, c->fl);
-      CKL();
-      k_faces<EOS, false><<<nblk(2 * nfy, 128), 128, 0, c->st>>>(d, a.Ub, a.w, a.tau, a.ffo, fhy, c->fl);
-      CKL();
+      int rc;
+      if (c->ft_cfg[0] == -2 && (rc = tune_faces<EOS>(c, a, fhx, fhy))) return rc;
+      if ((rc = launch_faces_dir<EOS, true>(c, a, c->ft_cfg[0], fhx))) return rc;
+      if ((rc = launch_faces_dir<EOS, false>(c, a, c->ft_cfg[1], fhy))) return rc;
     }
   }
   unsigned int* aq = c->queues + d.Ntot;
@@ -338,6 +515,7 @@ int sync_flags(fivo_ctx* c, bool read_amax) {
   CK(ctx_sync(c));
   const DevFlags& f = *c->flh;
   if (f.status == 3) return fail(FIVO_ERR_DEVICE, "learned recovery guess: a tensor-core wait gave up");
+  if (f.status == 4) return fail(FIVO_ERR_DEVICE, "face pass: a tile copy to shared memory did not complete");
   c->cnt.nprimfail = f.nprimfail;
   c->cnt.nvacuum = f.nvacuum;
   if (f.rep != (unsigned long long)REP_NONE) {
@@ -1221,7 +1399,6 @@ int fivo_cons_to_prim(const fivo_params* p, int64_t n, double tau, const double*
  * GPU race on it. A call is synchronous: it waits for its stream to read back the
  * signal speed and the recovery counters.
  */
-#include <mutex>
 
 namespace {
 constexpr size_t NOALLOC_PLANE_BYTES = (size_t)FIVO_NOALLOC_MAX_CELLS * 8;
@@ -1928,6 +2105,29 @@ int fivo_cooper_frye(fivo_fo* f, const fivo_cf_params* p, double* out) {
 }
 
 /* ------------------------------------------------ mixed precision */
+
+int fivo_ctx_set_face_pass(fivo_ctx* c, int x_cfg, int y_cfg) {
+  if (!c) return fail(FIVO_ERR_ARG, "null context");
+  const int cfg[2] = {x_cfg, y_cfg};
+  for (int dir = 0; dir < 2; ++dir) {
+    if (cfg[dir] < -2 || cfg[dir] >= FT_NSHAPES)
+      return fail(FIVO_ERR_ARG, "fivo_ctx_set_face_pass: configuration out of range");
+    if (cfg[dir] >= 0 && !(c->dp.Nytot % 2 == 0 && ft_encode(c, dir, cfg[dir])))
+      return fail(FIVO_ERR_ARG, "fivo_ctx_set_face_pass: the tiled face pass needs an even Ny + 6");
+  }
+  CK(ctx_sync(c));
+  c->ft_cfg[0] = x_cfg;
+  c->ft_cfg[1] = y_cfg;
+  if (x_cfg == -2 || y_cfg == -2) c->ft_cfg[0] = c->ft_cfg[1] = -2;
+  return FIVO_OK;
+}
+
+int fivo_ctx_face_pass(fivo_ctx* c, int* x_cfg, int* y_cfg) {
+  if (!c || !x_cfg || !y_cfg) return fail(FIVO_ERR_ARG, "null argument");
+  *x_cfg = c->ft_cfg[0];
+  *y_cfg = c->ft_cfg[1];
+  return FIVO_OK;
+}
 
 int fivo_ctx_set_precision(fivo_ctx* c, int mode) {
   if (!c) return fail(FIVO_ERR_ARG, "null context");

@@ -1458,33 +1458,48 @@ __global__ void __launch_bounds__(128) k_prim_slow(DevParams d, DevState U, DevP
  * face and the registers it needs. All lanes of the warp must call it.
  * Returns max(|sL|, |sR|); stores each row of the HLLE flux into its plane of
  * Fh (the lane of side a % 2 stores plane a) unless Fh is null. */
-template <int EOS, bool XDIR>
-__device__ __forceinline__ double face_flux_pair(const DevParams& d, const DevState& U, const DevPrims& w,
-                                                 long long i, long long st, int k, int kmax, double tau,
-                                                 const uint8_t* ffo, int side, double* Fh) {
+/* Where a face reads its stencil: the cells i - st, i, i + st, i + 2 st around the
+ * face between i and i + st, named by their position p = -1, 0, 1, 2. The
+ * primitives q = 0..3 are (yT, phi, u^x, u^y). FaceSrcGlobal reads the planes in
+ * global memory; k_faces_tile's source reads a tile staged in shared memory. */
+struct FaceSrcGlobal {
+  const DevParams& d;
+  const DevState& U;
+  const DevPrims& w;
+  long long i, st;
+  __device__ __forceinline__ double prim(int q, int p) const {
+    const double* f = q == 0 ? w.yT : (q == 1 ? w.phi : (q == 2 ? w.ux : w.uy));
+    return f[i + p * st];
+  }
+  __device__ __forceinline__ double mu(int p) const { return w.mu[i + p * st]; }
+  __device__ __forceinline__ void dis(int p, double out[7]) const { load_dis(d, U, i + p * st, out); }
+};
+
+template <int EOS, bool XDIR, class Src>
+__device__ __forceinline__ double face_flux_pair(const DevParams& d, const Src& src, long long i, long long st,
+                                                 int k, int kmax, double tau, const uint8_t* ffo, int side,
+                                                 double* Fh) {
   const long long ip = i + st;
-  const long long c0 = side ? ip : i;
+  const int p0 = side;             /* this lane's own cell: i (left) or i + st (right) */
   /* the two lanes of this pair; every branch below is taken by both or neither */
   const unsigned pm = 3u << (threadIdx.x & 30);
   const int ng = d.ng;
   double dis[7];
-  load_dis(d, U, c0, dis);
+  src.dis(p0, dis);
   const bool forced = ffo != nullptr && (ffo[i] || ffo[ip]);
   Prim p;
   double uc[4];
   bool good = false, floored = false;
   if (!forced) {
     double v[4];
-    const double* fld[4] = {w.yT, w.phi, w.ux, w.uy};
     const bool first = (k + 1 <= ng) || (k + 1 >= kmax - ng);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const double* f = fld[q];
       /* left: (vm, vi, vp) around vi; right: (vi, vp, vpp) around vp */
-      const double c = f[c0];
+      const double c = src.prim(q, p0);
       if (first) { v[q] = c; continue; }
-      const double a = side ? f[i] : f[i - st];
-      const double b = side ? f[ip + st] : f[ip];
+      const double a = src.prim(q, side ? 0 : -1);
+      const double b = src.prim(q, side ? 2 : 1);
       const double sl = mc_limiter(c - a, b - c);
       const double h = 0.5 * sl;
       const double val = side ? c - h : c + h;
@@ -1498,8 +1513,8 @@ __device__ __forceinline__ double face_flux_pair(const DevParams& d, const DevSt
     good = mine && theirs;
   }
   if (!good) {
-    const double Tc = fx_exp(w.yT[c0]), muc = w.mu[c0];
-    const bool ok = prim_to_cons<EOS>(uc, p, Tc, muc, w.ux[c0], w.uy[c0], dis, tau, d);
+    const double Tc = fx_exp(src.prim(0, p0)), muc = src.mu(p0);
+    const bool ok = prim_to_cons<EOS>(uc, p, Tc, muc, src.prim(2, p0), src.prim(3, p0), dis, tau, d);
     const int theirs = __shfl_xor_sync(pm, (int)ok, 1);
     const bool both = ok && theirs;
     if (!both && !ok) {
@@ -1565,8 +1580,9 @@ __global__ void __launch_bounds__(128, FV_FACE_MINB) k_faces(DevParams d, DevSta
     int ix = (int)(f / (d.Nytot - 1)), iy = (int)(f % (d.Nytot - 1));
     i = (long long)ix * d.Nytot + iy; k = iy; kmax = d.Nytot;
   }
-  double amax = face_flux_pair<EOS, XDIR>(d, Ub, w, i, XDIR ? d.Nytot : 1, k, kmax, tau, ffo, side,
-                                          valid ? Fh : nullptr);
+  const long long st = XDIR ? d.Nytot : 1;
+  const FaceSrcGlobal src{d, Ub, w, i, st};
+  double amax = face_flux_pair<EOS, XDIR>(d, src, i, st, k, kmax, tau, ffo, side, valid ? Fh : nullptr);
   for (int o = 16; o > 0; o >>= 1) amax = jmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
   __shared__ double red[4];
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = amax;

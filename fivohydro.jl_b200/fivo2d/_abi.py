@@ -90,6 +90,8 @@ KERNEL_CLASSES = ("prim_fast", "prim_slow", "faces", "update", "adm_slow", "rela
 
 FIVO_GUESS_NPARAM, FIVO_GUESS_NNORM, FIVO_GUESS_NSAMP = 6288, 22, 11
 FIVO_PRECISION_FP64, FIVO_PRECISION_FP32_FACES = 0, 1
+FIVO_FACES_AUTO, FIVO_FACES_GLOBAL = -2, -1
+FACE_TILE_SHAPES = ((4, 32), (2, 64), (8, 16), (8, 32))
 
 
 class FivoNewtonStats(C.Structure):
@@ -184,6 +186,8 @@ SIGNATURES = {
     "fivo_ctx_set_guess": (C.c_int, [C.c_void_p, C.c_void_p]),
     "fivo_newton_stats_read": (C.c_int, [C.c_void_p, C.POINTER(FivoNewtonStats), C.c_int]),
     "fivo_ctx_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
+    "fivo_ctx_set_face_pass": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "fivo_ctx_face_pass": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "fivo_cf_params_default": (None, [C.POINTER(FivoCFParams)]),
     "fivo_fo_create": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_void_p)]),
     "fivo_fo_destroy": (C.c_int, [C.c_void_p]),

@@ -177,6 +177,19 @@ class GPUWork2D:
         (the face pass of rhs_2d! in FP32, everything else FP64)"""
         self._ck(self.lib.fivo_ctx_set_precision(self.h, int(mode)), "fivo_ctx_set_precision")
 
+    def set_face_pass(self, x_cfg, y_cfg=None):
+        """Pin the kernel of the FP64 face pass (fivo_ctx_set_face_pass):
+        A.FIVO_FACES_AUTO (timed choice, the default), A.FIVO_FACES_GLOBAL, or the
+        index of a TMA tile shape in A.FACE_TILE_SHAPES; same bits either way."""
+        y_cfg = x_cfg if y_cfg is None else y_cfg
+        self._ck(self.lib.fivo_ctx_set_face_pass(self.h, int(x_cfg), int(y_cfg)), "fivo_ctx_set_face_pass")
+
+    def face_pass(self):
+        """(x, y) face-pass choice in force (-2 until the first stage has tuned it)"""
+        x, y = C.c_int(0), C.c_int(0)
+        self._ck(self.lib.fivo_ctx_face_pass(self.h, C.byref(x), C.byref(y)), "fivo_ctx_face_pass")
+        return x.value, y.value
+
     def sync(self):
         self._ck(self.lib.fivo_sync(self.h), "fivo_sync")
 

@@ -434,6 +434,19 @@ int  fivo_newton_stats_read(fivo_ctx* ctx, fivo_newton_stats* out, int reset);
 #define FIVO_PRECISION_FP32_FACES  1
 int  fivo_ctx_set_precision(fivo_ctx* ctx, int mode);
 
+/* --- which kernel runs the FP64 face pass of rhs_2d! (_faces_2d!, src2d/rhs2d.jl:282-371) ---
+ * Both give the same bits. FIVO_FACES_GLOBAL reads each face's stencil from global
+ * memory; FIVO_FACES_TILE_* stages a halo tile of every plane the faces read in
+ * shared memory by TMA first (needs Ny + 6 even), in tiles of TX x TY faces:
+ * 0 = 4 x 32, 1 = 2 x 64, 2 = 8 x 16, 3 = 8 x 32. FIVO_FACES_AUTO (the default) times
+ * every candidate on the context's first stage and keeps the fastest, one choice
+ * per grid and layout shared by the contexts of the process. x_cfg and y_cfg are
+ * the x- and y-face passes; fivo_ctx_face_pass reports the current choice. */
+#define FIVO_FACES_AUTO    (-2)
+#define FIVO_FACES_GLOBAL  (-1)
+int  fivo_ctx_set_face_pass(fivo_ctx* ctx, int x_cfg, int y_cfg);
+int  fivo_ctx_face_pass(fivo_ctx* ctx, int* x_cfg, int* y_cfg);
+
 /* --- the freeze-out surface and its Cooper-Frye pion yield (freezeout2d.jl) ---
  * The surface tau = tau_fo(x, y) over ctx's interior cells: each record takes the
  * primitives of ctx's last primitive pass (fivo_update_primitives first, as
