@@ -53,10 +53,12 @@ int fail(int code, const std::string& msg) {
 
 inline unsigned nblk(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 
+/* history planes of a context: x0_yT, x0_phi, x0_ux, x0_uy, ux_prev, uy_prev,
+ * alpha_prev, T_prev, nux_prev, nuy_prev */
+constexpr size_t NHIST = 10;
+
 /* reject_unwired_knobs_2d + check_terms (src2d/primitives2d.jl:246-272, src/terms.jl) */
 int validate(const fivo_params* p) {
-  if (p->consistent_m2)
-    return fail(FIVO_ERR_CONFIG, "consistent_m2 (the charm second moment) is not built");
   if (p->consistent_fm && p->tauN_coeff != 1.0)   /* reject_unwired_knobs_2d, src2d/primitives2d.jl:263-269 */
     return fail(FIVO_ERR_CONFIG, "tauN_coeff cannot be combined with consistent_fm = true (the closure ties "
                                  "tau_n = D_s h / T with h in closed form)");
@@ -79,8 +81,8 @@ int validate(const fivo_params* p) {
     return fail(FIVO_ERR_CONFIG, "Terms: shear_vorticity switched but enable_shear is off");
   if ((diff & fm) && !p->consistent_fm)
     return fail(FIVO_ERR_CONFIG, "Terms: a consistent-first-moment term is switched but consistent_fm is off");
-  if (diff & m2)
-    return fail(FIVO_ERR_CONFIG, "Terms: a second-moment term is switched but its sector is not built");
+  if ((diff & m2) && !p->consistent_m2)
+    return fail(FIVO_ERR_CONFIG, "Terms: a second-moment term is switched but consistent_m2 is off");
   if (p->primrec_maxit < 1 || !(p->primrec_tol > 0))
     return fail(FIVO_ERR_CONFIG, "primrec_maxit must be >= 1 and primrec_tol > 0");
   return FIVO_OK;
@@ -99,6 +101,11 @@ DevParams make_devparams(const fivo_params* p, int nx, int ny, int ng, double xm
   d.hasShear = p->enable_shear != 0;
   d.iPixx = d.hasShear ? k++ : -1; d.iPixy = d.hasShear ? k++ : -1;
   d.iPiyy = d.hasShear ? k++ : -1; d.iPieta = d.hasShear ? k++ : -1;
+  d.nvf = k;
+  /* the charm second moment's rows follow the medium's (make_layout2d with_m2) */
+  d.hasM2 = p->consistent_m2 != 0;
+  d.iPQxx = d.hasM2 ? k++ : -1; d.iPQxy = d.hasM2 ? k++ : -1; d.iPQyy = d.hasM2 ? k++ : -1;
+  d.iPQeta = d.hasM2 ? k++ : -1; d.iPiQ = d.hasM2 ? k++ : -1;
   d.nv = k;
   d.ncharge = (p->eos_kind == FIVO_EOS_CONFORMAL_HQ) ? (p->g_hq > 0.0) : 1;
   d.Nx = nx; d.Ny = ny; d.ng = ng; d.Nxtot = nx + 2 * ng; d.Nytot = ny + 2 * ng;
@@ -175,7 +182,7 @@ struct fivo_ctx {
    * planes of each of the four state buffers */
   int ft_cfg[2] = {-2, -2};
   CUtensorMap ft_prim[2][5];
-  CUtensorMap ft_slab[2][4 * FV_MAXV];   /* every plane of the state slab: the relaxation swaps
+  CUtensorMap ft_slab[2][4 * FV_MAXP];   /* every plane of the state slab: the relaxation swaps
                                            the dissipative planes between state buffers */
 };
 
@@ -720,10 +727,17 @@ int relax_project(fivo_ctx* c, double tau, double D, int do_relax, int do_projec
   unsigned g = nblk(d.Ntot, 128);
   {
   KTimer t_(c, FIVO_KCLASS_RELAX, 1, d.Ntot);
-  if (d.p.eos_kind == FIVO_EOS_LATTICE_HRG)
-    k_relax<FIVO_EOS_LATTICE_HRG><<<g, 128, 0, c->st>>>(d, Uq, Uo, c->w, c->h, tau, D, do_relax, do_project, c->fl);
-  else
-    k_relax<FIVO_EOS_CONFORMAL_HQ><<<g, 128, 0, c->st>>>(d, Uq, Uo, c->w, c->h, tau, D, do_relax, do_project, c->fl);
+  if (d.p.eos_kind == FIVO_EOS_LATTICE_HRG) {
+    if (d.hasM2)
+      k_relax<FIVO_EOS_LATTICE_HRG, true><<<g, 128, 0, c->st>>>(d, Uq, Uo, c->w, c->h, tau, D, do_relax, do_project, c->fl);
+    else
+      k_relax<FIVO_EOS_LATTICE_HRG, false><<<g, 128, 0, c->st>>>(d, Uq, Uo, c->w, c->h, tau, D, do_relax, do_project, c->fl);
+  } else {
+    if (d.hasM2)
+      k_relax<FIVO_EOS_CONFORMAL_HQ, true><<<g, 128, 0, c->st>>>(d, Uq, Uo, c->w, c->h, tau, D, do_relax, do_project, c->fl);
+    else
+      k_relax<FIVO_EOS_CONFORMAL_HQ, false><<<g, 128, 0, c->st>>>(d, Uq, Uo, c->w, c->h, tau, D, do_relax, do_project, c->fl);
+  }
   CKL();
   }
   /* the dissipative planes of U are now those of the scratch state */
@@ -756,8 +770,8 @@ int fill_nan(fivo_ctx* c, double* p, long long n) {
 int reset_history(fivo_ctx* c) {
   int rc;
   c->nsteps_run = 0;
-  /* x0_* and the four *_prev planes are contiguous in hbuf */
-  if ((rc = fill_nan(c, c->hbuf, 8 * c->dp.Ntot))) return rc;
+  /* x0_* and the six *_prev planes are contiguous in hbuf */
+  if ((rc = fill_nan(c, c->hbuf, NHIST * c->dp.Ntot))) return rc;
   c->hist_valid = false;
   return FIVO_OK;
 }
@@ -809,6 +823,7 @@ void fivo_params_default(fivo_params* p) {
   p->r_domain = fx::inf_(); p->T_vac_cut = 0.05; p->E_vac_cut = -1.0;
   p->primrec_tol = 1e-12; p->primrec_maxit = 80;
   p->relax_advect_nu = 1; p->relax_advect_pi = 1; p->relax_advect_Pi = 1; p->vacuum_ramp_relax = 1;
+  p->relax_advect_m2 = 1;
   p->shear_projected_deriv = 1; p->diff_projected_deriv = 1; p->shear_constraint_project = 1;
   p->terms = FIVO_TERMS_DEFAULT;
 }
@@ -835,7 +850,7 @@ int fivo_ctx_create(const fivo_params* p, int nx, int ny, int nghost, double xma
   size_t N = (size_t)d.Ntot;
   if (cudaMalloc(&c->slab, 4 * (size_t)d.nv * N * 8) != cudaSuccess ||
       cudaMalloc(&c->pbuf, 9 * N * 8 + N) != cudaSuccess ||
-      cudaMalloc(&c->hbuf, 8 * N * 8) != cudaSuccess ||
+      cudaMalloc(&c->hbuf, NHIST * N * 8) != cudaSuccess ||
       cudaMalloc(&c->masks, 3 * N) != cudaSuccess ||
       cudaMalloc(&c->fl, sizeof(DevFlags)) != cudaSuccess ||
       cudaMalloc(&c->stage, (size_t)d.nv * N * 8) != cudaSuccess ||
@@ -848,14 +863,15 @@ int fivo_ctx_create(const fivo_params* p, int nx, int ny, int nghost, double xma
   if (cudaMallocHost(&c->flh, sizeof(DevFlags)) != cudaSuccess)
     return cleanup(fail(FIVO_ERR_NOMEM, "pinned allocation failed"));
   for (int s = 0; s < 4; ++s)
-    for (int a = 0; a < FV_MAXV; ++a) c->S[s].f[a] = a < d.nv ? c->slab + ((size_t)s * d.nv + a) * N : nullptr;
+    for (int a = 0; a < FV_MAXP; ++a) c->S[s].f[a] = a < d.nv ? c->slab + ((size_t)s * d.nv + a) * N : nullptr;
   double* q = c->pbuf;
   c->w.yT = q; q += N; c->w.phi = q; q += N; c->w.mu = q; q += N; c->w.alpha = q; q += N;
   c->w.ux = q; q += N; c->w.uy = q; q += N; c->w.P = q; q += N; c->w.n = q; q += N; c->w.e = q; q += N;
   c->w.ok = (uint8_t*)q;
   q = c->hbuf;
   c->h.x0_yT = q; q += N; c->h.x0_phi = q; q += N; c->h.x0_ux = q; q += N; c->h.x0_uy = q; q += N;
-  c->h.ux_prev = q; q += N; c->h.uy_prev = q; q += N; c->h.alpha_prev = q; q += N; c->h.T_prev = q;
+  c->h.ux_prev = q; q += N; c->h.uy_prev = q; q += N; c->h.alpha_prev = q; q += N; c->h.T_prev = q; q += N;
+  c->h.nux_prev = q; q += N; c->h.nuy_prev = q;
   /* Work2D(): zeros, NaN history (src2d/work2d.jl:115-139) */
   if (cudaMemsetAsync(c->slab, 0, 4 * (size_t)d.nv * N * 8, c->st) != cudaSuccess ||
       cudaMemsetAsync(c->pbuf, 0, 9 * N * 8 + N, c->st) != cudaSuccess ||
@@ -904,11 +920,11 @@ int fivo_ctx_clone_state(fivo_ctx* dst, const fivo_ctx* src) {
   CK(cudaStreamSynchronize(src->st));
   CK(cudaMemcpyAsync(dst->slab, src->slab, 4 * (size_t)a.nv * N * 8, cudaMemcpyDeviceToDevice, dst->st));
   CK(cudaMemcpyAsync(dst->pbuf, src->pbuf, 9 * N * 8 + N, cudaMemcpyDeviceToDevice, dst->st));
-  CK(cudaMemcpyAsync(dst->hbuf, src->hbuf, 8 * N * 8, cudaMemcpyDeviceToDevice, dst->st));
+  CK(cudaMemcpyAsync(dst->hbuf, src->hbuf, NHIST * N * 8, cudaMemcpyDeviceToDevice, dst->st));
   CK(cudaMemcpyAsync(dst->masks, src->masks, 3 * N, cudaMemcpyDeviceToDevice, dst->st));
   /* the role indices and the plane permutation of the relaxation double buffer */
   for (int s = 0; s < 4; ++s)
-    for (int k = 0; k < FV_MAXV; ++k)
+    for (int k = 0; k < FV_MAXP; ++k)
       dst->S[s].f[k] = src->S[s].f[k] ? dst->slab + (src->S[s].f[k] - src->slab) : nullptr;
   dst->iU = src->iU; dst->iU1 = src->iU1; dst->iU2 = src->iU2; dst->iT = src->iT;
   dst->hist_valid = src->hist_valid;
@@ -967,6 +983,24 @@ int fivo_download_history(fivo_ctx* c, int64_t ntot, double* x0_yT, double* x0_p
                           c->h.alpha_prev, c->h.T_prev};
   for (int k = 0; k < 8; ++k)
     if (dst[k]) CK(cudaMemcpyAsync(dst[k], src[k], (size_t)ntot * 8, cudaMemcpyDeviceToHost, c->st));
+  CK(ctx_sync(c));
+  return FIVO_OK;
+}
+
+int fivo_upload_nu_history(fivo_ctx* c, int64_t ntot, const double* nux_prev, const double* nuy_prev) {
+  if (!c) return fail(FIVO_ERR_ARG, "null context");
+  if (ntot != c->dp.Ntot) return fail(FIVO_ERR_ARG, "history size mismatch");
+  if (nux_prev) CK(cudaMemcpyAsync(c->h.nux_prev, nux_prev, (size_t)ntot * 8, cudaMemcpyHostToDevice, c->st));
+  if (nuy_prev) CK(cudaMemcpyAsync(c->h.nuy_prev, nuy_prev, (size_t)ntot * 8, cudaMemcpyHostToDevice, c->st));
+  CK(ctx_sync(c));
+  return FIVO_OK;
+}
+
+int fivo_download_nu_history(fivo_ctx* c, int64_t ntot, double* nux_prev, double* nuy_prev) {
+  if (!c) return fail(FIVO_ERR_ARG, "null context");
+  if (ntot != c->dp.Ntot) return fail(FIVO_ERR_ARG, "history size mismatch");
+  if (nux_prev) CK(cudaMemcpyAsync(nux_prev, c->h.nux_prev, (size_t)ntot * 8, cudaMemcpyDeviceToHost, c->st));
+  if (nuy_prev) CK(cudaMemcpyAsync(nuy_prev, c->h.nuy_prev, (size_t)ntot * 8, cudaMemcpyDeviceToHost, c->st));
   CK(ctx_sync(c));
   return FIVO_OK;
 }
@@ -1447,14 +1481,14 @@ extern "C" int fivo_rhs_noalloc(const fivo_params* p, int nx, int ny, double xma
   DevParams d = make_devparams(p, nx, ny, 3, xmax, ymax);
   const size_t N = (size_t)d.Ntot;
   DevState S;
-  for (int a = 0; a < FV_MAXV; ++a) S.f[a] = a < d.nv ? U + (size_t)a * N : nullptr;
+  for (int a = 0; a < FV_MAXP; ++a) S.f[a] = a < d.nv ? U + (size_t)a * N : nullptr;
   double* q = (double*)base;
   DevPrims w;
   w.yT = q; q += N; w.phi = q; q += N; w.mu = q; q += N; w.alpha = q; q += N;
   w.ux = q; q += N; w.uy = q; q += N; w.P = q; q += N; w.n = q; q += N; w.e = q; q += N;
   DevHist h;
   h.x0_yT = q; q += N; h.x0_phi = q; q += N; h.x0_ux = q; q += N; h.x0_uy = q; q += N;
-  h.ux_prev = h.uy_prev = h.alpha_prev = h.T_prev = nullptr;
+  h.ux_prev = h.uy_prev = h.alpha_prev = h.T_prev = h.nux_prev = h.nuy_prev = nullptr;
   unsigned char* okb = base + 13 * NOALLOC_PLANE_BYTES;
   w.ok = (uint8_t*)okb;
   DevFlags* fl = (DevFlags*)(okb + (((size_t)FIVO_NOALLOC_MAX_CELLS + 255) / 256) * 256);
@@ -1479,7 +1513,7 @@ extern "C" int fivo_rhs_noalloc(const fivo_params* p, int nx, int ny, double xma
   StageArgs a;
   a.Ub = S; a.Uold = S; a.Uout = S; a.w = w; a.ffo = nullptr; a.bad = nullptr; a.dU = dU;
   a.tau = tau; a.tau_state = tau; a.dt = 0.0; a.wold = 0.0; a.wnew = 0.0; a.mode = COMB_RHS_ONLY; a.fl = fl;
-  size_t smem = (size_t)(ST_NFX + ST_NFY) * d.nv * sizeof(double);
+  size_t smem = (size_t)(ST_NFX + ST_NFY) * d.nvf * sizeof(double);
   dim3 grid((d.Nxtot + ST_CX - 1) / ST_CX, (d.Nytot + ST_CY - 1) / ST_CY);
   if (d.p.eos_kind == FIVO_EOS_LATTICE_HRG) {
     CK(cudaFuncSetAttribute(k_stage<FIVO_EOS_LATTICE_HRG, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

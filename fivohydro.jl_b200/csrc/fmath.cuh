@@ -189,6 +189,9 @@ FX_HD double fx_pow5(double x) {
   return x4 * x;
 }
 
+/* x^(3/2) as x sqrt(x) (IEEE square root and product) */
+FX_HD double fx_pow15(double x) { return x * sqrt_(x); }
+
 /* Julia's hypot (correctly rounded branch with fma) */
 FX_HD double fx_hypot(double x, double y) {
   if (isinf_(x) || isinf_(y)) return inf_();

@@ -36,16 +36,20 @@
 
 namespace fv {
 
-#define FV_MAXV 11
+#define FV_MAXV 11   /* rows of the flow: conserved four + the medium's dissipative seven */
+#define FV_MAXP 16   /* every row of a state: + the charm second moment's five */
 
-struct DevState { double* f[FV_MAXV]; };
+struct DevState { double* f[FV_MAXP]; };
 
 struct DevPrims {
   double *yT, *phi, *mu, *alpha, *ux, *uy, *P, *n, *e;
   uint8_t* ok;
 };
 
-struct DevHist { double *x0_yT, *x0_phi, *x0_ux, *x0_uy, *ux_prev, *uy_prev, *alpha_prev, *T_prev; };
+struct DevHist {
+  double *x0_yT, *x0_phi, *x0_ux, *x0_uy, *ux_prev, *uy_prev, *alpha_prev, *T_prev;
+  double *nux_prev, *nuy_prev;   /* the charge current after the last relaxation (second moment) */
+};
 
 /* device-side flags and reductions, mirrored into pinned host memory */
 struct DevFlags {
@@ -251,12 +255,12 @@ __device__ double face_flux(const DevParams& d, const DevState& U, const DevPrim
 #pragma unroll
   for (int q = 0; q < 7; ++q) { cl[4 + q] = floorL ? 0.0 : disL[q]; cr[4 + q] = floorR ? 0.0 : disR[q]; }
   if (sL >= 0) {
-    for (int a = 0; a < d.nv; ++a) Fh[a] = FL[slot_of(d, a)];
+    for (int a = 0; a < d.nvf; ++a) Fh[a] = FL[slot_of(d, a)];
   } else if (sR <= 0) {
-    for (int a = 0; a < d.nv; ++a) Fh[a] = FR[slot_of(d, a)];
+    for (int a = 0; a < d.nvf; ++a) Fh[a] = FR[slot_of(d, a)];
   } else {
     double inv = 1.0 / ((sR - sL) + FV_TINY);
-    for (int a = 0; a < d.nv; ++a) {
+    for (int a = 0; a < d.nvf; ++a) {
       int s = slot_of(d, a);
       Fh[a] = (((sR * FL[s]) - (sL * FR[s])) + ((sR * sL) * (cr[s] - cl[s]))) * inv;
     }
@@ -330,7 +334,7 @@ __device__ void sanitize_cell(const DevParams& d, double u[FV_MAXV], int ix, int
     if (!isfinite_(Di) || Di < 0.0) u[d.iDtau] = 0.0;
     if (!isfinite_(u[d.iSx])) u[d.iSx] = 0.0;
     if (!isfinite_(u[d.iSy])) u[d.iSy] = 0.0;
-    for (int a = 4; a < d.nv; ++a) if (!isfinite_(u[a])) u[a] = 0.0;
+    for (int a = 4; a < d.nvf; ++a) if (!isfinite_(u[a])) u[a] = 0.0;
   }
   /* S-E bound */
   {
@@ -372,7 +376,7 @@ __device__ bool cell_admissible(const DevParams& d, const double u[FV_MAXV], dou
   if (!(isfinite_(E) && isfinite_(Sx) && isfinite_(Sy) && isfinite_(Dt))) return false;
   if (!(E >= Emin)) return false;
   if (!(Dt >= 0.0)) return false;
-  for (int a = 4; a < d.nv; ++a) if (!isfinite_(u[a])) return false;
+  for (int a = 4; a < d.nvf; ++a) if (!isfinite_(u[a])) return false;
   if (E <= 1e6 * Emin) return true;
   if (okw) {
     double ut = utau(ux, uy);
@@ -394,14 +398,34 @@ __device__ bool cell_admissible(const DevParams& d, const double u[FV_MAXV], dou
   return r.ok || r.reason == PRR_VACUUM;
 }
 
+/* The charm second moment's rows in a stage (rows nvf..nv-1). flux_cell_2d! gives
+ * them no entries and prim_to_cons_2d! never writes their face columns (zero), so
+ * every branch of hlle_flux_2d! returns +0 for them, the assembly gives dU = +0
+ * (src2d/rhs2d.jl:240-243) and the rows only pass through the stage combination,
+ * with the same arithmetic as every other row. The floors and the admissibility
+ * test do not read them (src2d/floors2d.jl). */
+__device__ __forceinline__ void stage_m2_rows(const DevParams& d, const StageArgs& s, long long i) {
+  const size_t N = (size_t)d.Ntot;
+  for (int a = d.nvf; a < d.nv; ++a) {
+    const double k = 0.0;
+    if (s.dU) s.dU[(size_t)a * N + i] = k;
+    const double ub = s.Ub.f[a][i];
+    double u = ub;
+    if (s.mode == COMB_EULER) u = ub + (s.dt * k);
+    else if (s.mode == COMB_BLEND) u = (s.wold * s.Uold.f[a][i]) + (s.wnew * (ub + (s.dt * k)));
+    else if (s.mode == COMB_THIRD) u = (s.Uold.f[a][i] + (2.0 * (ub + (s.dt * k)))) / 3.0;
+    if (s.mode != COMB_RHS_ONLY) s.Uout.f[a][i] = u;
+  }
+}
+
 /* rhs_2d! (faces, sources, assembly) fused with the stage combination, the
  * sanitiser and the admissibility test. One CTA per ST_CX x ST_CY tile of the
  * full (ghost-inclusive) grid. */
 template <int EOS, bool NCH>
 __global__ void __launch_bounds__(256) k_stage(DevParams d, StageArgs s) {
   extern __shared__ double sm[];
-  double* Fx = sm;                              /* ST_NFX x nv */
-  double* Fy = sm + (size_t)ST_NFX * d.nv;      /* ST_NFY x nv */
+  double* Fx = sm;                              /* ST_NFX x nvf */
+  double* Fy = sm + (size_t)ST_NFX * d.nvf;     /* ST_NFY x nvf */
   const int cx0 = blockIdx.x * ST_CX, cy0 = blockIdx.y * ST_CY;
   const int tid = threadIdx.x;
   double amax = 0.0;
@@ -413,7 +437,7 @@ __global__ void __launch_bounds__(256) k_stage(DevParams d, StageArgs s) {
       if (ix < 0 || ix > d.Nxtot - 2 || iy >= d.Nytot) continue;
       long long i = (long long)ix * d.Nytot + iy;
       double a = face_flux<EOS, true>(d, s.Ub, s.w, i, d.Nytot, ix, d.Nxtot, s.tau, s.ffo,
-                                      Fx + (size_t)f * d.nv);
+                                      Fx + (size_t)f * d.nvf);
       if (a > amax) amax = a;
     } else {
       int g = f - ST_NFX;
@@ -422,7 +446,7 @@ __global__ void __launch_bounds__(256) k_stage(DevParams d, StageArgs s) {
       if (iy < 0 || iy > d.Nytot - 2 || ix >= d.Nxtot) continue;
       long long i = (long long)ix * d.Nytot + iy;
       double a = face_flux<EOS, false>(d, s.Ub, s.w, i, 1, iy, d.Nytot, s.tau, s.ffo,
-                                       Fy + (size_t)g * d.nv);
+                                       Fy + (size_t)g * d.nvf);
       if (a > amax) amax = a;
     }
   }
@@ -442,7 +466,7 @@ __global__ void __launch_bounds__(256) k_stage(DevParams d, StageArgs s) {
   const int ng = d.ng;
   if (ix < ng || ix >= ng + d.Nx || iy < ng || iy >= ng + d.Ny) return;
   const long long i = (long long)ix * d.Nytot + iy;
-  const int nv = d.nv;
+  const int nv = d.nvf;
   const double invdx = 1.0 / d.dx, invdy = 1.0 / d.dy;
   const double* fxR = Fx + (size_t)((lx + 1) * ST_CY + ly) * nv;
   const double* fxL = Fx + (size_t)(lx * ST_CY + ly) * nv;
@@ -485,6 +509,7 @@ __global__ void __launch_bounds__(256) k_stage(DevParams d, StageArgs s) {
     else if (s.mode == COMB_BLEND) u[a] = (s.wold * s.Uold.f[a][i]) + (s.wnew * (ub[a] + (s.dt * k)));
     else if (s.mode == COMB_THIRD) u[a] = (s.Uold.f[a][i] + (2.0 * (ub[a] + (s.dt * k)))) / 3.0;
   }
+  if (d.hasM2) stage_m2_rows(d, s, i);
   if (s.mode == COMB_RHS_ONLY) return;
   sanitize_cell(d, u, ix, iy, s.tau_state, Pw, true, FV_E_FLOOR);
   bool adm = cell_admissible<EOS, NCH>(d, u, s.tau_state, s.w.ok[i] != 0, s.w.ux[i], s.w.uy[i], Pw);
@@ -511,9 +536,9 @@ __global__ void k_finalize_ic(DevParams d, DevState U, double tau0) {
   int ix = d.ng + (int)(t / d.Ny), iy = d.ng + (int)(t % d.Ny);
   long long i = (long long)ix * d.Nytot + iy;
   double u[FV_MAXV];
-  for (int a = 0; a < d.nv; ++a) u[a] = U.f[a][i];
+  for (int a = 0; a < d.nvf; ++a) u[a] = U.f[a][i];
   sanitize_cell(d, u, ix, iy, tau0, 0.0, false, FV_E_FLOOR);
-  for (int a = 0; a < d.nv; ++a) U.f[a][i] = u[a];
+  for (int a = 0; a < d.nvf; ++a) U.f[a][i] = u[a];
 }
 
 /* ------------------------------------------------------------- relaxation */
@@ -690,12 +715,169 @@ __device__ void vorticity_coupling(double ux, double uy, double ut, double pxx, 
   *wxx = 2.0 * Mxx; *wxy = Mxy + Myx; *wyy = 2.0 * Myy;
 }
 
+/* ---- the consistent charm second moment (src2d/hq_consistent_m2_2d.jl) ---- */
+
+/* hq_h_hprime_2d, src2d/hq_consistent_firstmoment2d.jl:145-160: h = m K3/K2 and dh/dT */
+__device__ __forceinline__ void hq_h_hp(double T, const DevParams& d, double* h, double* hp) {
+  const double Tm = jmax(T, FV_T_MIN);
+  const double m = d.p.m_hq;
+  const double z = m / Tm;
+  *h = 0.0; *hp = 0.0;
+  if (z <= 0.0) return;
+  const double K1 = fx_besselkx(1, z), K2 = fx_besselkx(2, z), K3 = fx_besselkx(3, z), K4 = fx_besselkx(4, z);
+  if (fabs_(K2) <= FV_TINY) return;
+  const double hv = (m * K3) / K2;
+  const double hpv = ((m * z) / Tm) * ((((K2 + K4) * K2) - ((K1 + K3) * K3))) / ((2.0 * K2) * K2);
+  *h = isfinite_(hv) ? hv : 0.0;
+  *hp = isfinite_(hpv) ? hpv : 0.0;
+}
+
+/* tauM_charm_2d, src2d/transport2d.jl:177-184: tau_M = tau_n K4 K2 / (2 K3^2) */
+__device__ __forceinline__ double tauM_charm(double T, double tn, double m) {
+  const double Tm = jmax(T, FV_T_MIN), z = m / Tm;
+  const double K2 = fx_besselkx(2, z), K3 = fx_besselkx(3, z), K4 = fx_besselkx(4, z);
+  if (fabs_(K3) <= FV_TINY) return 0.0;
+  const double v = ((tn * K4) * K2) / ((2.0 * K3) * K3);
+  return (isfinite_(v) && v > 0) ? v : 0.0;
+}
+
+/* sigma_nu_2d, src2d/hq_consistent_m2_2d.jl:171-182 (the generated closed forms, in
+ * their order; the eta-eta entry is not read by the source and is not formed) */
+__device__ __noinline__ void sigma_nu(double uxv, double uyv, double uT, double tau, double nux, double nuy,
+                                      double dtnx, double dxnx, double dynx, double dtny, double dxny, double dyny,
+                                      double dtux, double dxux, double dyux, double dtuy, double dxuy, double dyuy,
+                                      double* oxx, double* oxy, double* oyy) {
+  const double sxx = (((((tau * ((1.0 + (uxv * uxv)) + (uyv * uyv))) * (((((((2.0 * dtnx) * ((uxv * uxv) * uxv)) - (dtny * uyv)) + ((2.0 * dxnx) * uT)) - (dyny * uT)) - ((uxv * uxv) * (((dtny * uyv) - ((2.0 * dxnx) * uT)) + (dyny * uT)))) + (uxv * (((2.0 * dtnx) + ((3.0 * dtnx) * (uyv * uyv))) + (((3.0 * dynx) * uyv) * uT))))) + (nuy * ((((((((-1.0) - ((dtux * tau) * uxv)) - (uxv * uxv)) + (((2.0 * dtux) * tau) * ((uxv * uxv) * uxv))) * ((uyv * uyv) * uyv)) - ((((2.0 * tau) * uxv) * ((1.0 + (uxv * uxv)) * (1.0 + (uxv * uxv)))) * ((dtuy * uxv) + (dxuy * uT)))) - (((tau * ((-1.0) + (2.0 * (uxv * uxv)))) * (uyv * uyv)) * ((dtuy + (dtuy * (uxv * uxv))) - ((dyux * uxv) * uT)))) + (((1.0 + (uxv * uxv)) * uyv) * ((((-1.0) + (((2.0 * dtux) * tau) * ((uxv * uxv) * uxv))) + ((dyuy * tau) * uT)) + ((uxv * uxv) * (((-1.0) + (((2.0 * dxux) * tau) * uT)) - (((2.0 * dyuy) * tau) * uT)))))))) + (nux * ((((((fx_pow5(uxv) * ((-1.0) + (((2.0 * dtuy) * tau) * uyv))) + (((tau * uyv) * (1.0 + (uyv * uyv))) * ((dtux * uyv) + (dyux * uT)))) + (((2.0 * tau) * fx_pow4(uxv)) * (((-dtux) - (dtux * (uyv * uyv))) + ((dxuy * uyv) * uT)))) - (((2.0 * tau) * (uxv * uxv)) * ((((dtux + ((2.0 * dtux) * (uyv * uyv))) + (dtux * fx_pow4(uyv))) + ((((-dxuy) + dyux) * uyv) * uT)) + ((dyux * ((uyv * uyv) * uyv)) * uT)))) - (uxv * (((1.0 + ((dtuy * tau) * ((uyv * uyv) * uyv))) + (((2.0 * dxux) * tau) * uT)) + ((uyv * uyv) * ((1.0 + (((2.0 * dxux) * tau) * uT)) + ((dyuy * tau) * uT)))))) + (((uxv * uxv) * uxv) * ((((((2.0 * dtuy) * tau) * uyv) + (((2.0 * dtuy) * tau) * ((uyv * uyv) * uyv))) - (2.0 * (1.0 + ((dxux * tau) * uT)))) + ((uyv * uyv) * (((-1.0) - (((2.0 * dxux) * tau) * uT)) + (((2.0 * dyuy) * tau) * uT)))))))) / ((3.0 * tau) * fx_pow15(((1.0 + (uxv * uxv)) + (uyv * uyv)))));
+  const double sxy = (((((tau * ((1.0 + (uxv * uxv)) + (uyv * uyv))) * ((((((3.0 * dtny) * ((uxv * uxv) * uxv)) + (((3.0 * dynx) * (1.0 + (uyv * uyv))) * uT)) + (3.0 * (((dtnx * uyv) * (1.0 + (uyv * uyv))) + (dxny * uT)))) + ((uxv * uxv) * ((dtnx * uyv) + ((3.0 * dxny) * uT)))) + (uxv * (((3.0 * dtny) + (dtny * (uyv * uyv))) + (((dxnx + dyny) * uyv) * uT))))) - (nuy * (((((((((4.0 * dtuy) * tau) * fx_pow5(uxv)) * uyv) + ((((3.0 * dxuy) * tau) * uyv) * uT)) + ((((4.0 * tau) * fx_pow4(uxv)) * uyv) * ((-(dtux * uyv)) + (dxuy * uT)))) - (((tau * (uxv * uxv)) * uyv) * (((((-7.0) * dxuy) * uT) + (((2.0 * dtux) * uyv) * (3.0 + (2.0 * (uyv * uyv))))) + ((dyux * uT) * (3.0 + (4.0 * (uyv * uyv))))))) + (((uxv * uxv) * uxv) * ((((((10.0 * dtuy) * tau) * uyv) + (((4.0 * dtuy) * tau) * ((uyv * uyv) * uyv))) + (((3.0 * dyuy) * tau) * uT)) + ((uyv * uyv) * ((2.0 - (((4.0 * dxux) * tau) * uT)) + (((4.0 * dyuy) * tau) * uT)))))) + (uxv * (((((((6.0 * dtuy) * tau) * uyv) + (((4.0 * dtuy) * tau) * ((uyv * uyv) * uyv))) + (2.0 * fx_pow4(uyv))) + (((3.0 * dyuy) * tau) * uT)) + ((uyv * uyv) * ((2.0 - (((3.0 * dxux) * tau) * uT)) + (((4.0 * dyuy) * tau) * uT)))))))) + (nux * (((((((2.0 * fx_pow4(uxv)) * uyv) * ((-1.0) + (((2.0 * dtuy) * tau) * uyv))) - (((((3.0 * dxux) * tau) * uyv) * (1.0 + (uyv * uyv))) * uT)) - ((((4.0 * tau) * ((uxv * uxv) * uxv)) * uyv) * ((dtux + (dtux * (uyv * uyv))) - ((dxuy * uyv) * uT)))) + (((uxv * uxv) * uyv) * ((((((-2.0) + (((6.0 * dtuy) * tau) * uyv)) + (((4.0 * dtuy) * tau) * ((uyv * uyv) * uyv))) - (((4.0 * dxux) * tau) * uT)) + (((3.0 * dyuy) * tau) * uT)) + ((uyv * uyv) * (((-2.0) - (((4.0 * dxux) * tau) * uT)) + (((4.0 * dyuy) * tau) * uT)))))) - ((tau * uxv) * (((dyux * uT) * ((3.0 + (7.0 * (uyv * uyv))) + (4.0 * fx_pow4(uyv)))) + (uyv * ((((6.0 * dtux) + ((10.0 * dtux) * (uyv * uyv))) + ((4.0 * dtux) * fx_pow4(uyv))) - (((3.0 * dxuy) * uyv) * uT)))))))) / ((6.0 * tau) * fx_pow15(((1.0 + (uxv * uxv)) + (uyv * uyv)))));
+  const double syy = (((((tau * ((1.0 + (uxv * uxv)) + (uyv * uyv))) * ((((((((-(dtnx * uxv)) + ((2.0 * dtny) * uyv)) + (((3.0 * dtny) * (uxv * uxv)) * uyv)) - ((dtnx * uxv) * (uyv * uyv))) + ((2.0 * dtny) * ((uyv * uyv) * uyv))) + ((((3.0 * dxny) * uxv) * uyv) * uT)) - ((dxnx * (1.0 + (uyv * uyv))) * uT)) + (((2.0 * dyny) * (1.0 + (uyv * uyv))) * uT))) + (nux * ((((((uxv * uxv) * uxv) * ((((-1.0) - ((dtuy * tau) * uyv)) - (uyv * uyv)) + (((2.0 * dtuy) * tau) * ((uyv * uyv) * uyv)))) - ((((2.0 * tau) * uyv) * ((1.0 + (uyv * uyv)) * (1.0 + (uyv * uyv)))) * ((dtux * uyv) + (dyux * uT)))) - (((tau * (uxv * uxv)) * ((-1.0) + (2.0 * (uyv * uyv)))) * ((dtux + (dtux * (uyv * uyv))) - ((dxuy * uyv) * uT)))) + ((uxv * (1.0 + (uyv * uyv))) * ((((-1.0) + (((2.0 * dtuy) * tau) * ((uyv * uyv) * uyv))) + ((dxux * tau) * uT)) + ((uyv * uyv) * (((-1.0) - (((2.0 * dxux) * tau) * uT)) + (((2.0 * dyuy) * tau) * uT)))))))) + (nuy * ((((((((-1.0) + (((2.0 * dtux) * tau) * uxv)) * fx_pow5(uyv)) + (((tau * uxv) * (1.0 + (uxv * uxv))) * ((dtuy * uxv) + (dxuy * uT)))) + (((2.0 * tau) * fx_pow4(uyv)) * (((-dtuy) - (dtuy * (uxv * uxv))) + ((dyux * uxv) * uT)))) - (((2.0 * tau) * (uyv * uyv)) * ((((dtuy + ((2.0 * dtuy) * (uxv * uxv))) + (dtuy * fx_pow4(uxv))) + (((dxuy - dyux) * uxv) * uT)) + ((dxuy * ((uxv * uxv) * uxv)) * uT)))) + (((uyv * uyv) * uyv) * ((((((2.0 * dtux) * tau) * uxv) + (((2.0 * dtux) * tau) * ((uxv * uxv) * uxv))) + ((uxv * uxv) * (((-1.0) + (((2.0 * dxux) * tau) * uT)) - (((2.0 * dyuy) * tau) * uT)))) - (2.0 * (1.0 + ((dyuy * tau) * uT)))))) - (uyv * (((1.0 + ((dtux * tau) * ((uxv * uxv) * uxv))) + (((2.0 * dyuy) * tau) * uT)) + ((uxv * uxv) * ((1.0 + ((dxux * tau) * uT)) + (((2.0 * dyuy) * tau) * uT)))))))) / ((3.0 * tau) * fx_pow15(((1.0 + (uxv * uxv)) + (uyv * uyv)))));
+  *oxx = sxx; *oxy = sxy; *oyy = syy;
+}
+
+/* rank1_traceless_2d, src2d/hq_consistent_m2_2d.jl:225-234 */
+__device__ __forceinline__ void rank1_traceless(double Ax, double Ay, double Bx, double By, double ux, double uy,
+                                                double ut, double* qxx, double* qxy, double* qyy) {
+  const double u2 = ut * ut;
+  const double tr = ((Ay * ((By + (By * (ux * ux))) - ((Bx * ux) * uy))) + (Ax * ((Bx - ((By * ux) * uy)) + (Bx * (uy * uy))))) / u2;
+  *qxx = (Ax * Bx) - (((1.0 + (ux * ux)) * tr) / 3.0);
+  *qyy = (Ay * By) - (((1.0 + (uy * uy)) * tr) / 3.0);
+  *qxy = (((Ay * Bx) + (Ax * By)) / 2.0) - (((ux * uy) * tr) / 3.0);
+}
+
+/* consistent_m2_source_2d (src2d/hq_consistent_m2_2d.jl:247-404), split in two: the
+ * parts that do not depend on the moment's own fields (the coefficients, the medium's
+ * and the current's shear, the rank-1 drives), computed once per cell, and the rows
+ * as functions of (pxx, pxy, pyy, peta, PiQ), evaluated five times (once, and once
+ * per perturbed channel for the implicit coefficients). Every expression is the
+ * single-function form's, in its order, so the bits are the same. */
+struct M2Cell {
+  double ux, uy, ut, tau, tM, Tm;
+  double sxx, sxy, syy, seta;      /* the medium's shear (unit viscosity) */
+  double snxx, snxy, snyy;         /* the current's shear */
+  double geo, DlnT, etabar, ABr, etaQ, zetaQ;
+  double qxx, qxy, qyy;            /* class (iv) */
+  double tB1, tB4, tB5, tB6, tB7;  /* the trace row's field-independent terms, in order */
+  double th, ax, ay, dtux, dtuy, dxux, dxuy, dyux, dyuy;
+  uint32_t t;
+};
+
+__device__ __noinline__ void m2_cell_prepare(M2Cell& c, double ux, double uy, double ut, double tau, double T,
+                                             double dxT, double dyT, double dtT, double nux, double nuy, double dta,
+                                             double dxa, double dya, double thnu, double dtnux, double dtnuy,
+                                             double dxnux, double dxnuy, double dynux, double dynuy, const Kin& k,
+                                             double dtux, double dtuy, double n, double tn, double Ds, double h,
+                                             double hp, double tM, double etaM, double m, uint32_t t) {
+  c.ux = ux; c.uy = uy; c.ut = ut; c.tau = tau; c.tM = tM; c.t = t;
+  c.th = k.th; c.ax = k.ax; c.ay = k.ay; c.dtux = dtux; c.dtuy = dtuy;
+  c.dxux = k.dxux; c.dxuy = k.dxuy; c.dyux = k.dyux; c.dyuy = k.dyuy;
+  const double Tm = jmax(T, FV_T_MIN);
+  c.Tm = Tm;
+  c.etaQ = etaM;
+  c.zetaQ = (5.0 / 3.0) * c.etaQ;
+  /* hq_m2_coeffs_2d, :125-142 */
+  const double T2 = jmax(Tm, FV_T_MIN), z = m / T2;
+  const double K2 = fx_besselkx(2, z), K3 = fx_besselkx(3, z), K4 = fx_besselkx(4, z);
+  const double K5 = K3 + ((8.0 * K4) / z);
+  const double dl = (fabs_(K4) > FV_TINY && fabs_(K3) > FV_TINY)
+                        ? z * (((K3 + K5) / (2.0 * K4)) - ((K2 + K4) / (2.0 * K3))) : 0.0;
+  c.etabar = ((tn * n) * T2) / 2.0;
+  const double lama = (Ds * ((m * m) + ((6.0 * T2) * h))) / (2.0 * T2);
+  const double Aco = (m * m) + ((5.0 * T2) * h);
+  const double abr = fabs_(K3) > FV_TINY ? 5.0 + ((z * K2) / K3) : 5.0;
+  const double dlnC = isfinite_(dl) ? dl : 0.0;
+  c.ABr = isfinite_(abr) ? abr : 5.0;
+  ns_shear(ux, uy, ut, tau, k, -0.5, &c.sxx, &c.sxy, &c.syy, &c.seta);
+  const double anudot = ((k.ax * nux) + (k.ay * nuy)) - ((((k.ax * ux) + (k.ay * uy)) * ((nux * ux) + (nuy * uy))) / (ut * ut));
+  sigma_nu(ux, uy, ut, tau, nux, nuy, dtnux, dxnux, dynux, dtnuy, dxnuy, dynuy, dtux, k.dxux, k.dyux, dtuy, k.dxuy,
+           k.dyuy, &c.snxx, &c.snxy, &c.snyy);
+  const double DT = ((ut * dtT) + (ux * dxT)) + (uy * dyT);
+  c.DlnT = DT / Tm;
+  const double DlnC = dlnC * c.DlnT;
+  const double Da = ((ut * dta) + (ux * dxa)) + (uy * dya);
+  c.geo = (t & FIVO_TERM_M2_EXPANSION) ? tM * (((5.0 / 3.0) * k.th) + DlnC) : 0.0;
+  const double gTx = (h + (Tm * hp)) * (dxT + (ux * DT));
+  const double gTy = (h + (Tm * hp)) * (dyT + (uy * DT));
+  double qaxx, qaxy, qayy, qgxx, qgxy, qgyy;
+  rank1_traceless(k.ax, k.ay, nux, nuy, ux, uy, ut, &qaxx, &qaxy, &qayy);
+  rank1_traceless(nux, nuy, gTx, gTy, ux, uy, ut, &qgxx, &qgxy, &qgyy);
+  const bool ia = t & FIVO_TERM_M2_ACCEL_NU, ig = t & FIVO_TERM_M2_NU_GRADTH;
+  c.qxx = (ia ? (2.0 * lama) * qaxx : 0.0) + (ig ? (Ds / Tm) * qgxx : 0.0);
+  c.qyy = (ia ? (2.0 * lama) * qayy : 0.0) + (ig ? (Ds / Tm) * qgyy : 0.0);
+  c.qxy = (ia ? (2.0 * lama) * qaxy : 0.0) + (ig ? (Ds / Tm) * qgxy : 0.0);
+  const bool i1 = t & FIVO_TERM_M2_NU_GRADIENT, i2 = t & FIVO_TERM_M2_BG_GRADU;
+  c.tB1 = i1 ? c.zetaQ * thnu : 0.0;
+  c.tB4 = c.etabar * (((t & FIVO_TERM_M2_BG_DLNT) ? c.ABr * c.DlnT : 0.0) + (i2 ? (5.0 / 3.0) * k.th : 0.0));
+  c.tB5 = ia ? ((Ds * Aco) / (3.0 * Tm)) * anudot : 0.0;
+  c.tB6 = ig ? ((5.0 / 6.0) * (Ds / Tm)) *
+                   (((nux * gTx) + (nuy * gTy)) - ((((nux * ux) + (nuy * uy)) * ((gTx * ux) + (gTy * uy))) / (ut * ut)))
+             : 0.0;
+  c.tB7 = (t & FIVO_TERM_M2_BG_DALPHA) ? c.etabar * Da : 0.0;
+}
+
+/* the rows d_tau (pQxx, pQxy, pQyy, PiQ) at the given fields */
+__device__ __noinline__ void m2_cell_rows(const M2Cell& c, double pxx, double pxy, double pyy, double peta,
+                                          double PiQ, double out[4]) {
+  const double ux = c.ux, uy = c.uy, tM = c.tM;
+  const uint32_t t = c.t;
+  double ps, cxx, cxy, cyy;
+  pi_sigma(ux, uy, pxx, pxy, pyy, peta, c.sxx, c.sxy, c.syy, c.seta, &ps, &cxx, &cxy, &cyy);
+  const bool i1 = t & FIVO_TERM_M2_NU_GRADIENT, i2 = t & FIVO_TERM_M2_BG_GRADU;
+  const bool i3 = t & FIVO_TERM_M2_PI_SIGMA, i4 = t & FIVO_TERM_M2_PIQ_SIGMA;
+  double sxx = ((((((pxx + (i1 ? (2.0 * c.etaQ) * c.snxx : 0.0)) + (c.geo * pxx)) +
+                  (i3 ? (2.0 * tM) * (cxx - (((1.0 + (ux * ux)) * ps) / 3.0)) : 0.0)) +
+                 (i4 ? ((2.0 * tM) * PiQ) * c.sxx : 0.0)) + (i2 ? (2.0 * c.etabar) * c.sxx : 0.0)) + c.qxx);
+  double syy = ((((((pyy + (i1 ? (2.0 * c.etaQ) * c.snyy : 0.0)) + (c.geo * pyy)) +
+                  (i3 ? (2.0 * tM) * (cyy - (((1.0 + (uy * uy)) * ps) / 3.0)) : 0.0)) +
+                 (i4 ? ((2.0 * tM) * PiQ) * c.syy : 0.0)) + (i2 ? (2.0 * c.etabar) * c.syy : 0.0)) + c.qyy);
+  double sxy = ((((((pxy + (i1 ? (2.0 * c.etaQ) * c.snxy : 0.0)) + (c.geo * pxy)) +
+                  (i3 ? (2.0 * tM) * (cxy - (((ux * uy) * ps) / 3.0)) : 0.0)) +
+                 (i4 ? ((2.0 * tM) * PiQ) * c.sxy : 0.0)) + (i2 ? (2.0 * c.etabar) * c.sxy : 0.0)) + c.qxy);
+  if (t & FIVO_TERM_M2_VORTICITY) {
+    double wxx, wxy, wyy;
+    vorticity_coupling(ux, uy, c.ut, pxx, pxy, pyy, c.ax, c.ay, c.dtux, c.dtuy, c.dxux, c.dxuy, c.dyux, c.dyuy,
+                       &wxx, &wxy, &wyy);
+    sxx += tM * wxx; sxy += tM * wxy; syy += tM * wyy;
+  }
+  if (t & FIVO_TERM_M2_PROJECTOR) {
+    const double at = ((ux * c.ax) + (uy * c.ay)) / c.ut;
+    const PiC Q = shear_tensor(ux, uy, c.ut, pxx, pxy, pyy);
+    const double cx = (((-Q.tx) * at) + (Q.xx * c.ax)) + (Q.xy * c.ay);
+    const double cy = (((-Q.ty) * at) + (Q.xy * c.ax)) + (Q.yy * c.ay);
+    sxx -= tM * ((2.0 * ux) * cx);
+    sxy -= tM * ((ux * cy) + (uy * cx));
+    syy -= tM * ((2.0 * uy) * cy);
+  }
+  const double sB = (((((((PiQ + c.tB1) + (c.geo * PiQ)) + (i3 ? ((2.0 / 3.0) * tM) * ps : 0.0)) + c.tB4) + c.tB5) +
+                      c.tB6) + c.tB7);
+  const double den = tM * c.ut;
+  out[0] = (-sxx) / den; out[1] = (-sxy) / den; out[2] = (-syy) / den; out[3] = (-sB) / den;
+}
+
 /* relax_dissipative_2d! (src2d/dissipation2d.jl:293-705) fused with
  * project_shear! (main2D.jl:332-358). Reads the dissipative planes of Uq (the
  * pre-relaxation snapshot), writes them to Uo; the conserved planes are shared.
  * Every cell writes its dissipative rows: interior ok cells relaxed, the rest
  * copied. Then the shear projection of every interior cell. */
-template <int EOS>
+template <int EOS, bool M2>
 __device__ __forceinline__ double relax_cell(const DevParams& d, const DevState& Uq, const DevState& Uo,
                                              const DevPrims& w, const DevHist& h, double tau, double D,
                                              int do_relax, int do_project, long long i) {
@@ -716,6 +898,12 @@ __device__ __forceinline__ double relax_cell(const DevParams& d, const DevState&
   double v_Pi = d.hasPi ? QPi[i] : 0.0;
   double v_pixx = d.hasShear ? QPixx[i] : 0.0, v_pixy = d.hasShear ? QPixy[i] : 0.0;
   double v_piyy = d.hasShear ? QPiyy[i] : 0.0, v_pieta = d.hasShear ? QPieta[i] : 0.0;
+  /* the charm second moment's rows pQxx, pQxy, pQyy, pQeta, PiQ (consecutive) */
+  double v_pQ[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  if (M2) {
+#pragma unroll
+    for (int j = 0; j < 5; ++j) v_pQ[j] = Uq.f[d.iPQxx + j][i];
+  }
   const fivo_params& p = d.p;
   const double ux = w.ux[i], uy = w.uy[i];
   const double ut = utau(ux, uy);
@@ -898,6 +1086,71 @@ __device__ __forceinline__ double relax_cell(const DevParams& d, const DevState&
           if (mag > cap && mag > FV_TINY) { double sc = cap / mag; nux *= sc; nuy *= sc; }
         }
         v_nux = nux; v_nuy = nuy;
+        /* the charm second moment: relax_charm_m2_cell_2d!, src2d/dissipation2d.jl:722-888,
+         * handed the ramped tau_n and this cell's relaxed current */
+        if (M2) {
+          const double mq = p.transport_mass > 0.0 ? p.transport_mass : p.m_hq;
+          const double tMq = tauM_charm(T, tn, mq);
+          const bool have_hist = isfinite_(h.alpha_prev[i]) && isfinite_(h.T_prev[i]);
+          if (tMq > 0.0 && have_hist) {
+            const double nxp = h.nux_prev[i], nyp = h.nuy_prev[i];
+            const double dtnx = isfinite_(nxp) ? (nux - nxp) / D : 0.0;
+            const double dtny = isfinite_(nyp) ? (nuy - nyp) / D : 0.0;
+            const double dxnx = ((QNux[i + st] - QNux[i - st]) * 0.5) * invdx;
+            const double dxny = ((QNuy[i + st] - QNuy[i - st]) * 0.5) * invdx;
+            const double dynx = ((QNux[i + 1] - QNux[i - 1]) * 0.5) * invdy;
+            const double dyny = ((QNuy[i + 1] - QNuy[i - 1]) * 0.5) * invdy;
+            const double uxp = h.ux_prev[i], uyp = h.uy_prev[i];
+            const double dtux2 = isfinite_(uxp) ? (ux - uxp) / D : 0.0;
+            const double dtuy2 = isfinite_(uyp) ? (uy - uyp) / D : 0.0;
+            const double nut2 = nu_tau(ux, uy, ut, nux, nuy);
+            const double thnu = ((((((((ux * dtnx) + (uy * dtny)) + (nux * dtux2)) + (nuy * dtuy2)) * safe_inv(ut)) -
+                                   ((nut2 * ((ux * dtux2) + (uy * dtuy2))) * safe_inv(ut * ut))) + dxnx) + dyny) +
+                                (nut2 * safe_inv(tau));
+            const double Tp2 = h.T_prev[i];
+            const double dtT2 = isfinite_(Tp2) ? (T - Tp2) / D : 0.0;
+            const double dxT2 = ((fx_exp(w.yT[i + st]) - fx_exp(w.yT[i - st])) * 0.5) * invdx;
+            const double dyT2 = ((fx_exp(w.yT[i + 1]) - fx_exp(w.yT[i - 1])) * 0.5) * invdy;
+            double h2, hp2;
+            hq_h_hp(T, d, &h2, &hp2);
+            const double Ds2 = safe_div(p.kappa_coeff, T) / FV_FMGEV;
+            M2Cell mc;
+            m2_cell_prepare(mc, ux, uy, ut, tau, T, dxT2, dyT2, dtT2, nux, nuy, dta, dxa, dya, thnu, dtnx, dtny,
+                            dxnx, dxny, dynx, dyny, k, dtux2, dtuy2, n, tn, Ds2, h2, hp2, tMq,
+                            (jmax(T, FV_T_MIN) * tn) / 2.0, mq, p.terms);
+            double pQxx = v_pQ[0], pQxy = v_pQ[1], pQyy = v_pQ[2], pQeta = v_pQ[3], PiQv = v_pQ[4];
+            double s0[4], s1[4];
+            m2_cell_rows(mc, pQxx, pQxy, pQyy, pQeta, PiQv, s0);
+            const double A2 = safe_div(tMq * ut, D);
+            const double dp = 1e-7 * jmax(jmax(jmax(jmax(1.0, fabs_(pQxx)), fabs_(pQxy)), fabs_(pQyy)), fabs_(PiQv));
+            /* one perturbed evaluation per channel: each row's slope in its own field */
+            double c[4];
+            m2_cell_rows(mc, pQxx + dp, pQxy, pQyy, pQeta, PiQv, s1);
+            c[0] = (((-(s1[0] - s0[0])) / dp) * tMq) * ut;
+            m2_cell_rows(mc, pQxx, pQxy + dp, pQyy, pQeta, PiQv, s1);
+            c[1] = (((-(s1[1] - s0[1])) / dp) * tMq) * ut;
+            m2_cell_rows(mc, pQxx, pQxy, pQyy + dp, pQeta, PiQv, s1);
+            c[2] = (((-(s1[2] - s0[2])) / dp) * tMq) * ut;
+            m2_cell_rows(mc, pQxx, pQxy, pQyy, pQeta, PiQv + dp, s1);
+            c[3] = (((-(s1[3] - s0[3])) / dp) * tMq) * ut;
+            const bool ram = p.relax_advect_m2 != 0;
+            const double amxx = ram ? (-tMq) * upw(Uq.f[d.iPQxx], pQxx) : 0.0;
+            const double amxy = ram ? (-tMq) * upw(Uq.f[d.iPQxy], pQxy) : 0.0;
+            const double amyy = ram ? (-tMq) * upw(Uq.f[d.iPQyy], pQyy) : 0.0;
+            const double amB = ram ? (-tMq) * upw(Uq.f[d.iPiQ], PiQv) : 0.0;
+            const double Rxx = ((((-tMq) * ut) * s0[0]) - (c[0] * pQxx)) - amxx;
+            const double Rxy = ((((-tMq) * ut) * s0[1]) - (c[1] * pQxy)) - amxy;
+            const double Ryy = ((((-tMq) * ut) * s0[2]) - (c[2] * pQyy)) - amyy;
+            const double RB = ((((-tMq) * ut) * s0[3]) - (c[3] * PiQv)) - amB;
+            const double half = 0.5 * (A2 + 1.0);
+            pQxx = ((A2 * pQxx) - Rxx) / jmax(A2 + c[0], half);
+            pQxy = ((A2 * pQxy) - Rxy) / jmax(A2 + c[1], half);
+            pQyy = ((A2 * pQyy) - Ryy) / jmax(A2 + c[2], half);
+            PiQv = ((A2 * PiQv) - RB) / jmax(A2 + c[3], half);
+            pQeta = project_traceless(ux, uy, ut, pQxx, pQxy, pQyy);
+            v_pQ[0] = pQxx; v_pQ[1] = pQxy; v_pQ[2] = pQyy; v_pQ[3] = pQeta; v_pQ[4] = PiQv;
+          }
+        }
       }
     }
   }
@@ -912,19 +1165,26 @@ __device__ __forceinline__ double relax_cell(const DevParams& d, const DevState&
   if (d.hasShear) {
     Uo.f[d.iPixx][i] = v_pixx; Uo.f[d.iPixy][i] = v_pixy; Uo.f[d.iPiyy][i] = v_piyy; Uo.f[d.iPieta][i] = v_pieta;
   }
+  if (M2) {
+#pragma unroll
+    for (int j = 0; j < 5; ++j) Uo.f[d.iPQxx + j][i] = v_pQ[j];
+    /* the current's history for the next relaxation's d_tau nu (dissipation2d.jl:354-359):
+     * every cell's nu after this relaxation */
+    if (do_relax && d.hasNu) { h.nux_prev[i] = v_nux; h.nuy_prev[i] = v_nuy; }
+  }
   return rel_out;
 }
 
 /* relax_dissipative_2d! + project_shear! on every cell. The shear-residual
  * monitor (max and sum over interior cells) is reduced over the warp before
  * its atomics: one per warp instead of one per cell on a single address. */
-template <int EOS>
+template <int EOS, bool M2>
 __global__ void __launch_bounds__(128) k_relax(DevParams d, DevState Uq, DevState Uo, DevPrims w,
                                                DevHist h, double tau, double D, int do_relax,
                                                int do_project, DevFlags* fl) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double rel = -1.0;
-  if (i < d.Ntot) rel = relax_cell<EOS>(d, Uq, Uo, w, h, tau, D, do_relax, do_project, i);
+  if (i < d.Ntot) rel = relax_cell<EOS, M2>(d, Uq, Uo, w, h, tau, D, do_relax, do_project, i);
   if (do_project && d.hasShear) {
     double mx = rel > 0.0 ? rel : 0.0, sm = rel >= 0.0 ? rel : 0.0;
     for (int o = 16; o > 0; o >>= 1) {
@@ -1602,7 +1862,7 @@ __device__ __forceinline__ int adm_prefilter(const DevParams& d, const double u[
   if (!(isfinite_(E) && isfinite_(Sx) && isfinite_(Sy) && isfinite_(Dt))) return 0;
   if (!(E >= Emin)) return 0;
   if (!(Dt >= 0.0)) return 0;
-  for (int a = 4; a < d.nv; ++a) if (!isfinite_(u[a])) return 0;
+  for (int a = 4; a < d.nvf; ++a) if (!isfinite_(u[a])) return 0;
   if (E <= 1e6 * Emin) return 1;
   if (okw) {
     double ut = utau(ux, uy);
@@ -1630,7 +1890,7 @@ __global__ void __launch_bounds__(128) k_update(DevParams d, StageArgs s, const 
   if (t < (long long)d.Nx * d.Ny) {
     const int ix = d.ng + (int)(t / d.Ny), iy = d.ng + (int)(t % d.Ny);
     i = (long long)ix * d.Nytot + iy;
-    const int nv = d.nv;
+    const int nv = d.nvf;
     const size_t N = (size_t)d.Ntot;
     const double invdx = 1.0 / d.dx, invdy = 1.0 / d.dy;
     double ub[FV_MAXV];
@@ -1673,6 +1933,7 @@ __global__ void __launch_bounds__(128) k_update(DevParams d, StageArgs s, const 
       else if (s.mode == COMB_BLEND) u[a] = (s.wold * s.Uold.f[a][i]) + (s.wnew * (ub[a] + (s.dt * k)));
       else if (s.mode == COMB_THIRD) u[a] = (s.Uold.f[a][i] + (2.0 * (ub[a] + (s.dt * k)))) / 3.0;
     }
+    if (d.hasM2) stage_m2_rows(d, s, i);
     if (s.mode != COMB_RHS_ONLY) {
       sanitize_cell(d, u, ix, iy, s.tau_state, Pw, true, FV_E_FLOOR);
       verdict = adm_prefilter(d, u, s.w.ok[i] != 0, s.w.ux[i], s.w.uy[i], Pw);

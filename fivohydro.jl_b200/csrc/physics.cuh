@@ -44,6 +44,9 @@ struct DevParams {
   fivo_params p;
   int nv, iDtau, iSx, iSy, iE, iNux, iNuy, iPi, iPixx, iPixy, iPiyy, iPieta;
   int hasNu, hasPi, hasShear, ncharge;
+  /* nv counts every state row; the first nvf take part in the fluxes, floors and
+   * admissibility, the charm second moment's five rows (hasM2) come after them */
+  int nvf, hasM2, iPQxx, iPQxy, iPQyy, iPQeta, iPiQ;
   int Nx, Ny, ng, Nxtot, Nytot;
   long long Ntot;
   double dx, dy, xmin, ymin;

@@ -10,7 +10,7 @@ import ctypes as C
 import os
 import pathlib
 
-FIVO_ABI_VERSION = 1
+FIVO_ABI_VERSION = 2
 
 FIVO_OK, FIVO_ERR_ARG, FIVO_ERR_CONFIG, FIVO_ERR_CUDA, FIVO_ERR_NOMEM, FIVO_ERR_DEVICE = range(6)
 
@@ -47,7 +47,7 @@ class FivoParams(C.Structure):
         ("bulk_width", C.c_double), ("deltaPi_factor", C.c_double),
         ("lambda_Pi_pi_factor", C.c_double), ("Pi_clip_factor", C.c_double),
         ("r_domain", C.c_double), ("T_vac_cut", C.c_double), ("E_vac_cut", C.c_double),
-        ("primrec_tol", C.c_double),
+        ("primrec_tol", C.c_double), ("transport_mass", C.c_double),
         ("eos_kind", C.c_int32), ("hq_times_fmGeV3", C.c_int32), ("with_charge", C.c_int32),
         ("enable_diff", C.c_int32), ("enable_shear", C.c_int32), ("enable_bulk", C.c_int32),
         ("shear_kind", C.c_int32), ("bulk_kind", C.c_int32),
@@ -59,6 +59,7 @@ class FivoParams(C.Structure):
         ("shear_constraint_project", C.c_int32),
         ("consistent_fm", C.c_int32), ("consistent_m2", C.c_int32),
         ("primrec_maxit", C.c_int32), ("terms", C.c_uint32),
+        ("relax_advect_m2", C.c_int32), ("reserved0", C.c_int32),
     ]
 
 
@@ -144,6 +145,8 @@ SIGNATURES = {
     "fivo_download_state": (C.c_int, [C.c_void_p, _D, C.c_int, _I64]),
     "fivo_upload_history": (C.c_int, [C.c_void_p, _I64] + [_D] * 8),
     "fivo_download_history": (C.c_int, [C.c_void_p, _I64] + [_D] * 8),
+    "fivo_upload_nu_history": (C.c_int, [C.c_void_p, _I64, _D, _D]),
+    "fivo_download_nu_history": (C.c_int, [C.c_void_p, _I64, _D, _D]),
     "fivo_reset_history": (C.c_int, [C.c_void_p]),
     "fivo_get_primitives": (C.c_int, [C.c_void_p, _I64] + [_D] * 9 + [_U8]),
     "fivo_get_counters": (C.c_int, [C.c_void_p, C.POINTER(FivoCounters)]),

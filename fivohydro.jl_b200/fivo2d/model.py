@@ -76,12 +76,13 @@ make_grid_2d = make_grid2d
 
 @dataclass
 class StateLayout2D:
-    """Dense field order Dtau, Sx, Sy, E, [nux, nuy], [Pi], [pixx, pixy, piyy, pieta]
-    (src2d/state_layout2d.jl:61-84); indices are 0-based."""
+    """Dense field order Dtau, Sx, Sy, E, [nux, nuy], [Pi], [pixx, pixy, piyy, pieta],
+    [pQxx, pQxy, pQyy, pQeta, PiQ] (src2d/state_layout2d.jl:61-84); indices are 0-based."""
     names: list
     hasNu: bool
     hasPi: bool
     hasShear: bool
+    hasM2: bool = False
 
     @property
     def nv(self):
@@ -92,8 +93,6 @@ class StateLayout2D:
 
 
 def make_layout2d(*, with_charge=True, with_bulk=True, with_shear=True, with_m2=False) -> StateLayout2D:
-    if with_m2:
-        raise NotImplementedError("make_layout2d: the charm second moment (with_m2) is not built")
     names = ["Dtau", "Sx", "Sy", "E"]
     if with_charge:
         names += ["nux", "nuy"]
@@ -101,7 +100,9 @@ def make_layout2d(*, with_charge=True, with_bulk=True, with_shear=True, with_m2=
         names += ["Pi"]
     if with_shear:
         names += ["pixx", "pixy", "piyy", "pieta"]
-    return StateLayout2D(names, with_charge, with_bulk, with_shear)
+    if with_m2:
+        names += ["pQxx", "pQxy", "pQyy", "pQeta", "PiQ"]
+    return StateLayout2D(names, with_charge, with_bulk, with_shear, with_m2)
 
 
 @dataclass
@@ -258,12 +259,11 @@ def build_model_2d(*, eos=None, r_domain: float = math.inf, enable_shear: bool =
                              f"2-D solver; use the default ({default}).")
     if knobs["consistent_fm"] and knobs["tauN_coeff"] != 1.0:
         raise ValueError("IdealDiffVisc2DModel: `tauN_coeff` cannot be combined with `consistent_fm = true`.")
-    if knobs["consistent_m2"]:
-        raise NotImplementedError("consistent_m2 (the charm second moment) is not built")
     if knobs["shear_constraint"] not in ("project", "monitor"):
         raise ValueError("shear_constraint must be 'project' or 'monitor'")
 
-    L = make_layout2d(with_charge=with_charge, with_bulk=enable_bulk, with_shear=enable_shear)
+    L = make_layout2d(with_charge=with_charge, with_bulk=enable_bulk, with_shear=enable_shear,
+                      with_m2=bool(knobs["consistent_m2"]))
     p = eos_params(eos)
     p.with_charge = int(with_charge)
     p.enable_diff, p.enable_shear, p.enable_bulk = int(enable_diff), int(enable_shear), int(enable_bulk)
@@ -283,16 +283,16 @@ def build_model_2d(*, eos=None, r_domain: float = math.inf, enable_shear: bool =
     for name in ("kappa_coeff", "tauN_coeff", "deltaN_factor", "nu_clip_factor", "vacuum_n_lo",
                  "vacuum_n_hi", "deltaShear_factor", "taupi_pi_factor", "lambda_pi_Pi_factor",
                  "pi_clip_factor", "deltaPi_factor", "lambda_Pi_pi_factor", "Pi_clip_factor",
-                 "r_domain", "T_vac_cut", "E_vac_cut"):
+                 "r_domain", "T_vac_cut", "E_vac_cut", "transport_mass"):
         setattr(p, name, float(knobs[name]))
     for name in ("advect_nu", "relax_advect_nu", "advect_pi", "relax_advect_pi", "advect_Pi",
                  "relax_advect_Pi", "vacuum_ramp_relax", "shear_projected_deriv",
-                 "diff_projected_deriv", "consistent_fm", "consistent_m2"):
+                 "diff_projected_deriv", "consistent_fm", "consistent_m2", "relax_advect_m2"):
         setattr(p, name, int(bool(knobs[name])))
     p.shear_constraint_project = int(knobs["shear_constraint"] == "project")
     p.primrec_maxit, p.primrec_tol = int(primrec_maxit), float(primrec_tol)
     sectors = dict(enable_diff=enable_diff, enable_shear=enable_shear, consistent_fm=bool(knobs["consistent_fm"]),
-                   consistent_m2=False)
+                   consistent_m2=bool(knobs["consistent_m2"]))
     p.terms = _resolve_terms(terms, lambda s: sectors[s])
     return IdealDiffVisc2DModel(eos=eos, layout=L, params=p, knobs=knobs)
 

@@ -100,6 +100,17 @@ class GPUWork2D:
     def reset_history(self):
         self._ck(self.lib.fivo_reset_history(self.h), "fivo_reset_history")
 
+    def set_nu_history(self, nux_prev=None, nuy_prev=None):
+        """Work2D nux_prev / nuy_prev: the charge current after the previous relaxation
+        (the charm second moment's d_tau nu, src2d/work2d.jl:46-47)"""
+        a, b = _f64(nux_prev), _f64(nuy_prev)
+        self._ck(self.lib.fivo_upload_nu_history(self.h, self.N, _ptr(a), _ptr(b)), "fivo_upload_nu_history")
+
+    def get_nu_history(self):
+        a, b = np.empty(self.N), np.empty(self.N)
+        self._ck(self.lib.fivo_download_nu_history(self.h, self.N, _ptr(a), _ptr(b)), "fivo_download_nu_history")
+        return dict(nux_prev=a, nuy_prev=b)
+
     def primitives(self):
         arrs = [np.empty(self.N) for _ in PRIMS]
         ok = np.empty(self.N, dtype=np.uint8)

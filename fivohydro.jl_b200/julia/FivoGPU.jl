@@ -31,6 +31,7 @@ mutable struct FivoParams
     zeta_over_s::Float64; tauPi_coeff::Float64; bulk_T0::Float64; bulk_width::Float64
     deltaPi_factor::Float64; lambda_Pi_pi_factor::Float64; Pi_clip_factor::Float64
     r_domain::Float64; T_vac_cut::Float64; E_vac_cut::Float64; primrec_tol::Float64
+    transport_mass::Float64
     eos_kind::Int32; hq_times_fmGeV3::Int32; with_charge::Int32
     enable_diff::Int32; enable_shear::Int32; enable_bulk::Int32
     shear_kind::Int32; bulk_kind::Int32
@@ -38,6 +39,7 @@ mutable struct FivoParams
     advect_Pi::Int32; relax_advect_Pi::Int32; vacuum_ramp_relax::Int32
     shear_projected_deriv::Int32; diff_projected_deriv::Int32; shear_constraint_project::Int32
     consistent_fm::Int32; consistent_m2::Int32; primrec_maxit::Int32; terms::UInt32
+    relax_advect_m2::Int32; reserved0::Int32
     FivoParams() = new()
 end
 
@@ -85,11 +87,13 @@ function fivo_params(model)
     end
     for f in (:kappa_coeff, :tauN_coeff, :deltaN_factor, :nu_clip_factor, :vacuum_n_lo, :vacuum_n_hi,
               :deltaShear_factor, :taupi_pi_factor, :lambda_pi_Pi_factor, :pi_clip_factor,
-              :deltaPi_factor, :lambda_Pi_pi_factor, :Pi_clip_factor, :r_domain, :T_vac_cut, :E_vac_cut)
+              :deltaPi_factor, :lambda_Pi_pi_factor, :Pi_clip_factor, :r_domain, :T_vac_cut, :E_vac_cut,
+              :transport_mass)
         setfield!(p, f, Float64(getfield(model, f)))
     end
     for f in (:advect_nu, :relax_advect_nu, :advect_pi, :relax_advect_pi, :advect_Pi, :relax_advect_Pi,
-              :vacuum_ramp_relax, :shear_projected_deriv, :diff_projected_deriv, :consistent_fm, :consistent_m2)
+              :vacuum_ramp_relax, :shear_projected_deriv, :diff_projected_deriv, :consistent_fm, :consistent_m2,
+              :relax_advect_m2)
         setfield!(p, f, _b(getfield(model, f)))
     end
     p.shear_constraint_project = _b(model.shear_constraint === :project)

@@ -18,7 +18,8 @@
  *     cell i, field a lives at U[i*nv + a] (AoS per cell). Flat cell index
  *     i = ix*Nytot + iy (0-based; y is the fast index), src2d/grid2d.jl:85.
  *   - Field order is StateLayout2D's (src2d/state_layout2d.jl:61-84):
- *     Dtau, Sx, Sy, E, [nux, nuy], [Pi], [pixx, pixy, piyy, pieta].
+ *     Dtau, Sx, Sy, E, [nux, nuy], [Pi], [pixx, pixy, piyy, pieta],
+ *     [pQxx, pQxy, pQyy, pQeta, PiQ] (the last five when consistent_m2 = 1).
  *   - Every function returns an int status: FIVO_OK (0) or a positive error
  *     code; fivo_last_error() returns the message of the last failure on the
  *     calling thread. A time step that the scheme cannot accept is NOT an
@@ -36,7 +37,7 @@
 extern "C" {
 #endif
 
-#define FIVO_ABI_VERSION 1
+#define FIVO_ABI_VERSION 2
 
 /* status codes */
 #define FIVO_OK              0
@@ -130,6 +131,9 @@ typedef struct fivo_params {
   double E_vac_cut;         /* vacuum cut energy; <= 0 derives it from T_vac_cut */
   /* --- primitive recovery numerics (src2d/primrec2d.jl:465-472) --- */
   double primrec_tol;       /* row-scaled residual tolerance (1e-12)             */
+  /* --- charm second moment --- */
+  double transport_mass;    /* charm mass of the m2 transport coefficients [GeV];
+                               <= 0 takes the EOS mass m_hq (0)                   */
   /* --- integers --- */
   int32_t eos_kind;         /* FIVO_EOS_*                                        */
   int32_t hq_times_fmGeV3;  /* multiply HQ (P,n,e) by fmGeV3                     */
@@ -145,9 +149,12 @@ typedef struct fivo_params {
   int32_t vacuum_ramp_relax;
   int32_t shear_projected_deriv, diff_projected_deriv;
   int32_t shear_constraint_project; /* 1 = :project, 0 = :monitor                */
-  int32_t consistent_fm, consistent_m2; /* charm closures (first, second moment) */
+  int32_t consistent_fm, consistent_m2; /* charm closures (first, second moment);
+                               consistent_m2 adds the five rows pQxx..PiQ          */
   int32_t primrec_maxit;    /* Newton iteration cap (80)                         */
   uint32_t terms;           /* FIVO_TERM_* bitmask                               */
+  int32_t relax_advect_m2;  /* tau_M u^k d_k of the m2 rows inside the relaxation (1) */
+  int32_t reserved0;        /* 0                                                 */
 } fivo_params;
 
 /* Diagnostics of the last call (run_sim_2d! NamedTuple, main2D.jl:558-560). */
@@ -234,6 +241,11 @@ int  fivo_download_history(fivo_ctx* ctx, int64_t ntot,
                            double* x0_yT, double* x0_phi, double* x0_ux, double* x0_uy,
                            double* ux_prev, double* uy_prev,
                            double* alpha_prev, double* T_prev);
+/* The charge-current history of the charm second moment (Work2D nux_prev,
+ * nuy_prev, src2d/work2d.jl:46-47: nu after the previous relaxation, for d_tau nu);
+ * any pointer may be NULL. Meaningful when consistent_m2 = 1. */
+int  fivo_upload_nu_history(fivo_ctx* ctx, int64_t ntot, const double* nux_prev, const double* nuy_prev);
+int  fivo_download_nu_history(fivo_ctx* ctx, int64_t ntot, double* nux_prev, double* nuy_prev);
 /* NaN-seed every history vector (run_sim_2d! reset_history, main2D.jl:407-415). */
 int  fivo_reset_history(fivo_ctx* ctx);
 /* Cell primitives of the last recovery (Work2D yT..ok); any pointer may be NULL. */

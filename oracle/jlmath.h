@@ -152,6 +152,23 @@ static inline double o_pow4(double x) {
   return x4;
 }
 
+/* Julia `x^5` for Float64 (pow_body(x, 5)): the square and the fourth power carry
+ * their low parts, the last product is fused. */
+static inline double o_pow5(double x) {
+  double x2 = x * x;
+  double e2 = std::fma(x, x, -x2);
+  double err = (x2 * 2.0) * e2;
+  double x4 = x2 * x2;
+  double lo = std::fma(x2, x2, -x4) + err;
+  double err2 = x * lo;
+  if (o_isfinite(x4) && o_isfinite(err2)) return std::fma(x4, x, err2);
+  return x4 * x;
+}
+
+/* x^(3/2) as x sqrt(x) (both roundings IEEE). Julia's Float64^Float64 is a
+ * double-double log/exp that can differ from this in the last bit. */
+static inline double o_pow15(double x) { return x * std::sqrt(x); }
+
 static inline double o_hypot(double x, double y) {
   if (std::isinf(x) || std::isinf(y)) return O_INF;
   double ax = std::fabs(x), ay = std::fabs(y);

@@ -84,8 +84,22 @@ void oracle_reset_history(void* h) {
   OCtx* c = (OCtx*)h;
   c->nsteps_run = 0;
   for (auto* v : {&c->w.x0_yT, &c->w.x0_phi, &c->w.x0_ux, &c->w.x0_uy, &c->w.ux_prev, &c->w.uy_prev,
-                  &c->w.alpha_prev, &c->w.T_prev})
+                  &c->w.alpha_prev, &c->w.T_prev, &c->w.nux_prev, &c->w.nuy_prev})
     std::fill(v->begin(), v->end(), O_NAN);
+}
+
+void oracle_set_nu_history(void* h, const double* nux_prev, const double* nuy_prev) {
+  OCtx* c = (OCtx*)h;
+  size_t n = c->w.nux_prev.size() * 8;
+  if (nux_prev) std::memcpy(c->w.nux_prev.data(), nux_prev, n);
+  if (nuy_prev) std::memcpy(c->w.nuy_prev.data(), nuy_prev, n);
+}
+
+void oracle_get_nu_history(void* h, double* nux_prev, double* nuy_prev) {
+  OCtx* c = (OCtx*)h;
+  size_t n = c->w.nux_prev.size() * 8;
+  if (nux_prev) std::memcpy(nux_prev, c->w.nux_prev.data(), n);
+  if (nuy_prev) std::memcpy(nuy_prev, c->w.nuy_prev.data(), n);
 }
 
 void oracle_get_primitives(void* h, double* yT, double* phi, double* mu, double* alpha, double* ux,
@@ -238,6 +252,14 @@ void oracle_cfm_source(const double* in, uint32_t terms, double* sx, double* sy)
   cfm_source(v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7], v[8], v[9], v[10], v[11], v[12], v[13], v[14],
              v[15], v[16], v[17], v[18], v[19], v[20], terms, sx, sy);
 }
+void oracle_m2_source(const double* in44, uint32_t terms, double* out5) { m2_source(in44, terms, out5); }
+void oracle_m2_coeffs(double T, double n, double tn, double Ds, double h, double m, double* out5) {
+  m2_coeffs(T, n, tn, Ds, h, m, out5);
+}
+double oracle_m2_tauM(double T, double tn, double m) { return m2_tauM(T, tn, m); }
+void oracle_m2_sigma_nu(const double* in18, double* out4) { m2_sigma_nu(in18, out4); }
+void oracle_m2_rank1_traceless(const double* in7, double* out3) { m2_rank1_traceless(in7, out3); }
+
 void oracle_cfm_h_hprime(const fivo_params* p, double T, double* h, double* hp) { cfm_h_hprime(T, *p, h, hp); }
 double oracle_cfm_dn_dT(const fivo_params* p, double T, double n) { return cfm_dn_dT(T, n, *p); }
 void oracle_diff_coeffs(const fivo_params* p, double T, double mu, double n, double* kappa, double* taun,

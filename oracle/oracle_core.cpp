@@ -573,8 +573,11 @@ bool make_model(const fivo_params& p, Model& m, const char** err) {
   L.hasShear = p.enable_shear != 0;
   L.iPixx = L.hasShear ? k++ : -1; L.iPixy = L.hasShear ? k++ : -1;
   L.iPiyy = L.hasShear ? k++ : -1; L.iPieta = L.hasShear ? k++ : -1;
+  /* the charm second moment's rows follow the medium's (make_layout2d with_m2) */
+  L.hasM2 = p.consistent_m2 != 0;
+  L.iPQxx = L.hasM2 ? k++ : -1; L.iPQxy = L.hasM2 ? k++ : -1; L.iPQyy = L.hasM2 ? k++ : -1;
+  L.iPQeta = L.hasM2 ? k++ : -1; L.iPiQ = L.hasM2 ? k++ : -1;
   L.nv = k;
-  if (p.consistent_m2) { if (err) *err = "consistent_m2 is not built"; return false; }
   /* reject_unwired_knobs_2d, src2d/primitives2d.jl:263-269 */
   if (p.consistent_fm && p.tauN_coeff != 1.0) {
     if (err) *err = "tauN_coeff cannot be combined with consistent_fm = true";
@@ -604,7 +607,7 @@ void make_work(const Grid& g, const Model& m, Work& w) {
   vz(w.yT, N); vz(w.phi, N); vz(w.mu, N); vz(w.alpha, N); vz(w.ux, N); vz(w.uy, N);
   vz(w.P, N); vz(w.n, N); vz(w.e, N); w.ok.assign(N, 0);
   vn(w.x0_yT); vn(w.x0_phi); vn(w.x0_ux); vn(w.x0_uy);
-  vn(w.ux_prev); vn(w.uy_prev); vn(w.alpha_prev); vn(w.T_prev);
+  vn(w.ux_prev); vn(w.uy_prev); vn(w.alpha_prev); vn(w.T_prev); vn(w.nux_prev); vn(w.nuy_prev);
   vz(w.sigx, 4 * N); vz(w.sigy, 4 * N); vz(w.ULpx, 4 * N); vz(w.URpx, 4 * N); vz(w.ULpy, 4 * N); vz(w.URpy, 4 * N);
   vz(w.ULcx, nv * N); vz(w.URcx, nv * N); vz(w.ULcy, nv * N); vz(w.URcy, nv * N);
   vz(w.Fhx, nv * N); vz(w.Fhy, nv * N); vz(w.S, nv * N); vz(w.diss_snap, nv * N);
@@ -1216,19 +1219,6 @@ bool step_ssprk3_2d(double* U, const Grid& g, double tau, double dtau, const Mod
 
 /* ======================= transport coefficients ======================= */
 
-/* pow_body(x, 5) as Julia's x^5 (src/eos.jl constants use m^5) */
-static inline double o_pow5(double x) {
-  double x2 = x * x;
-  double e2 = std::fma(x, x, -x2);
-  double err = (x2 * 2.0) * e2;
-  double x4 = x2 * x2;
-  double lo = std::fma(x2, x2, -x4) + err;
-  double err2 = x * lo;
-  double x4f = x4;
-  if (o_isfinite(x4f) && o_isfinite(err2)) return std::fma(x4f, x, err2);
-  return x4f * x;
-}
-
 /* _fluidum_single_hadron_normalization_2d, src2d/transport2d.jl:19-26 */
 static double fluidum_norm(double T, double alpha, const fivo_params& e) {
   double Tm = o_max(T, T_MIN);
@@ -1527,6 +1517,160 @@ void cfm_source(double ux, double uy, double ut, double T, double dxT, double dy
   consistent_fm_source(ux, uy, ut, T, dxT, dyT, dtT, nux, nuy, n, dn_dT, tn, Ds, hp, k, terms, sx, sy);
 }
 
+/* ---- the consistent charm second moment, src2d/hq_consistent_m2_2d.jl ---- */
+
+/* hq_m2_coeffs_2d, src2d/hq_consistent_m2_2d.jl:125-142: dlnC/dlnT, eta_bar, lambda_a, A, A/B */
+struct M2Coeffs { double dlnC, etabar, lama, Aco, ABr; };
+static M2Coeffs hq_m2_coeffs(double T, double n, double tn, double Ds, double h, double m) {
+  double Tm = o_max(T, T_MIN);
+  double z = m / Tm;
+  double K2 = o_besselkx(2, z), K3 = o_besselkx(3, z), K4 = o_besselkx(4, z);
+  double K5 = K3 + ((8.0 * K4) / z);
+  double dl = (std::fabs(K4) > TINY && std::fabs(K3) > TINY)
+                  ? z * (((K3 + K5) / (2.0 * K4)) - ((K2 + K4) / (2.0 * K3))) : 0.0;
+  M2Coeffs c;
+  c.etabar = ((tn * n) * Tm) / 2.0;
+  c.lama = (Ds * ((m * m) + ((6.0 * Tm) * h))) / (2.0 * Tm);
+  c.Aco = (m * m) + ((5.0 * Tm) * h);
+  double abr = std::fabs(K3) > TINY ? 5.0 + ((z * K2) / K3) : 5.0;
+  c.dlnC = o_isfinite(dl) ? dl : 0.0;
+  c.ABr = o_isfinite(abr) ? abr : 5.0;
+  return c;
+}
+
+/* tauM_charm_2d, src2d/transport2d.jl:177-184: tau_M = tau_n K4 K2 / (2 K3^2) */
+static double tauM_charm(double T, double tn, double m) {
+  double Tm = o_max(T, T_MIN), z = m / Tm;
+  double K2 = o_besselkx(2, z), K3 = o_besselkx(3, z), K4 = o_besselkx(4, z);
+  if (std::fabs(K3) <= TINY) return 0.0;
+  double v = ((tn * K4) * K2) / ((2.0 * K3) * K3);
+  return (o_isfinite(v) && v > 0) ? v : 0.0;
+}
+
+/* etaM_charm_2d, src2d/transport2d.jl:186 */
+static inline double etaM_charm(double T, double tn) { return (o_max(T, T_MIN) * tn) / 2.0; }
+
+/* sigma_nu_2d, src2d/hq_consistent_m2_2d.jl:171-182: the transverse-projected
+ * traceless gradient of the current (the generated closed forms, in their order) */
+static void sigma_nu(double uxv, double uyv, double uT, double tau, double nux, double nuy, double dtnx,
+                     double dxnx, double dynx, double dtny, double dxny, double dyny, double dtux, double dxux,
+                     double dyux, double dtuy, double dxuy, double dyuy, double* oxx, double* oxy, double* oyy,
+                     double* oeta) {
+  const double sxx = (((((tau * ((1.0 + (uxv * uxv)) + (uyv * uyv))) * (((((((2.0 * dtnx) * ((uxv * uxv) * uxv)) - (dtny * uyv)) + ((2.0 * dxnx) * uT)) - (dyny * uT)) - ((uxv * uxv) * (((dtny * uyv) - ((2.0 * dxnx) * uT)) + (dyny * uT)))) + (uxv * (((2.0 * dtnx) + ((3.0 * dtnx) * (uyv * uyv))) + (((3.0 * dynx) * uyv) * uT))))) + (nuy * ((((((((-1.0) - ((dtux * tau) * uxv)) - (uxv * uxv)) + (((2.0 * dtux) * tau) * ((uxv * uxv) * uxv))) * ((uyv * uyv) * uyv)) - ((((2.0 * tau) * uxv) * ((1.0 + (uxv * uxv)) * (1.0 + (uxv * uxv)))) * ((dtuy * uxv) + (dxuy * uT)))) - (((tau * ((-1.0) + (2.0 * (uxv * uxv)))) * (uyv * uyv)) * ((dtuy + (dtuy * (uxv * uxv))) - ((dyux * uxv) * uT)))) + (((1.0 + (uxv * uxv)) * uyv) * ((((-1.0) + (((2.0 * dtux) * tau) * ((uxv * uxv) * uxv))) + ((dyuy * tau) * uT)) + ((uxv * uxv) * (((-1.0) + (((2.0 * dxux) * tau) * uT)) - (((2.0 * dyuy) * tau) * uT)))))))) + (nux * ((((((o_pow5(uxv) * ((-1.0) + (((2.0 * dtuy) * tau) * uyv))) + (((tau * uyv) * (1.0 + (uyv * uyv))) * ((dtux * uyv) + (dyux * uT)))) + (((2.0 * tau) * o_pow4(uxv)) * (((-dtux) - (dtux * (uyv * uyv))) + ((dxuy * uyv) * uT)))) - (((2.0 * tau) * (uxv * uxv)) * ((((dtux + ((2.0 * dtux) * (uyv * uyv))) + (dtux * o_pow4(uyv))) + ((((-dxuy) + dyux) * uyv) * uT)) + ((dyux * ((uyv * uyv) * uyv)) * uT)))) - (uxv * (((1.0 + ((dtuy * tau) * ((uyv * uyv) * uyv))) + (((2.0 * dxux) * tau) * uT)) + ((uyv * uyv) * ((1.0 + (((2.0 * dxux) * tau) * uT)) + ((dyuy * tau) * uT)))))) + (((uxv * uxv) * uxv) * ((((((2.0 * dtuy) * tau) * uyv) + (((2.0 * dtuy) * tau) * ((uyv * uyv) * uyv))) - (2.0 * (1.0 + ((dxux * tau) * uT)))) + ((uyv * uyv) * (((-1.0) - (((2.0 * dxux) * tau) * uT)) + (((2.0 * dyuy) * tau) * uT)))))))) / ((3.0 * tau) * o_pow15(((1.0 + (uxv * uxv)) + (uyv * uyv)))));
+  const double sxy = (((((tau * ((1.0 + (uxv * uxv)) + (uyv * uyv))) * ((((((3.0 * dtny) * ((uxv * uxv) * uxv)) + (((3.0 * dynx) * (1.0 + (uyv * uyv))) * uT)) + (3.0 * (((dtnx * uyv) * (1.0 + (uyv * uyv))) + (dxny * uT)))) + ((uxv * uxv) * ((dtnx * uyv) + ((3.0 * dxny) * uT)))) + (uxv * (((3.0 * dtny) + (dtny * (uyv * uyv))) + (((dxnx + dyny) * uyv) * uT))))) - (nuy * (((((((((4.0 * dtuy) * tau) * o_pow5(uxv)) * uyv) + ((((3.0 * dxuy) * tau) * uyv) * uT)) + ((((4.0 * tau) * o_pow4(uxv)) * uyv) * ((-(dtux * uyv)) + (dxuy * uT)))) - (((tau * (uxv * uxv)) * uyv) * (((((-7.0) * dxuy) * uT) + (((2.0 * dtux) * uyv) * (3.0 + (2.0 * (uyv * uyv))))) + ((dyux * uT) * (3.0 + (4.0 * (uyv * uyv))))))) + (((uxv * uxv) * uxv) * ((((((10.0 * dtuy) * tau) * uyv) + (((4.0 * dtuy) * tau) * ((uyv * uyv) * uyv))) + (((3.0 * dyuy) * tau) * uT)) + ((uyv * uyv) * ((2.0 - (((4.0 * dxux) * tau) * uT)) + (((4.0 * dyuy) * tau) * uT)))))) + (uxv * (((((((6.0 * dtuy) * tau) * uyv) + (((4.0 * dtuy) * tau) * ((uyv * uyv) * uyv))) + (2.0 * o_pow4(uyv))) + (((3.0 * dyuy) * tau) * uT)) + ((uyv * uyv) * ((2.0 - (((3.0 * dxux) * tau) * uT)) + (((4.0 * dyuy) * tau) * uT)))))))) + (nux * (((((((2.0 * o_pow4(uxv)) * uyv) * ((-1.0) + (((2.0 * dtuy) * tau) * uyv))) - (((((3.0 * dxux) * tau) * uyv) * (1.0 + (uyv * uyv))) * uT)) - ((((4.0 * tau) * ((uxv * uxv) * uxv)) * uyv) * ((dtux + (dtux * (uyv * uyv))) - ((dxuy * uyv) * uT)))) + (((uxv * uxv) * uyv) * ((((((-2.0) + (((6.0 * dtuy) * tau) * uyv)) + (((4.0 * dtuy) * tau) * ((uyv * uyv) * uyv))) - (((4.0 * dxux) * tau) * uT)) + (((3.0 * dyuy) * tau) * uT)) + ((uyv * uyv) * (((-2.0) - (((4.0 * dxux) * tau) * uT)) + (((4.0 * dyuy) * tau) * uT)))))) - ((tau * uxv) * (((dyux * uT) * ((3.0 + (7.0 * (uyv * uyv))) + (4.0 * o_pow4(uyv)))) + (uyv * ((((6.0 * dtux) + ((10.0 * dtux) * (uyv * uyv))) + ((4.0 * dtux) * o_pow4(uyv))) - (((3.0 * dxuy) * uyv) * uT)))))))) / ((6.0 * tau) * o_pow15(((1.0 + (uxv * uxv)) + (uyv * uyv)))));
+  const double syy = (((((tau * ((1.0 + (uxv * uxv)) + (uyv * uyv))) * ((((((((-(dtnx * uxv)) + ((2.0 * dtny) * uyv)) + (((3.0 * dtny) * (uxv * uxv)) * uyv)) - ((dtnx * uxv) * (uyv * uyv))) + ((2.0 * dtny) * ((uyv * uyv) * uyv))) + ((((3.0 * dxny) * uxv) * uyv) * uT)) - ((dxnx * (1.0 + (uyv * uyv))) * uT)) + (((2.0 * dyny) * (1.0 + (uyv * uyv))) * uT))) + (nux * ((((((uxv * uxv) * uxv) * ((((-1.0) - ((dtuy * tau) * uyv)) - (uyv * uyv)) + (((2.0 * dtuy) * tau) * ((uyv * uyv) * uyv)))) - ((((2.0 * tau) * uyv) * ((1.0 + (uyv * uyv)) * (1.0 + (uyv * uyv)))) * ((dtux * uyv) + (dyux * uT)))) - (((tau * (uxv * uxv)) * ((-1.0) + (2.0 * (uyv * uyv)))) * ((dtux + (dtux * (uyv * uyv))) - ((dxuy * uyv) * uT)))) + ((uxv * (1.0 + (uyv * uyv))) * ((((-1.0) + (((2.0 * dtuy) * tau) * ((uyv * uyv) * uyv))) + ((dxux * tau) * uT)) + ((uyv * uyv) * (((-1.0) - (((2.0 * dxux) * tau) * uT)) + (((2.0 * dyuy) * tau) * uT)))))))) + (nuy * ((((((((-1.0) + (((2.0 * dtux) * tau) * uxv)) * o_pow5(uyv)) + (((tau * uxv) * (1.0 + (uxv * uxv))) * ((dtuy * uxv) + (dxuy * uT)))) + (((2.0 * tau) * o_pow4(uyv)) * (((-dtuy) - (dtuy * (uxv * uxv))) + ((dyux * uxv) * uT)))) - (((2.0 * tau) * (uyv * uyv)) * ((((dtuy + ((2.0 * dtuy) * (uxv * uxv))) + (dtuy * o_pow4(uxv))) + (((dxuy - dyux) * uxv) * uT)) + ((dxuy * ((uxv * uxv) * uxv)) * uT)))) + (((uyv * uyv) * uyv) * ((((((2.0 * dtux) * tau) * uxv) + (((2.0 * dtux) * tau) * ((uxv * uxv) * uxv))) + ((uxv * uxv) * (((-1.0) + (((2.0 * dxux) * tau) * uT)) - (((2.0 * dyuy) * tau) * uT)))) - (2.0 * (1.0 + ((dyuy * tau) * uT)))))) - (uyv * (((1.0 + ((dtux * tau) * ((uxv * uxv) * uxv))) + (((2.0 * dyuy) * tau) * uT)) + ((uxv * uxv) * ((1.0 + ((dxux * tau) * uT)) + (((2.0 * dyuy) * tau) * uT)))))))) / ((3.0 * tau) * o_pow15(((1.0 + (uxv * uxv)) + (uyv * uyv)))));
+  const double seta = (((((((((-dxnx) - dyny) + ((((dtux * uxv) + (dtuy * uyv)) * ((nux * uxv) + (nuy * uyv))) / o_pow15(((1.0 + (uxv * uxv)) + (uyv * uyv))))) - (((((dtux * nux) + (dtuy * nuy)) + (dtnx * uxv)) + (dtny * uyv)) / uT)) + ((2.0 * ((nux * uxv) + (nuy * uyv))) / (tau * uT))) + (nux * (((dxux * uxv) + (dyux * uyv)) + (dtux * uT)))) + (nuy * (((dxuy * uxv) + (dyuy * uyv)) + (dtuy * uT)))) - ((((nux * uxv) + (nuy * uyv)) * (((dxux * (uxv * uxv)) + (uxv * (((dxuy + dyux) * uyv) + (dtux * uT)))) + (uyv * ((dyuy * uyv) + (dtuy * uT))))) / ((1.0 + (uxv * uxv)) + (uyv * uyv)))) / 3.0);
+  *oxx = sxx; *oxy = sxy; *oyy = syy; *oeta = seta;
+}
+
+/* rank1_traceless_2d, src2d/hq_consistent_m2_2d.jl:225-234: A^<i B^j> for two u-orthogonal transverse vectors */
+static void rank1_traceless(double Ax, double Ay, double Bx, double By, double ux, double uy, double ut,
+                            double* qxx, double* qxy, double* qyy) {
+  double u2 = ut * ut;
+  double tr = ((Ay * ((By + (By * (ux * ux))) - ((Bx * ux) * uy))) + (Ax * ((Bx - ((By * ux) * uy)) + (Bx * (uy * uy))))) / u2;
+  *qxx = (Ax * Bx) - (((1.0 + (ux * ux)) * tr) / 3.0);
+  *qyy = (Ay * By) - (((1.0 + (uy * uy)) * tr) / 3.0);
+  *qxy = (((Ay * Bx) + (Ax * By)) / 2.0) - (((ux * uy) * tr) / 3.0);
+}
+
+/* consistent_m2_source_2d, src2d/hq_consistent_m2_2d.jl:247-404: d_tau of (pQxx, pQxy, pQyy, PiQ) and geo, each
+ * term behind its Terms switch. a[] holds the 44 positional arguments in order. */
+enum {
+  M2_UX, M2_UY, M2_UT, M2_TAU, M2_T, M2_DXT, M2_DYT, M2_DTT, M2_NUX, M2_NUY, M2_PXX, M2_PXY, M2_PYY, M2_PETA,
+  M2_PIQ, M2_DTA, M2_DXA, M2_DYA, M2_THNU, M2_ANUX, M2_ANUY, M2_DTNUX, M2_DTNUY, M2_DXNUX, M2_DXNUY, M2_DYNUX,
+  M2_DYNUY, M2_TH, M2_AX, M2_AY, M2_DTUX, M2_DTUY, M2_DXUX, M2_DXUY, M2_DYUX, M2_DYUY, M2_N, M2_TN, M2_DS, M2_H,
+  M2_HP, M2_TM, M2_ETAM, M2_M, M2_NARG
+};
+static void consistent_m2_source(const double* a, uint32_t t, double* out) {
+  const double ux = a[M2_UX], uy = a[M2_UY], ut = a[M2_UT], tau = a[M2_TAU];
+  const double Tm = o_max(a[M2_T], T_MIN);
+  const double tM = a[M2_TM];
+  if (!(tM > 0.0)) { for (int j = 0; j < 5; ++j) out[j] = 0.0; return; }
+  const double nux = a[M2_NUX], nuy = a[M2_NUY];
+  const double pxx = a[M2_PXX], pxy = a[M2_PXY], pyy = a[M2_PYY], peta = a[M2_PETA], PiQ = a[M2_PIQ];
+  const double th = a[M2_TH], ax = a[M2_AX], ay = a[M2_AY];
+  const double Ds = a[M2_DS], h = a[M2_H], hp = a[M2_HP];
+  const double etaQ = a[M2_ETAM];
+  const double zetaQ = (5.0 / 3.0) * etaQ;
+  const M2Coeffs cf = hq_m2_coeffs(Tm, a[M2_N], a[M2_TN], Ds, h, a[M2_M]);
+  /* the medium's shear at unit viscosity: ns_shear_target_2d(..., -1/2) */
+  const Kin k{th, ax, ay, 0.0, a[M2_DXUX], a[M2_DXUY], a[M2_DYUX], a[M2_DYUY]};
+  double sxx_, sxy_, syy_, seta_;
+  ns_shear_target(ux, uy, ut, tau, k, -0.5, &sxx_, &sxy_, &syy_, &seta_);
+  const double anudot = ((ax * nux) + (ay * nuy)) - ((((ax * ux) + (ay * uy)) * ((nux * ux) + (nuy * uy))) / (ut * ut));
+  double snxx, snxy, snyy, sneta;
+  sigma_nu(ux, uy, ut, tau, nux, nuy, a[M2_DTNUX], a[M2_DXNUX], a[M2_DYNUX], a[M2_DTNUY], a[M2_DXNUY],
+           a[M2_DYNUY], a[M2_DTUX], a[M2_DXUX], a[M2_DYUX], a[M2_DTUY], a[M2_DXUY], a[M2_DYUY], &snxx, &snxy,
+           &snyy, &sneta);
+  const double DT = ((ut * a[M2_DTT]) + (ux * a[M2_DXT])) + (uy * a[M2_DYT]);
+  const double DlnT = DT / Tm;
+  const double DlnC = cf.dlnC * DlnT;
+  const double Da = ((ut * a[M2_DTA]) + (ux * a[M2_DXA])) + (uy * a[M2_DYA]);
+  const double geo = (t & FIVO_TERM_M2_EXPANSION) ? tM * (((5.0 / 3.0) * th) + DlnC) : 0.0;
+  double ps, cxx, cxy, cyy;
+  pi_sigma(ux, uy, pxx, pxy, pyy, peta, sxx_, sxy_, syy_, seta_, &ps, &cxx, &cxy, &cyy);
+  const double gTx = (h + (Tm * hp)) * (a[M2_DXT] + (ux * DT));
+  const double gTy = (h + (Tm * hp)) * (a[M2_DYT] + (uy * DT));
+  double qaxx, qaxy, qayy, qgxx, qgxy, qgyy;
+  rank1_traceless(ax, ay, nux, nuy, ux, uy, ut, &qaxx, &qaxy, &qayy);
+  rank1_traceless(nux, nuy, gTx, gTy, ux, uy, ut, &qgxx, &qgxy, &qgyy);
+  const bool ia = t & FIVO_TERM_M2_ACCEL_NU, ig = t & FIVO_TERM_M2_NU_GRADTH;
+  const double qxx = (ia ? (2.0 * cf.lama) * qaxx : 0.0) + (ig ? (Ds / Tm) * qgxx : 0.0);
+  const double qyy = (ia ? (2.0 * cf.lama) * qayy : 0.0) + (ig ? (Ds / Tm) * qgyy : 0.0);
+  const double qxy = (ia ? (2.0 * cf.lama) * qaxy : 0.0) + (ig ? (Ds / Tm) * qgxy : 0.0);
+  const bool i1 = t & FIVO_TERM_M2_NU_GRADIENT, i2 = t & FIVO_TERM_M2_BG_GRADU;
+  const bool i3 = t & FIVO_TERM_M2_PI_SIGMA, i4 = t & FIVO_TERM_M2_PIQ_SIGMA;
+  double sxx = ((((((pxx + (i1 ? (2.0 * etaQ) * snxx : 0.0)) + (geo * pxx)) +
+                  (i3 ? (2.0 * tM) * (cxx - (((1.0 + (ux * ux)) * ps) / 3.0)) : 0.0)) +
+                 (i4 ? ((2.0 * tM) * PiQ) * sxx_ : 0.0)) + (i2 ? (2.0 * cf.etabar) * sxx_ : 0.0)) + qxx);
+  double syy = ((((((pyy + (i1 ? (2.0 * etaQ) * snyy : 0.0)) + (geo * pyy)) +
+                  (i3 ? (2.0 * tM) * (cyy - (((1.0 + (uy * uy)) * ps) / 3.0)) : 0.0)) +
+                 (i4 ? ((2.0 * tM) * PiQ) * syy_ : 0.0)) + (i2 ? (2.0 * cf.etabar) * syy_ : 0.0)) + qyy);
+  double sxy = ((((((pxy + (i1 ? (2.0 * etaQ) * snxy : 0.0)) + (geo * pxy)) +
+                  (i3 ? (2.0 * tM) * (cxy - (((ux * uy) * ps) / 3.0)) : 0.0)) +
+                 (i4 ? ((2.0 * tM) * PiQ) * sxy_ : 0.0)) + (i2 ? (2.0 * cf.etabar) * sxy_ : 0.0)) + qxy);
+  if (t & FIVO_TERM_M2_VORTICITY) {
+    double wxx, wxy, wyy;
+    vorticity_coupling(ux, uy, ut, tau, pxx, pxy, pyy, peta, ax, ay, a[M2_DTUX], a[M2_DTUY], a[M2_DXUX],
+                       a[M2_DXUY], a[M2_DYUX], a[M2_DYUY], &wxx, &wxy, &wyy);
+    sxx += tM * wxx; sxy += tM * wxy; syy += tM * wyy;
+  }
+  if (t & FIVO_TERM_M2_PROJECTOR) {
+    const double at = ((ux * ax) + (uy * ay)) / ut;
+    const PiC Q = shear_tensor(ux, uy, ut, tau, pxx, pxy, pyy, peta);
+    const double cx = (((-Q.tx) * at) + (Q.xx * ax)) + (Q.xy * ay);
+    const double cy = (((-Q.ty) * at) + (Q.xy * ax)) + (Q.yy * ay);
+    sxx -= tM * ((2.0 * ux) * cx);
+    sxy -= tM * ((ux * cy) + (uy * cx));
+    syy -= tM * ((2.0 * uy) * cy);
+  }
+  const double sB =
+      (((((((PiQ + (i1 ? zetaQ * a[M2_THNU] : 0.0)) + (geo * PiQ)) + (i3 ? ((2.0 / 3.0) * tM) * ps : 0.0)) +
+          (cf.etabar * (((t & FIVO_TERM_M2_BG_DLNT) ? cf.ABr * DlnT : 0.0) + (i2 ? (5.0 / 3.0) * th : 0.0)))) +
+         (ia ? ((Ds * cf.Aco) / (3.0 * Tm)) * anudot : 0.0)) +
+        (ig ? ((5.0 / 6.0) * (Ds / Tm)) *
+                  (((nux * gTx) + (nuy * gTy)) - ((((nux * ux) + (nuy * uy)) * ((gTx * ux) + (gTy * uy))) / (ut * ut)))
+            : 0.0)) +
+       ((t & FIVO_TERM_M2_BG_DALPHA) ? cf.etabar * Da : 0.0));
+  const double den = tM * ut;
+  out[0] = (-sxx) / den; out[1] = (-sxy) / den; out[2] = (-syy) / den; out[3] = (-sB) / den; out[4] = geo;
+}
+
+/* the second moment's pieces with plain arguments, for the gate tests */
+void m2_source(const double* in44, uint32_t terms, double* out5) { consistent_m2_source(in44, terms, out5); }
+void m2_coeffs(double T, double n, double tn, double Ds, double h, double m, double* out5) {
+  M2Coeffs c = hq_m2_coeffs(T, n, tn, Ds, h, m);
+  out5[0] = c.dlnC; out5[1] = c.etabar; out5[2] = c.lama; out5[3] = c.Aco; out5[4] = c.ABr;
+}
+double m2_tauM(double T, double tn, double m) { return tauM_charm(T, tn, m); }
+void m2_sigma_nu(const double* a, double* out4) {
+  sigma_nu(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8], a[9], a[10], a[11], a[12], a[13], a[14], a[15],
+           a[16], a[17], &out4[0], &out4[1], &out4[2], &out4[3]);
+}
+void m2_rank1_traceless(const double* a, double* out3) {
+  rank1_traceless(a[0], a[1], a[2], a[3], a[4], a[5], a[6], &out3[0], &out3[1], &out3[2]);
+}
+
 /* relax_dissipative_2d! and the per-cell sector updates, src2d/dissipation2d.jl:293-705 */
 int64_t relax_dissipative_2d(double* U, const Grid& g, double tau, double D, const Model& m, Work& w) {
   const Layout& L = m.L;
@@ -1671,10 +1815,81 @@ int64_t relax_dissipative_2d(double* U, const Grid& g, double tau, double D, con
           if (mag > cap && mag > TINY) { double sc = cap / mag; nux *= sc; nuy *= sc; }
         }
         u[L.iNux] = nux; u[L.iNuy] = nuy;
+        /* ---- the charm second moment: relax_charm_m2_cell_2d!, :722-888 (given the
+         * ramped tau_n and the relaxed current of this cell) ---- */
+        if (p.consistent_m2 && L.hasM2) {
+          double pQxx = u[L.iPQxx], pQxy = u[L.iPQxy], pQyy = u[L.iPQyy], pQeta = u[L.iPQeta];
+          double PiQv = u[L.iPiQ];
+          const double mq = p.transport_mass > 0.0 ? p.transport_mass : p.m_hq;
+          const double tMq = tauM_charm(T, tn, mq);
+          const bool have_hist = o_isfinite(w.alpha_prev[i]) && o_isfinite(w.T_prev[i]);
+          if (tMq > 0.0 && have_hist) {
+            const double dtnx = o_isfinite(w.nux_prev[i]) ? (nux - w.nux_prev[i]) / D : 0.0;
+            const double dtny = o_isfinite(w.nuy_prev[i]) ? (nuy - w.nuy_prev[i]) / D : 0.0;
+            const int64_t ixm = i - g.Nytot, ixp = i + g.Nytot;
+            const double dxnx = ((Q[ixp * nv + L.iNux] - Q[ixm * nv + L.iNux]) * 0.5) * invdx;
+            const double dxny = ((Q[ixp * nv + L.iNuy] - Q[ixm * nv + L.iNuy]) * 0.5) * invdx;
+            const double dynx = ((Q[(i + 1) * nv + L.iNux] - Q[(i - 1) * nv + L.iNux]) * 0.5) * invdy;
+            const double dyny = ((Q[(i + 1) * nv + L.iNuy] - Q[(i - 1) * nv + L.iNuy]) * 0.5) * invdy;
+            const double dtux2 = o_isfinite(w.ux_prev[i]) ? (ux - w.ux_prev[i]) / D : 0.0;
+            const double dtuy2 = o_isfinite(w.uy_prev[i]) ? (uy - w.uy_prev[i]) / D : 0.0;
+            const double anx = ((ut * dtnx) + (ux * dxnx)) + (uy * dynx);
+            const double any2 = ((ut * dtny) + (ux * dxny)) + (uy * dyny);
+            const double nut2 = nu_tau(ux, uy, ut, nux, nuy);
+            const double thnu = ((((((((ux * dtnx) + (uy * dtny)) + (nux * dtux2)) + (nuy * dtuy2)) * safe_inv(ut)) -
+                                   ((nut2 * ((ux * dtux2) + (uy * dtuy2))) * safe_inv(ut * ut))) + dxnx) + dyny) +
+                                (nut2 * safe_inv(tau));
+            const double Tp2 = w.T_prev[i];
+            const double dtT2 = o_isfinite(Tp2) ? (T - Tp2) / D : 0.0;
+            const double dxT2 = ((o_exp(w.yT[ixp]) - o_exp(w.yT[ixm])) * 0.5) * invdx;
+            const double dyT2 = ((o_exp(w.yT[i + 1]) - o_exp(w.yT[i - 1])) * 0.5) * invdy;
+            double h2, hp2;
+            hq_h_hprime(T, p, &h2, &hp2);
+            const double Ds2 = safe_div(p.kappa_coeff, T) / FMGEV;
+            double a[M2_NARG] = {ux, uy, ut, tau, T, dxT2, dyT2, dtT2, nux, nuy, pQxx, pQxy, pQyy, pQeta, PiQv,
+                                 dta, dxa, dya, thnu, anx, any2, dtnx, dtny, dxnx, dxny, dynx, dyny,
+                                 k.th, k.ax, k.ay, dtux2, dtuy2, k.dxux, k.dxuy, k.dyux, k.dyuy,
+                                 n, tn, Ds2, h2, hp2, tMq, etaM_charm(T, tn), mq};
+            double s0[5], s1[5];
+            consistent_m2_source(a, p.terms, s0);
+            const double A2 = safe_div(tMq * ut, D);
+            const double dp = 1e-7 * o_max(o_max(o_max(o_max(1.0, std::fabs(pQxx)), std::fabs(pQxy)), std::fabs(pQyy)),
+                                           std::fabs(PiQv));
+            /* one perturbed evaluation per channel: the slope of each row in its own field */
+            double c[4];
+            const int slot[4] = {M2_PXX, M2_PXY, M2_PYY, M2_PIQ};
+            for (int j = 0; j < 4; ++j) {
+              const double keep = a[slot[j]];
+              a[slot[j]] = keep + dp;
+              consistent_m2_source(a, p.terms, s1);
+              a[slot[j]] = keep;
+              c[j] = (((-(s1[j] - s0[j])) / dp) * tMq) * ut;
+            }
+            auto dn = [&](double cc) { return o_max(A2 + cc, 0.5 * (A2 + 1.0)); };
+            const bool ram = p.relax_advect_m2 != 0;
+            const double amxx = ram ? (-tMq) * upw(L.iPQxx, i, ux, uy) : 0.0;
+            const double amxy = ram ? (-tMq) * upw(L.iPQxy, i, ux, uy) : 0.0;
+            const double amyy = ram ? (-tMq) * upw(L.iPQyy, i, ux, uy) : 0.0;
+            const double amB = ram ? (-tMq) * upw(L.iPiQ, i, ux, uy) : 0.0;
+            const double Rxx = ((((-tMq) * ut) * s0[0]) - (c[0] * pQxx)) - amxx;
+            const double Rxy = ((((-tMq) * ut) * s0[1]) - (c[1] * pQxy)) - amxy;
+            const double Ryy = ((((-tMq) * ut) * s0[2]) - (c[2] * pQyy)) - amyy;
+            const double RB = ((((-tMq) * ut) * s0[3]) - (c[3] * PiQv)) - amB;
+            pQxx = ((A2 * pQxx) - Rxx) / dn(c[0]);
+            pQxy = ((A2 * pQxy) - Rxy) / dn(c[1]);
+            pQyy = ((A2 * pQyy) - Ryy) / dn(c[2]);
+            PiQv = ((A2 * PiQv) - RB) / dn(c[3]);
+            pQeta = project_traceless(ux, uy, ut, pQxx, pQxy, pQyy);
+            u[L.iPQxx] = pQxx; u[L.iPQxy] = pQxy; u[L.iPQyy] = pQyy; u[L.iPQeta] = pQeta; u[L.iPiQ] = PiQv;
+          }
+        }
       }
     }
   w.ux_prev = w.ux;
   w.uy_prev = w.uy;
+  /* the current's history for the second moment's d_tau nu, :354-359 */
+  if (p.consistent_m2 && L.hasNu)
+    for (int64_t j = 0; j < g.Ntot; ++j) { w.nux_prev[j] = U[j * nv + L.iNux]; w.nuy_prev[j] = U[j * nv + L.iNuy]; }
   return (int64_t)g.Nx * g.Ny;
 }
 
@@ -1760,6 +1975,7 @@ void run_sim_2d(double* U, const Grid& g, const Model& m, Work& w, double tau0, 
     std::fill(w.x0_ux.begin(), w.x0_ux.end(), O_NAN); std::fill(w.x0_uy.begin(), w.x0_uy.end(), O_NAN);
     std::fill(w.ux_prev.begin(), w.ux_prev.end(), O_NAN); std::fill(w.uy_prev.begin(), w.uy_prev.end(), O_NAN);
     std::fill(w.alpha_prev.begin(), w.alpha_prev.end(), O_NAN); std::fill(w.T_prev.begin(), w.T_prev.end(), O_NAN);
+    std::fill(w.nux_prev.begin(), w.nux_prev.end(), O_NAN); std::fill(w.nuy_prev.begin(), w.nuy_prev.end(), O_NAN);
   }
   rhs_2d(w.k.data(), U, g, tau0, m, w, bc, E_FLOOR, nullptr);
   double Qin = 0.0;

@@ -68,6 +68,7 @@ struct Layout {               /* src2d/state_layout2d.jl:23-84 (0-based rows) */
   bool hasNu; int iNux, iNuy;
   bool hasPi; int iPi;
   bool hasShear; int iPixx, iPixy, iPiyy, iPieta;
+  bool hasM2; int iPQxx, iPQxy, iPQyy, iPQeta, iPiQ;
 };
 
 struct EOSCache {             /* src2d/primrec2d.jl:115-130 */
@@ -94,6 +95,7 @@ struct Work {                 /* src2d/work2d.jl:15-139 */
   std::vector<uint8_t> ok;
   std::vector<double> x0_yT, x0_phi, x0_ux, x0_uy;
   std::vector<double> ux_prev, uy_prev, alpha_prev, T_prev;
+  std::vector<double> nux_prev, nuy_prev;                      /* the charm second moment's d_tau nu */
   std::vector<double> sigx, sigy, ULpx, URpx, ULpy, URpy;      /* 4 x Ntot */
   std::vector<double> ULcx, URcx, ULcy, URcy, Fhx, Fhy, S, diss_snap, k, U1, U2;  /* nv x Ntot */
   std::vector<uint8_t> bad, bad_tmp;
@@ -162,6 +164,15 @@ void cell_ns_diffusion_target(double ux, double uy, double ut, double dxa, doubl
 void cell_pi_sigma(const double* in10, double* out4);
 void cell_shear_tensor(double ux, double uy, double ut, double tau, double pixx, double pixy, double piyy,
                        double pieta, double* out7);
+
+/* the consistent charm second moment (src2d/hq_consistent_m2_2d.jl), for the gate tests:
+ * in[44] = the 44 positional arguments of consistent_m2_source_2d in their order;
+ * out[5] = (dpxx, dpxy, dpyy, dPiQ, geo) */
+void m2_source(const double* in44, uint32_t terms, double* out5);
+void m2_coeffs(double T, double n, double tn, double Ds, double h, double m, double* out5);
+double m2_tauM(double T, double tn, double m);
+void m2_sigma_nu(const double* in18, double* out4);
+void m2_rank1_traceless(const double* in7, double* out3);
 
 }  // namespace orc
 #endif

@@ -15,6 +15,10 @@
  *                              coefficient closures of test/test_dnmr2d.jl:47-60
  *   oracle_ref_gubser_viscous  G1v: test/test_gubser_viscous2d.jl:78-102
  *                              (= gubser_viscous, test/analytic_referees.jl:141-152)
+ *   oracle_ref_m2_rhs_1d       Gm1: the 1+1D second moment on its transported triad,
+ *                              hq_consistent_m2_rhs (src/hq_consistent_m2.jl:138-252),
+ *                              all terms on; the 2+1D tensor source must reduce to it
+ *                              (test/test_consistent_m22d.jl:85-198)
  */
 #include <cmath>
 #include <vector>
@@ -207,6 +211,56 @@ void oracle_ref_gubser_viscous(double etas, double TH0, double rhomin, double rh
 }
 
 /* ---- cell-level functions of the relaxation (the oracle's own code paths) ---- */
+/* Gm1's referee. in[27] = (tau, r, ur, T, dtT, drT, drur, dtur, p_l, p_phi, PiQ, nu,
+ * dtalpha, dralpha, dtnu, drnu, drp_l, drp_phi, drPiQ, n, tau_n, Ds, h, hp, tau_M, eta_M, m);
+ * out[3] = (dp_l, dp_phi, dPiQ) / dtau. The coefficient closed forms are the 2+1D
+ * ones (hq_m2_coeffs and hq_m2_coeffs_2d are the same expressions). */
+void oracle_ref_m2_rhs_1d(const double* in, double* out) {
+  const double tau = in[0], r = in[1], ur = in[2], T = in[3], dtT = in[4], drT = in[5], drur = in[6];
+  const double dtur = in[7], pl = in[8], pf = in[9], PiQ = in[10], nu = in[11], dta = in[12], dra = in[13];
+  const double dtnu = in[14], drnu = in[15], n = in[19], tn = in[20], Ds = in[21], h = in[22], hp = in[23];
+  const double tM = in[24], etaM = in[25], m = in[26];
+  const double Tm = std::fmax(T, 1e-20);
+  const double ut = std::sqrt(1.0 + ur * ur);
+  if (!(tM > 0.0 && r > 0.0)) { out[0] = out[1] = out[2] = 0.0; return; }
+  const double peta = -(pl + pf);
+  /* background kinematics on the triad (l, phi, eta) */
+  const double Dlur = ur * dtur + ut * drur;
+  const double thl = Dlur / ut, thf = ur / r, the = ut / tau;
+  const double th = thl + thf + the;
+  const double sl = thl - th / 3.0, sf = thf - th / 3.0, se = the - th / 3.0;
+  const double al = (ut * dtur + ur * drur) / ut;
+  const double nul = nu / ut;
+  /* the current's gradient on the triad */
+  const double Dlnu = ur * dtnu + ut * drnu;
+  const double gll = Dlnu / ut - ur * nu * Dlur / (ut * ut * ut);
+  const double gff = nu / r;
+  const double anu = al * nul;
+  const double thnu = (ur / ut) * dtnu + nu * dtur / (ut * ut * ut) + drnu + ur * nu / (ut * tau) + nu / r;
+  const double trnu = thnu - anu;
+  const double snl = gll - trnu / 3.0, snf = gff - trnu / 3.0;
+  const double etaQ = etaM, zetaQ = (5.0 / 3.0) * etaQ;
+  double cf[5];
+  m2_coeffs(Tm, n, tn, Ds, h, m, cf);   /* dlnC, etabar, lambda_a, A, A/B */
+  const double DlnT = (ut * dtT + ur * drT) / Tm;
+  const double DlnC = cf[0] * DlnT;
+  const double DlTh = (h + Tm * hp) * (ur * dtT + ut * drT);
+  const double ps = pl * sl + pf * sf + peta * se;
+  const double geo = tM * ((5.0 / 3.0) * th + DlnC);
+  const double rank1 = 2.0 * cf[2] * al * nul + (Ds / Tm) * nul * DlTh;
+  const double srcl = pl + 2.0 * etaQ * snl + geo * pl + 2.0 * tM * (pl * sl - ps / 3.0) + 2.0 * tM * PiQ * sl +
+                      2.0 * cf[1] * sl + rank1 * (2.0 / 3.0);
+  const double srcf = pf + 2.0 * etaQ * snf + geo * pf + 2.0 * tM * (pf * sf - ps / 3.0) + 2.0 * tM * PiQ * sf +
+                      2.0 * cf[1] * sf + rank1 * (-1.0 / 3.0);
+  double srcB = PiQ + zetaQ * thnu + geo * PiQ + (2.0 / 3.0) * tM * ps + cf[1] * (cf[4] * DlnT + (5.0 / 3.0) * th) +
+                (Ds * cf[3] / (3.0 * Tm)) * anu + (5.0 / 6.0) * (Ds / Tm) * nul * DlTh;
+  srcB += cf[1] * (ut * dta + ur * dra);
+  const double den = tM * ut;
+  out[0] = -(tM * ur * in[16] + srcl) / den;
+  out[1] = -(tM * ur * in[17] + srcf) / den;
+  out[2] = -(tM * ur * in[18] + srcB) / den;
+}
+
 void oracle_shear_coeffs(const fivo_params* p, double T, double mu, double n, double e, double P, double* out3) {
   cell_shear_coeffs(T, mu, n, e, P, *p, out3);
 }

@@ -100,6 +100,14 @@ def lib():
             "oracle_ns_diffusion_target": (None, [C.c_int64, _D, _D]),
             "oracle_pi_sigma": (None, [C.c_int64, _D, _D]),
             "oracle_shear_tensor": (None, [C.c_int64, _D, _D]),
+            "oracle_set_nu_history": (None, [C.c_void_p, _D, _D]),
+            "oracle_get_nu_history": (None, [C.c_void_p, _D, _D]),
+            "oracle_m2_source": (None, [_D, C.c_uint32, _D]),
+            "oracle_m2_coeffs": (None, [C.c_double] * 6 + [_D]),
+            "oracle_m2_tauM": (C.c_double, [C.c_double] * 3),
+            "oracle_m2_sigma_nu": (None, [_D, _D]),
+            "oracle_m2_rank1_traceless": (None, [_D, _D]),
+            "oracle_ref_m2_rhs_1d": (None, [_D, _D]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -205,6 +213,15 @@ class OracleSolver:
     def reset_history(self):
         lib().oracle_reset_history(self.h)
 
+    def set_nu_history(self, nux_prev=None, nuy_prev=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (nux_prev, nuy_prev)]
+        lib().oracle_set_nu_history(self.h, *[_ptr(a) for a in arrs])
+
+    def get_nu_history(self):
+        arrs = [np.empty(self.N), np.empty(self.N)]
+        lib().oracle_get_nu_history(self.h, *[_ptr(a) for a in arrs])
+        return dict(nux_prev=arrs[0], nuy_prev=arrs[1])
+
     def primitives(self):
         names = ("yT", "phi", "mu", "alpha", "ux", "uy", "P", "n", "e")
         arrs = [np.empty(self.N) for _ in names]
@@ -291,6 +308,56 @@ def pi_sigma(rows10):
 
 def shear_tensor(rows8):
     return _rows(lib().oracle_shear_tensor, rows8, 7)
+
+
+# consistent_m2_source_2d's 44 positional arguments, in order (src2d/hq_consistent_m2_2d.jl:247-262)
+M2_ARGS = ("ux", "uy", "ut", "tau", "T", "dxT", "dyT", "dtT", "nux", "nuy", "pxx", "pxy", "pyy", "peta", "PiQ",
+           "dta", "dxa", "dya", "thnu", "anux", "anuy", "dtnux", "dtnuy", "dxnux", "dxnuy", "dynux", "dynuy",
+           "th", "ax", "ay", "dtux", "dtuy", "dxux", "dxuy", "dyux", "dyuy", "n", "tn", "Ds", "h", "hp", "tM",
+           "etaM", "m")
+
+
+def m2_source(args, terms=A.FIVO_TERMS_DEFAULT):
+    """consistent_m2_source_2d: a dict (or sequence) of the 44 arguments -> (dpxx, dpxy, dpyy, dPiQ, geo)"""
+    a = np.array([args[k] for k in M2_ARGS] if isinstance(args, dict) else args, dtype=np.float64)
+    assert a.size == 44
+    out = np.empty(5)
+    lib().oracle_m2_source(_ptr(a), terms, _ptr(out))
+    return out
+
+
+def m2_coeffs(T, n, tn, Ds, h, m):
+    out = np.empty(5)
+    lib().oracle_m2_coeffs(T, n, tn, Ds, h, m, _ptr(out))
+    return dict(zip(("dlnC_dlnT", "etabar", "lambda_a", "Aco", "ABr"), out))
+
+
+def m2_tauM(T, tn, m=1.5):
+    return lib().oracle_m2_tauM(T, tn, m)
+
+
+def m2_sigma_nu(*a18):
+    a = np.array(a18, dtype=np.float64)
+    out = np.empty(4)
+    lib().oracle_m2_sigma_nu(_ptr(a), _ptr(out))
+    return out
+
+
+def m2_rank1_traceless(*a7):
+    a = np.array(a7, dtype=np.float64)
+    out = np.empty(3)
+    lib().oracle_m2_rank1_traceless(_ptr(a), _ptr(out))
+    return out
+
+
+def ref_m2_rhs_1d(**kw):
+    """hq_consistent_m2_rhs (src/hq_consistent_m2.jl:138-252), all terms on -> (dp_l, dp_phi, dPiQ)"""
+    names = ("tau", "r", "ur", "T", "dtT", "drT", "drur", "dtur", "p_l", "p_phi", "PiQ", "nu", "dta", "dra",
+             "dtnu", "drnu", "drp_l", "drp_phi", "drPiQ", "n", "tn", "Ds", "h", "hp", "tM", "etaM", "m")
+    a = np.array([kw.get(k, 0.0) for k in names], dtype=np.float64)
+    out = np.empty(3)
+    lib().oracle_ref_m2_rhs_1d(_ptr(a), _ptr(out))
+    return out
 
 
 def shear_coeffs(params, T, mu, n, e, P):

@@ -79,7 +79,7 @@ def test_config_refusals_are_status_codes(lib):
     base = fivo2d.build_model_2d(eos=fivo2d.LatticeHRGEOS()).params
     cases = []
     p = A.FivoParams.from_buffer_copy(base); p.consistent_fm = 1; p.tauN_coeff = 1.5; cases.append(p)
-    p = A.FivoParams.from_buffer_copy(base); p.consistent_m2 = 1; cases.append(p)
+    p = A.FivoParams.from_buffer_copy(base); p.terms = A.FIVO_TERMS_DEFAULT | A.TERM_BIT["m2_vorticity"]; cases.append(p)
     p = A.FivoParams.from_buffer_copy(base); p.terms = A.FIVO_TERMS_DEFAULT & ~A.TERM_BIT["fm_dlnh"]; cases.append(p)
     p = A.FivoParams.from_buffer_copy(base); p.terms = A.FIVO_TERMS_DEFAULT | A.TERM_BIT["shear_vorticity"]; cases.append(p)
     p = A.FivoParams.from_buffer_copy(base); p.terms = A.FIVO_TERMS_DEFAULT & ~A.TERM_BIT["nu_gradalpha"]; cases.append(p)

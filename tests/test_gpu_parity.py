@@ -149,6 +149,9 @@ def _assert_same_work(w, o, what=""):
         assert bits_equal(pw[k], po[k]), f"{what} primitive {k}: {where_differs(pw[k], po[k])}"
     assert np.array_equal(pw["ok"], po["ok"]), what
     hw, ho = w.get_history(), o.get_history()
+    if w.model.layout.hasM2:
+        hw.update(w.get_nu_history())
+        ho.update(o.get_nu_history())
     for k in hw:
         assert bits_equal(hw[k], ho[k]), f"{what} history {k}: {where_differs(hw[k], ho[k])}"
     Uw, Uo = w.get_state(), o.get_state()

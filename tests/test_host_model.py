@@ -43,9 +43,13 @@ def test_layout_rows(charge, bulk, shear, nv):
     assert (L.hasNu, L.hasPi, L.hasShear) == (charge, bulk, shear)
 
 
-def test_layout_refuses_the_charm_second_moment():
-    with pytest.raises(NotImplementedError):
-        make_layout2d(with_m2=True)
+def test_layout_appends_the_charm_second_moment():
+    """make_layout2d(with_m2 = true) appends pQxx, pQxy, pQyy, pQeta, PiQ after the
+    medium's rows (src2d/state_layout2d.jl:61-84)"""
+    L = make_layout2d(with_m2=True)
+    assert L.names == ["Dtau", "Sx", "Sy", "E", "nux", "nuy", "Pi", "pixx", "pixy", "piyy", "pieta",
+                       "pQxx", "pQxy", "pQyy", "pQeta", "PiQ"]
+    assert L.hasM2 and L.nv == 16 and L.idx("PiQ") == 15
 
 
 def test_model_flattens_to_params():
@@ -80,8 +84,13 @@ def test_refusals_follow_the_reference():
         fivo2d.build_model_2d(terms={"fm_dlnh": False})           # its sector (consistent_fm) is off
     assert fivo2d.build_model_2d(consistent_fm=True, terms={"fm_dlnh": False}).params.terms & \
         A.TERM_BIT["fm_dlnh"] == 0
-    with pytest.raises((ValueError, NotImplementedError)):
-        fivo2d.build_model_2d(consistent_m2=True)
+    m2 = fivo2d.build_model_2d(enable_diff=True, consistent_m2=True)
+    assert m2.params.consistent_m2 == 1 and m2.nv == 6 + 5 and m2.layout.names[-5:] == \
+        ["pQxx", "pQxy", "pQyy", "pQeta", "PiQ"]
+    with pytest.raises(ValueError):
+        fivo2d.build_model_2d(terms={"m2_vorticity": True})       # its sector (consistent_m2) is off
+    assert fivo2d.build_model_2d(consistent_m2=True, terms={"m2_vorticity": True}).params.terms & \
+        A.TERM_BIT["m2_vorticity"]
     with pytest.raises(ValueError):
         fivo2d.build_model_2d(enable_bulk=True, bulk_model="triangular")
     with pytest.raises(ValueError):
