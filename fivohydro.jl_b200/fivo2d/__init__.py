@@ -6,8 +6,9 @@ of include/fivo2d.h, implemented by csrc/libfivo2d.so (CUDA, sm_100a).
 from .model import (Grid2D, make_grid2d, make_grid_2d, make_layout2d, ConformalHQEOS, LatticeHRGEOS,
                     build_model_2d, allocate_state, IdealDiffVisc2DModel, eos_params)
 from . import ic
+from .fields_io import save_fields, load_fields
 from ._abi import FivoError, load_library
 
 __all__ = ["Grid2D", "make_grid2d", "make_grid_2d", "make_layout2d", "ConformalHQEOS", "LatticeHRGEOS",
            "build_model_2d", "allocate_state", "IdealDiffVisc2DModel", "eos_params", "ic", "FivoError",
-           "load_library"]
+           "load_library", "save_fields", "load_fields"]

@@ -228,6 +228,32 @@ function run_sim_2d_gpu!(U::AbstractMatrix, g::Grid2D, model, work::GPUWork2D;
             minPtot = r.minPtot)
 end
 
+"""
+    fields_2d(g, U, work::GPUWork2D, model) -> NamedTuple
+
+The reference's readout (main2D.jl:588-600) from the device's primitives: the same
+NamedTuple (x, y, T, mu, alpha, n, e, P, ux, uy and every stored dissipative row by
+its layout name, in physical units), so the reference's own
+`save_fields(path, fields_2d(g, U, res.work, m); model = m)` writes it unchanged.
+"""
+function fields_2d(g::Grid2D, U::AbstractMatrix, work::GPUWork2D, model)
+    N = work.ntot
+    yT, φ, μ, α, ux, uy, P, n, e = (Vector{Float64}(undef, N) for _ in 1:9)
+    ok = Vector{UInt8}(undef, N)
+    fivocheck(ccall((:fivo_get_primitives, LIBFIVO2D), Cint,
+                    (Ptr{Cvoid}, Int64, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64},
+                     Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{UInt8}),
+                    work.h, N, yT, φ, μ, α, ux, uy, P, n, e, ok), "fivo_get_primitives")
+    L = model.layout; ng = g.nghost
+    ixs = (ng+1):(ng+g.Nx); iys = (ng+1):(ng+g.Ny)
+    grab(f) = [f(lin(g, ix, iy)) for ix in ixs, iy in iys]
+    prim = (x = g.xC[ixs], y = g.yC[iys],
+            T = grab(i -> exp(yT[i])), mu = grab(i -> μ[i]), alpha = grab(i -> α[i]), n = grab(i -> n[i]),
+            e = grab(i -> e[i]), P = grab(i -> P[i]), ux = grab(i -> ux[i]), uy = grab(i -> uy[i]))
+    diss = [s => grab(i -> phys_from_stored(U[L.idx[s], i])) for s in L.names[5:end]]
+    return merge(prim, NamedTuple(diss))
+end
+
 """Device checkpoint: `dst` continues bit for bit as `src` would (same grid and model)."""
 clone_state!(dst::GPUWork2D, src::GPUWork2D) =
     fivocheck(ccall((:fivo_ctx_clone_state, LIBFIVO2D), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), dst.h, src.h),

@@ -103,3 +103,27 @@ def test_rhs_rows_of_the_second_moment_are_zero(gpu_lib):
     assert not np.any(dw[:, m.layout.idx("pQxx"):].view(np.int64))
     w.close()
     o.close()
+
+
+def test_readout_and_record_of_a_device_run(gpu_lib, tmp_path):
+    """fields_2d (main2D.jl:588-600) of a device run carries the second moment's rows by
+    their layout names, equals the same readout of the oracle's run, and survives
+    save_fields / load_fields bit for bit"""
+    from fivo2d.solver import fields_2d
+    g = fivo2d.make_grid2d(48, 48, xmax=6.0, ymax=6.0)
+    m = fivo2d.build_model_2d(eos=fivo2d.LatticeHRGEOS(), enable_diff=True, kappa_coeff=0.2, consistent_fm=True,
+                              consistent_m2=True)
+    w, o = _pair(m, g, _gm5_state(g, m))
+    w.run(0.4, 0.6, 0.2, 0.05, A.FIVO_SSPRK2)
+    o.run(0.4, 0.6, 0.2, 0.05, A.FIVO_SSPRK2)
+    fw = fields_2d(g, w.get_state(), w, m)
+    fo = fields_2d(g, o.get_state(), o, m)
+    assert {"pQxx", "pQxy", "pQyy", "pQeta", "PiQ"} <= set(fw)
+    for k in fw:
+        assert bits_equal(fw[k], fo[k]), k
+    d = fivo2d.load_fields(fivo2d.save_fields(tmp_path / "f.npz", fw, model=m, meta={"tau": 0.6}))
+    for k in fw:
+        assert bits_equal(d["fields"][k], fw[k]), k
+    assert d["model_fields"]["consistent_m2"] == "True" and d["meta"]["tau"] == 0.6
+    w.close()
+    o.close()

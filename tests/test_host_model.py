@@ -144,3 +144,26 @@ def test_terms_switches_and_refusals():
         fivo2d.build_model_2d(terms={"no_such_term": True})
     with pytest.raises(ValueError):
         fivo2d.build_model_2d(terms=3.5)
+
+
+def test_save_fields_round_trip(tmp_path):
+    """save_fields / load_fields (src/fields_io.jl:70-106): the arrays come back
+    bit for bit with the record of the model that made them"""
+    g = fivo2d.make_grid2d(16, 12, xmax=2.0, ymax=1.5)
+    m = fivo2d.build_model_2d(enable_diff=True, enable_shear=True, consistent_fm=True, consistent_m2=True,
+                              terms={"m2_vorticity": True})
+    rng = np.random.default_rng(5)
+    f = {"x": g.xC[3:-3].copy(), "y": g.yC[3:-3].copy()}
+    for name in ["T", "mu", "alpha", "n", "e", "P", "ux", "uy"] + m.layout.names[4:]:
+        f[name] = rng.normal(size=(g.Nx, g.Ny))
+    path = fivo2d.save_fields(tmp_path / "run" / "fields.npz", f, model=m, meta={"event": 3, "note": "m2 on"})
+    d = fivo2d.load_fields(path)
+    assert set(d["fields"]) == set(f)
+    for k, v in f.items():
+        assert np.array_equal(d["fields"][k].view(np.int64), np.asarray(v).view(np.int64)), k
+    assert d["solver"] == "FiVo 2+1D"
+    assert d["terms"]["m2_vorticity"] is True and d["terms"]["shear_vorticity"] is False
+    assert d["model_fields"]["consistent_m2"] == "True" and d["model_fields"]["eos"] == "LatticeHRGEOS"
+    assert "[x] m2_vorticity" in d["model"]
+    assert d["meta"] == {"event": 3, "note": "m2 on"}
+    assert d["created"] and d["fivo_revision"]
