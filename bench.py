@@ -809,6 +809,94 @@ def run_freezeout(args):
     }
 
 
+# ----------------------------------------------------------------------------- mixed precision at scale
+
+def _precision_fields(b):
+    """T, u^x, u^y, pibar = pi^eta_eta/(e+P) and n of every event's interior, and the
+    recovered-cell mask, one array per event"""
+    import numpy as np
+    m = b.model
+    iE = m.layout.idx("pieta")
+    out = []
+    for e, g in zip(b.events, b.grids):
+        p = e.primitives()
+        U = e.get_state()
+        sx, sy = g.interior()
+        r = lambda a: np.asarray(a).reshape(g.Nxtot, g.Nytot)[sx, sy].ravel()  # noqa: E731
+        wpl = r(p["e"]) + r(p["P"])
+        out.append({"ok": r(p["ok"]) == 1, "T": np.exp(r(p["yT"])), "ux": r(p["ux"]), "uy": r(p["uy"]),
+                    "pibar": U.reshape(g.Nxtot, g.Nytot, m.nv)[sx, sy, iE].ravel() / wpl, "n": r(p["n"])})
+    return out
+
+
+def run_precision(args):
+    """The mixed-precision form at scale: the viscous event's physics on 512^2 cells over
+    [-15, 15] fm, args.precision_events seeded events (device IC, seed 1000 + k),
+    advanced to tau = 4 and on to 10 fm/c in plain FP64 (bitwise the oracle), with the
+    FP32 face pass, and with the face pass and the relaxation's sources in FP32. Per
+    event and field (T, u^x, u^y, pibar, n) the relative L2 and Linf deviation from the
+    FP64 run over the cells recovered in both; the line gives the median and the
+    largest over the events, and the time of each form's run."""
+    import numpy as np
+    import torch
+
+    import fivo2d
+    from fivo2d import _abi as A
+    from fivo2d.solver import GPUBatch2D
+
+    lib = A.load_library()
+    _, m = model_and_grid()
+    nev = args.precision_events
+    grids = [fivo2d.make_grid2d(512, 512, xmax=15.0, ymax=15.0) for _ in range(nev)]
+    fields, runs = {}, {}
+    for name, mode in (("fp64", A.FIVO_PRECISION_FP64), ("fp32_faces", A.FIVO_PRECISION_FP32_FACES),
+                       ("fp32", A.FIVO_PRECISION_FP32)):
+        b = GPUBatch2D(m, grids, lib=lib)
+        for k, e in enumerate(b.events):
+            e.glauber_ic(TAU0, 1000 + k)
+            e.set_precision(mode)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r4 = b.run(TAU0, 4.0, CFL, CFLTAU, A.FIVO_SSPRK3)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        if not all(x["ok"] and x["tau"] == 4.0 for x in r4):
+            raise RuntimeError(f"an event failed before tau = 4 ({name})")
+        f4 = _precision_fields(b)
+        r10 = b.advance([x["tau"] for x in r4], 10.0, CFL, CFLTAU, A.FIVO_SSPRK3, max_steps=10 ** 9)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        if not all(x["ok"] and x["tau"] == 10.0 for x in r10):
+            raise RuntimeError(f"an event failed before tau = 10 ({name})")
+        fields[name] = {4.0: f4, 10.0: _precision_fields(b)}
+        steps = sum(x["nsteps"] for x in r4) + sum(x["nsteps"] for x in r10)
+        runs[name] = {"run_s": t2 - t0, "to_tau4_s": t1 - t0, "steps": steps,
+                      "zone_updates_per_s": steps * 512 * 512 / (t2 - t0)}
+        b.close()
+    errors = {}
+    for name in ("fp32_faces", "fp32"):
+        errors[name] = {}
+        for tau in (4.0, 10.0):
+            per = {k: ([], []) for k in ("T", "ux", "uy", "pibar", "n")}
+            for a, b_ in zip(fields[name][tau], fields["fp64"][tau]):
+                ok = a["ok"] & b_["ok"]
+                for k in per:
+                    x, y = a[k][ok], b_[k][ok]
+                    per[k][0].append(float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300)))
+                    per[k][1].append(float(np.max(np.abs(x - y)) / max(np.max(np.abs(y)), 1e-300)))
+            errors[name][f"tau_{tau:g}"] = {k: {"L2_median": float(np.median(v[0])), "L2_max": float(np.max(v[0])),
+                                                "Linf_median": float(np.median(v[1])),
+                                                "Linf_max": float(np.max(v[1]))} for k, v in per.items()}
+    return {
+        "metric": "relative L2 / Linf deviation of the FP32 forms from FP64 (T, u^x, u^y, pibar, n) at tau = 4, 10",
+        "value": errors["fp32"]["tau_4"]["T"]["L2_median"], "unit": "relative L2(T), median over events, tau = 4",
+        "n_gpus": 1, "higher_is_better": False, "dtype": "f32/f64", "data": "synthetic (seeded MC-Glauber events)",
+        "config": {"workload": f"precision_{nev}x512x512_box15_tau0.6-10_ssprk3", "events": nev, "grid": [512, 512],
+                   "reference": "the FP64 run, bitwise the oracle's arithmetic"},
+        "errors": errors, "runs": runs,
+    }
+
+
 # ----------------------------------------------------------------------------- CPU legs
 
 def oracle_event():
@@ -877,9 +965,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=30)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="event", choices=["event", "batch", "freezeout"],
+    ap.add_argument("--workload", default="event", choices=["event", "batch", "freezeout", "precision"],
                     help="event: the 384^2 viscous event (default); batch: many uneven events")
     ap.add_argument("--events", type=int, default=32, help="batch workload: number of events")
+    ap.add_argument("--precision-events", type=int, default=64, help="precision workload: number of 512^2 events")
     ap.add_argument("--workers", type=int, default=0, help="batch workload: host threads (0: library default)")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the FP32-faces replay and the batched forms comparison of the default line")
@@ -891,7 +980,7 @@ def main():
     ap.add_argument("--guess", action="store_true",
                     help="train the learned recovery guess on other seeded events and time with it attached")
     args = ap.parse_args()
-    if args.workload == "batch":
+    if args.workload in ("batch", "precision"):
         # more hardware queues for the per-event streams (read when CUDA initialises)
         os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     if args.warmup < 3:
@@ -902,6 +991,8 @@ def main():
         line = run_batch(args)
     elif args.workload == "freezeout":
         line = run_freezeout(args)
+    elif args.workload == "precision":
+        line = run_precision(args)
     else:
         line = run_gpu(args)
     if line is not None:

@@ -27,6 +27,7 @@
 #include "freezeout.cuh"
 #include "face32.cuh"
 #include "facetile.cuh"
+#include "relax32.cuh"
 
 using namespace fv;
 
@@ -478,7 +479,7 @@ int launch_stage_t(fivo_ctx* c, const StageArgs& a) {
   double* fhy = c->fh + (size_t)d.nv * d.Ntot;
   float* fhx32 = c->fh32;
   float* fhy32 = c->fh32 ? c->fh32 + (size_t)d.nv * d.Ntot : nullptr;
-  const bool f32 = c->precision == FIVO_PRECISION_FP32_FACES;
+  const bool f32 = c->precision != FIVO_PRECISION_FP64;
   {
     long long nfx = (long long)(d.Nxtot - 1) * d.Nytot, nfy = (long long)d.Nxtot * (d.Nytot - 1);
     KTimer t_(c, FIVO_KCLASS_FACES, 2, nfx + nfy);
@@ -727,7 +728,12 @@ int relax_project(fivo_ctx* c, double tau, double D, int do_relax, int do_projec
   unsigned g = nblk(d.Ntot, 128);
   {
   KTimer t_(c, FIVO_KCLASS_RELAX, 1, d.Ntot);
-  if (d.p.eos_kind == FIVO_EOS_LATTICE_HRG) {
+  if (c->precision == FIVO_PRECISION_FP32 && do_relax) {
+    if (d.p.eos_kind == FIVO_EOS_LATTICE_HRG)
+      k_relax32<FIVO_EOS_LATTICE_HRG><<<g, 128, 0, c->st>>>(d, Uq, Uo, c->w, c->h, tau, D, do_relax, do_project, c->fl);
+    else
+      k_relax32<FIVO_EOS_CONFORMAL_HQ><<<g, 128, 0, c->st>>>(d, Uq, Uo, c->w, c->h, tau, D, do_relax, do_project, c->fl);
+  } else if (d.p.eos_kind == FIVO_EOS_LATTICE_HRG) {
     if (d.hasM2)
       k_relax<FIVO_EOS_LATTICE_HRG, true><<<g, 128, 0, c->st>>>(d, Uq, Uo, c->w, c->h, tau, D, do_relax, do_project, c->fl);
     else
@@ -2165,10 +2171,12 @@ int fivo_ctx_face_pass(fivo_ctx* c, int* x_cfg, int* y_cfg) {
 
 int fivo_ctx_set_precision(fivo_ctx* c, int mode) {
   if (!c) return fail(FIVO_ERR_ARG, "null context");
-  if (mode != FIVO_PRECISION_FP64 && mode != FIVO_PRECISION_FP32_FACES)
+  if (mode != FIVO_PRECISION_FP64 && mode != FIVO_PRECISION_FP32_FACES && mode != FIVO_PRECISION_FP32)
     return fail(FIVO_ERR_ARG, "fivo_ctx_set_precision: unknown mode");
+  if (mode == FIVO_PRECISION_FP32 && c->dp.hasM2)
+    return fail(FIVO_ERR_CONFIG, "fivo_ctx_set_precision: the FP32 relaxation sources do not cover consistent_m2");
   CK(ctx_sync(c));
-  if (mode == FIVO_PRECISION_FP32_FACES && !c->fh32) {
+  if (mode != FIVO_PRECISION_FP64 && !c->fh32) {
     if (cudaMalloc(&c->fh32, 2 * (size_t)c->dp.nv * c->dp.Ntot * sizeof(float)) != cudaSuccess) {
       c->fh32 = nullptr;
       return fail(FIVO_ERR_NOMEM, "fivo_ctx_set_precision: device allocation failed");

@@ -90,7 +90,7 @@ KERNEL_CLASSES = ("prim_fast", "prim_slow", "faces", "update", "adm_slow", "rela
 
 
 FIVO_GUESS_NPARAM, FIVO_GUESS_NNORM, FIVO_GUESS_NSAMP = 6288, 22, 11
-FIVO_PRECISION_FP64, FIVO_PRECISION_FP32_FACES = 0, 1
+FIVO_PRECISION_FP64, FIVO_PRECISION_FP32_FACES, FIVO_PRECISION_FP32 = 0, 1, 2
 FIVO_FACES_AUTO, FIVO_FACES_GLOBAL = -2, -1
 FACE_TILE_SHAPES = ((4, 32), (2, 64), (8, 16), (8, 32))
 

@@ -184,8 +184,10 @@ class GPUWork2D:
         self._ck(self.lib.fivo_finalize_ic(self.h, tau0, bc), "fivo_finalize_ic")
 
     def set_precision(self, mode):
-        """FIVO_PRECISION_FP64 (the reference's arithmetic) or FIVO_PRECISION_FP32_FACES
-        (the face pass of rhs_2d! in FP32, everything else FP64)"""
+        """FIVO_PRECISION_FP64 (the reference's arithmetic), FIVO_PRECISION_FP32_FACES (the
+        face pass of rhs_2d! in FP32, everything else FP64) or FIVO_PRECISION_FP32 (the
+        face pass and the relaxation's sources in FP32; recovery, SSPRK combination,
+        transport coefficients and the relaxation's implicit update FP64)"""
         self._ck(self.lib.fivo_ctx_set_precision(self.h, int(mode)), "fivo_ctx_set_precision")
 
     def set_face_pass(self, x_cfg, y_cfg=None):

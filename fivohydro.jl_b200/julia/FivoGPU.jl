@@ -368,8 +368,8 @@ attach!(w::GPUWork2D, gg::Union{GPURecoveryGuess,Nothing}) =
 """The face pass of rhs_2d! in FP32 (`:fp32_faces`) or the reference's FP64 (`:fp64`);
 recovery, SSPRK combination, floors and relaxation stay FP64 either way."""
 function set_precision!(w::GPUWork2D, mode::Symbol)
-    m = mode === :fp32_faces ? Cint(1) : mode === :fp64 ? Cint(0) :
-        throw(ArgumentError("precision must be :fp64 or :fp32_faces"))
+    m = mode === :fp32_faces ? Cint(1) : mode === :fp64 ? Cint(0) : mode === :fp32 ? Cint(2) :
+        throw(ArgumentError("precision must be :fp64, :fp32_faces or :fp32"))
     fivocheck(ccall((:fivo_ctx_set_precision, LIBFIVO2D), Cint, (Ptr{Cvoid}, Cint), w.h, m),
               "fivo_ctx_set_precision")
 end

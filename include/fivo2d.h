@@ -441,9 +441,15 @@ int  fivo_newton_stats_read(fivo_ctx* ctx, fivo_newton_stats* out, int reset);
  * the EOS at the faces, physical fluxes, wave speeds, HLLE) in FP32 and stores FP32
  * face fluxes; the recovery, the divergence and sources, the SSPRK combination,
  * the floors and the relaxation stay FP64. Results then differ from the FP64 path
- * at the FP32 rounding level of the fluxes (not bitwise). */
+ * at the FP32 rounding level of the fluxes (not bitwise).
+ * FIVO_PRECISION_FP32 adds the relaxation's sources in FP32 (kinematics, the
+ * Navier-Stokes targets, the projected-derivative, advection and coupling terms and
+ * the consistent first moment's sources); the transport coefficients and the
+ * backward-Euler update of each dissipative field stay FP64. Not available with
+ * consistent_m2 (FIVO_ERR_CONFIG). */
 #define FIVO_PRECISION_FP64        0
 #define FIVO_PRECISION_FP32_FACES  1
+#define FIVO_PRECISION_FP32        2
 int  fivo_ctx_set_precision(fivo_ctx* ctx, int mode);
 
 /* --- which kernel runs the FP64 face pass of rhs_2d! (_faces_2d!, src2d/rhs2d.jl:282-371) ---

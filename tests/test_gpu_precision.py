@@ -1,5 +1,6 @@
-"""The mixed-precision form (fivo_ctx_set_precision: the face pass of rhs_2d! in
-FP32, everything else FP64) against the FP64 path and the reference's gates:
+"""The mixed-precision forms (fivo_ctx_set_precision: the face pass of rhs_2d! in
+FP32; and the face pass plus the relaxation's sources in FP32) against the FP64 path
+and the reference's gates:
 
   - the Gubser gate G1 (test/test_gubser2d.jl:97-246): L2(T) and L2(u) against the
     exact solution stay at the published values (the FP32 fluxes move them by far
@@ -98,9 +99,11 @@ def test_bjorken_order_in_fp32_faces(gpu_lib, integrator, expect):
     assert abs(p2 - GATES["bjorken"]["order"][expect]) < 0.15, (errs, p2)
 
 
-def test_viscous_event_error_against_fp64(gpu_lib):
+@pytest.mark.parametrize("form", [A.FIVO_PRECISION_FP32_FACES, A.FIVO_PRECISION_FP32], ids=["fp32_faces", "fp32"])
+def test_viscous_event_error_against_fp64(gpu_lib, form):
     """the bench workload's physics on a 192^2 event (dx = 30/384 fm), 30 SSPRK3 steps
-    from tau0 = 0.6"""
+    from tau0 = 0.6, with the FP32 face pass alone and with the relaxation's sources
+    in FP32 as well"""
     m = fivo2d.build_model_2d(eos=fivo2d.LatticeHRGEOS(), enable_shear=True, enable_bulk=True,
                               enable_diff=True, eta_over_s=0.16, tauShear_coeff=0.2, deltaShear_factor=4 / 3,
                               zeta_over_s=0.05, bulk_model="gaussian", bulk_T0=0.180, bulk_width=0.024,
@@ -110,7 +113,7 @@ def test_viscous_event_error_against_fp64(gpu_lib):
     T, a, ux, uy, _ = ic.glauber_fields(g, 0.6, 1001)
     U, _ = set_cells(m, 0.6, T, a, ux, uy, lib=gpu_lib)
     out = {}
-    for mode in (A.FIVO_PRECISION_FP64, A.FIVO_PRECISION_FP32_FACES):
+    for mode in (A.FIVO_PRECISION_FP64, form):
         w = GPUWork2D(m, g, lib=gpu_lib)
         w.set_precision(mode)
         w.set_state(U)
@@ -119,7 +122,7 @@ def test_viscous_event_error_against_fp64(gpu_lib):
         assert r["ok"] and r["nsteps"] == 30
         out[mode] = (w.primitives(), w.get_state())
         w.close()
-    (p64, U64), (p32, U32) = out[A.FIVO_PRECISION_FP64], out[A.FIVO_PRECISION_FP32_FACES]
+    (p64, U64), (p32, U32) = out[A.FIVO_PRECISION_FP64], out[form]
     sx, sy = g.interior()
     ok = ((p64["ok"] == 1) & (p32["ok"] == 1)).reshape(g.Nxtot, g.Nytot)[sx, sy]
     T64 = np.exp(p64["yT"]).reshape(g.Nxtot, g.Nytot)[sx, sy][ok]
@@ -129,8 +132,54 @@ def test_viscous_event_error_against_fp64(gpu_lib):
     pi64 = U64.reshape(g.Nxtot, g.Nytot, m.nv)[sx, sy, iP:iP + 3][ok]
     pi32 = U32.reshape(g.Nxtot, g.Nytot, m.nv)[sx, sy, iP:iP + 3][ok]
     l2pi = np.linalg.norm(pi32 - pi64) / np.linalg.norm(pi64)
-    print(f"FP32 faces vs FP64 after 30 steps: L2(T) {l2T:.3e}, L2(pi) {l2pi:.3e}")
-    assert 0 < l2T <= 1e-6 and l2pi <= 1e-4, (l2T, l2pi)
+    w64 = (p64["e"] + p64["P"]).reshape(g.Nxtot, g.Nytot)[sx, sy][ok]
+    w32 = (p32["e"] + p32["P"]).reshape(g.Nxtot, g.Nytot)[sx, sy][ok]
+    ie = m.layout.idx("pieta")
+    pb64 = U64.reshape(g.Nxtot, g.Nytot, m.nv)[sx, sy, ie][ok] / w64
+    pb32 = U32.reshape(g.Nxtot, g.Nytot, m.nv)[sx, sy, ie][ok] / w32
+    l2pb = np.linalg.norm(pb32 - pb64) / np.linalg.norm(pb64)
+    print(f"form {form} vs FP64 after 30 steps: L2(T) {l2T:.3e}, L2(pi) {l2pi:.3e}, L2(pibar) {l2pb:.3e}")
+    assert 0 < l2T <= 1e-6 and l2pi <= 1e-4 and l2pb <= 1e-4, (l2T, l2pi, l2pb)
+
+
+def test_relaxation_sources_in_fp32(gpu_lib):
+    """one relaxation on the same evolved state: the FP32 sources move every dissipative
+    row by FP32 rounding of the sources only (relative to the row's scale), the medium's
+    rows not at all; consistent_m2 is refused in this mode"""
+    m = fivo2d.build_model_2d(eos=fivo2d.LatticeHRGEOS(), enable_shear=True, enable_bulk=True,
+                              enable_diff=True, eta_over_s=0.16, zeta_over_s=0.05, kappa_coeff=0.5,
+                              consistent_fm=True, taupi_pi_factor=0.5, lambda_pi_Pi_factor=0.3,
+                              lambda_Pi_pi_factor=0.2)
+    g = fivo2d.make_grid2d(64, 64, xmax=64 * 15.0 / 384, ymax=64 * 15.0 / 384)
+    T, a, ux, uy, _ = ic.glauber_fields(g, 0.6, 1005)
+    U, _ = set_cells(m, 0.6, T, a, ux, uy, lib=gpu_lib)
+    w = GPUWork2D(m, g, lib=gpu_lib)
+    w.set_state(U)
+    w.finalize_ic(0.6)
+    r = w.run(0.6, 10.0, 0.2, 0.05, A.FIVO_SSPRK3, max_steps=6)
+    mid, hist = w.get_state(), w.get_history()
+    out = {}
+    for mode in (A.FIVO_PRECISION_FP64, A.FIVO_PRECISION_FP32):
+        v = GPUWork2D(m, g, lib=gpu_lib)
+        v.set_precision(mode)
+        v.set_state(mid)
+        v.set_history(**hist)
+        v.update_primitives(r["tau"])
+        v.relax(r["tau"], 0.02)
+        out[mode] = v.get_state()
+        v.close()
+    w.close()
+    a64, a32 = out[A.FIVO_PRECISION_FP64], out[A.FIVO_PRECISION_FP32]
+    assert np.array_equal(a32[:, :4], a64[:, :4])
+    for k in range(4, m.nv):
+        scale = max(np.abs(a64[:, k]).max(), 1e-300)
+        rel = np.abs(a32[:, k] - a64[:, k]).max() / scale
+        assert rel <= 1e-5, (m.layout.names[k], rel)
+    assert not np.array_equal(a32, a64)
+    m2 = fivo2d.build_model_2d(enable_diff=True, consistent_m2=True)
+    v = GPUWork2D(m2, g, lib=gpu_lib)
+    assert gpu_lib.fivo_ctx_set_precision(v.h, A.FIVO_PRECISION_FP32) == A.FIVO_ERR_CONFIG
+    v.close()
 
 
 def test_precision_switch_and_refusal(gpu_lib):
