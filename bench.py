@@ -556,8 +556,9 @@ def _batch_fields(b, m):
 
 def batch_forms(lib, m, nevents, steps, single_value, warmup=3):
     """The metric's comparison on one GPU: the same nevents seeded events (the
-    event-by-event sizes, device IC, seed 1000 + k) advanced in plain FP64, with
-    the FP32 face pass, and with the learned guess plus FP32 faces; zone-updates/s
+    event-by-event sizes, device IC, seed 1000 + k) advanced in plain FP64, in FP32
+    (face pass and relaxation sources), and with the learned guess plus FP32, the
+    guess used for every cell or for the cells the warm start defers; zone-updates/s
     of each (host wall clock around the synchronous batch call, one stream per
     event) and each form's L2(T), L2(pibar) and L2(pi) against the plain run."""
     import numpy as np
@@ -576,15 +577,17 @@ def batch_forms(lib, m, nevents, steps, single_value, warmup=3):
            "zone_updates_per_step": cells, "single_event_plain_fp64": single_value,
            "timing": "host wall clock around the synchronous batch call (one stream per event)"}
     ref = None
-    for form in ("plain_fp64", "fp32_faces", "learned_fp32"):
+    for form in ("plain_fp64", "fp32", "learned_fp32", "learned_deferred_fp32"):
         b = GPUBatch2D(m, grids, lib=lib)
         for k, e in enumerate(b.events):
             e.glauber_ic(TAU0, 1000 + k)
             e.rhs(TAU0)
             if form != "plain_fp64":
-                e.set_precision(A.FIVO_PRECISION_FP32_FACES)
+                e.set_precision(A.FIVO_PRECISION_FP32)
             if form == "learned_fp32":
-                guess.attach(e)
+                guess.attach(e, A.FIVO_GUESS_EVERY_CELL)
+            if form == "learned_deferred_fp32":
+                guess.attach(e, A.FIVO_GUESS_DEFERRED)
         taus = [TAU0] * len(grids)
 
         def adv(n):
@@ -612,13 +615,15 @@ def batch_forms(lib, m, nevents, steps, single_value, warmup=3):
             row["L2_pi"] = l2_rel(f["pi"][ok], ref["pi"][ok])
             row["speedup_vs_plain_batch"] = row["value"] / out["plain_fp64"]["value"]
             row["meets_L2T_1e-6"] = bool(row["L2_T"] <= 1e-6)
-        if form == "learned_fp32":
+        if form.startswith("learned"):
             st = {}
             for e in b.events:
                 for key, v in newton_stats(e).items():
                     st[key] = st.get(key, 0) + v
-            row["guess"] = dict(ginfo, accept_rate=st["ok_learn"] / max(1, st["n_learn"]),
-                                updates_per_cell=(st["it_learn"] + st["it_fb"]) / max(1, st["n_learn"]))
+            row["guess"] = dict(ginfo if form == "learned_fp32" else {}, mode=form,
+                                guesses=st["n_learn"], accept_rate=st["ok_learn"] / max(1, st["n_learn"]),
+                                updates_per_guess=(st["it_learn"] + st["it_fb"]) / max(1, st["n_learn"]),
+                                full_recoveries=st["deferred"])
         out[form] = row
         b.close()
     guess.close()

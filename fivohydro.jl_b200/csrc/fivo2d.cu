@@ -49,7 +49,9 @@ int fail(int code, const std::string& msg) {
 #define CKL()                                                                             \
   do {                                                                                    \
     cudaError_t e_ = cudaGetLastError();                                                  \
-    if (e_ != cudaSuccess) return fail(FIVO_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+    if (e_ != cudaSuccess)                                                                \
+      return fail(FIVO_ERR_CUDA, std::string("kernel launch at fivo2d.cu:") + std::to_string(__LINE__) + ": " + \
+                                     cudaGetErrorString(e_));                             \
   } while (0)
 
 inline unsigned nblk(long long n, int b) { return (unsigned)((n + b - 1) / b); }
@@ -172,6 +174,7 @@ struct fivo_ctx {
   int64_t tot_base_p = 0, tot_base_a = 0;   /* device deferred-cell totals at the last reset */
   /* the learned recovery guess (fivo_ctx_set_guess): k_prim_learned replaces k_prim_fast */
   bool learned = false;
+  int guess_mode = FIVO_GUESS_EVERY_CELL;
   guess::Net gnet{};
   int64_t stats_base_p = 0;                 /* deferred-cell total at the last Newton-statistics reset */
   /* the mixed-precision face pass (fivo_ctx_set_precision): FP32 face fluxes */
@@ -271,6 +274,31 @@ template <int EOS, bool NCH>
 int launch_primitive_t(fivo_ctx* c, const DevState& U, double tau) {
   const DevParams& d = c->dp;
   unsigned int* q = c->queues;
+  if (c->learned && c->guess_mode == FIVO_GUESS_DEFERRED) {
+    /* the plain fast pass, the network's guess for the cells it deferred, then the
+     * full recovery of what is left (second queue) */
+    unsigned int* q2 = c->queues + 2 * d.Ntot;
+    {
+      KTimer t_(c, FIVO_KCLASS_PRIM_FAST, 1, d.Ntot);
+      k_prim_fast<EOS, NCH><<<nblk(d.Ntot, 128), 128, 0, c->st>>>(d, U, c->w, c->h, tau, c->fl, q);
+      CKL();
+    }
+    {
+      const int dyn = LEARNED_SMEM - (int)sizeof(guess::FwdSmem) - 128;
+      CK(cudaFuncSetAttribute(k_prim_learned_retry<EOS, NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+      KTimer t_(c, FIVO_KCLASS_PRIM_SLOW);
+      k_prim_learned_retry<EOS, NCH><<<nblk(d.Ntot, 128), 128, dyn, c->st>>>(d, U, c->w, c->h, tau, c->fl, q, q2,
+                                                                               c->gnet);
+      CKL();
+    }
+    {
+      KTimer t_(c, FIVO_KCLASS_PRIM_SLOW);
+      k_prim_slow<EOS, NCH><<<2 * c->nsm, 128, 0, c->st>>>(d, U, c->w, c->h, tau, c->fl, q2, &c->fl->qcount_q,
+                                                           &c->fl->qnext_q);
+      CKL();
+    }
+    return FIVO_OK;
+  }
   if (c->learned) {
     /* at most 4 blocks per SM (4 x 128 tensor-memory columns): the launch reserves
      * shared memory up to LEARNED_SMEM per block */
@@ -287,7 +315,8 @@ int launch_primitive_t(fivo_ctx* c, const DevState& U, double tau) {
   }
   {
     KTimer t_(c, FIVO_KCLASS_PRIM_SLOW);
-    k_prim_slow<EOS, NCH><<<2 * c->nsm, 128, 0, c->st>>>(d, U, c->w, c->h, tau, c->fl, q);
+    k_prim_slow<EOS, NCH><<<2 * c->nsm, 128, 0, c->st>>>(d, U, c->w, c->h, tau, c->fl, q, &c->fl->qcount_p,
+                                                         &c->fl->qnext_p);
     CKL();
   }
   return FIVO_OK;
@@ -442,7 +471,7 @@ int tune_faces(fivo_ctx* c, const StageArgs& a, double* fhx, double* fhy) {
     for (int dir = 0; dir < 2; ++dir) {
       double* Fh = dir == 0 ? fhx : fhy;
       int best = -1;
-      float best_ms = 1e30f;
+      float best_ms = 1e30f, glob_ms = 1e30f;
       for (int cfg = -1; cfg < (tile_ok ? FT_NSHAPES : 0); ++cfg) {
         if (cfg >= 0 && !ft_encode(c, dir, cfg)) continue;
         float tmin = 1e30f;
@@ -456,7 +485,10 @@ int tune_faces(fivo_ctx* c, const StageArgs& a, double* fhx, double* fhy) {
           CK(cudaEventElapsedTime(&ms, e0, e1));
           if (rep > 0) tmin = std::min(tmin, ms);
         }
-        if (tmin < best_ms) { best_ms = tmin; best = cfg; }
+        /* a tile shape replaces the global-load kernel only when it is clearly faster
+         * (3 %): the two are often within the timing noise of each other */
+        if (cfg < 0 ? tmin < best_ms : tmin < best_ms && tmin < 0.97f * glob_ms) { best_ms = tmin; best = cfg; }
+        if (cfg < 0) glob_ms = tmin;
       }
       c->ft_cfg[dir] = best;
     }
@@ -861,7 +893,7 @@ int fivo_ctx_create(const fivo_params* p, int nx, int ny, int nghost, double xma
       cudaMalloc(&c->fl, sizeof(DevFlags)) != cudaSuccess ||
       cudaMalloc(&c->stage, (size_t)d.nv * N * 8) != cudaSuccess ||
       cudaMalloc(&c->fh, 2 * (size_t)d.nv * N * 8) != cudaSuccess ||
-      cudaMalloc(&c->queues, 2 * N * sizeof(unsigned int)) != cudaSuccess ||
+      cudaMalloc(&c->queues, 3 * N * sizeof(unsigned int)) != cudaSuccess ||
       cudaMalloc(&c->part, (size_t)nblk((long long)d.Nx * d.Ny, 256) * 8 * sizeof(double)) != cudaSuccess)
     return cleanup(fail(FIVO_ERR_NOMEM, "device allocation failed"));
   if (cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess || c->nsm < 1)
@@ -1977,6 +2009,15 @@ int fivo_ctx_set_guess(fivo_ctx* c, fivo_guess* g) {
   if (g) CK(cudaStreamSynchronize(g->st));
   c->learned = g != nullptr;
   c->gnet = g ? net_of(g) : guess::Net{};
+  return FIVO_OK;
+}
+
+int fivo_ctx_set_guess_mode(fivo_ctx* c, int mode) {
+  if (!c) return fail(FIVO_ERR_ARG, "null context");
+  if (mode != FIVO_GUESS_EVERY_CELL && mode != FIVO_GUESS_DEFERRED)
+    return fail(FIVO_ERR_ARG, "fivo_ctx_set_guess_mode: unknown mode");
+  CK(ctx_sync(c));
+  c->guess_mode = mode;
   return FIVO_OK;
 }
 

@@ -63,6 +63,7 @@ struct DevFlags {
   int status;                     /* nonzero: a device loop hit its cap                 */
   int pad;
   unsigned int qcount_p, qnext_p; /* deferred recoveries of the current pass           */
+  unsigned int qcount_q, qnext_q; /* the learned retry's leftovers for the full recovery */
   unsigned int qcount_a, qnext_a; /* deferred admissibility inversions of the stage     */
   unsigned long long tot_p, tot_a;/* deferred cells summed over passes (kernel timing)   */
   /* Newton statistics, cumulative until reset (what & 32): updates and attempts of
@@ -1208,6 +1209,7 @@ __global__ void k_reset_flags(DevFlags* fl, int what, unsigned long long amax_bi
   if (what & 1) {
     fl->nprimfail = 0; fl->nvacuum = 0; fl->rep = 0x7fffffffffffffffULL;
     fl->qcount_p = 0; fl->qnext_p = 0; fl->qcount_a = 0; fl->qnext_a = 0;
+    fl->qcount_q = 0; fl->qnext_q = 0;
   }
   if (what & 64) fl->nbad = 0;      /* inadmissible cells: accumulate over a step's stages otherwise */
   if (what & 2) fl->amax_bits = amax_bits;
@@ -1649,6 +1651,97 @@ __global__ void k_guess_harvest(DevParams d, DevState U, DevPrims w, double tau,
     for (int q = 0; q < guess::NSAMP; ++q) out[k * guess::NSAMP + q] = f[q];
 }
 
+/* The learned guess for the deferred cells only (FIVO_GUESS_DEFERRED): the fast pass
+ * ran the warm starts as in the plain path; CTA b takes the 128 cells b*128 .. of its
+ * queue (the cells without a warm start, and the warm attempts over budget or failed),
+ * infers their starting points with the network on the tensor cores and runs the
+ * Newton from there with the guess check (GUESS_CHECK_IT, GUESS_CHECK_TOL). A cell
+ * that converges is stored; the rest go on to a second queue, which the full
+ * recovery (k_prim_slow) then takes. The grid covers the largest possible queue and
+ * the CTAs past its end return at once (all threads alike). One tile per CTA: the
+ * forward pass gives up the CTA's tensor-memory allocation permit after its one
+ * allocation, so a CTA cannot allocate for a second tile. */
+template <int EOS, bool NCH>
+__global__ void __launch_bounds__(128, 4) k_prim_learned_retry(DevParams d, DevState U, DevPrims w, DevHist h,
+                                                             double tau, DevFlags* fl, const unsigned int* queue,
+                                                             unsigned int* queue2, guess::Net net) {
+  __shared__ __align__(128) guess::FwdSmem s;
+  const unsigned n = *(volatile unsigned int*)&fl->qcount_p;
+  const unsigned lane = threadIdx.x & 31;
+  bool net_ok = true;
+  {
+    const unsigned base = blockIdx.x * 128u;
+    if (base >= n) return;
+    const unsigned qi = base + threadIdx.x;
+    const bool live = qi < n;
+    const long long i = live ? (long long)queue[qi] : 0;
+    CellCons c;
+    float xn[guess::NIN];
+#pragma unroll
+    for (int q = 0; q < guess::NIN; ++q) xn[q] = 0.0f;
+    if (live) {
+      load_cons(d, U, i, tau, c);
+      if (c.E > 0.0) {
+        float r[guess::NIN];
+        guess::features(c.E, c.Sx, c.Sy, c.Pi, c.pixx, c.pixy, c.piyy, r);
+#pragma unroll
+        for (int q = 0; q < guess::NIN; ++q) xn[q] = guess::nrm_in(net.norm, q, r[q]);
+      }
+    }
+    float y[guess::NOUT] = {0.0f, 0.0f, 0.0f};
+    const bool tile_ok = guess::forward_tile(s, net, xn, y);
+    net_ok = net_ok && tile_ok;
+    bool pass_on = live, done = false;
+    unsigned it_l = 0, n_l = 0, ok_l = 0;
+    if (live && tile_ok && c.E > 0.0) {
+      double g[4];
+      g[0] = ((double)y[0] * (double)net.norm.out_std[0] + (double)net.norm.out_mean[0]) + 0.25 * log(c.E);
+      g[2] = (double)y[1] * (double)net.norm.out_std[1] + (double)net.norm.out_mean[1];
+      g[3] = (double)y[2] * (double)net.norm.out_std[2] + (double)net.norm.out_mean[2];
+      const double phw = h.x0_phi[i];
+      g[1] = isfinite_(phw) ? phw : 0.0;
+      if (NCH && EOS == FIVO_EOS_LATTICE_HRG) {
+        const double T0 = jclamp(exp(g[0]), FV_T_MIN, FV_T_SOLVE_MAX);
+        const double K2 = lhrg_K2(lhrg_x(T0, d));
+        double Cn = (d.A_lhrg * T0) * K2;
+        if (d.p.hq_times_fmGeV3) Cn *= d.fmgev3;
+        const double ut = utau(g[2], g[3]);
+        const double nt = (c.D - nu_tau(g[2], g[3], ut, c.nux, c.nuy)) / ut;
+        if (nt > 0.0 && Cn > 0.0) g[1] = log(nt / Cn);
+      }
+      if (isfinite_(g[0]) && isfinite_(g[1]) && isfinite_(g[2]) && isfinite_(g[3])) {
+        bool over = false;
+        int it = 0;
+        Recovery r = recover_fast<EOS, NCH>(c, d, g[0], g[1], g[2], g[3], d.p.primrec_maxit, d.p.primrec_tol,
+                                            d.p.primrec_maxit, &over, GUESS_CHECK_IT, GUESS_CHECK_TOL, &it);
+        it_l = (unsigned)it; n_l = 1;
+        if (!over && r.ok) {
+          store_recovery<EOS>(d, w, h, i, r);
+          done = true;
+          ok_l = 1;
+        }
+      }
+    }
+    pass_on = live && !done;
+    {
+      const unsigned a = __reduce_add_sync(0xffffffffu, it_l), b = __reduce_add_sync(0xffffffffu, n_l);
+      const unsigned e = __reduce_add_sync(0xffffffffu, ok_l);
+      if (lane == 0 && b) {
+        atomicAdd(&fl->it_learn, (unsigned long long)a); atomicAdd(&fl->n_learn, (unsigned long long)b);
+        atomicAdd(&fl->ok_learn, (unsigned long long)e);
+      }
+    }
+    const unsigned md = __ballot_sync(0xffffffffu, pass_on);
+    if (md) {
+      unsigned b2 = 0;
+      if (lane == 0) b2 = atomicAdd(&fl->qcount_q, (unsigned)__popc(md));
+      b2 = __shfl_sync(0xffffffffu, b2, 0);
+      if (pass_on) queue2[b2 + __popc(md & ((1u << lane) - 1u))] = (unsigned)i;
+    }
+  }
+  if (!net_ok && threadIdx.x == 0) atomicExch(&fl->status, 3);
+}
+
 /* Barrier of the two warps of pair p of a block (named barrier 1 + p, 64 threads). */
 __device__ __forceinline__ void pair_sync(int p) {
   asm volatile("bar.sync %0, 64;" :: "r"(1 + p) : "memory");
@@ -1661,18 +1754,19 @@ __device__ __forceinline__ void pair_sync(int p) {
  * that long and short recoveries balance over the pairs. */
 template <int EOS, bool NCH>
 __global__ void __launch_bounds__(128) k_prim_slow(DevParams d, DevState U, DevPrims w, DevHist h, double tau,
-                                                   DevFlags* fl, const unsigned int* queue) {
+                                                   DevFlags* fl, const unsigned int* queue, const unsigned int* qcount,
+                                                   unsigned int* qnext) {
   __shared__ unsigned int s_q[2];
   __shared__ int s_stop[2];
   __shared__ Recovery s_cold[2];
-  const unsigned n = *(volatile unsigned int*)&fl->qcount_p;
+  const unsigned n = *(volatile const unsigned int*)qcount;
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&fl->tot_p, (unsigned long long)n);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int pair = warp >> 1;
   const bool lead = (warp & 1) == 0;
   while (true) {
     if (lead && lane == 0) {
-      s_q[pair] = atomicAdd(&fl->qnext_p, 1u);
+      s_q[pair] = atomicAdd(qnext, 1u);
       s_stop[pair] = 0;
     }
     pair_sync(pair);

@@ -92,6 +92,7 @@ KERNEL_CLASSES = ("prim_fast", "prim_slow", "faces", "update", "adm_slow", "rela
 FIVO_GUESS_NPARAM, FIVO_GUESS_NNORM, FIVO_GUESS_NSAMP = 6288, 22, 11
 FIVO_PRECISION_FP64, FIVO_PRECISION_FP32_FACES, FIVO_PRECISION_FP32 = 0, 1, 2
 FIVO_FACES_AUTO, FIVO_FACES_GLOBAL = -2, -1
+FIVO_GUESS_EVERY_CELL, FIVO_GUESS_DEFERRED = 0, 1
 FACE_TILE_SHAPES = ((4, 32), (2, 64), (8, 16), (8, 32))
 
 
@@ -146,6 +147,7 @@ SIGNATURES = {
     "fivo_upload_history": (C.c_int, [C.c_void_p, _I64] + [_D] * 8),
     "fivo_download_history": (C.c_int, [C.c_void_p, _I64] + [_D] * 8),
     "fivo_upload_nu_history": (C.c_int, [C.c_void_p, _I64, _D, _D]),
+    "fivo_ctx_set_guess_mode": (C.c_int, [C.c_void_p, C.c_int]),
     "fivo_download_nu_history": (C.c_int, [C.c_void_p, _I64, _D, _D]),
     "fivo_reset_history": (C.c_int, [C.c_void_p]),
     "fivo_get_primitives": (C.c_int, [C.c_void_p, _I64] + [_D] * 9 + [_U8]),

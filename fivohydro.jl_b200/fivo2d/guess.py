@@ -124,8 +124,12 @@ class RecoveryGuess:
         return out
 
     # ---- use in a solver
-    def attach(self, work):
+    def attach(self, work, mode=A.FIVO_GUESS_EVERY_CELL):
+        """use the network in `work`'s recovery: for every cell (FIVO_GUESS_EVERY_CELL, the
+        warm start as the fallback) or for the cells the warm start leaves
+        (FIVO_GUESS_DEFERRED)"""
         self._ck(self.lib.fivo_ctx_set_guess(work.h, self.h), "fivo_ctx_set_guess")
+        self._ck(self.lib.fivo_ctx_set_guess_mode(work.h, int(mode)), "fivo_ctx_set_guess_mode")
 
     @staticmethod
     def detach(work):

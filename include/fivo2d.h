@@ -434,6 +434,14 @@ int  fivo_guess_grad(fivo_guess* g, const float* samples, int64_t n, float* grad
 int  fivo_guess_forward(fivo_guess* g, const float* raw, int64_t n, float* out);
 /* attach (g) or detach (NULL) the guess; the context keeps no ownership */
 int  fivo_ctx_set_guess(fivo_ctx* ctx, fivo_guess* g);
+/* where the attached guess is used. FIVO_GUESS_EVERY_CELL (the default): the network's
+ * guess is the starting point of every cell's Newton, the previous step's warm start
+ * its per-cell fallback. FIVO_GUESS_DEFERRED: the warm starts run first as in the plain
+ * path, and the network's guess is tried on the cells the warm start leaves (no warm
+ * start, over the fast budget, failed) before the full cons_to_prim_2d!. */
+#define FIVO_GUESS_EVERY_CELL 0
+#define FIVO_GUESS_DEFERRED   1
+int  fivo_ctx_set_guess_mode(fivo_ctx* ctx, int mode);
 int  fivo_newton_stats_read(fivo_ctx* ctx, fivo_newton_stats* out, int reset);
 
 /* --- mixed precision (no counterpart in the reference, which is FP64 throughout) ---

@@ -121,10 +121,10 @@ def test_training_reduces_the_loss(trained):
     assert l1 < l0 / 50, (l0, l1)
 
 
-def _run(m, gr, U, lib, guess=None, steps=24):
+def _run(m, gr, U, lib, guess=None, steps=24, mode=A.FIVO_GUESS_EVERY_CELL):
     w = GPUWork2D(m, gr, lib=lib)
     if guess is not None:
-        guess.attach(w)
+        guess.attach(w, mode)
     w.set_state(U)
     w.finalize_ic(0.6)
     newton_stats(w, reset=True)
@@ -178,6 +178,46 @@ def test_trained_guess_run_agrees_and_saves_updates(trained, gpu_lib):
           f"deferred learned {sl['deferred']} plain {sp['deferred']}")
 
 
+def test_rejected_deferred_guesses_fall_back_bitwise(gpu_lib):
+    """the deferred mode with a network whose every guess is rejected: the deferred
+    cells all go on to the full recovery and the run is the plain run to the bit"""
+    m = _model()
+    gr, U = _event(m, 80, 2101)
+    g = RecoveryGuess(seed=1, lib=gpu_lib)
+    g.set_params(np.zeros(A.FIVO_GUESS_NPARAM, dtype=np.float32),
+                 np.concatenate([np.zeros(8), np.ones(8), [8.0, 900.0, -900.0], np.ones(3)]).astype(np.float32))
+    rp, Up, pp, sp = _run(m, gr, U, gpu_lib)
+    rl, Ul, pl, sl = _run(m, gr, U, gpu_lib, guess=g, mode=A.FIVO_GUESS_DEFERRED)
+    assert rp["nsteps"] == rl["nsteps"] and rp["tau"] == rl["tau"]
+    assert bits_equal(Up, Ul)
+    assert sl["n_learn"] > 0 and sl["ok_learn"] == 0
+    assert sl["n_fast"] == sp["n_fast"] and sl["deferred"] == sp["deferred"]
+    g.close()
+
+
+def test_deferred_guess_agrees_and_takes_cells_off_the_full_recovery(trained, gpu_lib):
+    """the deferred mode with the trained network, over a longer window (the fireball
+    edge forms and cells leave vacuum without a warm start): the same primitives as the
+    plain run to L2(T) <= 1e-6, and the network converges a share of the cells that the
+    plain path sends to the full cons_to_prim_2d!"""
+    m, g, _ = trained
+    gr, U = _event(m, 96, 2199)
+    rp, Up, pp, sp = _run(m, gr, U, gpu_lib, steps=80)
+    rl, Ul, pl, sl = _run(m, gr, U, gpu_lib, guess=g, steps=80, mode=A.FIVO_GUESS_DEFERRED)
+    assert rl["ok"] and rl["nsteps"] == rp["nsteps"]
+    sx, sy = gr.interior()
+    ok = ((pp["ok"] == 1) & (pl["ok"] == 1)).reshape(gr.Nxtot, gr.Nytot)[sx, sy]
+    T_p = np.exp(pp["yT"]).reshape(gr.Nxtot, gr.Nytot)[sx, sy][ok]
+    T_l = np.exp(pl["yT"]).reshape(gr.Nxtot, gr.Nytot)[sx, sy][ok]
+    l2T = np.linalg.norm(T_l - T_p) / np.linalg.norm(T_p)
+    print(f"deferred mode: {sl['n_learn']} guesses on deferred cells, {sl['ok_learn']} converged "
+          f"({sl['it_learn'] / max(1, sl['n_learn']):.2f} updates each); full recoveries: plain "
+          f"{sp['deferred']}, with the network {sl['deferred']}; L2(T) {l2T:.2e}")
+    assert l2T < 1e-6, l2T
+    assert sl["n_learn"] > 0 and sl["ok_learn"] > 0
+    assert sl["deferred"] < sp["deferred"]
+
+
 def test_guess_argument_refusals(gpu_lib):
     import ctypes as C
     g = RecoveryGuess(seed=2, lib=gpu_lib)
@@ -191,4 +231,8 @@ def test_guess_argument_refusals(gpu_lib):
     assert gpu_lib.fivo_guess_train(g.h, 10, 4, C.c_float(1e-3), 1, out.ctypes.data_as(A._D)) == A.FIVO_ERR_ARG  # no samples
     y = g.forward(np.zeros((1, 8), dtype=np.float32))      # one row, a ragged tile
     assert y.shape == (1, 3) and np.isfinite(y).all()
+    m = _model()
+    w = GPUWork2D(m, fivo2d.make_grid2d(16, 16), lib=gpu_lib)
+    assert gpu_lib.fivo_ctx_set_guess_mode(w.h, 5) == A.FIVO_ERR_ARG
+    w.close()
     g.close()
