@@ -530,10 +530,16 @@ int launch_stage_t(fivo_ctx* c, const StageArgs& a) {
   unsigned int* aq = c->queues + d.Ntot;
   {
     KTimer t_(c, FIVO_KCLASS_UPDATE, 1, (long long)d.Nx * d.Ny);
-    if (f32)
-      k_update<EOS, NCH, float><<<nblk((long long)d.Nx * d.Ny, 128), 128, 0, c->st>>>(d, a, fhx32, fhy32, aq);
+    const unsigned gu = nblk((long long)d.Nx * d.Ny, 128);
+    const bool full = d.hasNu && d.hasPi && d.hasShear;   /* the rows at fixed places (k_update FULL) */
+    if (f32 && full)
+      k_update<EOS, NCH, float, true><<<gu, 128, 0, c->st>>>(d, a, fhx32, fhy32, aq);
+    else if (f32)
+      k_update<EOS, NCH, float><<<gu, 128, 0, c->st>>>(d, a, fhx32, fhy32, aq);
+    else if (full)
+      k_update<EOS, NCH, double, true><<<gu, 128, 0, c->st>>>(d, a, fhx, fhy, aq);
     else
-      k_update<EOS, NCH><<<nblk((long long)d.Nx * d.Ny, 128), 128, 0, c->st>>>(d, a, fhx, fhy, aq);
+      k_update<EOS, NCH><<<gu, 128, 0, c->st>>>(d, a, fhx, fhy, aq);
     CKL();
   }
   if (a.mode != COMB_RHS_ONLY) {

@@ -308,7 +308,7 @@ __device__ __forceinline__ double peff_of(const DevParams& d, const double u[FV_
 
 /* enforce_floors_2d! + enforce_S_energy_constraint_2d! + enforce_nu_charge_constraint_2d!
  * for one interior cell (src2d/floors2d.jl:24-210). Pw = work.P (NaN if absent). */
-__device__ void sanitize_cell(const DevParams& d, double u[FV_MAXV], int ix, int iy, double tau_state,
+__device__ __forceinline__ void sanitize_cell(const DevParams& d, double u[FV_MAXV], int ix, int iy, double tau_state,
                               double Pw, bool haveP, double Emin) {
   double Evac = jmax(Emin, d.E_vac_cut);
   double rdom = d.p.r_domain;
@@ -1974,10 +1974,19 @@ __device__ __forceinline__ int adm_prefilter(const DevParams& d, const double u[
 /* per interior cell: flux divergence + source (rhs_2d! assembly), the stage
  * combination, sanitize_stage_2d!'s floors and bounds, and the admissibility
  * test up to the inversion */
-/* FT: the type of the face-flux planes (double; float for the mixed-precision face pass) */
-template <int EOS, bool NCH, typename FT = double>
-__global__ void __launch_bounds__(128) k_update(DevParams d, StageArgs s, const FT* Fhx, const FT* Fhy,
+/* FT: the type of the face-flux planes (double; float for the mixed-precision face pass).
+ * FULL: the layout carries charge, bulk and shear (the viscous event's), so every row
+ * index is a compile-time constant and the per-cell row arrays live in registers; the
+ * arithmetic is the same. */
+template <int EOS, bool NCH, typename FT = double, bool FULL = false>
+__global__ void __launch_bounds__(128) k_update(DevParams d0, StageArgs s, const FT* Fhx, const FT* Fhy,
                                                 unsigned int* aqueue) {
+  DevParams d = d0;
+  if (FULL) {
+    d.iDtau = 0; d.iSx = 1; d.iSy = 2; d.iE = 3; d.iNux = 4; d.iNuy = 5; d.iPi = 6;
+    d.iPixx = 7; d.iPixy = 8; d.iPiyy = 9; d.iPieta = 10; d.nvf = 11;
+    d.hasNu = 1; d.hasPi = 1; d.hasShear = 1;
+  }
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int verdict = 1;
   long long i = 0;
