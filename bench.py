@@ -28,10 +28,12 @@ so it runs to the configured tau = 10 fm/c.
             every step uploads U, advances, downloads U (the drop-in usage from a
             host driver that keeps U on the host).
   metric_comparison  the metric's own comparison: 256 events of the event-by-event
-            sizes (N in {96..400}, dx = 30/384 fm, one stream per event) advanced in
-            plain FP64, with the FP32 face pass, and with the learned recovery guess
-            plus FP32 faces, on the same events; each form's L2(T) and L2(pibar) against
-            the plain run after the window.
+            sizes (N in {96..400}, dx = 30/384 fm) advanced in plain FP64, in FP32 (faces
+            and relaxation sources) and with the learned recovery guess plus FP32, one
+            stream per event, then plain FP64 and FP32 in lockstep (each kernel of a
+            step launched once over all events, replayed from CUDA graphs, schedule
+            tuned on the warm-up steps), on the same events; each form's L2(T) and
+            L2(pibar) against the plain run after the window.
 
 `--impl reference` times the reference's CPU path (the C++ restatement in
 oracle/, all host threads) on the same workload.
@@ -554,13 +556,20 @@ def _batch_fields(b, m):
     return {k: np.concatenate(v) for k, v in out.items()}
 
 
-def batch_forms(lib, m, nevents, steps, single_value, warmup=3):
+LOCKSTEP_FORMS = ("plain_fp64_lockstep", "fp32_lockstep", "plain_fp64_lockstep_nograph")
+
+
+def batch_forms(lib, m, nevents, steps, single_value, warmup=15):
     """The metric's comparison on one GPU: the same nevents seeded events (the
     event-by-event sizes, device IC, seed 1000 + k) advanced in plain FP64, in FP32
     (face pass and relaxation sources), and with the learned guess plus FP32, the
-    guess used for every cell or for the cells the warm start defers; zone-updates/s
-    of each (host wall clock around the synchronous batch call, one stream per
-    event) and each form's L2(T), L2(pibar) and L2(pi) against the plain run."""
+    guess used for every cell or for the cells the warm start defers, each with one
+    stream per event; then plain FP64 and FP32 in lockstep (one launch per kernel
+    over all events, replayed from CUDA graphs, the schedule tuned on the first 12
+    warm-up steps), and plain lockstep without graphs. Zone-updates/s of each (host
+    wall clock around the synchronous batch call), each form's L2(T), L2(pibar) and
+    L2(pi) against the plain run, and for the lockstep forms whether every event's
+    fields equal those of the stream batch of the same precision bit for bit."""
     import numpy as np
     import torch
 
@@ -575,14 +584,18 @@ def batch_forms(lib, m, nevents, steps, single_value, warmup=3):
     guess, ginfo = train_guess(lib, m, g384)
     out = {"events": nevents, "steps": steps, "warmup": warmup, "grids": sorted({g.Nx for g in grids}),
            "zone_updates_per_step": cells, "single_event_plain_fp64": single_value,
-           "timing": "host wall clock around the synchronous batch call (one stream per event)"}
+           "timing": "host wall clock around the synchronous batch call"}
     ref = None
-    for form in ("plain_fp64", "fp32", "learned_fp32", "learned_deferred_fp32"):
+    stream_fields = {}
+    for form in ("plain_fp64", "fp32", "learned_fp32", "learned_deferred_fp32") + LOCKSTEP_FORMS:
         b = GPUBatch2D(m, grids, lib=lib)
+        lockstep = form in LOCKSTEP_FORMS
+        if lockstep:
+            b.set_lockstep(True, graphs=not form.endswith("nograph"), tune=True)
         for k, e in enumerate(b.events):
             e.glauber_ic(TAU0, 1000 + k)
             e.rhs(TAU0)
-            if form != "plain_fp64":
+            if not form.startswith("plain_fp64"):
                 e.set_precision(A.FIVO_PRECISION_FP32)
             if form == "learned_fp32":
                 guess.attach(e, A.FIVO_GUESS_EVERY_CELL)
@@ -603,8 +616,17 @@ def batch_forms(lib, m, nevents, steps, single_value, warmup=3):
         adv(steps)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
-        row = {"value": steps * cells / dt, "unit": UNIT, "ms_per_step": 1e3 * dt / steps}
+        row = {"value": steps * cells / dt, "unit": UNIT, "ms_per_step": 1e3 * dt / steps,
+               "schedule": "lockstep" if lockstep else "stream per event"}
         f = _batch_fields(b, m)
+        if lockstep:
+            info = b.lockstep_info()
+            row["lockstep"] = {k: info[k] for k in ("graphs", "chosen", "candidates", "fallbacks")}
+            twin = stream_fields["plain_fp64" if form.startswith("plain_fp64") else "fp32"]
+            row["bitwise_equal_stream_batch"] = bool(
+                all(np.array_equal(f[k].view(np.int64), twin[k].view(np.int64)) for k in ("T", "pibar", "pi")))
+        elif form in ("plain_fp64", "fp32"):
+            stream_fields[form] = f
         if ref is None:
             ref = f
         else:
@@ -628,6 +650,8 @@ def batch_forms(lib, m, nevents, steps, single_value, warmup=3):
         b.close()
     guess.close()
     out["plain_batch_vs_single_event"] = out["plain_fp64"]["value"] / single_value
+    out["best_form_vs_plain_batch"] = max(out[f]["value"] for f in out if isinstance(out[f], dict)
+                                          and "value" in out[f]) / out["plain_fp64"]["value"]
     return out
 
 
@@ -666,6 +690,8 @@ def run_batch(args):
         g384, _ = model_and_grid()
         guess, ginfo = train_guess(lib, m, g384)
     b = GPUBatch2D(m, my_grids, nworkers=args.workers, lib=lib)
+    if args.lockstep:
+        b.set_lockstep(True, graphs=True, tune=True)
     for e, k in zip(b.events, mine):
         e.glauber_ic(TAU0, 1000 + k)      # the MC-Glauber IC built on the device
         e.rhs(TAU0)
@@ -682,7 +708,7 @@ def run_batch(args):
             raise RuntimeError("a batch event failed a step")
         taus = [x["tau"] for x in r]
 
-    adv(args.warmup)
+    adv(max(args.warmup, 15) if args.lockstep else args.warmup)   # lockstep: the 12 tuning steps are warm-up
     if guess is not None:
         from fivo2d.guess import newton_stats
         for e in b.events:
@@ -746,7 +772,9 @@ def run_batch(args):
         "config": {"workload": f"batch_{args.events}_events_N{sizes[0]}-{sizes[-1]}_dx0.078125_ssprk3_lhrg",
                    "events": args.events, "grids": [g.Nx for g in grids], "tau0": TAU0, "integrator": "ssprk3",
                    "cfl": CFL, "cfltau": CFLTAU, "workers": args.workers, "parallelism": f"events over {world} GPUs",
-                   "timing": "host wall clock around the synchronous batch call (one stream per event)",
+                   "timing": "host wall clock around the synchronous batch call",
+                   "schedule": "lockstep (one launch per kernel over all events, CUDA graphs, tuned)"
+                   if args.lockstep else "one stream per event",
                    "l2": "inputs (all events' state) larger than L2"},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
                 "steps": e2e_steps},
@@ -757,6 +785,8 @@ def run_batch(args):
     if learned is not None:
         line["learned_guess"] = learned
         line["config"]["workload"] += "_learned_guess"
+    if args.lockstep:
+        line["config"]["workload"] += "_lockstep"
     return line
 
 
@@ -982,6 +1012,8 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=30, help="timed steps of the batched comparison")
     ap.add_argument("--fp32-faces", action="store_true",
                     help="the mixed-precision form: the face pass in FP32 (fivo_ctx_set_precision)")
+    ap.add_argument("--lockstep", action="store_true",
+                    help="batch workload: lockstep mode (one launch per kernel over all events, CUDA graphs)")
     ap.add_argument("--guess", action="store_true",
                     help="train the learned recovery guess on other seeded events and time with it attached")
     args = ap.parse_args()

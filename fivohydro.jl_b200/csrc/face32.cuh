@@ -273,9 +273,9 @@ __device__ __forceinline__ float face_flux_pair_f(const fv::DevParams& d, const 
 }
 
 template <int EOS, bool XDIR>
-__global__ void __launch_bounds__(128, 8) k_faces32(fv::DevParams d, fv::DevState Ub, fv::DevPrims w, double tau,
-                                                   const uint8_t* ffo, float* Fh, fv::DevFlags* fl) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void faces32_body(const fv::DevParams& d, const fv::DevState& Ub, const fv::DevPrims& w,
+                                             double tau, const uint8_t* ffo, float* Fh, fv::DevFlags* fl,
+                                             long long t) {
   const long long nf = XDIR ? (long long)(d.Nxtot - 1) * d.Nytot : (long long)d.Nxtot * (d.Nytot - 1);
   const int side = (int)(t & 1);
   long long f = t >> 1;
@@ -298,6 +298,12 @@ __global__ void __launch_bounds__(128, 8) k_faces32(fv::DevParams d, fv::DevStat
     const float m = jmaxf(jmaxf(red[0], red[1]), jmaxf(red[2], red[3]));
     fv::atomic_max_pos(&fl->amax_bits, (double)m);
   }
+}
+
+template <int EOS, bool XDIR>
+__global__ void __launch_bounds__(128, 8) k_faces32(fv::DevParams d, fv::DevState Ub, fv::DevPrims w, double tau,
+                                                   const uint8_t* ffo, float* Fh, fv::DevFlags* fl) {
+  faces32_body<EOS, XDIR>(d, Ub, w, tau, ffo, Fh, fl, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 }  // namespace f32

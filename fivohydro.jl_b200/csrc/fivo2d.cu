@@ -18,6 +18,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <numeric>
+#include <tuple>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -28,6 +31,7 @@
 #include "face32.cuh"
 #include "facetile.cuh"
 #include "relax32.cuh"
+#include "batch.cuh"
 
 using namespace fv;
 
@@ -556,9 +560,16 @@ int launch_stage(fivo_ctx* c, const StageArgs& a) {
   return launch_stage_t<FIVO_EOS_CONFORMAL_HQ, false>(c, a);
 }
 
+int parse_flags(fivo_ctx* c, bool read_amax);
+
 int sync_flags(fivo_ctx* c, bool read_amax) {
   CK(cudaMemcpyAsync(c->flh, c->fl, sizeof(DevFlags), cudaMemcpyDeviceToHost, c->st));
   CK(ctx_sync(c));
+  return parse_flags(c, read_amax);
+}
+
+/* the host mirror c->flh of the flag block, just read back: errors, counters, amax */
+int parse_flags(fivo_ctx* c, bool read_amax) {
   const DevFlags& f = *c->flh;
   if (f.status == 3) return fail(FIVO_ERR_DEVICE, "learned recovery guess: a tensor-core wait gave up");
   if (f.status == 4) return fail(FIVO_ERR_DEVICE, "face pass: a tile copy to shared memory did not complete");
@@ -665,6 +676,9 @@ int copy_state(fivo_ctx* c, int dst, int src) {
   return FIVO_OK;
 }
 
+int step2_rest(fivo_ctx* c, double tau, double D, int max_halve, int max_mood, int bc, double* used, int* okout);
+int step3_rest(fivo_ctx* c, double tau, double D, int max_halve, int bc, double* used, int* okout);
+
 /* step_ssprk2_2d!, src2d/timestepper2d.jl:74-103 */
 int step2(fivo_ctx* c, double tau, double dtau, int max_halve, int max_mood, int bc, double* used, int* okout) {
   double D = dtau;
@@ -685,6 +699,12 @@ int step2(fivo_ctx* c, double tau, double dtau, int max_halve, int max_mood, int
     if (nbad == 0) { std::swap(c->iU, c->iT); *used = D; *okout = 1; return FIVO_OK; }
     if ((rc = restore_warm(c))) return rc;
   }
+  return step2_rest(c, tau, D, max_halve, max_mood, bc, used, okout);
+}
+
+/* step_ssprk2_2d!'s stage-by-stage procedure with MOOD and halving (after the
+ * optimistic pass found an inadmissible cell and was undone) */
+int step2_rest(fivo_ctx* c, double tau, double D, int max_halve, int max_mood, int bc, double* used, int* okout) {
   for (int h = 0; h <= max_halve; ++h) {
     int rc;
     if ((rc = copy_state(c, c->iU2, c->iU))) return rc;
@@ -726,6 +746,12 @@ int step3(fivo_ctx* c, double tau, double dtau, int max_halve, int bc, double* u
     std::swap(c->iU, c->iU2);    /* the state before the step */
     if ((rc = restore_warm(c))) return rc;
   }
+  return step3_rest(c, tau, D, max_halve, bc, used, okout);
+}
+
+/* step_ssprk3_2d!'s stage-by-stage procedure with halving (after the optimistic
+ * pass found an inadmissible cell and was undone) */
+int step3_rest(fivo_ctx* c, double tau, double D, int max_halve, int bc, double* used, int* okout) {
   for (int h = 0; h <= max_halve; ++h) {
     int rc;
     long long nbad = 0;
@@ -1201,20 +1227,20 @@ int advance_loop(fivo_ctx* c, double tau, double taufinal, double cfl, double cf
 }
 }  // namespace
 
-int fivo_run(fivo_ctx* c, double tau0, double taufinal, double cfl, double cfltau, int integrator, int bc,
-             int64_t max_steps, int reset_hist, fivo_run_result* out) {
-  if (!c || !out) return fail(FIVO_ERR_ARG, "null argument");
-  if (integrator != FIVO_SSPRK2 && integrator != FIVO_SSPRK3)
-    return fail(FIVO_ERR_ARG, "integrator must be FIVO_SSPRK2 or FIVO_SSPRK3");
+namespace {
+/* run_sim_2d! before its loop: the history reset, one RHS pass to populate the
+ * primitives and signal speeds (main2D.jl:418), the initial total charge */
+int run_begin(fivo_ctx* c, double tau0, int bc, int reset_hist, double* Qin) {
   int rc;
-  std::memset(out, 0, sizeof(*out));
   if (reset_hist && (rc = reset_history(c))) return rc;
   c->nsteps_run = 0;
-  /* one RHS pass to populate primitives and signal speeds (main2D.jl:418) */
   if ((rc = run_stage(c, c->iU, c->iT, c->iU, tau0, tau0, 0.0, 0.0, 0.0, COMB_RHS_ONLY, nullptr, bc, nullptr, nullptr))) return rc;
-  double Qin = 0.0;
-  if ((rc = diag(c, false, &Qin, nullptr, nullptr))) return rc;
-  if ((rc = advance_loop(c, tau0, taufinal, cfl, cfltau, integrator, bc, max_steps, out))) return rc;
+  return diag(c, false, Qin, nullptr, nullptr);
+}
+
+/* run_sim_2d! after its loop: the result's bulk diagnostics */
+int run_end(fivo_ctx* c, double Qin, fivo_run_result* out) {
+  int rc;
   out->Q0 = Qin;
   if (!out->ok) {
     out->maxu = fx::nan_(); out->dQ = fx::nan_(); out->Q1 = fx::nan_(); out->minPtot = fx::nan_();
@@ -1226,6 +1252,20 @@ int fivo_run(fivo_ctx* c, double tau0, double taufinal, double cfl, double cflta
   out->dQ = fx::fabs_(Qin) > 0 ? fx::fabs_(Qout - Qin) / fx::fabs_(Qin) : 0.0;
   out->Q1 = Qout; out->minPtot = minPtot;
   return FIVO_OK;
+}
+}  // namespace
+
+int fivo_run(fivo_ctx* c, double tau0, double taufinal, double cfl, double cfltau, int integrator, int bc,
+             int64_t max_steps, int reset_hist, fivo_run_result* out) {
+  if (!c || !out) return fail(FIVO_ERR_ARG, "null argument");
+  if (integrator != FIVO_SSPRK2 && integrator != FIVO_SSPRK3)
+    return fail(FIVO_ERR_ARG, "integrator must be FIVO_SSPRK2 or FIVO_SSPRK3");
+  int rc;
+  std::memset(out, 0, sizeof(*out));
+  double Qin = 0.0;
+  if ((rc = run_begin(c, tau0, bc, reset_hist, &Qin))) return rc;
+  if ((rc = advance_loop(c, tau0, taufinal, cfl, cfltau, integrator, bc, max_steps, out))) return rc;
+  return run_end(c, Qin, out);
 }
 
 int fivo_advance(fivo_ctx* c, double tau, double taufinal, double cfl, double cfltau, int integrator, int bc,
@@ -1600,10 +1640,15 @@ extern "C" int fivo_rhs_noalloc(const fivo_params* p, int nx, int ny, double xma
  * Events share the model parameters; each has its own grid, dt and control
  * flow, exactly as separate run_sim_2d! calls.
  * ---------------------------------------------------------------------- */
+struct Lockstep;
+int ls_destroy(Lockstep* L);
+
 struct fivo_batch {
   std::vector<fivo_ctx*> ev;
   int nworkers = 1;
   int device = 0;
+  Lockstep* ls = nullptr;     /* lockstep mode (fivo_batch_set_lockstep) */
+  bool lockstep = false;
 };
 
 int fivo_batch_create(const fivo_params* p, int nevents, const int* nx, const int* ny, const double* xmax,
@@ -1634,6 +1679,7 @@ int fivo_batch_create(const fivo_params* p, int nevents, const int* nx, const in
 
 int fivo_batch_destroy(fivo_batch* b) {
   if (!b) return FIVO_OK;
+  ls_destroy(b->ls);
   for (fivo_ctx* c : b->ev) fivo_ctx_destroy(c);
   delete b;
   return FIVO_OK;
@@ -1679,9 +1725,558 @@ int batch_for_each(fivo_batch* b, int* status, F fn) {
 }
 }  // namespace
 
+/* ------------------------------------------------------------------------
+ * Lockstep batches (fivo_batch_set_lockstep): the events' steps taken together,
+ * each kernel of a step launched once over every event's blocks (batch.cuh).
+ * A step is two launch sequences with one host read after each:
+ *   STEP  the optimistic SSPRK step of every active event: k_snapshot (when
+ *         due), the warm-start save and copy_state, then per stage the ghost
+ *         fill, flag reset, fast recovery, deferred recoveries, faces, update,
+ *         admissibility inversions and the output's ghost fill; the flag blocks
+ *         of all events gathered and read back at once.
+ *   POST  update_primitives_2d! and relax_dissipative_2d! (+ project_shear!) on
+ *         the events whose step was accepted, then the flags again.
+ * Between them the host settles, per event, what advance_loop settles after
+ * step2/step3: an event with an inadmissible cell is undone (roles, warm
+ * starts) and stepped by step2_rest/step3_rest on its own stream, exactly as
+ * a separate run would after its optimistic pass. So every event sees the same
+ * kernels on the same inputs in the same order as in fivo_run, and its results
+ * are bitwise those of a separate run.
+ * ---------------------------------------------------------------------- */
+enum { LS_STEP = 0, LS_POST = 1 };
+
+struct Lockstep {
+  int flags = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t done = nullptr;                /* blocking: the host thread sleeps while it waits */
+  cudaEvent_t ta = nullptr, tb = nullptr;    /* device time of a launch sequence */
+  int nev = 0, nsm = 148;
+  DevParams d0;                              /* the shared model; grid fields come from Geo */
+  bt::Geo* geo_d[2] = {nullptr, nullptr};    /* per block order */
+  unsigned short* eob_d[2][bt::NSHAPE] = {};
+  int nblocks[bt::NSHAPE] = {};
+  bt::Ev* tab_d = nullptr;
+  bt::Ev* tab_h = nullptr;                   /* pinned; copied in by each launch sequence */
+  unsigned int* pre_d = nullptr;
+  bt::Ctl* ctl_d = nullptr;
+  DevFlags* flg_d = nullptr;
+  DevFlags* flg_h = nullptr;                 /* pinned */
+  std::vector<std::pair<int, int>> cands;    /* (block order, deferred-pass blocks per SM) */
+  std::vector<double> cand_ms;
+  int chosen = -1;
+  int tuned_steps = 0;
+  std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs;  /* (sequence, integrator, candidate, precision) */
+  int64_t steps = 0, fallbacks = 0;
+  double ms_step = 0.0, ms_post = 0.0;
+};
+
+constexpr int LS_TUNE_ROUNDS = 2;
+
+int ls_destroy(Lockstep* L) {
+  if (!L) return FIVO_OK;
+  if (L->st) cudaStreamSynchronize(L->st);
+  for (auto& g : L->graphs) cudaGraphExecDestroy(g.second);
+  for (int o = 0; o < 2; ++o) {
+    cudaFree(L->geo_d[o]);
+    for (int s = 0; s < bt::NSHAPE; ++s) cudaFree(L->eob_d[o][s]);
+  }
+  cudaFree(L->tab_d); cudaFree(L->pre_d); cudaFree(L->ctl_d); cudaFree(L->flg_d);
+  if (L->tab_h) cudaFreeHost(L->tab_h);
+  if (L->flg_h) cudaFreeHost(L->flg_h);
+  if (L->done) cudaEventDestroy(L->done);
+  if (L->ta) cudaEventDestroy(L->ta);
+  if (L->tb) cudaEventDestroy(L->tb);
+  if (L->st) cudaStreamDestroy(L->st);
+  delete L;
+  return FIVO_OK;
+}
+
+namespace {
+
+/* the units of each launch shape for one event */
+void ls_units(const DevParams& d, long long u[bt::NSHAPE]) {
+  u[bt::SH_CELL] = d.Ntot;
+  u[bt::SH_FRAME] = d.Ntot - (long long)d.Nx * d.Ny;
+  u[bt::SH_FACEX] = 2LL * (d.Nxtot - 1) * d.Nytot;
+  u[bt::SH_FACEY] = 2LL * d.Nxtot * (d.Nytot - 1);
+  u[bt::SH_INT] = (long long)d.Nx * d.Ny;
+}
+
+int ls_create(fivo_batch* b, int flags, Lockstep** out) {
+  const int n = (int)b->ev.size();
+  if (n > 65535) return fail(FIVO_ERR_ARG, "fivo_batch_set_lockstep: at most 65535 events");
+  Lockstep* L = new Lockstep();
+  auto cleanup = [&](int code) { ls_destroy(L); return code; };
+  L->flags = flags;
+  L->nev = n;
+  L->d0 = b->ev[0]->dp;
+  L->nsm = b->ev[0]->nsm;
+  if (cudaStreamCreateWithFlags(&L->st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&L->done, cudaEventBlockingSync | cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreate(&L->ta) != cudaSuccess || cudaEventCreate(&L->tb) != cudaSuccess)
+    return cleanup(fail(FIVO_ERR_CUDA, "fivo_batch_set_lockstep: stream or event creation failed"));
+  for (int order = 0; order < 2; ++order) {
+    std::vector<int> perm(n);
+    std::iota(perm.begin(), perm.end(), 0);
+    if (order == 1)
+      std::stable_sort(perm.begin(), perm.end(),
+                       [&](int a, int c) { return b->ev[a]->dp.Ntot > b->ev[c]->dp.Ntot; });
+    std::vector<bt::Geo> geo(n);
+    std::vector<unsigned short> eob[bt::NSHAPE];
+    long long cnt[bt::NSHAPE] = {0, 0, 0, 0, 0};
+    for (int e : perm) {
+      const DevParams& d = b->ev[e]->dp;
+      bt::Geo& g = geo[e];
+      std::memset(&g, 0, sizeof(g));
+      g.Nx = d.Nx; g.Ny = d.Ny; g.Nxtot = d.Nxtot; g.Nytot = d.Nytot; g.Ntot = d.Ntot;
+      g.dx = d.dx; g.dy = d.dy; g.xmin = d.xmin; g.ymin = d.ymin;
+      long long u[bt::NSHAPE];
+      ls_units(d, u);
+      for (int s = 0; s < bt::NSHAPE; ++s) {
+        const long long nb = (u[s] + 127) / 128;
+        g.b0[s] = (int)cnt[s];
+        eob[s].insert(eob[s].end(), (size_t)nb, (unsigned short)e);
+        cnt[s] += nb;
+      }
+    }
+    for (int s = 0; s < bt::NSHAPE; ++s) {
+      if (cnt[s] >= 0x7fffffffLL) return cleanup(fail(FIVO_ERR_ARG, "fivo_batch_set_lockstep: batch too large"));
+      L->nblocks[s] = (int)cnt[s];
+      if (cudaMalloc(&L->eob_d[order][s], std::max<size_t>(1, eob[s].size()) * sizeof(unsigned short)) != cudaSuccess)
+        return cleanup(fail(FIVO_ERR_NOMEM, "fivo_batch_set_lockstep: device allocation failed"));
+      if (!eob[s].empty())
+        CK(cudaMemcpy(L->eob_d[order][s], eob[s].data(), eob[s].size() * sizeof(unsigned short),
+                      cudaMemcpyHostToDevice));
+    }
+    if (cudaMalloc(&L->geo_d[order], n * sizeof(bt::Geo)) != cudaSuccess)
+      return cleanup(fail(FIVO_ERR_NOMEM, "fivo_batch_set_lockstep: device allocation failed"));
+    CK(cudaMemcpy(L->geo_d[order], geo.data(), n * sizeof(bt::Geo), cudaMemcpyHostToDevice));
+  }
+  if (cudaMalloc(&L->tab_d, n * sizeof(bt::Ev)) != cudaSuccess ||
+      cudaMalloc(&L->pre_d, (n + 1) * sizeof(unsigned int)) != cudaSuccess ||
+      cudaMalloc(&L->ctl_d, sizeof(bt::Ctl)) != cudaSuccess ||
+      cudaMalloc(&L->flg_d, n * sizeof(DevFlags)) != cudaSuccess)
+    return cleanup(fail(FIVO_ERR_NOMEM, "fivo_batch_set_lockstep: device allocation failed"));
+  if (cudaMallocHost(&L->tab_h, n * sizeof(bt::Ev)) != cudaSuccess ||
+      cudaMallocHost(&L->flg_h, n * sizeof(DevFlags)) != cudaSuccess)
+    return cleanup(fail(FIVO_ERR_NOMEM, "fivo_batch_set_lockstep: pinned allocation failed"));
+  std::memset(L->tab_h, 0, n * sizeof(bt::Ev));
+  for (int order = 0; order < 2; ++order)
+    for (int slow : {1, 2, 4}) L->cands.push_back({order, slow});
+  L->cand_ms.assign(L->cands.size(), 0.0);
+  /* untuned: batch order, 2 blocks per SM (the single-event deferred pass's grid) */
+  L->chosen = (flags & FIVO_LOCKSTEP_TUNE) ? -1 : 1;
+  *out = L;
+  return FIVO_OK;
+}
+
+/* the buffers of event c in its record (everything but the per-pass arguments) */
+void ls_fill_common(fivo_ctx* c, bt::Ev& e) {
+  const DevParams& d = c->dp;
+  std::memset(&e, 0, sizeof(e));
+  e.w = c->w; e.h = c->h; e.fl = c->fl;
+  e.qp = c->queues; e.qa = c->queues + d.Ntot;
+  e.fhx = c->fh; e.fhy = c->fh + (size_t)d.nv * d.Ntot;
+  e.fhx32 = c->fh32; e.fhy32 = c->fh32 ? c->fh32 + (size_t)d.nv * d.Ntot : nullptr;
+  e.x0save = c->x0save;
+}
+
+/* the optimistic step of step2/step3 on the context's current roles */
+void ls_fill_step(fivo_ctx* c, bt::Ev& e, int integrator, double tau, double D, bool snap) {
+  ls_fill_common(c, e);
+  e.active = 1;
+  e.snap = snap ? 1 : 0;
+  const int U = c->iU, U1 = c->iU1, U2 = c->iU2, T = c->iT;
+  e.cp_dst = c->S[U2]; e.cp_src = c->S[U];
+  auto stage = [&](int k, int ub, int uo, double t, double ts, double wold, double wnew, int mode) {
+    StageArgs& a = e.st[k];
+    a.Ub = c->S[ub]; a.Uold = c->S[U2]; a.Uout = c->S[uo]; a.w = c->w; a.ffo = nullptr; a.bad = c->masks;
+    a.dU = nullptr; a.tau = t; a.tau_state = ts; a.dt = D; a.wold = wold; a.wnew = wnew; a.mode = mode;
+    a.fl = c->fl;
+    e.pU[k] = c->S[ub];
+    e.ptau[k] = t;
+  };
+  if (integrator == FIVO_SSPRK3) {
+    stage(0, U, U1, tau, tau + D, 1.0, 0.0, COMB_EULER);
+    stage(1, U1, T, tau + D, tau + D, 0.75, 0.25, COMB_BLEND);
+    /* step3 swaps U1 and T here: the third stage reads the second's output */
+    stage(2, T, U1, tau + (0.5 * D), tau + D, 0.0, 0.0, COMB_THIRD);
+  } else {
+    stage(0, U, U1, tau, tau + D, 1.0, 0.0, COMB_EULER);
+    stage(1, U1, T, tau + D, tau + D, 0.5, 0.5, COMB_BLEND);
+  }
+}
+
+/* update_prims + relax_project after an accepted step (state U at time tau) */
+void ls_fill_post(fivo_ctx* c, bt::Ev& e, double tau, double used, int do_relax, int do_project) {
+  ls_fill_common(c, e);
+  e.active = 1;
+  e.pU[3] = c->S[c->iU];
+  e.ptau[3] = tau;
+  e.rq = c->S[c->iU]; e.ro = c->S[c->iT];
+  e.rtau = tau; e.rD = used;
+  e.do_relax = do_relax; e.do_project = do_project;
+}
+
+#define LS_GRID(s) L.nblocks[s] ? L.nblocks[s] : 1
+
+/* enqueue one launch sequence on L.st (recorded into a graph or run directly) */
+template <int EOS, bool NCH>
+int ls_launch_t(fivo_batch* b, int seq, int integrator, int bc, int cand, int prec, bool any_sector, bool relax_on) {
+  Lockstep& L = *b->ls;
+  const int n = L.nev;
+  const int order = L.cands[cand].first;
+  const unsigned slow_blocks = (unsigned)(L.cands[cand].second * L.nsm);
+  const bt::Geo* geo = L.geo_d[order];
+  unsigned short* const* eob = L.eob_d[order];
+  const DevParams& d0 = L.d0;
+  cudaStream_t st = L.st;
+  const bool f32 = prec != FIVO_PRECISION_FP64;
+  const unsigned gr = nblk(n, 256);
+  CK(cudaMemcpyAsync(L.tab_d, L.tab_h, n * sizeof(bt::Ev), cudaMemcpyHostToDevice, st));
+  auto prim_pass = [&](int which) -> int {
+    bt::kb_prim_fast<EOS, NCH><<<LS_GRID(bt::SH_CELL), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_CELL], which);
+    CKL();
+    bt::kb_scan<<<1, 1024, 0, st>>>(L.tab_d, n, 0, L.pre_d, L.ctl_d);
+    CKL();
+    bt::kb_prim_slow<EOS, NCH><<<slow_blocks, 128, 0, st>>>(d0, geo, L.tab_d, L.pre_d, n, L.ctl_d, which);
+    CKL();
+    return FIVO_OK;
+  };
+  int rc;
+  if (seq == LS_STEP) {
+    bt::kb_pre_step<<<LS_GRID(bt::SH_CELL), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_CELL]);
+    CKL();
+    const int nst = integrator == FIVO_SSPRK3 ? 3 : 2;
+    const bool full = d0.hasNu && d0.hasPi && d0.hasShear;
+    for (int k = 0; k < nst; ++k) {
+      if (k == 0) {
+        bt::kb_bc<<<LS_GRID(bt::SH_FRAME), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FRAME], 0, bc);
+        CKL();
+      }
+      bt::kb_reset<<<gr, 256, 0, st>>>(L.tab_d, n, k == 0 ? (1 | 2 | 64) : (1 | 2));
+      CKL();
+      if ((rc = prim_pass(k))) return rc;
+      if (f32) {
+        bt::kb_faces<EOS, true, true><<<LS_GRID(bt::SH_FACEX), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FACEX], k);
+        CKL();
+        bt::kb_faces<EOS, false, true><<<LS_GRID(bt::SH_FACEY), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FACEY], k);
+        CKL();
+        if (full) bt::kb_update<EOS, NCH, float, true><<<LS_GRID(bt::SH_INT), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_INT], k);
+        else bt::kb_update<EOS, NCH, float, false><<<LS_GRID(bt::SH_INT), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_INT], k);
+        CKL();
+      } else {
+        bt::kb_faces<EOS, true, false><<<LS_GRID(bt::SH_FACEX), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FACEX], k);
+        CKL();
+        bt::kb_faces<EOS, false, false><<<LS_GRID(bt::SH_FACEY), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FACEY], k);
+        CKL();
+        if (full) bt::kb_update<EOS, NCH, double, true><<<LS_GRID(bt::SH_INT), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_INT], k);
+        else bt::kb_update<EOS, NCH, double, false><<<LS_GRID(bt::SH_INT), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_INT], k);
+        CKL();
+      }
+      bt::kb_scan<<<1, 1024, 0, st>>>(L.tab_d, n, 1, L.pre_d, L.ctl_d);
+      CKL();
+      bt::kb_adm_slow<EOS, NCH><<<(unsigned)L.nsm, 128, 0, st>>>(d0, geo, L.tab_d, L.pre_d, n, L.ctl_d, k);
+      CKL();
+      bt::kb_bc<<<LS_GRID(bt::SH_FRAME), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FRAME], k + 1, bc);
+      CKL();
+    }
+  } else {
+    if (any_sector) {
+      bt::kb_reset<<<gr, 256, 0, st>>>(L.tab_d, n, 1 | 64);
+      CKL();
+      if ((rc = prim_pass(3))) return rc;
+    }
+    if (relax_on) {
+      bt::kb_reset<<<gr, 256, 0, st>>>(L.tab_d, n, 4);
+      CKL();
+      if (prec == FIVO_PRECISION_FP32 && any_sector)
+        bt::kb_relax<EOS, false, true><<<LS_GRID(bt::SH_CELL), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_CELL]);
+      else if (d0.hasM2)
+        bt::kb_relax<EOS, true, false><<<LS_GRID(bt::SH_CELL), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_CELL]);
+      else
+        bt::kb_relax<EOS, false, false><<<LS_GRID(bt::SH_CELL), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_CELL]);
+      CKL();
+      bt::kb_post_hist<<<LS_GRID(bt::SH_CELL), 128, 0, st>>>(geo, L.tab_d, eob[bt::SH_CELL]);
+      CKL();
+    }
+  }
+  bt::kb_gather_flags<<<nblk((long long)n * (sizeof(DevFlags) / 8), 256), 256, 0, st>>>(L.tab_d, n, L.flg_d);
+  CKL();
+  CK(cudaMemcpyAsync(L.flg_h, L.flg_d, n * sizeof(DevFlags), cudaMemcpyDeviceToHost, st));
+  return FIVO_OK;
+}
+
+int ls_launch(fivo_batch* b, int seq, int integrator, int bc, int cand, int prec, bool any_sector, bool relax_on) {
+  const DevParams& d = b->ls->d0;
+  if (d.p.eos_kind == FIVO_EOS_LATTICE_HRG)
+    return ls_launch_t<FIVO_EOS_LATTICE_HRG, true>(b, seq, integrator, bc, cand, prec, any_sector, relax_on);
+  if (d.ncharge) return ls_launch_t<FIVO_EOS_CONFORMAL_HQ, true>(b, seq, integrator, bc, cand, prec, any_sector, relax_on);
+  return ls_launch_t<FIVO_EOS_CONFORMAL_HQ, false>(b, seq, integrator, bc, cand, prec, any_sector, relax_on);
+}
+
+/* run one launch sequence (replaying its graph when graphs are on) and wait for it */
+int ls_exec(fivo_batch* b, int seq, int integrator, int bc, int cand, int prec, bool any_sector, bool relax_on,
+            float* ms) {
+  Lockstep& L = *b->ls;
+  CK(cudaEventRecord(L.ta, L.st));
+  if (L.flags & FIVO_LOCKSTEP_GRAPHS) {
+    const auto key = std::make_tuple(seq, integrator, cand, prec);
+    auto it = L.graphs.find(key);
+    if (it == L.graphs.end()) {
+      CK(cudaStreamBeginCapture(L.st, cudaStreamCaptureModeThreadLocal));
+      const int rc = ls_launch(b, seq, integrator, bc, cand, prec, any_sector, relax_on);
+      cudaGraph_t g = nullptr;
+      const cudaError_t ec = cudaStreamEndCapture(L.st, &g);
+      if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+      if (ec != cudaSuccess) return fail(FIVO_ERR_CUDA, std::string("lockstep graph capture: ") + cudaGetErrorString(ec));
+      cudaGraphExec_t x = nullptr;
+      const cudaError_t ei = cudaGraphInstantiate(&x, g, 0);
+      cudaGraphDestroy(g);
+      if (ei != cudaSuccess) return fail(FIVO_ERR_CUDA, std::string("lockstep graph instantiation: ") + cudaGetErrorString(ei));
+      it = L.graphs.emplace(key, x).first;
+    }
+    CK(cudaGraphLaunch(it->second, L.st));
+  } else {
+    const int rc = ls_launch(b, seq, integrator, bc, cand, prec, any_sector, relax_on);
+    if (rc) return rc;
+  }
+  CK(cudaEventRecord(L.tb, L.st));
+  CK(cudaEventRecord(L.done, L.st));
+  CK(cudaEventSynchronize(L.done));
+  CK(cudaEventElapsedTime(ms, L.ta, L.tb));
+  return FIVO_OK;
+}
+
+/* fn(k) for the listed events on the batch's worker threads */
+template <class F>
+void ls_parallel(fivo_batch* b, const std::vector<int>& ks, F fn) {
+  std::atomic<int> next{0};
+  auto worker = [&]() {
+    if (cudaSetDevice(b->device) != cudaSuccess) return;
+    for (;;) {
+      const int j = next.fetch_add(1);
+      if (j >= (int)ks.size()) break;
+      fn(ks[j]);
+    }
+  };
+  const int nw = std::min<int>(b->nworkers, (int)ks.size());
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nw; ++t) pool.emplace_back(worker);
+  worker();
+  for (auto& t : pool) t.join();
+}
+
+/* advance_loop (run_sim_2d!'s while loop, main2D.jl:436-513) for every event of
+ * the batch in lockstep; tau[k] is event k's time, advanced in place */
+int ls_loop(fivo_batch* b, std::vector<double>& tau, double taufinal, double cfl, double cfltau, int integrator,
+            int bc, int64_t max_steps, fivo_run_result* out, std::vector<int>& st, std::vector<std::string>& msg) {
+  Lockstep& L = *b->ls;
+  const int n = L.nev;
+  const DevParams& d = L.d0;
+  const fivo_params& p = d.p;
+  const bool any_sector = p.enable_shear || p.enable_bulk || p.enable_diff;
+  const bool relax_on = d.nv > 4 && (any_sector || d.hasShear);
+  const bool post = any_sector || d.hasShear;
+  const int prec = b->ev[0]->precision;
+  for (fivo_ctx* c : b->ev) {
+    if (c->learned) return fail(FIVO_ERR_CONFIG, "lockstep batch: the events must use the plain recovery (no learned guess)");
+    if (c->precision != prec) return fail(FIVO_ERR_CONFIG, "lockstep batch: every event must use the same precision");
+    if (!c->x0save) {
+      if (cudaMalloc(&c->x0save, 4 * (size_t)c->dp.Ntot * sizeof(double)) != cudaSuccess) {
+        c->x0save = nullptr;
+        return fail(FIVO_ERR_NOMEM, "device allocation failed");
+      }
+    }
+    /* the batch stream reads what the contexts' streams wrote */
+    CK(ctx_sync(c));
+  }
+  std::vector<char> done(n, 0), stepped(n, 0);
+  std::vector<double> D(n, 0.0), used(n, 0.0), msr(n, 0.0);
+  std::vector<int64_t> nsteps(n, 0), npf(n, 0), nvac(n, 0);
+  for (int k = 0; k < n; ++k) out[k].ok = 1;
+  while (true) {
+    int nact = 0;
+    for (int k = 0; k < n; ++k) {
+      fivo_ctx* c = b->ev[k];
+      bt::Ev& e = L.tab_h[k];
+      e.active = 0;
+      stepped[k] = 0;
+      if (done[k] || st[k] != FIVO_OK) continue;
+      if (!(tau[k] < taufinal && nsteps[k] < max_steps)) { done[k] = 1; continue; }
+      double Dk;
+      fivo_compute_dt(c, tau[k], cfl, cfltau, &Dk);
+      Dk = jmin(Dk, taufinal - tau[k]);
+      if (Dk <= 0) { done[k] = 1; continue; }
+      const bool snap = c->hist_valid || c->nsteps_run > 0;
+      if (snap) c->hist_valid = true;
+      c->cnt.nmood = 0; c->cnt.nhalve = 0;
+      ls_fill_step(c, e, integrator, tau[k], Dk, snap);
+      D[k] = Dk;
+      ++nact;
+    }
+    if (!nact) break;
+    /* the schedule: the chosen candidate, or the next one to time */
+    int cand = L.chosen;
+    const bool tuning = cand < 0;
+    if (tuning) cand = L.tuned_steps % (int)L.cands.size();
+    float ms = 0.f;
+    int rc = ls_exec(b, LS_STEP, integrator, bc, cand, prec, any_sector, relax_on, &ms);
+    if (rc) return rc;
+    L.ms_step += ms;
+    L.steps += 1;
+    if (tuning) {
+      double& best = L.cand_ms[cand];
+      if (best == 0.0 || ms < best) best = ms;
+      if (++L.tuned_steps >= LS_TUNE_ROUNDS * (int)L.cands.size())
+        L.chosen = (int)(std::min_element(L.cand_ms.begin(), L.cand_ms.end()) - L.cand_ms.begin());
+    }
+    std::vector<int> redo;
+    for (int k = 0; k < n; ++k) {
+      if (!L.tab_h[k].active) continue;
+      fivo_ctx* c = b->ev[k];
+      *c->flh = L.flg_h[k];
+      if ((rc = parse_flags(c, true))) { st[k] = rc; msg[k] = g_err; continue; }
+      const long long nbad = c->flh->nbad;
+      if (integrator == FIVO_SSPRK3) { std::swap(c->iU1, c->iT); std::swap(c->iU, c->iT); }
+      if (nbad == 0) {
+        if (integrator != FIVO_SSPRK3) std::swap(c->iU, c->iT);
+        used[k] = D[k];
+        stepped[k] = 1;
+      } else {
+        if (integrator == FIVO_SSPRK3) std::swap(c->iU, c->iU2);   /* the state before the step */
+        redo.push_back(k);
+      }
+    }
+    /* events whose optimistic step found an inadmissible cell: the rest of step2/step3 */
+    if (!redo.empty()) {
+      L.fallbacks += (int64_t)redo.size();
+      ls_parallel(b, redo, [&](int k) {
+        fivo_ctx* c = b->ev[k];
+        int ok = 0, r = restore_warm(c);
+        if (!r) {
+          r = integrator == FIVO_SSPRK3 ? step3_rest(c, tau[k], D[k], 12, bc, &used[k], &ok)
+                                        : step2_rest(c, tau[k], D[k], 12, 2, bc, &used[k], &ok);
+        }
+        if (!r && ctx_sync(c) != cudaSuccess) r = fail(FIVO_ERR_CUDA, "lockstep batch: stream synchronisation failed");
+        if (r) { st[k] = r; msg[k] = g_err; return; }
+        if (!ok) { out[k].ok = 0; done[k] = 1; return; }
+        stepped[k] = 1;
+      });
+    }
+    int npost = 0;
+    for (int k = 0; k < n; ++k) {
+      L.tab_h[k].active = 0;
+      if (!stepped[k]) continue;
+      fivo_ctx* c = b->ev[k];
+      tau[k] += used[k];
+      nsteps[k] += 1;
+      c->nsteps_run += 1;
+      if (post) {
+        ls_fill_post(c, L.tab_h[k], tau[k], used[k], any_sector ? 1 : 0, any_sector ? d.hasShear : 1);
+        ++npost;
+      }
+    }
+    if (npost) {
+      if ((rc = ls_exec(b, LS_POST, integrator, bc, L.chosen < 0 ? 1 : L.chosen, prec, any_sector, relax_on, &ms)))
+        return rc;
+      L.ms_post += ms;
+    }
+    for (int k = 0; k < n; ++k) {
+      if (!stepped[k]) continue;
+      fivo_ctx* c = b->ev[k];
+      if (post) {
+        if (relax_on)   /* relax_project: U's dissipative planes are now the scratch state's */
+          for (int a = 4; a < d.nv; ++a) std::swap(c->S[c->iU].f[a], c->S[c->iT].f[a]);
+        *c->flh = L.flg_h[k];
+        if (any_sector && (rc = parse_flags(c, false))) { st[k] = rc; msg[k] = g_err; continue; }
+        if (d.hasShear) {
+          uint64_t bits = c->flh->shear_max_bits;
+          double r;
+          std::memcpy(&r, &bits, 8);
+          msr[k] = jmax(msr[k], r);
+        }
+      }
+      npf[k] += c->cnt.nprimfail;
+      nvac[k] += c->cnt.nvacuum;
+    }
+  }
+  for (int k = 0; k < n; ++k) {
+    out[k].tau = tau[k]; out[k].nsteps = nsteps[k]; out[k].nprimfail = npf[k]; out[k].nvacuum = nvac[k];
+    out[k].max_shear_res = msr[k];
+  }
+  return FIVO_OK;
+}
+
+/* per-event statuses and messages of a lockstep call into the batch's convention */
+int ls_status(const std::vector<int>& st, const std::vector<std::string>& msg, int* status) {
+  int first = -1;
+  for (size_t k = 0; k < st.size(); ++k) {
+    if (status) status[k] = st[k];
+    if (st[k] != FIVO_OK && first < 0) first = (int)k;
+  }
+  if (first >= 0) return fail(st[first], "event " + std::to_string(first) + ": " + msg[first]);
+  return FIVO_OK;
+}
+
+}  // namespace
+
+int fivo_batch_set_lockstep(fivo_batch* b, int enable, int flags) {
+  if (!b) return fail(FIVO_ERR_ARG, "null argument");
+  if (flags & ~(FIVO_LOCKSTEP_GRAPHS | FIVO_LOCKSTEP_TUNE)) return fail(FIVO_ERR_ARG, "fivo_batch_set_lockstep: unknown flags");
+  if (!enable) { b->lockstep = false; return FIVO_OK; }
+  if (cudaSetDevice(b->device) != cudaSuccess) return fail(FIVO_ERR_CUDA, "cudaSetDevice failed");
+  if (b->ls && b->ls->flags != flags) { ls_destroy(b->ls); b->ls = nullptr; }
+  if (!b->ls) {
+    int rc = ls_create(b, flags, &b->ls);
+    if (rc) { b->ls = nullptr; return rc; }
+  }
+  b->lockstep = true;
+  return FIVO_OK;
+}
+
+int fivo_batch_lockstep_info(fivo_batch* b, fivo_lockstep_info* out) {
+  if (!b || !out) return fail(FIVO_ERR_ARG, "null argument");
+  std::memset(out, 0, sizeof(*out));
+  out->enabled = b->lockstep ? 1 : 0;
+  out->chosen = -1;
+  if (!b->ls) return FIVO_OK;
+  const Lockstep& L = *b->ls;
+  out->flags = L.flags;
+  out->ncand = std::min<int>((int)L.cands.size(), FIVO_LOCKSTEP_MAXCAND);
+  out->chosen = L.chosen;
+  for (int i = 0; i < out->ncand; ++i) {
+    out->cand_order[i] = L.cands[i].first;
+    out->cand_slow[i] = L.cands[i].second;
+    out->cand_ms[i] = L.cand_ms[i];
+  }
+  out->steps = L.steps;
+  out->fallbacks = L.fallbacks;
+  out->ms_step = L.ms_step;
+  out->ms_post = L.ms_post;
+  return FIVO_OK;
+}
+
 int fivo_batch_run(fivo_batch* b, double tau0, double taufinal, double cfl, double cfltau, int integrator, int bc,
                    int64_t max_steps, int reset_hist, fivo_run_result* results, int* status) {
   if (!b || !results) return fail(FIVO_ERR_ARG, "null argument");
+  if (integrator != FIVO_SSPRK2 && integrator != FIVO_SSPRK3)
+    return fail(FIVO_ERR_ARG, "integrator must be FIVO_SSPRK2 or FIVO_SSPRK3");
+  if (b->lockstep) {
+    const int n = (int)b->ev.size();
+    std::vector<double> Qin(n, 0.0), tau(n, tau0);
+    int rc = batch_for_each(b, status, [&](int k) {
+      std::memset(&results[k], 0, sizeof(results[k]));
+      return run_begin(b->ev[k], tau0, bc, reset_hist, &Qin[k]);
+    });
+    if (rc) return rc;
+    if (cudaSetDevice(b->device) != cudaSuccess) return fail(FIVO_ERR_CUDA, "cudaSetDevice failed");
+    std::vector<int> st(n, FIVO_OK);
+    std::vector<std::string> msg(n);
+    if ((rc = ls_loop(b, tau, taufinal, cfl, cfltau, integrator, bc, max_steps, results, st, msg))) return rc;
+    if ((rc = ls_status(st, msg, status))) return rc;
+    return batch_for_each(b, status, [&](int k) { return run_end(b->ev[k], Qin[k], &results[k]); });
+  }
   return batch_for_each(b, status, [&](int k) {
     return fivo_run(b->ev[k], tau0, taufinal, cfl, cfltau, integrator, bc, max_steps, reset_hist, &results[k]);
   });
@@ -1690,6 +2285,19 @@ int fivo_batch_run(fivo_batch* b, double tau0, double taufinal, double cfl, doub
 int fivo_batch_advance(fivo_batch* b, const double* tau, double taufinal, double cfl, double cfltau, int integrator,
                        int bc, int64_t max_steps, fivo_run_result* results, int* status) {
   if (!b || !tau || !results) return fail(FIVO_ERR_ARG, "null argument");
+  if (integrator != FIVO_SSPRK2 && integrator != FIVO_SSPRK3)
+    return fail(FIVO_ERR_ARG, "integrator must be FIVO_SSPRK2 or FIVO_SSPRK3");
+  if (b->lockstep) {
+    const int n = (int)b->ev.size();
+    std::vector<double> t(tau, tau + n);
+    for (int k = 0; k < n; ++k) std::memset(&results[k], 0, sizeof(results[k]));
+    if (cudaSetDevice(b->device) != cudaSuccess) return fail(FIVO_ERR_CUDA, "cudaSetDevice failed");
+    std::vector<int> st(n, FIVO_OK);
+    std::vector<std::string> msg(n);
+    int rc = ls_loop(b, t, taufinal, cfl, cfltau, integrator, bc, max_steps, results, st, msg);
+    if (rc) return rc;
+    return ls_status(st, msg, status);
+  }
   return batch_for_each(b, status, [&](int k) {
     return fivo_advance(b->ev[k], tau[k], taufinal, cfl, cfltau, integrator, bc, max_steps, &results[k]);
   });

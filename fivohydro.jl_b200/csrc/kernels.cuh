@@ -110,8 +110,7 @@ __device__ __forceinline__ void load_dis(const DevParams& d, const DevState& U, 
 /* apply_bc_2d!, src2d/bc2d.jl:14-65. Both passes together leave every ghost
  * cell equal to U[clamp(ix), clamp(iy)] (outflow) or U[wrap(ix), wrap(iy)]
  * (periodic), which is what one thread per ghost cell writes. */
-__global__ void k_bc(DevParams d, DevState U, int bc) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void bc_body(const DevParams& d, const DevState& U, int bc, long long t) {
   const int ng = d.ng, Nx = d.Nx, Ny = d.Ny;
   const long long nframe = (long long)d.Nxtot * d.Nytot - (long long)Nx * Ny;
   if (t >= nframe) return;
@@ -137,6 +136,10 @@ __global__ void k_bc(DevParams d, DevState U, int bc) {
   }
   long long dst = (long long)ix * d.Nytot + iy, src = (long long)sx * d.Nytot + sy;
   for (int a = 0; a < d.nv; ++a) U.f[a][dst] = U.f[a][src];
+}
+
+__global__ void k_bc(DevParams d, DevState U, int bc) {
+  bc_body(d, U, bc, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 /* ------------------------------------------------------- primitive recovery */
@@ -1180,10 +1183,9 @@ __device__ __forceinline__ double relax_cell(const DevParams& d, const DevState&
  * monitor (max and sum over interior cells) is reduced over the warp before
  * its atomics: one per warp instead of one per cell on a single address. */
 template <int EOS, bool M2>
-__global__ void __launch_bounds__(128) k_relax(DevParams d, DevState Uq, DevState Uo, DevPrims w,
-                                               DevHist h, double tau, double D, int do_relax,
-                                               int do_project, DevFlags* fl) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void relax_body(const DevParams& d, const DevState& Uq, const DevState& Uo,
+                                           const DevPrims& w, const DevHist& h, double tau, double D, int do_relax,
+                                           int do_project, DevFlags* fl, long long i) {
   double rel = -1.0;
   if (i < d.Ntot) rel = relax_cell<EOS, M2>(d, Uq, Uo, w, h, tau, D, do_relax, do_project, i);
   if (do_project && d.hasShear) {
@@ -1199,13 +1201,20 @@ __global__ void __launch_bounds__(128) k_relax(DevParams d, DevState Uq, DevStat
   }
 }
 
+template <int EOS, bool M2>
+__global__ void __launch_bounds__(128) k_relax(DevParams d, DevState Uq, DevState Uo, DevPrims w,
+                                               DevHist h, double tau, double D, int do_relax,
+                                               int do_project, DevFlags* fl) {
+  relax_body<EOS, M2>(d, Uq, Uo, w, h, tau, D, do_relax, do_project, fl,
+                      (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 /* --------------------------------------------------------------- utilities */
 
 /* flag resets on the device (no host staging, so nothing races a queued copy).
  * what: 1 = per-pass counters, 2 = amax (set to amax_bits), 4 = shear monitor,
  * 8 = end-of-run diagnostics */
-__global__ void k_reset_flags(DevFlags* fl, int what, unsigned long long amax_bits) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ void reset_flags_dev(DevFlags* fl, int what, unsigned long long amax_bits) {
   if (what & 1) {
     fl->nprimfail = 0; fl->nvacuum = 0; fl->rep = 0x7fffffffffffffffULL;
     fl->qcount_p = 0; fl->qnext_p = 0; fl->qcount_a = 0; fl->qnext_a = 0;
@@ -1220,17 +1229,26 @@ __global__ void k_reset_flags(DevFlags* fl, int what, unsigned long long amax_bi
   fl->status = 0;
 }
 
+__global__ void k_reset_flags(DevFlags* fl, int what, unsigned long long amax_bits) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  reset_flags_dev(fl, what, amax_bits);
+}
+
 __global__ void k_fill_nan(double* p, long long n) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) p[i] = nan_();
 }
 
 /* run_sim_2d! history snapshot (main2D.jl:458-463): alpha_prev = alpha, T_prev = exp(yT) */
+__device__ __forceinline__ void snapshot_cell(const DevPrims& w, const DevHist& h, long long i) {
+  h.alpha_prev[i] = w.alpha[i];
+  h.T_prev[i] = fx_exp(w.yT[i]);
+}
+
 __global__ void k_snapshot(DevParams d, DevPrims w, DevHist h) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.Ntot) return;
-  h.alpha_prev[i] = w.alpha[i];
-  h.T_prev[i] = fx_exp(w.yT[i]);
+  snapshot_cell(w, h, i);
 }
 
 __global__ void k_copy_planes(DevState dst, DevState src, int a0, int a1, long long n) {
@@ -1484,9 +1502,9 @@ __device__ __forceinline__ void load_cons(const DevParams& d, const DevState& U,
 }
 
 template <int EOS, bool NCH>
-__global__ void __launch_bounds__(128, FV_FAST_MINB) k_prim_fast(DevParams d, DevState U, DevPrims w, DevHist h, double tau,
-                                                   DevFlags* fl, unsigned int* queue) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void prim_fast_body(const DevParams& d, const DevState& U, const DevPrims& w,
+                                               const DevHist& h, double tau, DevFlags* fl, unsigned int* queue,
+                                               long long i) {
   bool vac = false, defer = false;
   unsigned nit = 0, natt = 0;
   if (i < d.Ntot) {
@@ -1523,6 +1541,12 @@ __global__ void __launch_bounds__(128, FV_FAST_MINB) k_prim_fast(DevParams d, De
     base = __shfl_sync(0xffffffffu, base, 0);
     if (defer) queue[base + __popc(md & ((1u << lane) - 1u))] = (unsigned)i;
   }
+}
+
+template <int EOS, bool NCH>
+__global__ void __launch_bounds__(128, FV_FAST_MINB) k_prim_fast(DevParams d, DevState U, DevPrims w, DevHist h, double tau,
+                                                   DevFlags* fl, unsigned int* queue) {
+  prim_fast_body<EOS, NCH>(d, U, w, h, tau, fl, queue, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 /* The warm pass with the learned guess in front of it. Every cell of a block of
@@ -1752,27 +1776,11 @@ __device__ __forceinline__ void pair_sync(int p) {
  * that cons_to_prim_2d! runs when the warm one fails; the second stops early
  * when the first succeeds. The pair takes cells from the queue one at a time so
  * that long and short recoveries balance over the pairs. */
+/* one queued cell i, taken by the warp pair `pair` of the block (both warps call it) */
 template <int EOS, bool NCH>
-__global__ void __launch_bounds__(128) k_prim_slow(DevParams d, DevState U, DevPrims w, DevHist h, double tau,
-                                                   DevFlags* fl, const unsigned int* queue, const unsigned int* qcount,
-                                                   unsigned int* qnext) {
-  __shared__ unsigned int s_q[2];
-  __shared__ int s_stop[2];
-  __shared__ Recovery s_cold[2];
-  const unsigned n = *(volatile const unsigned int*)qcount;
-  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&fl->tot_p, (unsigned long long)n);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int pair = warp >> 1;
-  const bool lead = (warp & 1) == 0;
-  while (true) {
-    if (lead && lane == 0) {
-      s_q[pair] = atomicAdd(qnext, 1u);
-      s_stop[pair] = 0;
-    }
-    pair_sync(pair);
-    const unsigned q = *(volatile unsigned int*)&s_q[pair];
-    if (q >= n) break;
-    const long long i = queue[q];
+__device__ __forceinline__ void slow_item(const DevParams& d, const DevState& U, const DevPrims& w, const DevHist& h,
+                                          double tau, DevFlags* fl, long long i, int lane, bool lead, int pair,
+                                          int* s_stop, Recovery* s_cold) {
     CellCons c;
     load_cons(d, U, i, tau, c);
     const double yT0 = h.x0_yT[i], phi0 = h.x0_phi[i], ux0 = h.x0_ux[i], uy0 = h.x0_uy[i];
@@ -1799,6 +1807,29 @@ __global__ void __launch_bounds__(128) k_prim_slow(DevParams d, DevState U, DevP
       }
       store_recovery<EOS>(d, w, h, i, r);
     }
+}
+
+template <int EOS, bool NCH>
+__global__ void __launch_bounds__(128) k_prim_slow(DevParams d, DevState U, DevPrims w, DevHist h, double tau,
+                                                   DevFlags* fl, const unsigned int* queue, const unsigned int* qcount,
+                                                   unsigned int* qnext) {
+  __shared__ unsigned int s_q[2];
+  __shared__ int s_stop[2];
+  __shared__ Recovery s_cold[2];
+  const unsigned n = *(volatile const unsigned int*)qcount;
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&fl->tot_p, (unsigned long long)n);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int pair = warp >> 1;
+  const bool lead = (warp & 1) == 0;
+  while (true) {
+    if (lead && lane == 0) {
+      s_q[pair] = atomicAdd(qnext, 1u);
+      s_stop[pair] = 0;
+    }
+    pair_sync(pair);
+    const unsigned q = *(volatile unsigned int*)&s_q[pair];
+    if (q >= n) break;
+    slow_item<EOS, NCH>(d, U, w, h, tau, fl, (long long)queue[q], lane, lead, pair, s_stop, s_cold);
   }
 }
 
@@ -1919,9 +1950,8 @@ __device__ __forceinline__ double face_flux_pair(const DevParams& d, const Src& 
 /* two lanes per face of one direction, every face of the (ghost-inclusive) grid;
  * the lane of the left state stores the even rows, its partner the odd ones */
 template <int EOS, bool XDIR>
-__global__ void __launch_bounds__(128, FV_FACE_MINB) k_faces(DevParams d, DevState Ub, DevPrims w, double tau,
-                                               const uint8_t* ffo, double* Fh, DevFlags* fl) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void faces_body(const DevParams& d, const DevState& Ub, const DevPrims& w, double tau,
+                                           const uint8_t* ffo, double* Fh, DevFlags* fl, long long t) {
   const long long nf = XDIR ? (long long)(d.Nxtot - 1) * d.Nytot : (long long)d.Nxtot * (d.Nytot - 1);
   const int side = (int)(t & 1);
   long long f = t >> 1;
@@ -1945,6 +1975,12 @@ __global__ void __launch_bounds__(128, FV_FACE_MINB) k_faces(DevParams d, DevSta
     double m = jmax(jmax(red[0], red[1]), jmax(red[2], red[3]));
     atomic_max_pos(&fl->amax_bits, m);
   }
+}
+
+template <int EOS, bool XDIR>
+__global__ void __launch_bounds__(128, FV_FACE_MINB) k_faces(DevParams d, DevState Ub, DevPrims w, double tau,
+                                               const uint8_t* ffo, double* Fh, DevFlags* fl) {
+  faces_body<EOS, XDIR>(d, Ub, w, tau, ffo, Fh, fl, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 /* cell_admissible_2d up to (not including) the inversion: 0 inadmissible,
@@ -1979,15 +2015,14 @@ __device__ __forceinline__ int adm_prefilter(const DevParams& d, const double u[
  * index is a compile-time constant and the per-cell row arrays live in registers; the
  * arithmetic is the same. */
 template <int EOS, bool NCH, typename FT = double, bool FULL = false>
-__global__ void __launch_bounds__(128) k_update(DevParams d0, StageArgs s, const FT* Fhx, const FT* Fhy,
-                                                unsigned int* aqueue) {
+__device__ __forceinline__ void update_body(const DevParams& d0, const StageArgs& s, const FT* Fhx, const FT* Fhy,
+                                            unsigned int* aqueue, long long t) {
   DevParams d = d0;
   if (FULL) {
     d.iDtau = 0; d.iSx = 1; d.iSy = 2; d.iE = 3; d.iNux = 4; d.iNuy = 5; d.iPi = 6;
     d.iPixx = 7; d.iPixy = 8; d.iPiyy = 9; d.iPieta = 10; d.nvf = 11;
     d.hasNu = 1; d.hasPi = 1; d.hasShear = 1;
   }
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int verdict = 1;
   long long i = 0;
   if (t < (long long)d.Nx * d.Ny) {
@@ -2056,6 +2091,26 @@ __global__ void __launch_bounds__(128) k_update(DevParams d0, StageArgs s, const
   }
 }
 
+template <int EOS, bool NCH, typename FT = double, bool FULL = false>
+__global__ void __launch_bounds__(128) k_update(DevParams d0, StageArgs s, const FT* Fhx, const FT* Fhy,
+                                                unsigned int* aqueue) {
+  update_body<EOS, NCH, FT, FULL>(d0, s, Fhx, Fhy, aqueue, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+/* the inversion of cell_admissible_2d for one queued cell i (src2d/floors2d.jl:329-335), by one warp */
+template <int EOS, bool NCH>
+__device__ __forceinline__ void adm_item(const DevParams& d, const DevState& Uout, double tau_state, uint8_t* bad,
+                                         DevFlags* fl, long long i, int lane) {
+  CellCons c;
+  load_cons(d, Uout, i, tau_state, c);
+  Recovery r = recover_warp<EOS, NCH>(c, d, nan_(), nan_(), nan_(), nan_(), 80, 1e-12, lane);
+  if (lane == 0) {
+    bool adm = r.ok || r.reason == PRR_VACUUM;
+    bad[i] = adm ? 0 : 1;
+    if (!adm) atomicAdd((unsigned long long*)&fl->nbad, 1ULL);
+  }
+}
+
 /* the inversion of cell_admissible_2d for the queued cells (src2d/floors2d.jl:329-335),
  * one warp per cell */
 template <int EOS, bool NCH>
@@ -2069,15 +2124,7 @@ __global__ void __launch_bounds__(128) k_adm_slow(DevParams d, DevState Uout, do
     if (lane == 0) q = atomicAdd(&fl->qnext_a, 1u);
     q = __shfl_sync(FV_FULL, q, 0);
     if (q >= n) break;
-    const long long i = aqueue[q];
-    CellCons c;
-    load_cons(d, Uout, i, tau_state, c);
-    Recovery r = recover_warp<EOS, NCH>(c, d, nan_(), nan_(), nan_(), nan_(), 80, 1e-12, lane);
-    if (lane == 0) {
-      bool adm = r.ok || r.reason == PRR_VACUUM;
-      bad[i] = adm ? 0 : 1;
-      if (!adm) atomicAdd((unsigned long long*)&fl->nbad, 1ULL);
-    }
+    adm_item<EOS, NCH>(d, Uout, tau_state, bad, fl, (long long)aqueue[q], lane);
   }
 }
 

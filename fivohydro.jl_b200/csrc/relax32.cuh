@@ -307,9 +307,9 @@ __device__ __forceinline__ double relax_cell32(const DevParams& d, const DevStat
 }
 
 template <int EOS>
-__global__ void __launch_bounds__(128) k_relax32(DevParams d, DevState Uq, DevState Uo, DevPrims w, DevHist h,
-                                                 double tau, double D, int do_relax, int do_project, DevFlags* fl) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void relax32_body(const DevParams& d, const DevState& Uq, const DevState& Uo,
+                                             const DevPrims& w, const DevHist& h, double tau, double D, int do_relax,
+                                             int do_project, DevFlags* fl, long long i) {
   double rel = -1.0;
   if (i < d.Ntot) rel = relax_cell32<EOS>(d, Uq, Uo, w, h, tau, D, do_relax, do_project, i);
   if (do_project && d.hasShear) {
@@ -323,6 +323,13 @@ __global__ void __launch_bounds__(128) k_relax32(DevParams d, DevState Uq, DevSt
       if (sm != 0.0) atomicAdd(&fl->shear_sum, sm);
     }
   }
+}
+
+template <int EOS>
+__global__ void __launch_bounds__(128) k_relax32(DevParams d, DevState Uq, DevState Uo, DevPrims w, DevHist h,
+                                                 double tau, double D, int do_relax, int do_project, DevFlags* fl) {
+  relax32_body<EOS>(d, Uq, Uo, w, h, tau, D, do_relax, do_project, fl,
+                    (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 }  // namespace fv

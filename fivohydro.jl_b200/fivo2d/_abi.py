@@ -31,6 +31,8 @@ TERM_NAMES = (
 TERM_BIT = {n: 1 << k for k, n in enumerate(TERM_NAMES)}
 FIVO_TERMS_DEFAULT = 0x1DFFF
 FIVO_NOALLOC_MAX_CELLS = 160000
+FIVO_LOCKSTEP_GRAPHS, FIVO_LOCKSTEP_TUNE = 1, 2
+FIVO_LOCKSTEP_MAXCAND = 16
 
 
 class FivoParams(C.Structure):
@@ -81,6 +83,25 @@ class FivoRunResult(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("pad")}
+
+
+class FivoLockstepInfo(C.Structure):
+    _fields_ = [
+        ("enabled", C.c_int32), ("flags", C.c_int32), ("ncand", C.c_int32), ("chosen", C.c_int32),
+        ("cand_order", C.c_int32 * FIVO_LOCKSTEP_MAXCAND), ("cand_slow", C.c_int32 * FIVO_LOCKSTEP_MAXCAND),
+        ("cand_ms", C.c_double * FIVO_LOCKSTEP_MAXCAND), ("steps", C.c_int64), ("fallbacks", C.c_int64),
+        ("ms_step", C.c_double), ("ms_post", C.c_double),
+    ]
+
+    def as_dict(self):
+        n = self.ncand
+        return {"enabled": bool(self.enabled), "graphs": bool(self.flags & FIVO_LOCKSTEP_GRAPHS),
+                "tune": bool(self.flags & FIVO_LOCKSTEP_TUNE), "chosen": self.chosen,
+                "candidates": [{"order": ("batch", "largest_first")[self.cand_order[i]],
+                                "slow_blocks_per_sm": self.cand_slow[i], "best_step_ms": self.cand_ms[i]}
+                               for i in range(n)],
+                "steps": self.steps, "fallbacks": self.fallbacks, "ms_step": self.ms_step,
+                "ms_post": self.ms_post}
 
 
 FIVO_KCLASS_N = 8
@@ -142,6 +163,8 @@ SIGNATURES = {
                                  C.c_int64, C.c_int, C.POINTER(FivoRunResult), C.POINTER(C.c_int)]),
     "fivo_batch_advance": (C.c_int, [C.c_void_p, _D, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
                                      C.c_int64, C.POINTER(FivoRunResult), C.POINTER(C.c_int)]),
+    "fivo_batch_set_lockstep": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "fivo_batch_lockstep_info": (C.c_int, [C.c_void_p, C.c_void_p]),
     "fivo_upload_state": (C.c_int, [C.c_void_p, _D, C.c_int, _I64]),
     "fivo_download_state": (C.c_int, [C.c_void_p, _D, C.c_int, _I64]),
     "fivo_upload_history": (C.c_int, [C.c_void_p, _I64] + [_D] * 8),

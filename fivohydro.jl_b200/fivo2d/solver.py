@@ -276,6 +276,19 @@ class GPUBatch2D:
     def _results(self, res, st):
         return [dict(r.as_dict(), status=int(s)) for r, s in zip(res, st)]
 
+    def set_lockstep(self, enable=True, graphs=True, tune=False):
+        """Lockstep mode (fivo_batch_set_lockstep): every kernel of a step launched
+        once over all events, optionally replayed from captured CUDA graphs, the
+        schedule optionally chosen by timing the candidates on the first steps."""
+        flags = (A.FIVO_LOCKSTEP_GRAPHS if graphs else 0) | (A.FIVO_LOCKSTEP_TUNE if tune else 0)
+        A.check(self.lib, self.lib.fivo_batch_set_lockstep(self.h, int(bool(enable)), flags),
+                "fivo_batch_set_lockstep")
+
+    def lockstep_info(self):
+        info = A.FivoLockstepInfo()
+        A.check(self.lib, self.lib.fivo_batch_lockstep_info(self.h, C.byref(info)), "fivo_batch_lockstep_info")
+        return info.as_dict()
+
     def run(self, tau0, taufinal, cfl=0.2, cfltau=0.05, integrator=A.FIVO_SSPRK2, bc=A.FIVO_BC_OUTFLOW,
             max_steps=10**9, reset_history=True):
         n = len(self)

@@ -377,6 +377,39 @@ int  fivo_batch_advance(fivo_batch* b, const double* tau, double taufinal, doubl
                         double CFLtau, int integrator, int bc, int64_t max_steps,
                         fivo_run_result* results, int* status);
 
+/* Lockstep mode of a batch (enable != 0): fivo_batch_run and fivo_batch_advance
+ * take every event's step at the same time, each kernel of the step launched
+ * once over the blocks of all events (the deferred recoveries and admissibility
+ * inversions as persistent kernels over the union of the events' queues), with
+ * ONE host read for the whole batch per step and one per post-step pass
+ * (update_primitives_2d! + relax_dissipative_2d!, main2D.jl:486-502). An event
+ * whose optimistic step has an inadmissible cell is undone and stepped alone by
+ * the usual stage-by-stage procedure with MOOD and halving; events that have
+ * reached taufinal or max_steps sit out the launches. Results per event are
+ * bitwise those of separate fivo_run calls. flags: FIVO_LOCKSTEP_GRAPHS
+ * replays each launch sequence as a captured CUDA graph; FIVO_LOCKSTEP_TUNE
+ * times the candidate schedules (block order of the events, blocks of the
+ * persistent deferred pass) on the first steps of the next run and keeps the
+ * fastest. Every event must use the plain recovery (no learned guess) and the
+ * same precision. Replaces the reference's per-event loop over run_sim_2d!. */
+#define FIVO_LOCKSTEP_GRAPHS 1
+#define FIVO_LOCKSTEP_TUNE   2
+int  fivo_batch_set_lockstep(fivo_batch* b, int enable, int flags);
+
+#define FIVO_LOCKSTEP_MAXCAND 16
+typedef struct fivo_lockstep_info {
+  int32_t enabled, flags;
+  int32_t ncand;            /* candidate schedules */
+  int32_t chosen;           /* index of the kept one, -1 before tuning */
+  int32_t cand_order[FIVO_LOCKSTEP_MAXCAND];    /* 0: events in batch order, 1: largest grid first */
+  int32_t cand_slow[FIVO_LOCKSTEP_MAXCAND];     /* persistent deferred-pass blocks per SM */
+  double  cand_ms[FIVO_LOCKSTEP_MAXCAND];       /* best step time measured (device, ms) */
+  int64_t steps;            /* lockstep steps taken (batch-wide) */
+  int64_t fallbacks;        /* event steps redone stage by stage */
+  double  ms_step, ms_post; /* device time of the step and post-step launch sequences */
+} fivo_lockstep_info;
+int  fivo_batch_lockstep_info(fivo_batch* b, fivo_lockstep_info* out);
+
 /* --- the learned starting guess of the primitive recovery (no counterpart in
  * the reference: its Newton starts from the previous step's primitives or the
  * closed-form seed, src2d/primrec2d.jl:300-347,465-486) ---

@@ -108,3 +108,133 @@ def test_batch_rejects_bad_event(gpu_lib):
     with pytest.raises(A.FivoError) as e:
         GPUBatch2D(m, grids, lib=gpu_lib)
     assert "event 1" in str(e.value)
+
+
+def _single_runs(gpu_lib, m, grids, states, tau0, taufinal, cfl, cfltau, integrator, max_steps, precision=None):
+    out = []
+    for g, U in zip(grids, states):
+        w = GPUWork2D(m, g, lib=gpu_lib)
+        if precision is not None:
+            w.set_precision(precision)
+        w.set_state(U)
+        w.finalize_ic(tau0)
+        r = w.run(tau0, taufinal, cfl, cfltau, integrator, max_steps=max_steps)
+        out.append((r, w.get_state(), w.get_history()))
+        w.close()
+    return out
+
+
+def _assert_batch_equals(b, rb, singles):
+    for k, (rw, Uw, hw) in enumerate(singles):
+        assert rb[k]["status"] == A.FIVO_OK
+        for key in ("ok", "tau", "nsteps", "nprimfail", "nvacuum", "maxu", "max_shear_res", "dQ", "Q0", "Q1",
+                    "minPtot"):
+            assert rb[k][key] == rw[key] or (np.isnan(rb[k][key]) and np.isnan(rw[key])), (k, key, rb[k][key], rw[key])
+        assert bits_equal(b.events[k].get_state(), Uw), k
+        hb = b.events[k].get_history()
+        for name in hb:
+            assert bits_equal(hb[name], hw[name]), (k, name)
+
+
+@pytest.mark.parametrize("integrator,graphs,tune", [(A.FIVO_SSPRK3, True, True), (A.FIVO_SSPRK3, False, False),
+                                                    (A.FIVO_SSPRK2, True, False)])
+def test_lockstep_batch_equals_single_runs(gpu_lib, integrator, graphs, tune):
+    """Lockstep mode: one launch per kernel over all events (uneven grids), the
+    launch sequences replayed from CUDA graphs or launched directly, the
+    schedule timed and chosen on the first steps. Every event equals its
+    separate fivo_run bit for bit (state, history and the run's results), events
+    leave the lockstep at different steps (taufinal), and one event also equals
+    the oracle."""
+    sizes = [(24, 24), (40, 32), (32, 48), (56, 56), (20, 28)]
+    m, grids, states = _events(sizes, seed0=1201)
+    b = GPUBatch2D(m, grids, nworkers=3, lib=gpu_lib)
+    b.set_lockstep(True, graphs=graphs, tune=tune)
+    for e, U in zip(b.events, states):
+        e.set_state(U)
+        e.finalize_ic(0.6)
+    rb = b.run(0.6, 1.2, 0.2, 0.05, integrator, max_steps=60)
+    info = b.lockstep_info()
+    assert info["enabled"] and info["graphs"] == graphs and info["steps"] >= 12
+    assert len({r["nsteps"] for r in rb}) > 1      # events leave the lockstep at different steps
+    if tune:
+        assert info["chosen"] >= 0 and all(c["best_step_ms"] > 0 for c in info["candidates"])
+    singles = _single_runs(gpu_lib, m, grids, states, 0.6, 1.2, 0.2, 0.05, integrator, 60)
+    _assert_batch_equals(b, rb, singles)
+    o = O.OracleSolver(m, grids[4])
+    o.set_state(states[4])
+    o.finalize_ic(0.6)
+    ro = o.run(0.6, 1.2, 0.2, 0.05, integrator, max_steps=60)
+    assert ro["tau"] == rb[4]["tau"] and ro["nsteps"] == rb[4]["nsteps"]
+    assert bits_equal(o.get_state(), b.events[4].get_state())
+    b.close()
+
+
+@pytest.mark.parametrize("integrator,cfl", [(A.FIVO_SSPRK2, 1.5), (A.FIVO_SSPRK3, 3.0)])
+def test_lockstep_fallback_steps(gpu_lib, integrator, cfl):
+    """A CFL number far above the stable one makes optimistic steps find
+    inadmissible cells: those events are undone and stepped alone with MOOD
+    retries and halvings, and still equal their separate runs bit for bit."""
+    sizes = [(32, 32), (24, 40), (36, 28)]
+    m, grids, states = _events(sizes, seed0=1201)
+    b = GPUBatch2D(m, grids, nworkers=2, lib=gpu_lib)
+    b.set_lockstep(True, graphs=True)
+    for e, U in zip(b.events, states):
+        e.set_state(U)
+        e.finalize_ic(0.6)
+    rb = b.run(0.6, 10.0, cfl, 0.5, integrator, max_steps=8)
+    assert b.lockstep_info()["fallbacks"] > 0
+    singles = _single_runs(gpu_lib, m, grids, states, 0.6, 10.0, cfl, 0.5, integrator, 8)
+    _assert_batch_equals(b, rb, singles)
+    b.close()
+
+
+def test_lockstep_fp32_and_advance(gpu_lib):
+    """The FP32 form in lockstep equals the FP32 form of separate runs bit for
+    bit, and lockstep advance in chunks equals one lockstep run."""
+    sizes = [(24, 32), (36, 36), (28, 20)]
+    m, grids, states = _events(sizes, seed0=1301)
+    b = GPUBatch2D(m, grids, nworkers=2, lib=gpu_lib)
+    b.set_lockstep(True, graphs=True)
+    for e, U in zip(b.events, states):
+        e.set_precision(A.FIVO_PRECISION_FP32)
+        e.set_state(U)
+        e.finalize_ic(0.6)
+    rb = b.run(0.6, 10.0, 0.2, 0.05, A.FIVO_SSPRK3, max_steps=6)
+    singles = _single_runs(gpu_lib, m, grids, states, 0.6, 10.0, 0.2, 0.05, A.FIVO_SSPRK3, 6,
+                           precision=A.FIVO_PRECISION_FP32)
+    _assert_batch_equals(b, rb, singles)
+    b.close()
+    ba = GPUBatch2D(m, grids, nworkers=2, lib=gpu_lib)
+    bb = GPUBatch2D(m, grids, nworkers=2, lib=gpu_lib)
+    ba.set_lockstep(True, graphs=True)
+    for bt in (ba, bb):
+        for e, U in zip(bt.events, states):
+            e.set_state(U)
+            e.finalize_ic(0.6)
+            e.rhs(0.6)
+    taus = [0.6] * len(sizes)
+    for _ in range(4):
+        r = ba.advance(taus, 10.0, 0.2, 0.05, A.FIVO_SSPRK3, max_steps=1)
+        assert all(x["ok"] and x["nsteps"] == 1 for x in r)
+        taus = [x["tau"] for x in r]
+    r4 = bb.advance([0.6] * len(sizes), 10.0, 0.2, 0.05, A.FIVO_SSPRK3, max_steps=4)
+    for k in range(len(sizes)):
+        assert r4[k]["tau"] == taus[k]
+        assert bits_equal(ba.events[k].get_state(), bb.events[k].get_state())
+    ba.close()
+    bb.close()
+
+
+def test_lockstep_refuses_mixed_precision(gpu_lib):
+    sizes = [(24, 24), (28, 28)]
+    m, grids, states = _events(sizes, seed0=1401)
+    b = GPUBatch2D(m, grids, lib=gpu_lib)
+    b.set_lockstep(True)
+    b.events[0].set_precision(A.FIVO_PRECISION_FP32)
+    for e, U in zip(b.events, states):
+        e.set_state(U)
+        e.finalize_ic(0.6)
+    with pytest.raises(A.FivoError) as e:
+        b.run(0.6, 10.0, 0.2, 0.05, A.FIVO_SSPRK3, max_steps=2)
+    assert "same precision" in str(e.value)
+    b.close()
