@@ -48,6 +48,13 @@ struct FivoRunResult
     max_shear_res::Float64; maxu::Float64; dQ::Float64; Q0::Float64; Q1::Float64; minPtot::Float64
 end
 
+# fivo_lockstep_info: the lockstep batch's candidate schedules and the one kept
+struct FivoLockstepInfo
+    enabled::Int32; flags::Int32; ncand::Int32; chosen::Int32
+    cand_order::NTuple{16,Int32}; cand_slow::NTuple{16,Int32}; cand_ms::NTuple{16,Float64}
+    steps::Int64; fallbacks::Int64; ms_step::Float64; ms_post::Float64
+end
+
 fivo_error() = unsafe_string(ccall((:fivo_last_error, LIBFIVO2D), Cstring, ()))
 fivocheck(st, what) = st == FIVO_OK || error("$what: status $st: $(fivo_error())")
 
