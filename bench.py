@@ -208,15 +208,20 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def traffic_from_profiles(kclass):
-    """Per-launch DRAM bytes from the committed ncu summary, if present."""
+def from_profiles(kclass, key):
+    """A figure of the committed ncu summary of a kernel class (`key: value` line), if present."""
     f = ROOT / "profiles" / f"{kclass}_kernel_traffic.txt"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
-        if line.startswith("traffic_bytes_per_launch_full_workload:"):
+        if line.startswith(key + ":"):
             return float(line.split(":")[1])
     return None
+
+
+def traffic_from_profiles(kclass):
+    """Per-launch DRAM bytes from the committed ncu summary, if present."""
+    return from_profiles(kclass, "traffic_bytes_per_launch_full_workload")
 
 
 # ----------------------------------------------------------------------------- our arm
@@ -491,10 +496,17 @@ def run_gpu(args):
                         "share": kt.ms[i] / max(1e-30, sum(tot.values())),
                         "units_per_launch": kt.units[i] / kt.launches[i],
                         "gbs": b / (kt.ms[i] / 1e3) / 1e9 if kt.ms[i] > 0 else None}
+    for c in per_class:
+        fp = from_profiles(c, "fp64_pipe_active_pct")
+        if fp is not None:
+            per_class[c]["fp64_pipe_active_pct_ncu"] = fp
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "kernel": dom, "peak_source": peak_kind,
             "bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms, "kernels": per_class,
-            "note": "FP64 Newton/EOS kernels, latency-bound; bytes-based fraction per the contract"}
+            "fp64_pipe_active_pct_ncu": from_profiles(dom, "fp64_pipe_active_pct"),
+            "note": "FP64 Newton/EOS kernels, bound by FP64 latency, not bytes: the bytes-based fraction per "
+                    "the contract, and the FP64-pipe activity of the same kernel from the committed ncu "
+                    "summary (profiles/<class>_kernel_traffic.txt)"}
 
     w.close()
     if dist:
