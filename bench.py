@@ -568,7 +568,17 @@ def _batch_fields(b, m):
     return {k: np.concatenate(v) for k, v in out.items()}
 
 
-LOCKSTEP_FORMS = ("plain_fp64_lockstep", "fp32_lockstep", "plain_fp64_lockstep_nograph")
+def _fields_digest(f):
+    """SHA-256 of the bits of T, pibar and the shear rows (bitwise comparison of two batches)"""
+    import hashlib
+    h = hashlib.sha256()
+    for k in ("T", "pibar", "pi"):
+        h.update(f[k].tobytes())
+    return h.hexdigest()
+
+
+LOCKSTEP_FORMS = ("plain_fp64_lockstep", "fp32_lockstep", "learned_fp32_lockstep", "learned_deferred_fp32_lockstep",
+                  "plain_fp64_lockstep_nograph")
 
 
 def batch_forms(lib, m, nevents, steps, single_value, warmup=15):
@@ -576,9 +586,10 @@ def batch_forms(lib, m, nevents, steps, single_value, warmup=15):
     event-by-event sizes, device IC, seed 1000 + k) advanced in plain FP64, in FP32
     (face pass and relaxation sources), and with the learned guess plus FP32, the
     guess used for every cell or for the cells the warm start defers, each with one
-    stream per event; then plain FP64 and FP32 in lockstep (one launch per kernel
-    over all events, replayed from CUDA graphs, the schedule tuned on the first 12
-    warm-up steps), and plain lockstep without graphs. Zone-updates/s of each (host
+    stream per event; then plain FP64, FP32 and the two learned+FP32 forms in
+    lockstep (one launch per kernel over all events, replayed from CUDA graphs, the
+    schedule tuned on the first 12 warm-up steps), plain lockstep without graphs,
+    and the plain path unbatched (the events one at a time, each alone on the GPU). Zone-updates/s of each (host
     wall clock around the synchronous batch call), each form's L2(T), L2(pibar) and
     L2(pi) against the plain run, and for the lockstep forms whether every event's
     fields equal those of the stream batch of the same precision bit for bit."""
@@ -599,8 +610,10 @@ def batch_forms(lib, m, nevents, steps, single_value, warmup=15):
            "timing": "host wall clock around the synchronous batch call"}
     ref = None
     stream_fields = {}
-    for form in ("plain_fp64", "fp32", "learned_fp32", "learned_deferred_fp32") + LOCKSTEP_FORMS:
-        b = GPUBatch2D(m, grids, lib=lib)
+    for form in ("plain_fp64", "fp32", "learned_fp32", "learned_deferred_fp32") + LOCKSTEP_FORMS + (
+            "plain_fp64_one_event_at_a_time",):
+        sequential = form == "plain_fp64_one_event_at_a_time"
+        b = GPUBatch2D(m, grids, nworkers=1 if sequential else 0, lib=lib)
         lockstep = form in LOCKSTEP_FORMS
         if lockstep:
             b.set_lockstep(True, graphs=not form.endswith("nograph"), tune=True)
@@ -609,9 +622,9 @@ def batch_forms(lib, m, nevents, steps, single_value, warmup=15):
             e.rhs(TAU0)
             if not form.startswith("plain_fp64"):
                 e.set_precision(A.FIVO_PRECISION_FP32)
-            if form == "learned_fp32":
+            if form.startswith("learned_fp32"):
                 guess.attach(e, A.FIVO_GUESS_EVERY_CELL)
-            if form == "learned_deferred_fp32":
+            if form.startswith("learned_deferred_fp32"):
                 guess.attach(e, A.FIVO_GUESS_DEFERRED)
         taus = [TAU0] * len(grids)
 
@@ -629,16 +642,18 @@ def batch_forms(lib, m, nevents, steps, single_value, warmup=15):
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         row = {"value": steps * cells / dt, "unit": UNIT, "ms_per_step": 1e3 * dt / steps,
-               "schedule": "lockstep" if lockstep else "stream per event"}
+               "schedule": "lockstep" if lockstep else ("one event at a time (the plain path, unbatched)"
+                                                         if sequential else "stream per event")}
         f = _batch_fields(b, m)
-        if lockstep:
+        if sequential:
+            row["bitwise_equal_stream_batch"] = _fields_digest(f) == stream_fields["plain_fp64"]
+        elif lockstep:
             info = b.lockstep_info()
             row["lockstep"] = {k: info[k] for k in ("graphs", "chosen", "candidates", "fallbacks")}
-            twin = stream_fields["plain_fp64" if form.startswith("plain_fp64") else "fp32"]
-            row["bitwise_equal_stream_batch"] = bool(
-                all(np.array_equal(f[k].view(np.int64), twin[k].view(np.int64)) for k in ("T", "pibar", "pi")))
-        elif form in ("plain_fp64", "fp32"):
-            stream_fields[form] = f
+            twin = stream_fields[form.replace("_lockstep", "").replace("_nograph", "")]
+            row["bitwise_equal_stream_batch"] = _fields_digest(f) == twin
+        else:
+            stream_fields[form] = _fields_digest(f)
         if ref is None:
             ref = f
         else:
@@ -662,8 +677,13 @@ def batch_forms(lib, m, nevents, steps, single_value, warmup=15):
         b.close()
     guess.close()
     out["plain_batch_vs_single_event"] = out["plain_fp64"]["value"] / single_value
-    out["best_form_vs_plain_batch"] = max(out[f]["value"] for f in out if isinstance(out[f], dict)
-                                          and "value" in out[f]) / out["plain_fp64"]["value"]
+    best = max((f for f in out if isinstance(out[f], dict) and "value" in out[f]), key=lambda f: out[f]["value"])
+    out["best_form"] = best
+    out["best_form_vs_plain_batch"] = out[best]["value"] / out["plain_fp64"]["value"]
+    seq = out["plain_fp64_one_event_at_a_time"]["value"]
+    for f in out:
+        if isinstance(out[f], dict) and "value" in out[f]:
+            out[f]["speedup_vs_plain_one_event_at_a_time"] = out[f]["value"] / seq
     return out
 
 

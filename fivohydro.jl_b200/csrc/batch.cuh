@@ -56,6 +56,7 @@ struct Ev {
   DevFlags* fl;
   unsigned int* qp;         /* deferred recoveries */
   unsigned int* qa;         /* deferred admissibility inversions */
+  unsigned int* qq;         /* what the learned retry leaves for the full recovery */
   double* fhx;
   double* fhy;
   float* fhx32;
@@ -183,10 +184,39 @@ __global__ void __launch_bounds__(128, FV_FAST_MINB) kb_prim_fast(DevParams d0, 
   prim_fast_body<EOS, NCH>(d, sU, sw, shh, stau, sfl, sq, blk * 128 + threadIdx.x);
 }
 
-/* Offsets of every active event's queue in the batch's union of queues
- * (kind 0: deferred recoveries, 1: admissibility inversions); pre[nev] = total.
- * Adds each event's count to its tot_p / tot_a, as the single-event deferred
- * kernels do. One block. */
+/* the warm pass with the learned guess in front of it (k_prim_learned) on each
+ * event's state pU[which]; one tensor-core tile per block (128 cells of one event) */
+template <int EOS, bool NCH>
+__global__ void __launch_bounds__(128, 4) kb_prim_learned(DevParams d0, const Geo* __restrict__ geo,
+                                                        const Ev* __restrict__ tab,
+                                                        const unsigned short* __restrict__ eob, int which,
+                                                        guess::Net net) {
+  __shared__ __align__(128) guess::FwdSmem s;
+  __shared__ BlockHead sh;
+  __shared__ DevState sU;
+  __shared__ DevPrims sw;
+  __shared__ DevHist shh;
+  __shared__ DevFlags* sfl;
+  __shared__ unsigned int* sq;
+  __shared__ double stau;
+  long long blk;
+  if (!block_head(&sh, geo, tab, eob, SH_CELL, &blk)) return;
+  const Ev& ev = tab[sh.e];
+  to_shared(&sU, &ev.pU[which]);
+  to_shared(&sw, &ev.w);
+  to_shared(&shh, &ev.h);
+  if (threadIdx.x == 0) { sfl = ev.fl; sq = ev.qp; stau = ev.ptau[which]; }
+  __syncthreads();
+  DevParams d = d0;
+  with_geo(d, sh.g);
+  prim_learned_body<EOS, NCH>(d, sU, sw, shh, stau, sfl, sq, net, s, blk * 128 + threadIdx.x);
+}
+
+/* Offsets of every active event's queue in the batch's union of queues; pre[nev] =
+ * total. kind 0: deferred recoveries (counted into tot_p, as k_prim_slow counts
+ * them), 1: admissibility inversions (into tot_a), 2: the learned retry's leftovers
+ * (into tot_p), 3: deferred recoveries without counting (the learned retry takes
+ * them; k_prim_learned_retry counts nothing). One block. */
 __global__ void __launch_bounds__(1024) kb_scan(const Ev* __restrict__ tab, int nev, int kind, unsigned int* pre,
                                                 Ctl* ctl) {
   __shared__ unsigned int s_warp[32];
@@ -199,8 +229,8 @@ __global__ void __launch_bounds__(1024) kb_scan(const Ev* __restrict__ tab, int 
     unsigned int cnt = 0;
     if (e < nev && tab[e].active) {
       DevFlags* fl = tab[e].fl;
-      cnt = *(volatile unsigned int*)(kind == 0 ? &fl->qcount_p : &fl->qcount_a);
-      if (cnt) atomicAdd(kind == 0 ? &fl->tot_p : &fl->tot_a, (unsigned long long)cnt);
+      cnt = *(volatile unsigned int*)(kind == 1 ? &fl->qcount_a : (kind == 2 ? &fl->qcount_q : &fl->qcount_p));
+      if (cnt && kind != 3) atomicAdd(kind == 1 ? &fl->tot_a : &fl->tot_p, (unsigned long long)cnt);
     }
     /* inclusive scan in the warp, then over the warps' totals */
     unsigned int v = cnt;
@@ -245,11 +275,11 @@ __device__ __forceinline__ int item_event(const unsigned int* pre, int nev, unsi
 }
 
 /* k_prim_slow over the union of the events' deferred recoveries (persistent;
- * one item per warp pair at a time) */
+ * one item per warp pair at a time); left: the learned retry's leftovers instead */
 template <int EOS, bool NCH>
 __global__ void __launch_bounds__(128) kb_prim_slow(DevParams d0, const Geo* __restrict__ geo,
                                                     const Ev* __restrict__ tab, const unsigned int* __restrict__ pre,
-                                                    int nev, Ctl* ctl, int which) {
+                                                    int nev, Ctl* ctl, int which, int left) {
   __shared__ unsigned int s_q[2];
   __shared__ int s_stop[2];
   __shared__ Recovery s_cold[2];
@@ -269,9 +299,64 @@ __global__ void __launch_bounds__(128) kb_prim_slow(DevParams d0, const Geo* __r
     const Ev& ev = tab[e];
     DevParams d = d0;
     with_geo(d, geo[e]);
-    slow_item<EOS, NCH>(d, ev.pU[which], ev.w, ev.h, ev.ptau[which], ev.fl, (long long)ev.qp[q - pre[e]], lane,
+    const unsigned int* qe = left ? ev.qq : ev.qp;
+    slow_item<EOS, NCH>(d, ev.pU[which], ev.w, ev.h, ev.ptau[which], ev.fl, (long long)qe[q - pre[e]], lane,
                         lead, pair, s_stop, s_cold);
   }
+}
+
+/* k_prim_learned_retry over the union of the events' deferred recoveries: CTA b
+ * takes items b*128 .. of the union (cells of several events may share a tile:
+ * the network does not depend on the grid), infers their starting points on the
+ * tensor cores and runs the Newton with the guess check; a cell that converges is
+ * stored, the rest go to its event's second queue. The grid covers the largest
+ * possible union and the CTAs past its end return at once (all threads alike);
+ * one tile per CTA, as in the single-event kernel. */
+template <int EOS, bool NCH>
+__global__ void __launch_bounds__(128, 4) kb_prim_learned_retry(DevParams d0, const Geo* __restrict__ geo,
+                                                              const Ev* __restrict__ tab,
+                                                              const unsigned int* __restrict__ pre, int nev,
+                                                              const Ctl* ctl, int which, guess::Net net) {
+  __shared__ __align__(128) guess::FwdSmem s;
+  const unsigned n = *(volatile const unsigned int*)&ctl->total;
+  const unsigned base = blockIdx.x * 128u;
+  if (base >= n) return;
+  const unsigned qi = base + threadIdx.x;
+  const bool live = qi < n;
+  int e = 0;
+  long long i = 0;
+  DevParams d = d0;
+  CellCons c;
+  float xn[guess::NIN];
+#pragma unroll
+  for (int q = 0; q < guess::NIN; ++q) xn[q] = 0.0f;
+  if (live) {
+    e = item_event(pre, nev, qi);
+    with_geo(d, geo[e]);
+    const Ev& ev = tab[e];
+    i = (long long)ev.qp[qi - pre[e]];
+    load_cons(d, ev.pU[which], i, ev.ptau[which], c);
+    if (c.E > 0.0) {
+      float r[guess::NIN];
+      guess::features(c.E, c.Sx, c.Sy, c.Pi, c.pixx, c.pixy, c.piyy, r);
+#pragma unroll
+      for (int q = 0; q < guess::NIN; ++q) xn[q] = guess::nrm_in(net.norm, q, r[q]);
+    }
+  }
+  float y[guess::NOUT] = {0.0f, 0.0f, 0.0f};
+  const bool tile_ok = guess::forward_tile(s, net, xn, y);
+  if (!live) return;
+  const Ev& ev = tab[e];
+  unsigned it_l = 0, n_l = 0, ok_l = 0;
+  bool done = false;
+  if (tile_ok && c.E > 0.0) done = guess_and_recover<EOS, NCH>(d, ev.w, ev.h, c, y, net, i, &it_l, &n_l, &ok_l);
+  if (n_l) {
+    atomicAdd(&ev.fl->it_learn, (unsigned long long)it_l);
+    atomicAdd(&ev.fl->n_learn, (unsigned long long)n_l);
+    atomicAdd(&ev.fl->ok_learn, (unsigned long long)ok_l);
+  }
+  if (!done) ev.qq[atomicAdd(&ev.fl->qcount_q, 1u)] = (unsigned)i;
+  if (!tile_ok) atomicExch(&ev.fl->status, 3);
 }
 
 /* the face pass of stage k in one direction (FP64 or FP32 planes) */

@@ -1765,7 +1765,8 @@ struct Lockstep {
   std::vector<double> cand_ms;
   int chosen = -1;
   int tuned_steps = 0;
-  std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs;  /* (sequence, integrator, candidate, precision) */
+  /* (sequence, integrator, candidate, precision, recovery, the learned guess's weights) */
+  std::map<std::tuple<int, int, int, int, int, std::string>, cudaGraphExec_t> graphs;
   int64_t steps = 0, fallbacks = 0;
   double ms_step = 0.0, ms_post = 0.0;
 };
@@ -1875,7 +1876,7 @@ void ls_fill_common(fivo_ctx* c, bt::Ev& e) {
   const DevParams& d = c->dp;
   std::memset(&e, 0, sizeof(e));
   e.w = c->w; e.h = c->h; e.fl = c->fl;
-  e.qp = c->queues; e.qa = c->queues + d.Ntot;
+  e.qp = c->queues; e.qa = c->queues + d.Ntot; e.qq = c->queues + 2 * d.Ntot;
   e.fhx = c->fh; e.fhy = c->fh + (size_t)d.nv * d.Ntot;
   e.fhx32 = c->fh32; e.fhy32 = c->fh32 ? c->fh32 + (size_t)d.nv * d.Ntot : nullptr;
   e.x0save = c->x0save;
@@ -1919,6 +1920,8 @@ void ls_fill_post(fivo_ctx* c, bt::Ev& e, double tau, double used, int do_relax,
 }
 
 #define LS_GRID(s) L.nblocks[s] ? L.nblocks[s] : 1
+constexpr int LS_LEARNED_DYN = LEARNED_SMEM - (int)sizeof(guess::FwdSmem) - 1024;
+constexpr int LS_RETRY_DYN = LEARNED_SMEM - (int)sizeof(guess::FwdSmem) - 128;
 
 /* enqueue one launch sequence on L.st (recorded into a graph or run directly) */
 template <int EOS, bool NCH>
@@ -1934,12 +1937,31 @@ int ls_launch_t(fivo_batch* b, int seq, int integrator, int bc, int cand, int pr
   const bool f32 = prec != FIVO_PRECISION_FP64;
   const unsigned gr = nblk(n, 256);
   CK(cudaMemcpyAsync(L.tab_d, L.tab_h, n * sizeof(bt::Ev), cudaMemcpyHostToDevice, st));
+  /* _primitive_pass!: as launch_primitive_t, with or without the learned guess */
+  const fivo_ctx* c0 = b->ev[0];
   auto prim_pass = [&](int which) -> int {
-    bt::kb_prim_fast<EOS, NCH><<<LS_GRID(bt::SH_CELL), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_CELL], which);
+    if (c0->learned && c0->guess_mode == FIVO_GUESS_EVERY_CELL) {
+      bt::kb_prim_learned<EOS, NCH><<<LS_GRID(bt::SH_CELL), 128, LS_LEARNED_DYN, st>>>(d0, geo, L.tab_d,
+                                                                                     eob[bt::SH_CELL], which, c0->gnet);
+      CKL();
+    } else {
+      bt::kb_prim_fast<EOS, NCH><<<LS_GRID(bt::SH_CELL), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_CELL], which);
+      CKL();
+    }
+    int left = 0;
+    if (c0->learned && c0->guess_mode == FIVO_GUESS_DEFERRED) {
+      /* the network's guess for the deferred cells of every event, then the full
+       * recovery of what it leaves */
+      bt::kb_scan<<<1, 1024, 0, st>>>(L.tab_d, n, 3, L.pre_d, L.ctl_d);
+      CKL();
+      bt::kb_prim_learned_retry<EOS, NCH><<<LS_GRID(bt::SH_CELL), 128, LS_RETRY_DYN, st>>>(
+          d0, geo, L.tab_d, L.pre_d, n, L.ctl_d, which, c0->gnet);
+      CKL();
+      left = 1;
+    }
+    bt::kb_scan<<<1, 1024, 0, st>>>(L.tab_d, n, left ? 2 : 0, L.pre_d, L.ctl_d);
     CKL();
-    bt::kb_scan<<<1, 1024, 0, st>>>(L.tab_d, n, 0, L.pre_d, L.ctl_d);
-    CKL();
-    bt::kb_prim_slow<EOS, NCH><<<slow_blocks, 128, 0, st>>>(d0, geo, L.tab_d, L.pre_d, n, L.ctl_d, which);
+    bt::kb_prim_slow<EOS, NCH><<<slow_blocks, 128, 0, st>>>(d0, geo, L.tab_d, L.pre_d, n, L.ctl_d, which, left);
     CKL();
     return FIVO_OK;
   };
@@ -2007,6 +2029,22 @@ int ls_launch_t(fivo_batch* b, int seq, int integrator, int bc, int cand, int pr
   return FIVO_OK;
 }
 
+/* dynamic shared memory of the learned kernels: with their static part, at most 4 CTAs
+ * per SM (4 x 128 tensor-memory columns), as the single-event launches reserve */
+template <int EOS, bool NCH>
+int ls_prepare_t() {
+  CK(cudaFuncSetAttribute(bt::kb_prim_learned<EOS, NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, LS_LEARNED_DYN));
+  CK(cudaFuncSetAttribute(bt::kb_prim_learned_retry<EOS, NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          LS_RETRY_DYN));
+  return FIVO_OK;
+}
+
+int ls_prepare(const DevParams& d) {
+  if (d.p.eos_kind == FIVO_EOS_LATTICE_HRG) return ls_prepare_t<FIVO_EOS_LATTICE_HRG, true>();
+  if (d.ncharge) return ls_prepare_t<FIVO_EOS_CONFORMAL_HQ, true>();
+  return ls_prepare_t<FIVO_EOS_CONFORMAL_HQ, false>();
+}
+
 int ls_launch(fivo_batch* b, int seq, int integrator, int bc, int cand, int prec, bool any_sector, bool relax_on) {
   const DevParams& d = b->ls->d0;
   if (d.p.eos_kind == FIVO_EOS_LATTICE_HRG)
@@ -2019,9 +2057,14 @@ int ls_launch(fivo_batch* b, int seq, int integrator, int bc, int cand, int prec
 int ls_exec(fivo_batch* b, int seq, int integrator, int bc, int cand, int prec, bool any_sector, bool relax_on,
             float* ms) {
   Lockstep& L = *b->ls;
+  int rc0 = ls_prepare(L.d0);
+  if (rc0) return rc0;
   CK(cudaEventRecord(L.ta, L.st));
   if (L.flags & FIVO_LOCKSTEP_GRAPHS) {
-    const auto key = std::make_tuple(seq, integrator, cand, prec);
+    const fivo_ctx* c0 = b->ev[0];
+    /* the guess's weights and normalisation are kernel arguments: a graph per attached network */
+    const std::string net = c0->learned ? std::string((const char*)&c0->gnet, sizeof(c0->gnet)) : std::string();
+    const auto key = std::make_tuple(seq, integrator, cand, prec, c0->learned ? 1 + c0->guess_mode : 0, net);
     auto it = L.graphs.find(key);
     if (it == L.graphs.end()) {
       CK(cudaStreamBeginCapture(L.st, cudaStreamCaptureModeThreadLocal));
@@ -2079,8 +2122,10 @@ int ls_loop(fivo_batch* b, std::vector<double>& tau, double taufinal, double cfl
   const bool relax_on = d.nv > 4 && (any_sector || d.hasShear);
   const bool post = any_sector || d.hasShear;
   const int prec = b->ev[0]->precision;
+  const fivo_ctx* c0 = b->ev[0];
   for (fivo_ctx* c : b->ev) {
-    if (c->learned) return fail(FIVO_ERR_CONFIG, "lockstep batch: the events must use the plain recovery (no learned guess)");
+    if (c->learned != c0->learned || (c->learned && (c->guess_mode != c0->guess_mode || c->gnet.img != c0->gnet.img)))
+      return fail(FIVO_ERR_CONFIG, "lockstep batch: every event must use the same recovery (one learned guess, one mode, or none)");
     if (c->precision != prec) return fail(FIVO_ERR_CONFIG, "lockstep batch: every event must use the same precision");
     if (!c->x0save) {
       if (cudaMalloc(&c->x0save, 4 * (size_t)c->dp.Ntot * sizeof(double)) != cudaSuccess) {

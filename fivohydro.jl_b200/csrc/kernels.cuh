@@ -1560,11 +1560,9 @@ __global__ void __launch_bounds__(128, FV_FAST_MINB) k_prim_fast(DevParams d, De
 #define GUESS_CHECK_IT 3
 #define GUESS_CHECK_TOL 1e-10
 template <int EOS, bool NCH>
-__global__ void __launch_bounds__(128, 4) k_prim_learned(DevParams d, DevState U, DevPrims w, DevHist h,
-                                                       double tau, DevFlags* fl, unsigned int* queue,
-                                                       guess::Net net) {
-  __shared__ __align__(128) guess::FwdSmem s;
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void prim_learned_body(const DevParams& d, const DevState& U, const DevPrims& w,
+                                                  const DevHist& h, double tau, DevFlags* fl, unsigned int* queue,
+                                                  const guess::Net& net, guess::FwdSmem& s, long long i) {
   const bool live = i < d.Ntot;
   CellCons c;
   bool vac = false;
@@ -1653,6 +1651,14 @@ __global__ void __launch_bounds__(128, 4) k_prim_learned(DevParams d, DevState U
   if (!net_ok && threadIdx.x == 0) atomicExch(&fl->status, 3);
 }
 
+template <int EOS, bool NCH>
+__global__ void __launch_bounds__(128, 4) k_prim_learned(DevParams d, DevState U, DevPrims w, DevHist h,
+                                                       double tau, DevFlags* fl, unsigned int* queue,
+                                                       guess::Net net) {
+  __shared__ __align__(128) guess::FwdSmem s;
+  prim_learned_body<EOS, NCH>(d, U, w, h, tau, fl, queue, net, s, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 /* (features, targets) pairs of the interior cells whose recovery succeeded, every
  * stride-th cell from phase on: out[k][11], k < cap, *count counts every offered
  * pair (it may pass cap) */
@@ -1685,6 +1691,41 @@ __global__ void k_guess_harvest(DevParams d, DevState U, DevPrims w, double tau,
  * the CTAs past its end return at once (all threads alike). One tile per CTA: the
  * forward pass gives up the CTA's tensor-memory allocation permit after its one
  * allocation, so a CTA cannot allocate for a second tile. */
+/* a deferred cell from the network's output y: its starting point (log T, u from the
+ * network, the charm chemical potential in closed form from N^tau), then the Newton
+ * with the guess check; true when the cell converged and is stored */
+template <int EOS, bool NCH>
+__device__ __forceinline__ bool guess_and_recover(const DevParams& d, const DevPrims& w, const DevHist& h,
+                                                  const CellCons& c, const float y[guess::NOUT],
+                                                  const guess::Net& net, long long i, unsigned* it_l, unsigned* n_l,
+                                                  unsigned* ok_l) {
+  double g[4];
+  g[0] = ((double)y[0] * (double)net.norm.out_std[0] + (double)net.norm.out_mean[0]) + 0.25 * log(c.E);
+  g[2] = (double)y[1] * (double)net.norm.out_std[1] + (double)net.norm.out_mean[1];
+  g[3] = (double)y[2] * (double)net.norm.out_std[2] + (double)net.norm.out_mean[2];
+  const double phw = h.x0_phi[i];
+  g[1] = isfinite_(phw) ? phw : 0.0;
+  if (NCH && EOS == FIVO_EOS_LATTICE_HRG) {
+    const double T0 = jclamp(exp(g[0]), FV_T_MIN, FV_T_SOLVE_MAX);
+    const double K2 = lhrg_K2(lhrg_x(T0, d));
+    double Cn = (d.A_lhrg * T0) * K2;
+    if (d.p.hq_times_fmGeV3) Cn *= d.fmgev3;
+    const double ut = utau(g[2], g[3]);
+    const double nt = (c.D - nu_tau(g[2], g[3], ut, c.nux, c.nuy)) / ut;
+    if (nt > 0.0 && Cn > 0.0) g[1] = log(nt / Cn);
+  }
+  if (!(isfinite_(g[0]) && isfinite_(g[1]) && isfinite_(g[2]) && isfinite_(g[3]))) return false;
+  bool over = false;
+  int it = 0;
+  Recovery r = recover_fast<EOS, NCH>(c, d, g[0], g[1], g[2], g[3], d.p.primrec_maxit, d.p.primrec_tol,
+                                      d.p.primrec_maxit, &over, GUESS_CHECK_IT, GUESS_CHECK_TOL, &it);
+  *it_l = (unsigned)it; *n_l = 1;
+  if (over || !r.ok) return false;
+  store_recovery<EOS>(d, w, h, i, r);
+  *ok_l = 1;
+  return true;
+}
+
 template <int EOS, bool NCH>
 __global__ void __launch_bounds__(128, 4) k_prim_learned_retry(DevParams d, DevState U, DevPrims w, DevHist h,
                                                              double tau, DevFlags* fl, const unsigned int* queue,
@@ -1717,35 +1758,7 @@ __global__ void __launch_bounds__(128, 4) k_prim_learned_retry(DevParams d, DevS
     net_ok = net_ok && tile_ok;
     bool pass_on = live, done = false;
     unsigned it_l = 0, n_l = 0, ok_l = 0;
-    if (live && tile_ok && c.E > 0.0) {
-      double g[4];
-      g[0] = ((double)y[0] * (double)net.norm.out_std[0] + (double)net.norm.out_mean[0]) + 0.25 * log(c.E);
-      g[2] = (double)y[1] * (double)net.norm.out_std[1] + (double)net.norm.out_mean[1];
-      g[3] = (double)y[2] * (double)net.norm.out_std[2] + (double)net.norm.out_mean[2];
-      const double phw = h.x0_phi[i];
-      g[1] = isfinite_(phw) ? phw : 0.0;
-      if (NCH && EOS == FIVO_EOS_LATTICE_HRG) {
-        const double T0 = jclamp(exp(g[0]), FV_T_MIN, FV_T_SOLVE_MAX);
-        const double K2 = lhrg_K2(lhrg_x(T0, d));
-        double Cn = (d.A_lhrg * T0) * K2;
-        if (d.p.hq_times_fmGeV3) Cn *= d.fmgev3;
-        const double ut = utau(g[2], g[3]);
-        const double nt = (c.D - nu_tau(g[2], g[3], ut, c.nux, c.nuy)) / ut;
-        if (nt > 0.0 && Cn > 0.0) g[1] = log(nt / Cn);
-      }
-      if (isfinite_(g[0]) && isfinite_(g[1]) && isfinite_(g[2]) && isfinite_(g[3])) {
-        bool over = false;
-        int it = 0;
-        Recovery r = recover_fast<EOS, NCH>(c, d, g[0], g[1], g[2], g[3], d.p.primrec_maxit, d.p.primrec_tol,
-                                            d.p.primrec_maxit, &over, GUESS_CHECK_IT, GUESS_CHECK_TOL, &it);
-        it_l = (unsigned)it; n_l = 1;
-        if (!over && r.ok) {
-          store_recovery<EOS>(d, w, h, i, r);
-          done = true;
-          ok_l = 1;
-        }
-      }
-    }
+    if (live && tile_ok && c.E > 0.0) done = guess_and_recover<EOS, NCH>(d, w, h, c, y, net, i, &it_l, &n_l, &ok_l);
     pass_on = live && !done;
     {
       const unsigned a = __reduce_add_sync(0xffffffffu, it_l), b = __reduce_add_sync(0xffffffffu, n_l);

@@ -390,8 +390,10 @@ int  fivo_batch_advance(fivo_batch* b, const double* tau, double taufinal, doubl
  * replays each launch sequence as a captured CUDA graph; FIVO_LOCKSTEP_TUNE
  * times the candidate schedules (block order of the events, blocks of the
  * persistent deferred pass) on the first steps of the next run and keeps the
- * fastest. Every event must use the plain recovery (no learned guess) and the
- * same precision. Replaces the reference's per-event loop over run_sim_2d!. */
+ * fastest. Every event must use the same recovery (the plain one, or one
+ * learned guess in one mode: its batched kernels take the network's tiles over
+ * the events' cells or over the union of their deferred cells) and the same
+ * precision. Replaces the reference's per-event loop over run_sim_2d!. */
 #define FIVO_LOCKSTEP_GRAPHS 1
 #define FIVO_LOCKSTEP_TUNE   2
 int  fivo_batch_set_lockstep(fivo_batch* b, int enable, int flags);

@@ -110,12 +110,15 @@ def test_batch_rejects_bad_event(gpu_lib):
     assert "event 1" in str(e.value)
 
 
-def _single_runs(gpu_lib, m, grids, states, tau0, taufinal, cfl, cfltau, integrator, max_steps, precision=None):
+def _single_runs(gpu_lib, m, grids, states, tau0, taufinal, cfl, cfltau, integrator, max_steps, precision=None,
+                 guess=None, mode=None):
     out = []
     for g, U in zip(grids, states):
         w = GPUWork2D(m, g, lib=gpu_lib)
         if precision is not None:
             w.set_precision(precision)
+        if guess is not None:
+            guess.attach(w, mode)
         w.set_state(U)
         w.finalize_ic(tau0)
         r = w.run(tau0, taufinal, cfl, cfltau, integrator, max_steps=max_steps)
@@ -223,6 +226,68 @@ def test_lockstep_fp32_and_advance(gpu_lib):
         assert bits_equal(ba.events[k].get_state(), bb.events[k].get_state())
     ba.close()
     bb.close()
+
+
+@pytest.fixture(scope="module")
+def small_guess(gpu_lib):
+    """a network trained briefly on pairs harvested from one small event"""
+    from fivo2d.guess import RecoveryGuess
+    m, grids, states = _events([(48, 48)], seed0=2301)
+    g = RecoveryGuess(seed=5, lib=gpu_lib)
+    g.reserve(400_000)
+    w = GPUWork2D(m, grids[0], lib=gpu_lib)
+    w.set_state(states[0])
+    w.finalize_ic(0.6)
+    tau = 0.6
+    for _ in range(12):
+        r = w.advance(tau, 10.0, 0.2, 0.05, A.FIVO_SSPRK3, max_steps=1)
+        assert r["ok"]
+        tau = r["tau"]
+        w.update_primitives(tau)
+        g.harvest(w, tau)
+    w.close()
+    g.fit_norm()
+    g.train(300, ctas_per_step=64, lr=2e-3, seed=9)
+    yield g
+    g.close()
+
+
+@pytest.mark.parametrize("mode", [A.FIVO_GUESS_EVERY_CELL, A.FIVO_GUESS_DEFERRED])
+def test_lockstep_learned_guess_equals_single_runs(gpu_lib, small_guess, mode):
+    """The learned guess in lockstep: every cell's tile (k_prim_learned's body per
+    block) or the union of the events' deferred cells in shared tensor-core tiles
+    (the retry across events), then the full recovery of what is left. Each event
+    equals its separate run with the same network attached, bit for bit, and the
+    Newton statistics of the guess agree event by event."""
+    from fivo2d.guess import newton_stats
+    g = small_guess
+    sizes = [(24, 24), (40, 32), (32, 48), (20, 28)]
+    m, grids, states = _events(sizes, seed0=1501)
+    b = GPUBatch2D(m, grids, nworkers=2, lib=gpu_lib)
+    b.set_lockstep(True, graphs=True)
+    for e, U in zip(b.events, states):
+        g.attach(e, mode)
+        e.set_state(U)
+        e.finalize_ic(0.6)
+        newton_stats(e, reset=True)
+    rb = b.run(0.6, 10.0, 0.2, 0.05, A.FIVO_SSPRK3, max_steps=10)
+    stats_b = [newton_stats(e) for e in b.events]
+    out = []
+    for gr, U in zip(grids, states):
+        w = GPUWork2D(m, gr, lib=gpu_lib)
+        g.attach(w, mode)
+        w.set_state(U)
+        w.finalize_ic(0.6)
+        newton_stats(w, reset=True)
+        r = w.run(0.6, 10.0, 0.2, 0.05, A.FIVO_SSPRK3, max_steps=10)
+        out.append((r, w.get_state(), w.get_history(), newton_stats(w)))
+        w.close()
+    _assert_batch_equals(b, rb, [o[:3] for o in out])
+    for k, o in enumerate(out):
+        for key in ("n_learn", "ok_learn", "it_learn", "deferred"):
+            assert stats_b[k][key] == o[3][key], (k, key, stats_b[k][key], o[3][key])
+    assert sum(s["n_learn"] for s in stats_b) > 0 and sum(s["ok_learn"] for s in stats_b) > 0
+    b.close()
 
 
 def test_lockstep_refuses_mixed_precision(gpu_lib):
