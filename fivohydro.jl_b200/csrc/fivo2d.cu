@@ -1765,7 +1765,7 @@ struct Lockstep {
   std::vector<double> cand_ms;
   int chosen = -1;
   int tuned_steps = 0;
-  /* (sequence, integrator, candidate, precision, recovery, the learned guess's weights) */
+  /* (sequence, integrator and boundary condition, candidate, precision, recovery, the learned guess's weights) */
   std::map<std::tuple<int, int, int, int, int, std::string>, cudaGraphExec_t> graphs;
   int64_t steps = 0, fallbacks = 0;
   double ms_step = 0.0, ms_post = 0.0;
@@ -2064,7 +2064,7 @@ int ls_exec(fivo_batch* b, int seq, int integrator, int bc, int cand, int prec, 
     const fivo_ctx* c0 = b->ev[0];
     /* the guess's weights and normalisation are kernel arguments: a graph per attached network */
     const std::string net = c0->learned ? std::string((const char*)&c0->gnet, sizeof(c0->gnet)) : std::string();
-    const auto key = std::make_tuple(seq, integrator, cand, prec, c0->learned ? 1 + c0->guess_mode : 0, net);
+    const auto key = std::make_tuple(seq, integrator * 16 + bc, cand, prec, c0->learned ? 1 + c0->guess_mode : 0, net);
     auto it = L.graphs.find(key);
     if (it == L.graphs.end()) {
       CK(cudaStreamBeginCapture(L.st, cudaStreamCaptureModeThreadLocal));

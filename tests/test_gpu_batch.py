@@ -290,6 +290,34 @@ def test_lockstep_learned_guess_equals_single_runs(gpu_lib, small_guess, mode):
     b.close()
 
 
+def test_lockstep_graphs_follow_the_boundary_condition(gpu_lib):
+    """Lockstep advances with outflow, then periodic, then outflow boundaries on the
+    same batch (each launch sequence is a graph per boundary condition): every event
+    equals a separate context advanced with the same boundaries, bit for bit."""
+    sizes = [(24, 24), (28, 20)]
+    m, grids, states = _events(sizes, seed0=1601)
+    b = GPUBatch2D(m, grids, lib=gpu_lib)
+    b.set_lockstep(True, graphs=True)
+    singles = [GPUWork2D(m, g, lib=gpu_lib) for g in grids]
+    for e, w, U in zip(b.events, singles, states):
+        for x in (e, w):
+            x.set_state(U)
+            x.finalize_ic(0.6)
+            x.rhs(0.6)
+    taus, tw = [0.6] * len(sizes), [0.6] * len(sizes)
+    for bc in (A.FIVO_BC_OUTFLOW, A.FIVO_BC_PERIODIC, A.FIVO_BC_OUTFLOW):
+        r = b.advance(taus, 10.0, 0.2, 0.05, A.FIVO_SSPRK3, bc=bc, max_steps=2)
+        assert all(x["ok"] and x["nsteps"] == 2 for x in r)
+        taus = [x["tau"] for x in r]
+        for k, w in enumerate(singles):
+            tw[k] = w.advance(tw[k], 10.0, 0.2, 0.05, A.FIVO_SSPRK3, bc=bc, max_steps=2)["tau"]
+    assert taus == tw
+    for e, w in zip(b.events, singles):
+        assert bits_equal(e.get_state(), w.get_state())
+        w.close()
+    b.close()
+
+
 def test_lockstep_refuses_mixed_precision(gpu_lib):
     sizes = [(24, 24), (28, 28)]
     m, grids, states = _events(sizes, seed0=1401)
