@@ -17,10 +17,13 @@ so it runs to the configured tau = 10 fm/c.
 
   value     device-resident: K steps after W warm-up steps, per-step CUDA events on
             the library's stream, L2 flushed (256 MB write) between steps, sum over
-            the K steps, max over ranks. The per-kernel times of the roofline come
+            the K steps, max over ranks. Each step's two launch sequences (the
+            optimistic SSPRK step, then the primitive refresh and relaxation) are
+            replayed as CUDA graphs (fivo_ctx_set_graphs; --no-graphs launches kernel
+            by kernel, the same bits). The per-kernel times of the roofline come
             from replaying the same K steps (a device copy of the state taken before
-            them) with the library's kernel timing on, so the timed run has no
-            profiling events.
+            them) kernel by kernel with the library's kernel timing on, so the timed
+            run has no profiling events.
   full_run  the whole configured run, tau0 = 0.6 -> 10 fm/c, timed the same way
             from a device copy of the initial state: the figure that does not
             depend on the window.
@@ -258,6 +261,8 @@ def run_gpu(args):
         w.set_precision(A.FIVO_PRECISION_FP32_FACES)
     stream = torch.cuda.Stream()
     A.check(lib, lib.fivo_ctx_set_stream(w.h, C.c_void_p(stream.cuda_stream)), "set_stream")
+    graphs = not args.no_graphs
+    w.set_graphs(graphs)       # each step's launch sequences replayed as CUDA graphs (same bits)
     w.set_state(U0)
     w.finalize_ic(TAU0)
     nint = g.Nx * g.Ny
@@ -273,6 +278,7 @@ def run_gpu(args):
     if not args.no_full_run:
         init = GPUWork2D(m, g, lib=lib)          # the state at tau0, for the full-run figure
         A.check(lib, lib.fivo_ctx_set_stream(init.h, C.c_void_p(stream.cuda_stream)), "set_stream")
+        init.set_graphs(graphs)
         init.clone_state_from(w)
 
     def step_on(h, tau_, n):
@@ -307,6 +313,7 @@ def run_gpu(args):
         form32 = GPUWork2D(m, g, lib=lib)
         A.check(lib, lib.fivo_ctx_set_stream(form32.h, C.c_void_p(stream.cuda_stream)), "set_stream")
         form32.clone_state_from(w)
+        form32.set_graphs(graphs)
         form32.set_precision(A.FIVO_PRECISION_FP32_FACES)
     plain = None
     if guess is not None or args.fp32_faces:
@@ -329,6 +336,7 @@ def run_gpu(args):
     # the clock samples span the timed steps and their profiled replay (the same work):
     # a window of a few tens of milliseconds alone is shorter than one sampling period
     clk = ClockSampler(local).__enter__()
+    kernels0 = w.lockstep_info()["kernels"]
     for k in range(args.steps):
         l2_flush()
         starts[k].record(stream)
@@ -338,6 +346,7 @@ def run_gpu(args):
     if dist:
         dist.barrier()
     ms = sum(s.elapsed_time(e) for s, e in zip(starts, stops))
+    graph_kernels = w.lockstep_info()["kernels"] - kernels0   # kernels the timed steps' graphs ran
 
     # ---------------- the same steps again on the twin, kernel by kernel
     A.check(lib, lib.fivo_profile(twin.h, 1), "profile")
@@ -520,11 +529,15 @@ def run_gpu(args):
         "config": {"workload": WORKLOAD, "grid": [N_CELLS, N_CELLS], "box_fm": BOX, "tau0": TAU0,
                    "tau_window": [tau_start, tau], "integrator": "ssprk3", "cfl": CFL, "cfltau": CFLTAU,
                    "events_per_gpu": 1, "seed": SEED, "l2": "flushed (256 MB write) between timed steps",
-                   "parallelism": f"replicas{world}", "face_pass_xy": face_pass},
+                   "parallelism": f"replicas{world}",
+                   "face_pass_xy": ["global", "global"] if graphs else face_pass,
+                   "launch": ("each step's two launch sequences replayed as CUDA graphs on the stream "
+                              "(fivo_ctx_set_graphs); the per-kernel roofline times come from the same "
+                              "steps replayed kernel by kernel") if graphs else "kernel by kernel"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes, "steps": e2e_steps},
         "full_run": full_run,
-        "gpu_launches": int(kt.total_launches),
+        "gpu_launches": int(graph_kernels) if graphs else int(kt.total_launches),
         "roofline": roof,
         "clocks": clocks,
     }
@@ -1044,6 +1057,8 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=30, help="timed steps of the batched comparison")
     ap.add_argument("--fp32-faces", action="store_true",
                     help="the mixed-precision form: the face pass in FP32 (fivo_ctx_set_precision)")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="event workload: launch each step kernel by kernel instead of replaying CUDA graphs")
     ap.add_argument("--lockstep", action="store_true",
                     help="batch workload: lockstep mode (one launch per kernel over all events, CUDA graphs)")
     ap.add_argument("--guess", action="store_true",

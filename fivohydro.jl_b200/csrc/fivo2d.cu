@@ -189,6 +189,10 @@ struct fivo_ctx {
    * the tensor maps of the chosen shape: the primitive planes, and the dissipative
    * planes of each of the four state buffers */
   int ft_cfg[2] = {-2, -2};
+  /* fivo_ctx_set_graphs: fivo_run / fivo_advance through the lockstep launch
+   * sequences of a batch of this one context, replayed as CUDA graphs */
+  bool graphs = false;
+  fivo_batch* solo = nullptr;
   CUtensorMap ft_prim[2][5];
   CUtensorMap ft_slab[2][4 * FV_MAXP];   /* every plane of the state slab: the relaxation swaps
                                            the dissipative planes between state buffers */
@@ -954,9 +958,12 @@ int fivo_ctx_create(const fivo_params* p, int nx, int ny, int nghost, double xma
   return FIVO_OK;
 }
 
+void solo_destroy(fivo_batch* b);
+
 int fivo_ctx_destroy(fivo_ctx* c) {
   if (!c) return FIVO_OK;
   if (c->st) cudaStreamSynchronize(c->st);
+  solo_destroy(c->solo);
   for (auto& q : c->pend) { cudaEventDestroy(q.a); cudaEventDestroy(q.b); }
   for (auto e : c->pool) cudaEventDestroy(e);
   cudaFree(c->slab); cudaFree(c->pbuf); cudaFree(c->hbuf); cudaFree(c->masks); cudaFree(c->fl);
@@ -1227,6 +1234,9 @@ int advance_loop(fivo_ctx* c, double tau, double taufinal, double cfl, double cf
 }
 }  // namespace
 
+int solo_advance(fivo_ctx* c, double tau, double taufinal, double cfl, double cfltau, int integrator, int bc,
+                 int64_t max_steps, fivo_run_result* out);
+
 namespace {
 /* run_sim_2d! before its loop: the history reset, one RHS pass to populate the
  * primitives and signal speeds (main2D.jl:418), the initial total charge */
@@ -1264,7 +1274,9 @@ int fivo_run(fivo_ctx* c, double tau0, double taufinal, double cfl, double cflta
   std::memset(out, 0, sizeof(*out));
   double Qin = 0.0;
   if ((rc = run_begin(c, tau0, bc, reset_hist, &Qin))) return rc;
-  if ((rc = advance_loop(c, tau0, taufinal, cfl, cfltau, integrator, bc, max_steps, out))) return rc;
+  if (c->graphs && !c->profiling) rc = solo_advance(c, tau0, taufinal, cfl, cfltau, integrator, bc, max_steps, out);
+  else rc = advance_loop(c, tau0, taufinal, cfl, cfltau, integrator, bc, max_steps, out);
+  if (rc) return rc;
   return run_end(c, Qin, out);
 }
 
@@ -1274,6 +1286,7 @@ int fivo_advance(fivo_ctx* c, double tau, double taufinal, double cfl, double cf
   if (integrator != FIVO_SSPRK2 && integrator != FIVO_SSPRK3)
     return fail(FIVO_ERR_ARG, "integrator must be FIVO_SSPRK2 or FIVO_SSPRK3");
   std::memset(out, 0, sizeof(*out));
+  if (c->graphs && !c->profiling) return solo_advance(c, tau, taufinal, cfl, cfltau, integrator, bc, max_steps, out);
   return advance_loop(c, tau, taufinal, cfl, cfltau, integrator, bc, max_steps, out);
 }
 
@@ -1747,7 +1760,10 @@ enum { LS_STEP = 0, LS_POST = 1 };
 
 struct Lockstep {
   int flags = 0;
-  cudaStream_t st = nullptr;
+  cudaStream_t st = nullptr;                 /* the lockstep's own stream */
+  cudaStream_t run_st = nullptr;             /* where the sequences run: st, or a single context's stream */
+  int64_t kernels = 0;                       /* kernels launched (graph nodes replayed included) */
+  int last_nk = 0;                           /* kernels of the sequence built last */
   cudaEvent_t done = nullptr;                /* blocking: the host thread sleeps while it waits */
   cudaEvent_t ta = nullptr, tb = nullptr;    /* device time of a launch sequence */
   int nev = 0, nsm = 148;
@@ -1766,7 +1782,7 @@ struct Lockstep {
   int chosen = -1;
   int tuned_steps = 0;
   /* (sequence, integrator and boundary condition, candidate, precision, recovery, the learned guess's weights) */
-  std::map<std::tuple<int, int, int, int, int, std::string>, cudaGraphExec_t> graphs;
+  std::map<std::tuple<int, int, int, int, int, std::string>, std::pair<cudaGraphExec_t, int>> graphs;
   int64_t steps = 0, fallbacks = 0;
   double ms_step = 0.0, ms_post = 0.0;
 };
@@ -1776,7 +1792,7 @@ constexpr int LS_TUNE_ROUNDS = 2;
 int ls_destroy(Lockstep* L) {
   if (!L) return FIVO_OK;
   if (L->st) cudaStreamSynchronize(L->st);
-  for (auto& g : L->graphs) cudaGraphExecDestroy(g.second);
+  for (auto& g : L->graphs) cudaGraphExecDestroy(g.second.first);
   for (int o = 0; o < 2; ++o) {
     cudaFree(L->geo_d[o]);
     for (int s = 0; s < bt::NSHAPE; ++s) cudaFree(L->eob_d[o][s]);
@@ -1816,6 +1832,7 @@ int ls_create(fivo_batch* b, int flags, Lockstep** out) {
       cudaEventCreateWithFlags(&L->done, cudaEventBlockingSync | cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreate(&L->ta) != cudaSuccess || cudaEventCreate(&L->tb) != cudaSuccess)
     return cleanup(fail(FIVO_ERR_CUDA, "fivo_batch_set_lockstep: stream or event creation failed"));
+  L->run_st = L->st;
   for (int order = 0; order < 2; ++order) {
     std::vector<int> perm(n);
     std::iota(perm.begin(), perm.end(), 0);
@@ -1920,10 +1937,15 @@ void ls_fill_post(fivo_ctx* c, bt::Ev& e, double tau, double used, int do_relax,
 }
 
 #define LS_GRID(s) L.nblocks[s] ? L.nblocks[s] : 1
+#define LS_K() \
+  do {         \
+    CKL();     \
+    ++nk;      \
+  } while (0)
 constexpr int LS_LEARNED_DYN = LEARNED_SMEM - (int)sizeof(guess::FwdSmem) - 1024;
 constexpr int LS_RETRY_DYN = LEARNED_SMEM - (int)sizeof(guess::FwdSmem) - 128;
 
-/* enqueue one launch sequence on L.st (recorded into a graph or run directly) */
+/* enqueue one launch sequence on L.run_st (recorded into a graph or run directly) */
 template <int EOS, bool NCH>
 int ls_launch_t(fivo_batch* b, int seq, int integrator, int bc, int cand, int prec, bool any_sector, bool relax_on) {
   Lockstep& L = *b->ls;
@@ -1933,9 +1955,10 @@ int ls_launch_t(fivo_batch* b, int seq, int integrator, int bc, int cand, int pr
   const bt::Geo* geo = L.geo_d[order];
   unsigned short* const* eob = L.eob_d[order];
   const DevParams& d0 = L.d0;
-  cudaStream_t st = L.st;
+  cudaStream_t st = L.run_st;
   const bool f32 = prec != FIVO_PRECISION_FP64;
   const unsigned gr = nblk(n, 256);
+  int nk = 0;   /* kernels of this sequence */
   CK(cudaMemcpyAsync(L.tab_d, L.tab_h, n * sizeof(bt::Ev), cudaMemcpyHostToDevice, st));
   /* _primitive_pass!: as launch_primitive_t, with or without the learned guess */
   const fivo_ctx* c0 = b->ev[0];
@@ -1943,89 +1966,90 @@ int ls_launch_t(fivo_batch* b, int seq, int integrator, int bc, int cand, int pr
     if (c0->learned && c0->guess_mode == FIVO_GUESS_EVERY_CELL) {
       bt::kb_prim_learned<EOS, NCH><<<LS_GRID(bt::SH_CELL), 128, LS_LEARNED_DYN, st>>>(d0, geo, L.tab_d,
                                                                                      eob[bt::SH_CELL], which, c0->gnet);
-      CKL();
+      LS_K();
     } else {
       bt::kb_prim_fast<EOS, NCH><<<LS_GRID(bt::SH_CELL), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_CELL], which);
-      CKL();
+      LS_K();
     }
     int left = 0;
     if (c0->learned && c0->guess_mode == FIVO_GUESS_DEFERRED) {
       /* the network's guess for the deferred cells of every event, then the full
        * recovery of what it leaves */
       bt::kb_scan<<<1, 1024, 0, st>>>(L.tab_d, n, 3, L.pre_d, L.ctl_d);
-      CKL();
+      LS_K();
       bt::kb_prim_learned_retry<EOS, NCH><<<LS_GRID(bt::SH_CELL), 128, LS_RETRY_DYN, st>>>(
           d0, geo, L.tab_d, L.pre_d, n, L.ctl_d, which, c0->gnet);
-      CKL();
+      LS_K();
       left = 1;
     }
     bt::kb_scan<<<1, 1024, 0, st>>>(L.tab_d, n, left ? 2 : 0, L.pre_d, L.ctl_d);
-    CKL();
+    LS_K();
     bt::kb_prim_slow<EOS, NCH><<<slow_blocks, 128, 0, st>>>(d0, geo, L.tab_d, L.pre_d, n, L.ctl_d, which, left);
-    CKL();
+    LS_K();
     return FIVO_OK;
   };
   int rc;
   if (seq == LS_STEP) {
     bt::kb_pre_step<<<LS_GRID(bt::SH_CELL), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_CELL]);
-    CKL();
+    LS_K();
     const int nst = integrator == FIVO_SSPRK3 ? 3 : 2;
     const bool full = d0.hasNu && d0.hasPi && d0.hasShear;
     for (int k = 0; k < nst; ++k) {
       if (k == 0) {
         bt::kb_bc<<<LS_GRID(bt::SH_FRAME), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FRAME], 0, bc);
-        CKL();
+        LS_K();
       }
       bt::kb_reset<<<gr, 256, 0, st>>>(L.tab_d, n, k == 0 ? (1 | 2 | 64) : (1 | 2));
-      CKL();
+      LS_K();
       if ((rc = prim_pass(k))) return rc;
       if (f32) {
         bt::kb_faces<EOS, true, true><<<LS_GRID(bt::SH_FACEX), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FACEX], k);
-        CKL();
+        LS_K();
         bt::kb_faces<EOS, false, true><<<LS_GRID(bt::SH_FACEY), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FACEY], k);
-        CKL();
+        LS_K();
         if (full) bt::kb_update<EOS, NCH, float, true><<<LS_GRID(bt::SH_INT), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_INT], k);
         else bt::kb_update<EOS, NCH, float, false><<<LS_GRID(bt::SH_INT), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_INT], k);
-        CKL();
+        LS_K();
       } else {
         bt::kb_faces<EOS, true, false><<<LS_GRID(bt::SH_FACEX), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FACEX], k);
-        CKL();
+        LS_K();
         bt::kb_faces<EOS, false, false><<<LS_GRID(bt::SH_FACEY), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FACEY], k);
-        CKL();
+        LS_K();
         if (full) bt::kb_update<EOS, NCH, double, true><<<LS_GRID(bt::SH_INT), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_INT], k);
         else bt::kb_update<EOS, NCH, double, false><<<LS_GRID(bt::SH_INT), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_INT], k);
-        CKL();
+        LS_K();
       }
       bt::kb_scan<<<1, 1024, 0, st>>>(L.tab_d, n, 1, L.pre_d, L.ctl_d);
-      CKL();
+      LS_K();
       bt::kb_adm_slow<EOS, NCH><<<(unsigned)L.nsm, 128, 0, st>>>(d0, geo, L.tab_d, L.pre_d, n, L.ctl_d, k);
-      CKL();
+      LS_K();
       bt::kb_bc<<<LS_GRID(bt::SH_FRAME), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FRAME], k + 1, bc);
-      CKL();
+      LS_K();
     }
   } else {
     if (any_sector) {
       bt::kb_reset<<<gr, 256, 0, st>>>(L.tab_d, n, 1 | 64);
-      CKL();
+      LS_K();
       if ((rc = prim_pass(3))) return rc;
     }
     if (relax_on) {
       bt::kb_reset<<<gr, 256, 0, st>>>(L.tab_d, n, 4);
-      CKL();
+      LS_K();
       if (prec == FIVO_PRECISION_FP32 && any_sector)
         bt::kb_relax<EOS, false, true><<<LS_GRID(bt::SH_CELL), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_CELL]);
       else if (d0.hasM2)
         bt::kb_relax<EOS, true, false><<<LS_GRID(bt::SH_CELL), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_CELL]);
       else
         bt::kb_relax<EOS, false, false><<<LS_GRID(bt::SH_CELL), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_CELL]);
-      CKL();
+      LS_K();
       bt::kb_post_hist<<<LS_GRID(bt::SH_CELL), 128, 0, st>>>(geo, L.tab_d, eob[bt::SH_CELL]);
-      CKL();
+      LS_K();
     }
   }
   bt::kb_gather_flags<<<nblk((long long)n * (sizeof(DevFlags) / 8), 256), 256, 0, st>>>(L.tab_d, n, L.flg_d);
-  CKL();
+  LS_K();
   CK(cudaMemcpyAsync(L.flg_h, L.flg_d, n * sizeof(DevFlags), cudaMemcpyDeviceToHost, st));
+  L.last_nk = nk;
   return FIVO_OK;
 }
 
@@ -2059,7 +2083,7 @@ int ls_exec(fivo_batch* b, int seq, int integrator, int bc, int cand, int prec, 
   Lockstep& L = *b->ls;
   int rc0 = ls_prepare(L.d0);
   if (rc0) return rc0;
-  CK(cudaEventRecord(L.ta, L.st));
+  CK(cudaEventRecord(L.ta, L.run_st));
   if (L.flags & FIVO_LOCKSTEP_GRAPHS) {
     const fivo_ctx* c0 = b->ev[0];
     /* the guess's weights and normalisation are kernel arguments: a graph per attached network */
@@ -2067,25 +2091,27 @@ int ls_exec(fivo_batch* b, int seq, int integrator, int bc, int cand, int prec, 
     const auto key = std::make_tuple(seq, integrator * 16 + bc, cand, prec, c0->learned ? 1 + c0->guess_mode : 0, net);
     auto it = L.graphs.find(key);
     if (it == L.graphs.end()) {
-      CK(cudaStreamBeginCapture(L.st, cudaStreamCaptureModeThreadLocal));
+      CK(cudaStreamBeginCapture(L.run_st, cudaStreamCaptureModeThreadLocal));
       const int rc = ls_launch(b, seq, integrator, bc, cand, prec, any_sector, relax_on);
       cudaGraph_t g = nullptr;
-      const cudaError_t ec = cudaStreamEndCapture(L.st, &g);
+      const cudaError_t ec = cudaStreamEndCapture(L.run_st, &g);
       if (rc) { if (g) cudaGraphDestroy(g); return rc; }
       if (ec != cudaSuccess) return fail(FIVO_ERR_CUDA, std::string("lockstep graph capture: ") + cudaGetErrorString(ec));
       cudaGraphExec_t x = nullptr;
       const cudaError_t ei = cudaGraphInstantiate(&x, g, 0);
       cudaGraphDestroy(g);
       if (ei != cudaSuccess) return fail(FIVO_ERR_CUDA, std::string("lockstep graph instantiation: ") + cudaGetErrorString(ei));
-      it = L.graphs.emplace(key, x).first;
+      it = L.graphs.emplace(key, std::make_pair(x, L.last_nk)).first;
     }
-    CK(cudaGraphLaunch(it->second, L.st));
+    CK(cudaGraphLaunch(it->second.first, L.run_st));
+    L.kernels += it->second.second;
   } else {
     const int rc = ls_launch(b, seq, integrator, bc, cand, prec, any_sector, relax_on);
     if (rc) return rc;
+    L.kernels += L.last_nk;
   }
-  CK(cudaEventRecord(L.tb, L.st));
-  CK(cudaEventRecord(L.done, L.st));
+  CK(cudaEventRecord(L.tb, L.run_st));
+  CK(cudaEventRecord(L.done, L.run_st));
   CK(cudaEventSynchronize(L.done));
   CK(cudaEventElapsedTime(ms, L.ta, L.tb));
   return FIVO_OK;
@@ -2264,6 +2290,22 @@ int ls_status(const std::vector<int>& st, const std::vector<std::string>& msg, i
   return FIVO_OK;
 }
 
+void ls_info(const Lockstep& L, bool enabled, fivo_lockstep_info* out) {
+  out->enabled = enabled ? 1 : 0;
+  out->flags = L.flags;
+  out->ncand = std::min<int>((int)L.cands.size(), FIVO_LOCKSTEP_MAXCAND);
+  out->chosen = L.chosen;
+  for (int i = 0; i < out->ncand; ++i) {
+    out->cand_order[i] = L.cands[i].first;
+    out->cand_slow[i] = L.cands[i].second;
+    out->cand_ms[i] = L.cand_ms[i];
+  }
+  out->steps = L.steps;
+  out->fallbacks = L.fallbacks;
+  out->ms_step = L.ms_step;
+  out->ms_post = L.ms_post;
+  out->kernels = L.kernels;
+}
 }  // namespace
 
 int fivo_batch_set_lockstep(fivo_batch* b, int enable, int flags) {
@@ -2286,19 +2328,7 @@ int fivo_batch_lockstep_info(fivo_batch* b, fivo_lockstep_info* out) {
   out->enabled = b->lockstep ? 1 : 0;
   out->chosen = -1;
   if (!b->ls) return FIVO_OK;
-  const Lockstep& L = *b->ls;
-  out->flags = L.flags;
-  out->ncand = std::min<int>((int)L.cands.size(), FIVO_LOCKSTEP_MAXCAND);
-  out->chosen = L.chosen;
-  for (int i = 0; i < out->ncand; ++i) {
-    out->cand_order[i] = L.cands[i].first;
-    out->cand_slow[i] = L.cands[i].second;
-    out->cand_ms[i] = L.cand_ms[i];
-  }
-  out->steps = L.steps;
-  out->fallbacks = L.fallbacks;
-  out->ms_step = L.ms_step;
-  out->ms_post = L.ms_post;
+  ls_info(*b->ls, b->lockstep, out);
   return FIVO_OK;
 }
 
@@ -2346,6 +2376,59 @@ int fivo_batch_advance(fivo_batch* b, const double* tau, double taufinal, double
   return batch_for_each(b, status, [&](int k) {
     return fivo_advance(b->ev[k], tau[k], taufinal, cfl, cfltau, integrator, bc, max_steps, &results[k]);
   });
+}
+
+/* ------------------------------------------------------------------------
+ * One context through the lockstep launch sequences (fivo_ctx_set_graphs): a
+ * batch of this one context, whose STEP and POST sequences run on the context's
+ * stream as captured CUDA graphs (two graph launches and two host reads per
+ * step instead of ~32 launches), with the lockstep's default schedule. The
+ * kernels and their inputs are those of the single-context path, so results are
+ * the same bits; the face pass is the global-load one.
+ * ---------------------------------------------------------------------- */
+void solo_destroy(fivo_batch* b) {
+  if (!b) return;
+  ls_destroy(b->ls);
+  delete b;   /* the batch does not own its one context */
+}
+
+int solo_advance(fivo_ctx* c, double tau, double taufinal, double cfl, double cfltau, int integrator, int bc,
+                 int64_t max_steps, fivo_run_result* out) {
+  if (!c->solo) {
+    fivo_batch* b = new fivo_batch();
+    b->ev.push_back(c);
+    b->nworkers = 1;
+    b->device = c->device;
+    int rc = ls_create(b, FIVO_LOCKSTEP_GRAPHS, &b->ls);
+    if (rc) { b->ls = nullptr; delete b; return rc; }
+    b->lockstep = true;
+    c->solo = b;
+  }
+  fivo_batch* b = c->solo;
+  b->ls->run_st = c->st;   /* the caller's stream (fivo_ctx_set_stream) orders the work */
+  std::vector<double> t(1, tau);
+  std::vector<int> st(1, FIVO_OK);
+  std::vector<std::string> msg(1);
+  int rc = ls_loop(b, t, taufinal, cfl, cfltau, integrator, bc, max_steps, out, st, msg);
+  if (rc) return rc;
+  if (st[0] != FIVO_OK) return fail(st[0], msg[0]);
+  return FIVO_OK;
+}
+
+int fivo_ctx_set_graphs(fivo_ctx* c, int enable) {
+  if (!c) return fail(FIVO_ERR_ARG, "null context");
+  c->graphs = enable != 0;
+  return FIVO_OK;
+}
+
+
+int fivo_ctx_lockstep_info(fivo_ctx* c, fivo_lockstep_info* out) {
+  if (!c || !out) return fail(FIVO_ERR_ARG, "null argument");
+  std::memset(out, 0, sizeof(*out));
+  out->enabled = c->graphs ? 1 : 0;
+  out->chosen = -1;
+  if (c->solo) ls_info(*c->solo->ls, c->graphs, out);
+  return FIVO_OK;
 }
 
 /* ------------------------------------------------ the learned recovery guess */

@@ -90,7 +90,7 @@ class FivoLockstepInfo(C.Structure):
         ("enabled", C.c_int32), ("flags", C.c_int32), ("ncand", C.c_int32), ("chosen", C.c_int32),
         ("cand_order", C.c_int32 * FIVO_LOCKSTEP_MAXCAND), ("cand_slow", C.c_int32 * FIVO_LOCKSTEP_MAXCAND),
         ("cand_ms", C.c_double * FIVO_LOCKSTEP_MAXCAND), ("steps", C.c_int64), ("fallbacks", C.c_int64),
-        ("ms_step", C.c_double), ("ms_post", C.c_double),
+        ("ms_step", C.c_double), ("ms_post", C.c_double), ("kernels", C.c_int64),
     ]
 
     def as_dict(self):
@@ -101,7 +101,7 @@ class FivoLockstepInfo(C.Structure):
                                 "slow_blocks_per_sm": self.cand_slow[i], "best_step_ms": self.cand_ms[i]}
                                for i in range(n)],
                 "steps": self.steps, "fallbacks": self.fallbacks, "ms_step": self.ms_step,
-                "ms_post": self.ms_post}
+                "ms_post": self.ms_post, "kernels": self.kernels}
 
 
 FIVO_KCLASS_N = 8
@@ -165,6 +165,8 @@ SIGNATURES = {
                                      C.c_int64, C.POINTER(FivoRunResult), C.POINTER(C.c_int)]),
     "fivo_batch_set_lockstep": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "fivo_batch_lockstep_info": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "fivo_ctx_set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
+    "fivo_ctx_lockstep_info": (C.c_int, [C.c_void_p, C.c_void_p]),
     "fivo_upload_state": (C.c_int, [C.c_void_p, _D, C.c_int, _I64]),
     "fivo_download_state": (C.c_int, [C.c_void_p, _D, C.c_int, _I64]),
     "fivo_upload_history": (C.c_int, [C.c_void_p, _I64] + [_D] * 8),

@@ -183,6 +183,16 @@ class GPUWork2D:
     def finalize_ic(self, tau0, bc=A.FIVO_BC_OUTFLOW):
         self._ck(self.lib.fivo_finalize_ic(self.h, tau0, bc), "fivo_finalize_ic")
 
+    def set_graphs(self, enable=True):
+        """fivo_ctx_set_graphs: run and advance through the lockstep launch sequences of
+        this one context, replayed as CUDA graphs on the context's stream (same bits)"""
+        self._ck(self.lib.fivo_ctx_set_graphs(self.h, int(bool(enable))), "fivo_ctx_set_graphs")
+
+    def lockstep_info(self):
+        info = A.FivoLockstepInfo()
+        self._ck(self.lib.fivo_ctx_lockstep_info(self.h, C.byref(info)), "fivo_ctx_lockstep_info")
+        return info.as_dict()
+
     def set_precision(self, mode):
         """FIVO_PRECISION_FP64 (the reference's arithmetic), FIVO_PRECISION_FP32_FACES (the
         face pass of rhs_2d! in FP32, everything else FP64) or FIVO_PRECISION_FP32 (the

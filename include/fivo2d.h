@@ -409,8 +409,20 @@ typedef struct fivo_lockstep_info {
   int64_t steps;            /* lockstep steps taken (batch-wide) */
   int64_t fallbacks;        /* event steps redone stage by stage */
   double  ms_step, ms_post; /* device time of the step and post-step launch sequences */
+  int64_t kernels;          /* kernels launched by the sequences (graph nodes replayed included) */
 } fivo_lockstep_info;
 int  fivo_batch_lockstep_info(fivo_batch* b, fivo_lockstep_info* out);
+
+/* One context through the same launch sequences (enable != 0): fivo_run and
+ * fivo_advance take each step as a batch of this one context, the step and the
+ * post-step pass replayed as CUDA graphs on the context's stream (two graph
+ * launches and two host reads per step instead of about 32 kernel launches),
+ * with the default schedule and the global-load face pass. Results are the same
+ * bits as without it. While fivo_profile is on the per-kernel path is taken.
+ * fivo_ctx_lockstep_info reports its sequences. Replaces nothing in the
+ * reference: its step is a sequence of Julia calls (main2D.jl:436-513). */
+int  fivo_ctx_set_graphs(fivo_ctx* c, int enable);
+int  fivo_ctx_lockstep_info(fivo_ctx* c, fivo_lockstep_info* out);
 
 /* --- the learned starting guess of the primitive recovery (no counterpart in
  * the reference: its Newton starts from the previous step's primitives or the

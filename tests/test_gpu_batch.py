@@ -331,3 +331,35 @@ def test_lockstep_refuses_mixed_precision(gpu_lib):
         b.run(0.6, 10.0, 0.2, 0.05, A.FIVO_SSPRK3, max_steps=2)
     assert "same precision" in str(e.value)
     b.close()
+
+
+@pytest.mark.parametrize("integrator", [A.FIVO_SSPRK2, A.FIVO_SSPRK3])
+def test_single_context_graphs_bitwise(gpu_lib, integrator):
+    """fivo_ctx_set_graphs: one context's run and advance through the lockstep
+    sequences replayed as CUDA graphs on the context's stream equal the
+    per-kernel path bit for bit (state, history, run results), and the graphs
+    count their kernels."""
+    m, grids, states = _events([(40, 36)], seed0=1701)
+    w1, w2 = GPUWork2D(m, grids[0], lib=gpu_lib), GPUWork2D(m, grids[0], lib=gpu_lib)
+    w2.set_graphs(True)
+    for w in (w1, w2):
+        w.set_state(states[0])
+        w.finalize_ic(0.6)
+    r1 = w1.run(0.6, 10.0, 0.2, 0.05, integrator, max_steps=15)
+    r2 = w2.run(0.6, 10.0, 0.2, 0.05, integrator, max_steps=15)
+    for key in ("ok", "tau", "nsteps", "nprimfail", "nvacuum", "maxu", "max_shear_res", "dQ"):
+        assert r1[key] == r2[key], (key, r1[key], r2[key])
+    t1, t2 = r1["tau"], r2["tau"]
+    for _ in range(3):
+        t1 = w1.advance(t1, 10.0, 0.2, 0.05, integrator, max_steps=1)["tau"]
+        t2 = w2.advance(t2, 10.0, 0.2, 0.05, integrator, max_steps=1)["tau"]
+    assert t1 == t2
+    assert bits_equal(w1.get_state(), w2.get_state())
+    h1, h2 = w1.get_history(), w2.get_history()
+    for name in h1:
+        assert bits_equal(h1[name], h2[name]), name
+    info = w2.lockstep_info()
+    assert info["enabled"] and info["graphs"] and info["steps"] == 18 and info["kernels"] > 18 * 20
+    assert not w1.lockstep_info()["enabled"]
+    w1.close()
+    w2.close()
