@@ -17,13 +17,13 @@ so it runs to the configured tau = 10 fm/c.
 
   value     device-resident: K steps after W warm-up steps, per-step CUDA events on
             the library's stream, L2 flushed (256 MB write) between steps, sum over
-            the K steps, max over ranks. Each step's two launch sequences (the
-            optimistic SSPRK step, then the primitive refresh and relaxation) are
-            replayed as CUDA graphs (fivo_ctx_set_graphs; --no-graphs launches kernel
-            by kernel, the same bits). The per-kernel times of the roofline come
-            from replaying the same K steps (a device copy of the state taken before
-            them) kernel by kernel with the library's kernel timing on, so the timed
-            run has no profiling events.
+            the K steps, max over ranks. Kernel by kernel; --graphs replays each step's
+            two launch sequences (the optimistic SSPRK step, then the primitive
+            refresh and relaxation) as CUDA graphs instead (fivo_ctx_set_graphs, the
+            same bits). The per-kernel times of the roofline come from replaying the
+            same K steps (a device copy of the state taken before them) kernel by
+            kernel with the library's kernel timing on, so the timed run has no
+            profiling events.
   full_run  the whole configured run, tau0 = 0.6 -> 10 fm/c, timed the same way
             from a device copy of the initial state: the figure that does not
             depend on the window.
@@ -261,8 +261,8 @@ def run_gpu(args):
         w.set_precision(A.FIVO_PRECISION_FP32_FACES)
     stream = torch.cuda.Stream()
     A.check(lib, lib.fivo_ctx_set_stream(w.h, C.c_void_p(stream.cuda_stream)), "set_stream")
-    graphs = not args.no_graphs
-    w.set_graphs(graphs)       # each step's launch sequences replayed as CUDA graphs (same bits)
+    graphs = args.graphs
+    w.set_graphs(graphs)       # --graphs: each step's launch sequences replayed as CUDA graphs (same bits)
     w.set_state(U0)
     w.finalize_ic(TAU0)
     nint = g.Nx * g.Ny
@@ -1057,8 +1057,9 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=30, help="timed steps of the batched comparison")
     ap.add_argument("--fp32-faces", action="store_true",
                     help="the mixed-precision form: the face pass in FP32 (fivo_ctx_set_precision)")
-    ap.add_argument("--no-graphs", action="store_true",
-                    help="event workload: launch each step kernel by kernel instead of replaying CUDA graphs")
+    ap.add_argument("--graphs", action="store_true",
+                    help="event workload: replay each step's launch sequences as CUDA graphs "
+                         "(fivo_ctx_set_graphs) instead of launching kernel by kernel")
     ap.add_argument("--lockstep", action="store_true",
                     help="batch workload: lockstep mode (one launch per kernel over all events, CUDA graphs)")
     ap.add_argument("--guess", action="store_true",

@@ -191,7 +191,7 @@ struct fivo_ctx {
   int ft_cfg[2] = {-2, -2};
   /* fivo_ctx_set_graphs: fivo_run / fivo_advance through the lockstep launch
    * sequences of a batch of this one context, replayed as CUDA graphs */
-  bool graphs = false;
+  int graphs = 0;                 /* 1: graphs; 2: the same sequences launched kernel by kernel */
   fivo_batch* solo = nullptr;
   CUtensorMap ft_prim[2][5];
   CUtensorMap ft_slab[2][4 * FV_MAXP];   /* every plane of the state slab: the relaxation swaps
@@ -1764,7 +1764,8 @@ struct Lockstep {
   cudaStream_t run_st = nullptr;             /* where the sequences run: st, or a single context's stream */
   int64_t kernels = 0;                       /* kernels launched (graph nodes replayed included) */
   int last_nk = 0;                           /* kernels of the sequence built last */
-  cudaEvent_t done = nullptr;                /* blocking: the host thread sleeps while it waits */
+  cudaEvent_t done = nullptr;                /* the end of a sequence; one host thread waits on it */
+  bool prepared = false;                     /* the learned kernels' shared-memory attributes are set */
   cudaEvent_t ta = nullptr, tb = nullptr;    /* device time of a launch sequence */
   int nev = 0, nsm = 148;
   DevParams d0;                              /* the shared model; grid fields come from Geo */
@@ -1829,7 +1830,7 @@ int ls_create(fivo_batch* b, int flags, Lockstep** out) {
   L->d0 = b->ev[0]->dp;
   L->nsm = b->ev[0]->nsm;
   if (cudaStreamCreateWithFlags(&L->st, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&L->done, cudaEventBlockingSync | cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&L->done, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreate(&L->ta) != cudaSuccess || cudaEventCreate(&L->tb) != cudaSuccess)
     return cleanup(fail(FIVO_ERR_CUDA, "fivo_batch_set_lockstep: stream or event creation failed"));
   L->run_st = L->st;
@@ -2081,8 +2082,11 @@ int ls_launch(fivo_batch* b, int seq, int integrator, int bc, int cand, int prec
 int ls_exec(fivo_batch* b, int seq, int integrator, int bc, int cand, int prec, bool any_sector, bool relax_on,
             float* ms) {
   Lockstep& L = *b->ls;
-  int rc0 = ls_prepare(L.d0);
-  if (rc0) return rc0;
+  if (!L.prepared) {
+    const int rc0 = ls_prepare(L.d0);
+    if (rc0) return rc0;
+    L.prepared = true;
+  }
   CK(cudaEventRecord(L.ta, L.run_st));
   if (L.flags & FIVO_LOCKSTEP_GRAPHS) {
     const fivo_ctx* c0 = b->ev[0];
@@ -2159,8 +2163,10 @@ int ls_loop(fivo_batch* b, std::vector<double>& tau, double taufinal, double cfl
         return fail(FIVO_ERR_NOMEM, "device allocation failed");
       }
     }
-    /* the batch stream reads what the contexts' streams wrote */
-    CK(ctx_sync(c));
+    /* the sequences' stream reads what the contexts' streams wrote (one host thread
+     * waits here, so it spins rather than sleeps as the batch workers do) */
+    CK(cudaStreamSynchronize(c->st));
+    prof_flush(c);
   }
   std::vector<char> done(n, 0), stepped(n, 0);
   std::vector<double> D(n, 0.0), used(n, 0.0), msr(n, 0.0);
@@ -2394,12 +2400,17 @@ void solo_destroy(fivo_batch* b) {
 
 int solo_advance(fivo_ctx* c, double tau, double taufinal, double cfl, double cfltau, int integrator, int bc,
                  int64_t max_steps, fivo_run_result* out) {
+  const int want = c->graphs == 2 ? 0 : FIVO_LOCKSTEP_GRAPHS;
+  if (c->solo && c->solo->ls->flags != want) {
+    solo_destroy(c->solo);
+    c->solo = nullptr;
+  }
   if (!c->solo) {
     fivo_batch* b = new fivo_batch();
     b->ev.push_back(c);
     b->nworkers = 1;
     b->device = c->device;
-    int rc = ls_create(b, FIVO_LOCKSTEP_GRAPHS, &b->ls);
+    int rc = ls_create(b, want, &b->ls);
     if (rc) { b->ls = nullptr; delete b; return rc; }
     b->lockstep = true;
     c->solo = b;
@@ -2415,9 +2426,10 @@ int solo_advance(fivo_ctx* c, double tau, double taufinal, double cfl, double cf
   return FIVO_OK;
 }
 
-int fivo_ctx_set_graphs(fivo_ctx* c, int enable) {
+int fivo_ctx_set_graphs(fivo_ctx* c, int mode) {
   if (!c) return fail(FIVO_ERR_ARG, "null context");
-  c->graphs = enable != 0;
+  if (mode < 0 || mode > 2) return fail(FIVO_ERR_ARG, "fivo_ctx_set_graphs: mode must be 0, 1 or 2");
+  c->graphs = mode;
   return FIVO_OK;
 }
 
@@ -2427,7 +2439,7 @@ int fivo_ctx_lockstep_info(fivo_ctx* c, fivo_lockstep_info* out) {
   std::memset(out, 0, sizeof(*out));
   out->enabled = c->graphs ? 1 : 0;
   out->chosen = -1;
-  if (c->solo) ls_info(*c->solo->ls, c->graphs, out);
+  if (c->solo) ls_info(*c->solo->ls, c->graphs != 0, out);
   return FIVO_OK;
 }
 

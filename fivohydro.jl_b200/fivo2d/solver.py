@@ -183,10 +183,12 @@ class GPUWork2D:
     def finalize_ic(self, tau0, bc=A.FIVO_BC_OUTFLOW):
         self._ck(self.lib.fivo_finalize_ic(self.h, tau0, bc), "fivo_finalize_ic")
 
-    def set_graphs(self, enable=True):
+    def set_graphs(self, mode=1):
         """fivo_ctx_set_graphs: run and advance through the lockstep launch sequences of
-        this one context, replayed as CUDA graphs on the context's stream (same bits)"""
-        self._ck(self.lib.fivo_ctx_set_graphs(self.h, int(bool(enable))), "fivo_ctx_set_graphs")
+        this one context, replayed as CUDA graphs on the context's stream (mode 1 or
+        True), launched kernel by kernel (2), or the context's own path (0 or False);
+        the same bits in every mode"""
+        self._ck(self.lib.fivo_ctx_set_graphs(self.h, int(mode)), "fivo_ctx_set_graphs")
 
     def lockstep_info(self):
         info = A.FivoLockstepInfo()

@@ -413,15 +413,17 @@ typedef struct fivo_lockstep_info {
 } fivo_lockstep_info;
 int  fivo_batch_lockstep_info(fivo_batch* b, fivo_lockstep_info* out);
 
-/* One context through the same launch sequences (enable != 0): fivo_run and
+/* One context through the same launch sequences (mode 1): fivo_run and
  * fivo_advance take each step as a batch of this one context, the step and the
  * post-step pass replayed as CUDA graphs on the context's stream (two graph
  * launches and two host reads per step instead of about 32 kernel launches),
- * with the default schedule and the global-load face pass. Results are the same
- * bits as without it. While fivo_profile is on the per-kernel path is taken.
- * fivo_ctx_lockstep_info reports its sequences. Replaces nothing in the
- * reference: its step is a sequence of Julia calls (main2D.jl:436-513). */
-int  fivo_ctx_set_graphs(fivo_ctx* c, int enable);
+ * with the default schedule and the global-load face pass; mode 2 launches the
+ * same sequences kernel by kernel; mode 0 (the default) is the context's own
+ * per-kernel path. Results are the same bits in every mode. While fivo_profile
+ * is on the per-kernel path is taken. fivo_ctx_lockstep_info reports the
+ * sequences. Replaces nothing in the reference: its step is a sequence of Julia
+ * calls (main2D.jl:436-513). */
+int  fivo_ctx_set_graphs(fivo_ctx* c, int mode);
 int  fivo_ctx_lockstep_info(fivo_ctx* c, fivo_lockstep_info* out);
 
 /* --- the learned starting guess of the primitive recovery (no counterpart in
