@@ -333,15 +333,15 @@ def test_lockstep_refuses_mixed_precision(gpu_lib):
     b.close()
 
 
-@pytest.mark.parametrize("integrator", [A.FIVO_SSPRK2, A.FIVO_SSPRK3])
-def test_single_context_graphs_bitwise(gpu_lib, integrator):
+@pytest.mark.parametrize("integrator,mode", [(A.FIVO_SSPRK2, 1), (A.FIVO_SSPRK3, 1), (A.FIVO_SSPRK3, 2)])
+def test_single_context_graphs_bitwise(gpu_lib, integrator, mode):
     """fivo_ctx_set_graphs: one context's run and advance through the lockstep
-    sequences replayed as CUDA graphs on the context's stream equal the
-    per-kernel path bit for bit (state, history, run results), and the graphs
-    count their kernels."""
+    sequences, replayed as CUDA graphs on the context's stream (mode 1) or launched
+    kernel by kernel (mode 2), equal the per-kernel path bit for bit (state,
+    history, run results), and the sequences count their kernels."""
     m, grids, states = _events([(40, 36)], seed0=1701)
     w1, w2 = GPUWork2D(m, grids[0], lib=gpu_lib), GPUWork2D(m, grids[0], lib=gpu_lib)
-    w2.set_graphs(True)
+    w2.set_graphs(mode)
     for w in (w1, w2):
         w.set_state(states[0])
         w.finalize_ic(0.6)
@@ -359,7 +359,7 @@ def test_single_context_graphs_bitwise(gpu_lib, integrator):
     for name in h1:
         assert bits_equal(h1[name], h2[name]), name
     info = w2.lockstep_info()
-    assert info["enabled"] and info["graphs"] and info["steps"] == 18 and info["kernels"] > 18 * 20
+    assert info["enabled"] and info["graphs"] == (mode == 1) and info["steps"] == 18 and info["kernels"] > 18 * 20
     assert not w1.lockstep_info()["enabled"]
     w1.close()
     w2.close()
