@@ -51,6 +51,8 @@ struct Geo {
 struct Ev {
   int active;               /* 0: every launch skips the event */
   int snap;                 /* the step starts with k_snapshot's copy */
+  int spec;                 /* the post-step pass follows in the same sequence: save the
+                               history planes it overwrites (for an undone step) */
   DevPrims w;
   DevHist h;
   DevFlags* fl;
@@ -62,6 +64,7 @@ struct Ev {
   float* fhx32;
   float* fhy32;
   double* x0save;           /* the warm starts before the step */
+  double* hsave;            /* ux_prev, uy_prev, nux_prev, nuy_prev before the step */
   DevState cp_dst, cp_src;  /* copy_state(U2 <- U) before the step */
   StageArgs st[3];          /* the step's stages */
   DevState pU[4];           /* recovery input: stage 0..2's Ub; 3 = the step's result */
@@ -110,8 +113,10 @@ __device__ __forceinline__ bool block_head(BlockHead* sh, const Geo* geo, const 
 
 /* ----------------------------------------------------------------- kernels */
 
-/* per event, before the step: k_snapshot (when due), save_warm (x0 -> x0save)
- * and copy_state (U2 <- U), fused over the cells (disjoint data) */
+/* per event, before the step: k_snapshot (when due), save_warm (x0 -> x0save),
+ * copy_state (U2 <- U) and, when the post-step pass follows in the same
+ * sequence, the history planes it overwrites (-> hsave), fused over the cells
+ * (disjoint data) */
 __global__ void __launch_bounds__(128) kb_pre_step(DevParams d0, const Geo* __restrict__ geo,
                                                    const Ev* __restrict__ tab, const unsigned short* __restrict__ eob) {
   __shared__ BlockHead sh;
@@ -119,7 +124,8 @@ __global__ void __launch_bounds__(128) kb_pre_step(DevParams d0, const Geo* __re
   __shared__ DevPrims sw;
   __shared__ DevHist shh;
   __shared__ double* sx0;
-  __shared__ int ssnap;
+  __shared__ double* shs;
+  __shared__ int ssnap, sspec;
   long long blk;
   if (!block_head(&sh, geo, tab, eob, SH_CELL, &blk)) return;
   const Ev& ev = tab[sh.e];
@@ -127,13 +133,17 @@ __global__ void __launch_bounds__(128) kb_pre_step(DevParams d0, const Geo* __re
   to_shared(&ssrc, &ev.cp_src);
   to_shared(&sw, &ev.w);
   to_shared(&shh, &ev.h);
-  if (threadIdx.x == 0) { sx0 = ev.x0save; ssnap = ev.snap; }
+  if (threadIdx.x == 0) { sx0 = ev.x0save; shs = ev.hsave; ssnap = ev.snap; sspec = ev.spec; }
   __syncthreads();
   const long long N = sh.g.Ntot;
   const long long i = blk * 128 + threadIdx.x;
   if (i >= N) return;
   if (ssnap) snapshot_cell(sw, shh, i);
   sx0[i] = shh.x0_yT[i]; sx0[N + i] = shh.x0_phi[i]; sx0[2 * N + i] = shh.x0_ux[i]; sx0[3 * N + i] = shh.x0_uy[i];
+  if (sspec) {
+    shs[i] = shh.ux_prev[i]; shs[N + i] = shh.uy_prev[i]; shs[2 * N + i] = shh.nux_prev[i];
+    shs[3 * N + i] = shh.nuy_prev[i];
+  }
   for (int a = 0; a < d0.nv; ++a) sdst.f[a][i] = ssrc.f[a][i];
 }
 

@@ -185,6 +185,7 @@ struct fivo_ctx {
   int precision = FIVO_PRECISION_FP64;
   float* fh32 = nullptr;                    /* x faces then y faces, nv FP32 planes each */
   double* x0save = nullptr;                 /* the warm starts before an optimistic step */
+  double* hsave = nullptr;                  /* history planes before a lockstep step with speculation */
   /* the face pass (x, y): -2 not chosen yet, -1 k_faces, k >= 0 k_faces_tile of FT_SHAPES[k];
    * the tensor maps of the chosen shape: the primitive planes, and the dissipative
    * planes of each of the four state buffers */
@@ -968,7 +969,7 @@ int fivo_ctx_destroy(fivo_ctx* c) {
   for (auto e : c->pool) cudaEventDestroy(e);
   cudaFree(c->slab); cudaFree(c->pbuf); cudaFree(c->hbuf); cudaFree(c->masks); cudaFree(c->fl);
   cudaFree(c->dU); cudaFree(c->stage); cudaFree(c->fh); cudaFree(c->queues); cudaFree(c->part);
-  cudaFree(c->fh32); cudaFree(c->x0save);
+  cudaFree(c->fh32); cudaFree(c->x0save); cudaFree(c->hsave);
   if (c->flh) cudaFreeHost(c->flh);
   if (c->own_st) cudaStreamDestroy(c->own_st);
   if (c->ev_sync) cudaEventDestroy(c->ev_sync);
@@ -1756,7 +1757,9 @@ int batch_for_each(fivo_batch* b, int* status, F fn) {
  * kernels on the same inputs in the same order as in fivo_run, and its results
  * are bitwise those of a separate run.
  * ---------------------------------------------------------------------- */
-enum { LS_STEP = 0, LS_POST = 1 };
+/* the launch sequences: the optimistic step; the post-step pass; both in one (the
+ * post-step pass speculating that the step is accepted, undone where it is not) */
+enum { LS_STEP = 0, LS_POST = 1, LS_FULL = 2 };
 
 struct Lockstep {
   int flags = 0;
@@ -1778,6 +1781,9 @@ struct Lockstep {
   bt::Ctl* ctl_d = nullptr;
   DevFlags* flg_d = nullptr;
   DevFlags* flg_h = nullptr;                 /* pinned */
+  DevFlags* flg2_d = nullptr;                /* the post-step flags of a LS_FULL sequence */
+  DevFlags* flg2_h = nullptr;                /* pinned */
+  bool speculate = true;                     /* LS_FULL where a post-step pass exists */
   std::vector<std::pair<int, int>> cands;    /* (block order, deferred-pass blocks per SM) */
   std::vector<double> cand_ms;
   int chosen = -1;
@@ -1798,9 +1804,10 @@ int ls_destroy(Lockstep* L) {
     cudaFree(L->geo_d[o]);
     for (int s = 0; s < bt::NSHAPE; ++s) cudaFree(L->eob_d[o][s]);
   }
-  cudaFree(L->tab_d); cudaFree(L->pre_d); cudaFree(L->ctl_d); cudaFree(L->flg_d);
+  cudaFree(L->tab_d); cudaFree(L->pre_d); cudaFree(L->ctl_d); cudaFree(L->flg_d); cudaFree(L->flg2_d);
   if (L->tab_h) cudaFreeHost(L->tab_h);
   if (L->flg_h) cudaFreeHost(L->flg_h);
+  if (L->flg2_h) cudaFreeHost(L->flg2_h);
   if (L->done) cudaEventDestroy(L->done);
   if (L->ta) cudaEventDestroy(L->ta);
   if (L->tb) cudaEventDestroy(L->tb);
@@ -1874,10 +1881,12 @@ int ls_create(fivo_batch* b, int flags, Lockstep** out) {
   if (cudaMalloc(&L->tab_d, n * sizeof(bt::Ev)) != cudaSuccess ||
       cudaMalloc(&L->pre_d, (n + 1) * sizeof(unsigned int)) != cudaSuccess ||
       cudaMalloc(&L->ctl_d, sizeof(bt::Ctl)) != cudaSuccess ||
-      cudaMalloc(&L->flg_d, n * sizeof(DevFlags)) != cudaSuccess)
+      cudaMalloc(&L->flg_d, n * sizeof(DevFlags)) != cudaSuccess ||
+      cudaMalloc(&L->flg2_d, n * sizeof(DevFlags)) != cudaSuccess)
     return cleanup(fail(FIVO_ERR_NOMEM, "fivo_batch_set_lockstep: device allocation failed"));
   if (cudaMallocHost(&L->tab_h, n * sizeof(bt::Ev)) != cudaSuccess ||
-      cudaMallocHost(&L->flg_h, n * sizeof(DevFlags)) != cudaSuccess)
+      cudaMallocHost(&L->flg_h, n * sizeof(DevFlags)) != cudaSuccess ||
+      cudaMallocHost(&L->flg2_h, n * sizeof(DevFlags)) != cudaSuccess)
     return cleanup(fail(FIVO_ERR_NOMEM, "fivo_batch_set_lockstep: pinned allocation failed"));
   std::memset(L->tab_h, 0, n * sizeof(bt::Ev));
   for (int order = 0; order < 2; ++order)
@@ -1898,6 +1907,7 @@ void ls_fill_common(fivo_ctx* c, bt::Ev& e) {
   e.fhx = c->fh; e.fhy = c->fh + (size_t)d.nv * d.Ntot;
   e.fhx32 = c->fh32; e.fhy32 = c->fh32 ? c->fh32 + (size_t)d.nv * d.Ntot : nullptr;
   e.x0save = c->x0save;
+  e.hsave = c->hsave;
 }
 
 /* the optimistic step of step2/step3 on the context's current roles */
@@ -1926,15 +1936,38 @@ void ls_fill_step(fivo_ctx* c, bt::Ev& e, int integrator, double tau, double D, 
   }
 }
 
+/* the post-step pass's arguments: update_prims + relax_project on state buffer u
+ * (scratch buffer t) at time tau after a step of length used */
+void ls_set_post(fivo_ctx* c, bt::Ev& e, int u, int t, double tau, double used, int do_relax, int do_project) {
+  e.pU[3] = c->S[u];
+  e.ptau[3] = tau;
+  e.rq = c->S[u]; e.ro = c->S[t];
+  e.rtau = tau; e.rD = used;
+  e.do_relax = do_relax; e.do_project = do_project;
+}
+
 /* update_prims + relax_project after an accepted step (state U at time tau) */
 void ls_fill_post(fivo_ctx* c, bt::Ev& e, double tau, double used, int do_relax, int do_project) {
   ls_fill_common(c, e);
   e.active = 1;
-  e.pU[3] = c->S[c->iU];
-  e.ptau[3] = tau;
-  e.rq = c->S[c->iU]; e.ro = c->S[c->iT];
-  e.rtau = tau; e.rD = used;
-  e.do_relax = do_relax; e.do_project = do_project;
+  ls_set_post(c, e, c->iU, c->iT, tau, used, do_relax, do_project);
+}
+
+/* the post-step pass in the step's own sequence, on the roles the step takes when it
+ * is accepted (step3: U <- U1, T <- U; step2: U <- T, T <- U) */
+void ls_fill_spec(fivo_ctx* c, bt::Ev& e, int integrator, double tau_post, double used, int do_relax,
+                  int do_project) {
+  e.spec = 1;
+  ls_set_post(c, e, integrator == FIVO_SSPRK3 ? c->iU1 : c->iT, c->iU, tau_post, used, do_relax, do_project);
+}
+
+/* the history planes the post-step pass overwrote, back from the copies taken
+ * before the step (an undone speculative step) */
+int restore_hist(fivo_ctx* c) {
+  const size_t N = (size_t)c->dp.Ntot;
+  CK(cudaMemcpyAsync(c->h.ux_prev, c->hsave, 2 * N * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaMemcpyAsync(c->h.nux_prev, c->hsave + 2 * N, 2 * N * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+  return FIVO_OK;
 }
 
 #define LS_GRID(s) L.nblocks[s] ? L.nblocks[s] : 1
@@ -1989,8 +2022,14 @@ int ls_launch_t(fivo_batch* b, int seq, int integrator, int bc, int cand, int pr
     LS_K();
     return FIVO_OK;
   };
+  auto gather = [&](DevFlags* dev, DevFlags* host) -> int {
+    bt::kb_gather_flags<<<nblk((long long)n * (sizeof(DevFlags) / 8), 256), 256, 0, st>>>(L.tab_d, n, dev);
+    LS_K();
+    CK(cudaMemcpyAsync(host, dev, n * sizeof(DevFlags), cudaMemcpyDeviceToHost, st));
+    return FIVO_OK;
+  };
   int rc;
-  if (seq == LS_STEP) {
+  if (seq == LS_STEP || seq == LS_FULL) {
     bt::kb_pre_step<<<LS_GRID(bt::SH_CELL), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_CELL]);
     LS_K();
     const int nst = integrator == FIVO_SSPRK3 ? 3 : 2;
@@ -2027,7 +2066,10 @@ int ls_launch_t(fivo_batch* b, int seq, int integrator, int bc, int cand, int pr
       bt::kb_bc<<<LS_GRID(bt::SH_FRAME), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FRAME], k + 1, bc);
       LS_K();
     }
-  } else {
+    /* the step's flags, before the post-step pass resets them */
+    if (seq == LS_FULL && (rc = gather(L.flg_d, L.flg_h))) return rc;
+  }
+  if (seq == LS_POST || seq == LS_FULL) {
     if (any_sector) {
       bt::kb_reset<<<gr, 256, 0, st>>>(L.tab_d, n, 1 | 64);
       LS_K();
@@ -2047,9 +2089,9 @@ int ls_launch_t(fivo_batch* b, int seq, int integrator, int bc, int cand, int pr
       LS_K();
     }
   }
-  bt::kb_gather_flags<<<nblk((long long)n * (sizeof(DevFlags) / 8), 256), 256, 0, st>>>(L.tab_d, n, L.flg_d);
-  LS_K();
-  CK(cudaMemcpyAsync(L.flg_h, L.flg_d, n * sizeof(DevFlags), cudaMemcpyDeviceToHost, st));
+  if (seq == LS_FULL) rc = gather(L.flg2_d, L.flg2_h);
+  else rc = gather(L.flg_d, L.flg_h);
+  if (rc) return rc;
   L.last_nk = nk;
   return FIVO_OK;
 }
@@ -2153,6 +2195,9 @@ int ls_loop(fivo_batch* b, std::vector<double>& tau, double taufinal, double cfl
   const bool post = any_sector || d.hasShear;
   const int prec = b->ev[0]->precision;
   const fivo_ctx* c0 = b->ev[0];
+  /* the post-step pass speculates in the step's sequence (one host read per step) */
+  const bool spec = L.speculate && post;
+  const int do_relax = any_sector ? 1 : 0, do_project = any_sector ? d.hasShear : 1;
   for (fivo_ctx* c : b->ev) {
     if (c->learned != c0->learned || (c->learned && (c->guess_mode != c0->guess_mode || c->gnet.img != c0->gnet.img)))
       return fail(FIVO_ERR_CONFIG, "lockstep batch: every event must use the same recovery (one learned guess, one mode, or none)");
@@ -2163,12 +2208,18 @@ int ls_loop(fivo_batch* b, std::vector<double>& tau, double taufinal, double cfl
         return fail(FIVO_ERR_NOMEM, "device allocation failed");
       }
     }
+    if (spec && !c->hsave) {
+      if (cudaMalloc(&c->hsave, 4 * (size_t)c->dp.Ntot * sizeof(double)) != cudaSuccess) {
+        c->hsave = nullptr;
+        return fail(FIVO_ERR_NOMEM, "device allocation failed");
+      }
+    }
     /* the sequences' stream reads what the contexts' streams wrote (one host thread
      * waits here, so it spins rather than sleeps as the batch workers do) */
     CK(cudaStreamSynchronize(c->st));
     prof_flush(c);
   }
-  std::vector<char> done(n, 0), stepped(n, 0);
+  std::vector<char> done(n, 0), stepped(n, 0), posted(n, 0);
   std::vector<double> D(n, 0.0), used(n, 0.0), msr(n, 0.0);
   std::vector<int64_t> nsteps(n, 0), npf(n, 0), nvac(n, 0);
   for (int k = 0; k < n; ++k) out[k].ok = 1;
@@ -2179,6 +2230,7 @@ int ls_loop(fivo_batch* b, std::vector<double>& tau, double taufinal, double cfl
       bt::Ev& e = L.tab_h[k];
       e.active = 0;
       stepped[k] = 0;
+      posted[k] = 0;
       if (done[k] || st[k] != FIVO_OK) continue;
       if (!(tau[k] < taufinal && nsteps[k] < max_steps)) { done[k] = 1; continue; }
       double Dk;
@@ -2189,6 +2241,7 @@ int ls_loop(fivo_batch* b, std::vector<double>& tau, double taufinal, double cfl
       if (snap) c->hist_valid = true;
       c->cnt.nmood = 0; c->cnt.nhalve = 0;
       ls_fill_step(c, e, integrator, tau[k], Dk, snap);
+      if (spec) ls_fill_spec(c, e, integrator, tau[k] + Dk, Dk, do_relax, do_project);
       D[k] = Dk;
       ++nact;
     }
@@ -2198,7 +2251,7 @@ int ls_loop(fivo_batch* b, std::vector<double>& tau, double taufinal, double cfl
     const bool tuning = cand < 0;
     if (tuning) cand = L.tuned_steps % (int)L.cands.size();
     float ms = 0.f;
-    int rc = ls_exec(b, LS_STEP, integrator, bc, cand, prec, any_sector, relax_on, &ms);
+    int rc = ls_exec(b, spec ? LS_FULL : LS_STEP, integrator, bc, cand, prec, any_sector, relax_on, &ms);
     if (rc) return rc;
     L.ms_step += ms;
     L.steps += 1;
@@ -2220,6 +2273,7 @@ int ls_loop(fivo_batch* b, std::vector<double>& tau, double taufinal, double cfl
         if (integrator != FIVO_SSPRK3) std::swap(c->iU, c->iT);
         used[k] = D[k];
         stepped[k] = 1;
+        posted[k] = spec ? 1 : 0;
       } else {
         if (integrator == FIVO_SSPRK3) std::swap(c->iU, c->iU2);   /* the state before the step */
         redo.push_back(k);
@@ -2231,6 +2285,10 @@ int ls_loop(fivo_batch* b, std::vector<double>& tau, double taufinal, double cfl
       ls_parallel(b, redo, [&](int k) {
         fivo_ctx* c = b->ev[k];
         int ok = 0, r = restore_warm(c);
+        /* a speculative post-step pass also wrote the history planes and, for step2,
+         * the relaxed rows into U itself (its scratch role); U2 holds U's copy */
+        if (!r && spec) r = restore_hist(c);
+        if (!r && spec && integrator != FIVO_SSPRK3) r = copy_state(c, c->iU, c->iU2);
         if (!r) {
           r = integrator == FIVO_SSPRK3 ? step3_rest(c, tau[k], D[k], 12, bc, &used[k], &ok)
                                         : step2_rest(c, tau[k], D[k], 12, 2, bc, &used[k], &ok);
@@ -2249,8 +2307,8 @@ int ls_loop(fivo_batch* b, std::vector<double>& tau, double taufinal, double cfl
       tau[k] += used[k];
       nsteps[k] += 1;
       c->nsteps_run += 1;
-      if (post) {
-        ls_fill_post(c, L.tab_h[k], tau[k], used[k], any_sector ? 1 : 0, any_sector ? d.hasShear : 1);
+      if (post && !posted[k]) {
+        ls_fill_post(c, L.tab_h[k], tau[k], used[k], do_relax, do_project);
         ++npost;
       }
     }
@@ -2265,7 +2323,7 @@ int ls_loop(fivo_batch* b, std::vector<double>& tau, double taufinal, double cfl
       if (post) {
         if (relax_on)   /* relax_project: U's dissipative planes are now the scratch state's */
           for (int a = 4; a < d.nv; ++a) std::swap(c->S[c->iU].f[a], c->S[c->iT].f[a]);
-        *c->flh = L.flg_h[k];
+        *c->flh = posted[k] ? L.flg2_h[k] : L.flg_h[k];
         if (any_sector && (rc = parse_flags(c, false))) { st[k] = rc; msg[k] = g_err; continue; }
         if (d.hasShear) {
           uint64_t bits = c->flh->shear_max_bits;
