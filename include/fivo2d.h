@@ -381,10 +381,11 @@ int  fivo_batch_advance(fivo_batch* b, const double* tau, double taufinal, doubl
  * take every event's step at the same time, each kernel of the step launched
  * once over the blocks of all events (the deferred recoveries and admissibility
  * inversions as persistent kernels over the union of the events' queues), with
- * ONE host read for the whole batch per step and one per post-step pass
- * (update_primitives_2d! + relax_dissipative_2d!, main2D.jl:486-502). An event
- * whose optimistic step has an inadmissible cell is undone and stepped alone by
- * the usual stage-by-stage procedure with MOOD and halving; events that have
+ * ONE host read for the whole batch per step: the post-step pass
+ * (update_primitives_2d! + relax_dissipative_2d!, main2D.jl:486-502) follows in
+ * the same sequence, speculating that the step is accepted. An event whose
+ * optimistic step has an inadmissible cell is undone (speculation included) and
+ * stepped alone by the usual stage-by-stage procedure with MOOD and halving; events that have
  * reached taufinal or max_steps sit out the launches. Results per event are
  * bitwise those of separate fivo_run calls. flags: FIVO_LOCKSTEP_GRAPHS
  * replays each launch sequence as a captured CUDA graph; FIVO_LOCKSTEP_TUNE
@@ -415,8 +416,8 @@ int  fivo_batch_lockstep_info(fivo_batch* b, fivo_lockstep_info* out);
 
 /* One context through the same launch sequences (mode 1): fivo_run and
  * fivo_advance take each step as a batch of this one context, the step and the
- * post-step pass replayed as CUDA graphs on the context's stream (two graph
- * launches and two host reads per step instead of about 32 kernel launches),
+ * post-step pass replayed as one CUDA graph on the context's stream (one graph
+ * launch and one host read per step instead of about 32 kernel launches),
  * with the default schedule and the global-load face pass; mode 2 launches the
  * same sequences kernel by kernel; mode 0 (the default) is the context's own
  * per-kernel path. Results are the same bits in every mode. While fivo_profile
