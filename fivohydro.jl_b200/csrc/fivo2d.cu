@@ -2163,12 +2163,13 @@ int ls_exec(fivo_batch* b, int seq, int integrator, int bc, int cand, int prec, 
   return FIVO_OK;
 }
 
-/* fn(k) for the listed events on the batch's worker threads */
+/* fn(k) for the listed events on the batch's worker threads (a thread that cannot
+ * select the device still runs fn: its CUDA calls then fail into the event's status) */
 template <class F>
 void ls_parallel(fivo_batch* b, const std::vector<int>& ks, F fn) {
   std::atomic<int> next{0};
   auto worker = [&]() {
-    if (cudaSetDevice(b->device) != cudaSuccess) return;
+    cudaSetDevice(b->device);
     for (;;) {
       const int j = next.fetch_add(1);
       if (j >= (int)ks.size()) break;
