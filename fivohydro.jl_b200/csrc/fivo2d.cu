@@ -1742,7 +1742,7 @@ int batch_for_each(fivo_batch* b, int* status, F fn) {
 /* ------------------------------------------------------------------------
  * Lockstep batches (fivo_batch_set_lockstep): the events' steps taken together,
  * each kernel of a step launched once over every event's blocks (batch.cuh).
- * A step is two launch sequences with one host read after each:
+ * The launch sequences:
  *   STEP  the optimistic SSPRK step of every active event: k_snapshot (when
  *         due), the warm-start save and copy_state, then per stage the ghost
  *         fill, flag reset, fast recovery, deferred recoveries, faces, update,
@@ -1750,12 +1750,16 @@ int batch_for_each(fivo_batch* b, int* status, F fn) {
  *         of all events gathered and read back at once.
  *   POST  update_primitives_2d! and relax_dissipative_2d! (+ project_shear!) on
  *         the events whose step was accepted, then the flags again.
- * Between them the host settles, per event, what advance_loop settles after
+ *   FULL  STEP then POST in one sequence (one host read per step), POST on the
+ *         roles an accepted step takes; the step's first kernel also copies the
+ *         history planes POST overwrites.
+ * After the read the host settles, per event, what advance_loop settles after
  * step2/step3: an event with an inadmissible cell is undone (roles, warm
- * starts) and stepped by step2_rest/step3_rest on its own stream, exactly as
- * a separate run would after its optimistic pass. So every event sees the same
- * kernels on the same inputs in the same order as in fivo_run, and its results
- * are bitwise those of a separate run.
+ * starts, and after FULL the history planes and, for step2, the state from its
+ * copy) and stepped by step2_rest/step3_rest on its own stream, exactly as a
+ * separate run would after its optimistic pass, and then gets its own POST. So
+ * every event sees the same kernels on the same inputs in the same order as in
+ * fivo_run, and its results are bitwise those of a separate run.
  * ---------------------------------------------------------------------- */
 /* the launch sequences: the optimistic step; the post-step pass; both in one (the
  * post-step pass speculating that the step is accepted, undone where it is not) */
