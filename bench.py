@@ -594,14 +594,14 @@ LOCKSTEP_FORMS = ("plain_fp64_lockstep", "fp32_lockstep", "learned_fp32_lockstep
                   "plain_fp64_lockstep_nograph")
 
 
-def batch_forms(lib, m, nevents, steps, single_value, warmup=15):
+def batch_forms(lib, m, nevents, steps, single_value, warmup=18):
     """The metric's comparison on one GPU: the same nevents seeded events (the
     event-by-event sizes, device IC, seed 1000 + k) advanced in plain FP64, in FP32
     (face pass and relaxation sources), and with the learned guess plus FP32, the
     guess used for every cell or for the cells the warm start defers, each with one
     stream per event; then plain FP64, FP32 and the two learned+FP32 forms in
     lockstep (one launch per kernel over all events, replayed from CUDA graphs, the
-    schedule tuned on the first 12 warm-up steps), plain lockstep without graphs,
+    schedule tuned on the first 16 warm-up steps), plain lockstep without graphs,
     and the plain path unbatched (the events one at a time, each alone on the GPU). Zone-updates/s of each (host
     wall clock around the synchronous batch call), each form's L2(T), L2(pibar) and
     L2(pi) against the plain run, and for the lockstep forms whether every event's
@@ -753,7 +753,7 @@ def run_batch(args):
             raise RuntimeError("a batch event failed a step")
         taus = [x["tau"] for x in r]
 
-    adv(max(args.warmup, 15) if args.lockstep else args.warmup)   # lockstep: the 12 tuning steps are warm-up
+    adv(max(args.warmup, 18) if args.lockstep else args.warmup)   # lockstep: the 16 tuning steps are warm-up
     if guess is not None:
         from fivo2d.guess import newton_stats
         for e in b.events:

@@ -34,8 +34,9 @@ namespace fv {
 namespace bt {
 
 /* the units one 128-thread block covers, per event: cells of the whole grid,
- * ghost cells, x-face lane pairs, y-face lane pairs, interior cells */
-enum { SH_CELL = 0, SH_FRAME = 1, SH_FACEX = 2, SH_FACEY = 3, SH_INT = 4, NSHAPE = 5 };
+ * ghost cells, x-face lane pairs, y-face lane pairs, interior cells, and both
+ * face directions in one launch (the event's x-face blocks, then its y-face blocks) */
+enum { SH_CELL = 0, SH_FRAME = 1, SH_FACEX = 2, SH_FACEY = 3, SH_INT = 4, SH_FACEXY = 5, NSHAPE = 6 };
 
 /* an event's grid (the DevParams fields that differ between events) and the
  * first block of the event in each shape's launch */
@@ -44,7 +45,7 @@ struct Geo {
   long long Ntot;
   double dx, dy, xmin, ymin;
   int b0[NSHAPE];
-  int pad;
+  int nbx;                  /* x-face blocks of the event (the first ones of its SH_FACEXY range) */
 };
 
 /* one event's arguments for a step and for the pass after it (host-built) */
@@ -396,6 +397,45 @@ __global__ void __launch_bounds__(128, FV_FACE_MINB) kb_faces(DevParams d0, cons
   const long long t = blk * 128 + threadIdx.x;
   if (F32) f32::faces32_body<EOS, XDIR>(d, sU, sw, stau, nullptr, (float*)sF, sfl, t);
   else faces_body<EOS, XDIR>(d, sU, sw, stau, nullptr, (double*)sF, sfl, t);
+}
+
+/* the face pass of stage k in both directions in one launch: an event's x-face
+ * blocks and then its y-face blocks, so both read the event's planes at about the
+ * same time (the second from L2 where the batch's planes do not fit in it) */
+template <int EOS, bool F32>
+__global__ void __launch_bounds__(128, FV_FACE_MINB) kb_faces_xy(DevParams d0, const Geo* __restrict__ geo,
+                                                                 const Ev* __restrict__ tab,
+                                                                 const unsigned short* __restrict__ eob, int k) {
+  __shared__ BlockHead sh;
+  __shared__ DevState sU;
+  __shared__ DevPrims sw;
+  __shared__ DevFlags* sfl;
+  __shared__ void* sFx;
+  __shared__ void* sFy;
+  __shared__ double stau;
+  long long blk;
+  if (!block_head(&sh, geo, tab, eob, SH_FACEXY, &blk)) return;
+  const Ev& ev = tab[sh.e];
+  to_shared(&sU, &ev.st[k].Ub);
+  to_shared(&sw, &ev.w);
+  if (threadIdx.x == 0) {
+    sfl = ev.fl;
+    stau = ev.st[k].tau;
+    sFx = F32 ? (void*)ev.fhx32 : (void*)ev.fhx;
+    sFy = F32 ? (void*)ev.fhy32 : (void*)ev.fhy;
+  }
+  __syncthreads();
+  DevParams d = d0;
+  with_geo(d, sh.g);
+  const bool xdir = blk < sh.g.nbx;   /* uniform over the block */
+  const long long t = (xdir ? blk : blk - sh.g.nbx) * 128 + threadIdx.x;
+  if (F32) {
+    if (xdir) f32::faces32_body<EOS, true>(d, sU, sw, stau, nullptr, (float*)sFx, sfl, t);
+    else f32::faces32_body<EOS, false>(d, sU, sw, stau, nullptr, (float*)sFy, sfl, t);
+  } else {
+    if (xdir) faces_body<EOS, true>(d, sU, sw, stau, nullptr, (double*)sFx, sfl, t);
+    else faces_body<EOS, false>(d, sU, sw, stau, nullptr, (double*)sFy, sfl, t);
+  }
 }
 
 /* k_update of stage k */

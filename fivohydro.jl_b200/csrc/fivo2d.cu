@@ -1788,7 +1788,8 @@ struct Lockstep {
   DevFlags* flg2_d = nullptr;                /* the post-step flags of a LS_FULL sequence */
   DevFlags* flg2_h = nullptr;                /* pinned */
   bool speculate = true;                     /* LS_FULL where a post-step pass exists */
-  std::vector<std::pair<int, int>> cands;    /* (block order, deferred-pass blocks per SM) */
+  struct Cand { int order, slow, fused; };   /* block order, deferred-pass blocks per SM, face pass in one launch */
+  std::vector<Cand> cands;
   std::vector<double> cand_ms;
   int chosen = -1;
   int tuned_steps = 0;
@@ -1828,6 +1829,7 @@ void ls_units(const DevParams& d, long long u[bt::NSHAPE]) {
   u[bt::SH_FRAME] = d.Ntot - (long long)d.Nx * d.Ny;
   u[bt::SH_FACEX] = 2LL * (d.Nxtot - 1) * d.Nytot;
   u[bt::SH_FACEY] = 2LL * d.Nxtot * (d.Nytot - 1);
+  u[bt::SH_FACEXY] = u[bt::SH_FACEX] + u[bt::SH_FACEY];   /* (blocks: those of x plus those of y) */
   u[bt::SH_INT] = (long long)d.Nx * d.Ny;
 }
 
@@ -1853,7 +1855,7 @@ int ls_create(fivo_batch* b, int flags, Lockstep** out) {
                        [&](int a, int c) { return b->ev[a]->dp.Ntot > b->ev[c]->dp.Ntot; });
     std::vector<bt::Geo> geo(n);
     std::vector<unsigned short> eob[bt::NSHAPE];
-    long long cnt[bt::NSHAPE] = {0, 0, 0, 0, 0};
+    long long cnt[bt::NSHAPE] = {0, 0, 0, 0, 0, 0};
     for (int e : perm) {
       const DevParams& d = b->ev[e]->dp;
       bt::Geo& g = geo[e];
@@ -1862,8 +1864,9 @@ int ls_create(fivo_batch* b, int flags, Lockstep** out) {
       g.dx = d.dx; g.dy = d.dy; g.xmin = d.xmin; g.ymin = d.ymin;
       long long u[bt::NSHAPE];
       ls_units(d, u);
+      g.nbx = (int)((u[bt::SH_FACEX] + 127) / 128);
       for (int s = 0; s < bt::NSHAPE; ++s) {
-        const long long nb = (u[s] + 127) / 128;
+        const long long nb = s == bt::SH_FACEXY ? g.nbx + (u[bt::SH_FACEY] + 127) / 128 : (u[s] + 127) / 128;
         g.b0[s] = (int)cnt[s];
         eob[s].insert(eob[s].end(), (size_t)nb, (unsigned short)e);
         cnt[s] += nb;
@@ -1894,10 +1897,12 @@ int ls_create(fivo_batch* b, int flags, Lockstep** out) {
     return cleanup(fail(FIVO_ERR_NOMEM, "fivo_batch_set_lockstep: pinned allocation failed"));
   std::memset(L->tab_h, 0, n * sizeof(bt::Ev));
   for (int order = 0; order < 2; ++order)
-    for (int slow : {1, 2, 4}) L->cands.push_back({order, slow});
+    for (int slow : {2, 4})
+      for (int fused = 0; fused < 2; ++fused) L->cands.push_back({order, slow, fused});
   L->cand_ms.assign(L->cands.size(), 0.0);
-  /* untuned: batch order, 2 blocks per SM (the single-event deferred pass's grid) */
-  L->chosen = (flags & FIVO_LOCKSTEP_TUNE) ? -1 : 1;
+  /* untuned: batch order, 2 blocks per SM (the single-event deferred pass's grid), the
+   * face directions in two launches (as the single-event path) */
+  L->chosen = (flags & FIVO_LOCKSTEP_TUNE) ? -1 : 0;
   *out = L;
   return FIVO_OK;
 }
@@ -1988,8 +1993,9 @@ template <int EOS, bool NCH>
 int ls_launch_t(fivo_batch* b, int seq, int integrator, int bc, int cand, int prec, bool any_sector, bool relax_on) {
   Lockstep& L = *b->ls;
   const int n = L.nev;
-  const int order = L.cands[cand].first;
-  const unsigned slow_blocks = (unsigned)(L.cands[cand].second * L.nsm);
+  const int order = L.cands[cand].order;
+  const unsigned slow_blocks = (unsigned)(L.cands[cand].slow * L.nsm);
+  const bool fused = L.cands[cand].fused != 0;
   const bt::Geo* geo = L.geo_d[order];
   unsigned short* const* eob = L.eob_d[order];
   const DevParams& d0 = L.d0;
@@ -2046,19 +2052,28 @@ int ls_launch_t(fivo_batch* b, int seq, int integrator, int bc, int cand, int pr
       bt::kb_reset<<<gr, 256, 0, st>>>(L.tab_d, n, k == 0 ? (1 | 2 | 64) : (1 | 2));
       LS_K();
       if ((rc = prim_pass(k))) return rc;
+      if (fused) {
+        if (f32) bt::kb_faces_xy<EOS, true><<<LS_GRID(bt::SH_FACEXY), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FACEXY], k);
+        else bt::kb_faces_xy<EOS, false><<<LS_GRID(bt::SH_FACEXY), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FACEXY], k);
+        LS_K();
+      }
       if (f32) {
-        bt::kb_faces<EOS, true, true><<<LS_GRID(bt::SH_FACEX), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FACEX], k);
-        LS_K();
-        bt::kb_faces<EOS, false, true><<<LS_GRID(bt::SH_FACEY), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FACEY], k);
-        LS_K();
+        if (!fused) {
+          bt::kb_faces<EOS, true, true><<<LS_GRID(bt::SH_FACEX), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FACEX], k);
+          LS_K();
+          bt::kb_faces<EOS, false, true><<<LS_GRID(bt::SH_FACEY), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FACEY], k);
+          LS_K();
+        }
         if (full) bt::kb_update<EOS, NCH, float, true><<<LS_GRID(bt::SH_INT), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_INT], k);
         else bt::kb_update<EOS, NCH, float, false><<<LS_GRID(bt::SH_INT), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_INT], k);
         LS_K();
       } else {
-        bt::kb_faces<EOS, true, false><<<LS_GRID(bt::SH_FACEX), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FACEX], k);
-        LS_K();
-        bt::kb_faces<EOS, false, false><<<LS_GRID(bt::SH_FACEY), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FACEY], k);
-        LS_K();
+        if (!fused) {
+          bt::kb_faces<EOS, true, false><<<LS_GRID(bt::SH_FACEX), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FACEX], k);
+          LS_K();
+          bt::kb_faces<EOS, false, false><<<LS_GRID(bt::SH_FACEY), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_FACEY], k);
+          LS_K();
+        }
         if (full) bt::kb_update<EOS, NCH, double, true><<<LS_GRID(bt::SH_INT), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_INT], k);
         else bt::kb_update<EOS, NCH, double, false><<<LS_GRID(bt::SH_INT), 128, 0, st>>>(d0, geo, L.tab_d, eob[bt::SH_INT], k);
         LS_K();
@@ -2318,7 +2333,7 @@ int ls_loop(fivo_batch* b, std::vector<double>& tau, double taufinal, double cfl
       }
     }
     if (npost) {
-      if ((rc = ls_exec(b, LS_POST, integrator, bc, L.chosen < 0 ? 1 : L.chosen, prec, any_sector, relax_on, &ms)))
+      if ((rc = ls_exec(b, LS_POST, integrator, bc, L.chosen < 0 ? 0 : L.chosen, prec, any_sector, relax_on, &ms)))
         return rc;
       L.ms_post += ms;
     }
@@ -2365,8 +2380,9 @@ void ls_info(const Lockstep& L, bool enabled, fivo_lockstep_info* out) {
   out->ncand = std::min<int>((int)L.cands.size(), FIVO_LOCKSTEP_MAXCAND);
   out->chosen = L.chosen;
   for (int i = 0; i < out->ncand; ++i) {
-    out->cand_order[i] = L.cands[i].first;
-    out->cand_slow[i] = L.cands[i].second;
+    out->cand_order[i] = L.cands[i].order;
+    out->cand_slow[i] = L.cands[i].slow;
+    out->cand_fused[i] = L.cands[i].fused;
     out->cand_ms[i] = L.cand_ms[i];
   }
   out->steps = L.steps;

@@ -89,6 +89,7 @@ class FivoLockstepInfo(C.Structure):
     _fields_ = [
         ("enabled", C.c_int32), ("flags", C.c_int32), ("ncand", C.c_int32), ("chosen", C.c_int32),
         ("cand_order", C.c_int32 * FIVO_LOCKSTEP_MAXCAND), ("cand_slow", C.c_int32 * FIVO_LOCKSTEP_MAXCAND),
+        ("cand_fused", C.c_int32 * FIVO_LOCKSTEP_MAXCAND),
         ("cand_ms", C.c_double * FIVO_LOCKSTEP_MAXCAND), ("steps", C.c_int64), ("fallbacks", C.c_int64),
         ("ms_step", C.c_double), ("ms_post", C.c_double), ("kernels", C.c_int64),
     ]
@@ -98,7 +99,8 @@ class FivoLockstepInfo(C.Structure):
         return {"enabled": bool(self.enabled), "graphs": bool(self.flags & FIVO_LOCKSTEP_GRAPHS),
                 "tune": bool(self.flags & FIVO_LOCKSTEP_TUNE), "chosen": self.chosen,
                 "candidates": [{"order": ("batch", "largest_first")[self.cand_order[i]],
-                                "slow_blocks_per_sm": self.cand_slow[i], "best_step_ms": self.cand_ms[i]}
+                                "slow_blocks_per_sm": self.cand_slow[i], "faces_one_launch": bool(self.cand_fused[i]),
+                                "best_step_ms": self.cand_ms[i]}
                                for i in range(n)],
                 "steps": self.steps, "fallbacks": self.fallbacks, "ms_step": self.ms_step,
                 "ms_post": self.ms_post, "kernels": self.kernels}

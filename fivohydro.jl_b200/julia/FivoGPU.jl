@@ -51,7 +51,8 @@ end
 # fivo_lockstep_info: the lockstep batch's candidate schedules and the one kept
 struct FivoLockstepInfo
     enabled::Int32; flags::Int32; ncand::Int32; chosen::Int32
-    cand_order::NTuple{16,Int32}; cand_slow::NTuple{16,Int32}; cand_ms::NTuple{16,Float64}
+    cand_order::NTuple{16,Int32}; cand_slow::NTuple{16,Int32}; cand_fused::NTuple{16,Int32}
+    cand_ms::NTuple{16,Float64}
     steps::Int64; fallbacks::Int64; ms_step::Float64; ms_post::Float64; kernels::Int64
 end
 

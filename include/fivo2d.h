@@ -390,8 +390,8 @@ int  fivo_batch_advance(fivo_batch* b, const double* tau, double taufinal, doubl
  * bitwise those of separate fivo_run calls. flags: FIVO_LOCKSTEP_GRAPHS
  * replays each launch sequence as a captured CUDA graph; FIVO_LOCKSTEP_TUNE
  * times the candidate schedules (block order of the events, blocks of the
- * persistent deferred pass) on the first steps of the next run and keeps the
- * fastest. Every event must use the same recovery (the plain one, or one
+ * persistent deferred pass, the face pass's two directions in one launch or two)
+ * on the first 16 steps of the next run and keeps the fastest. Every event must use the same recovery (the plain one, or one
  * learned guess in one mode: its batched kernels take the network's tiles over
  * the events' cells or over the union of their deferred cells) and the same
  * precision. Replaces the reference's per-event loop over run_sim_2d!. */
@@ -406,6 +406,7 @@ typedef struct fivo_lockstep_info {
   int32_t chosen;           /* index of the kept one, -1 before tuning */
   int32_t cand_order[FIVO_LOCKSTEP_MAXCAND];    /* 0: events in batch order, 1: largest grid first */
   int32_t cand_slow[FIVO_LOCKSTEP_MAXCAND];     /* persistent deferred-pass blocks per SM */
+  int32_t cand_fused[FIVO_LOCKSTEP_MAXCAND];    /* 1: both face directions in one launch */
   double  cand_ms[FIVO_LOCKSTEP_MAXCAND];       /* best step time measured (device, ms) */
   int64_t steps;            /* lockstep steps taken (batch-wide) */
   int64_t fallbacks;        /* event steps redone stage by stage */

@@ -159,8 +159,10 @@ def test_lockstep_batch_equals_single_runs(gpu_lib, integrator, graphs, tune):
     info = b.lockstep_info()
     assert info["enabled"] and info["graphs"] == graphs and info["steps"] >= 12
     assert len({r["nsteps"] for r in rb}) > 1      # events leave the lockstep at different steps
-    if tune:
-        assert info["chosen"] >= 0 and all(c["best_step_ms"] > 0 for c in info["candidates"])
+    if tune:   # every candidate timed; one kept once the 16 tuning steps are done
+        assert all(c["best_step_ms"] > 0 for c in info["candidates"])
+        assert info["chosen"] >= 0 or info["steps"] < 16
+        assert any(c["faces_one_launch"] for c in info["candidates"])
     singles = _single_runs(gpu_lib, m, grids, states, 0.6, 1.2, 0.2, 0.05, integrator, 60)
     _assert_batch_equals(b, rb, singles)
     o = O.OracleSolver(m, grids[4])
