@@ -54,6 +54,22 @@ def test_struct_layout_matches_c(tmp_path):
     assert int(out[4]) == A.FivoParams.terms.offset
 
 
+def test_lockstep_info_layout_matches_c(tmp_path):
+    """fivo_lockstep_info, field for field (the batch's and a context's sequences)"""
+    fields = ("enabled", "ncand", "chosen", "cand_order", "cand_slow", "cand_fused", "cand_ms", "steps",
+              "fallbacks", "ms_step", "ms_post", "kernels")
+    src = tmp_path / "li.c"
+    body = " ".join(f'printf("%zu ", offsetof(fivo_lockstep_info, {f}));' for f in fields)
+    src.write_text(f'#include "{HEADER}"\n#include <stdio.h>\n#include <stddef.h>\n'
+                   f'int main(void){{printf("%zu ", sizeof(fivo_lockstep_info)); {body} return 0;}}\n')
+    exe = tmp_path / "li"
+    subprocess.run(["gcc", str(src), "-o", str(exe)], check=True)
+    out = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert out[0] == C.sizeof(A.FivoLockstepInfo)
+    for f, off in zip(fields, out[1:]):
+        assert off == getattr(A.FivoLockstepInfo, f).offset, f
+
+
 def test_params_default_matches_build_model_2d(lib):
     """fivo_params_default == build_model_2d() defaults (main2D.jl:85-123)."""
     p = A.FivoParams()
