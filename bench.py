@@ -555,6 +555,7 @@ def run_gpu(args):
                                       "plain warm start; trained on seeds " + str(list(GUESS_SEEDS)))
     if world == 1 and not args.no_forms and guess is None and not args.fp32_faces and args.batch_events > 0:
         line["metric_comparison"] = batch_forms(lib, m, args.batch_events, args.batch_steps, value)
+        line["metric_summary"] = metric_summary(line["metric_comparison"])
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.cpu_steps)
     return line
@@ -579,6 +580,30 @@ def _batch_fields(b, m):
         out["pibar"].append(Ur[..., iE].ravel() / wpl)
         out["pi"].append(Ur[..., iP:iP + 3].reshape(-1, 3))
     return {k: np.concatenate(v) for k, v in out.items()}
+
+
+def metric_summary(mc):
+    """The metric's own ratio read off the comparison: batched learned+FP32 (the learned
+    guess on the deferred cells, FP32, lockstep) against plain FP64, both unbatched (the
+    events one at a time) and batched (one stream per event), with its accuracy, and the
+    best form beside it"""
+    def val(form):
+        row = mc.get(form)
+        return row.get("value") if isinstance(row, dict) else None
+
+    head = "learned_deferred_fp32_lockstep"
+    out = {"form": head, "value": val(head), "plain_unbatched": val("plain_fp64_one_event_at_a_time"),
+           "plain_batched": val("plain_fp64"), "best_form": mc.get("best_form"),
+           "best_value": val(mc.get("best_form")) if mc.get("best_form") else None}
+    if out["value"] and out["plain_unbatched"]:
+        out["vs_plain_unbatched"] = out["value"] / out["plain_unbatched"]
+    if out["value"] and out["plain_batched"]:
+        out["vs_plain_batched"] = out["value"] / out["plain_batched"]
+    row = mc.get(head) if isinstance(mc.get(head), dict) else {}
+    for k in ("L2_T", "L2_pibar", "meets_L2T_1e-6"):
+        if k in row:
+            out[k] = row[k]
+    return out
 
 
 def _fields_digest(f):
