@@ -554,8 +554,11 @@ def run_gpu(args):
         line["config"]["recovery"] = ("learned MLP guess (BF16 tcgen05, FP32 accumulate), fallback to the "
                                       "plain warm start; trained on seeds " + str(list(GUESS_SEEDS)))
     if world == 1 and not args.no_forms and guess is None and not args.fp32_faces and args.batch_events > 0:
-        line["metric_comparison"] = batch_forms(lib, m, args.batch_events, args.batch_steps, value)
-        line["metric_summary"] = metric_summary(line["metric_comparison"])
+        try:
+            line["metric_comparison"] = batch_forms(lib, m, args.batch_events, args.batch_steps, value)
+            line["metric_summary"] = metric_summary(line["metric_comparison"])
+        except Exception as exc:   # the single-event line above stands on its own
+            line["metric_comparison"] = {"error": f"{type(exc).__name__}: {exc}"}
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.cpu_steps)
     return line
